@@ -1,0 +1,361 @@
+"""Benchmark: exact top-k linear aggregation on B200.
+
+Default workload (one GPU): single-query exact top-k over a resident table of
+n = 2^28 objects x d = 16 FP32 attributes (column-major, 16 GiB, seeded
+independent U[0,1), generated on the device and normalised like TPAc::init).
+One step = 16 queries, the grid q in {2,4,8,16} x k in {16,64,256,1024} on the
+last q attributes with U(0,1] weights.  The table is far larger than L2, so no
+flush is needed between queries.
+
+  value   queries/s, device-timed with CUDA events on the launching stream, inputs
+          resident in HBM, outputs written to device buffers (topk_query_device).
+  e2e     the same queries through topk_query (the C-ABI call a caller makes) with
+          host weights/attrs and host result buffers; host wall time per step.
+  roofline  the fused scan kernel: algorithmic bytes 4*n*q per launch over its mean
+          launch time (per-launch CUDA events), against MEASURED_PEAKS.json hbm_gbs.
+  cpu_baseline  the reference's TPAc::findTopKthreads (compiled strict into
+          oracle/_ref) on this host, timed on a 2^25-row sample, scaled to n.
+
+Multi-GPU (torchrun): every rank holds its own replica and runs the same query
+steps (weak scaling, no collective on the data path); time = max over ranks.
+
+`--impl reference` runs the reference's own CPU TPAc on the host (rank 0 only).
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "exact top-k queries/s & scan GB/s vs HBM peak; learned+BF16 vs plain FTE speedup"
+FALLBACK_HBM_GBS = 6650.0
+N_FULL = 1 << 28
+D_FULL = 16
+QS = (2, 4, 8, 16)
+KS = (16, 64, 256, 1024)
+
+
+def weights_u01(d, seed):
+    """d weights i.i.d. U(0,1] on the 2^-24 grid (seeded)."""
+    u = np.random.default_rng(seed).integers(0, 1 << 24, size=d)
+    return ((u + 1) * 2.0 ** -24).astype(np.float32)
+
+
+def the_queries(d):
+    """The 16 queries of one step: last-q attributes (the reference harness's QM=0
+    attribute tables, validation/bench_cpu.h:25-45), U(0,1] weights."""
+    out = []
+    for q in QS:
+        w = weights_u01(d, 4000 + q)
+        a = np.arange(d - q, d, dtype=np.uint8)
+        for k in KS:
+            out.append((k, q, w, a))
+    return out
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the scan kernel by q, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "scan_select_n2e28_d16.md")
+    out = {}
+    try:
+        for line in open(p):
+            m = re.match(r"\s*traffic_bytes_per_launch\[q=(\d+)\]:\s*([0-9.eE+]+)", line)
+            if m:
+                out[int(m.group(1))] = float(m.group(2))
+    except OSError:
+        pass
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(n_full, d, queries, sample_rows=1 << 25, reps=2):
+    """Reference TPAc::findTopKthreads (oracle/_ref) on a sample, scaled to n_full."""
+    from oracle import oracle as O
+    if not O.RefTPAc.available():
+        return None
+    t = O.generate(sample_rows, d, 1, 0)
+    ref = O.RefTPAc(t)
+    del t
+    ref.init()
+    best = None
+    for _ in range(reps):
+        tot = 0.0
+        for k, q, w, a in queries:
+            tot += ref.query(2, k, w, a)[3]
+        best = tot if best is None else min(best, tot)
+    ref.close()
+    per_query_ms = best / len(queries) * (n_full / sample_rows)
+    return {
+        "value": 1000.0 / per_query_ms,
+        "unit": "queries/s",
+        "cores": int(O.RefTPAc.lib().ref_threads_constant()),
+        "host_cpus": os.cpu_count(),
+        "kind": "reference",
+        "sample": f"TPAc::findTopKthreads (THREADS=16 as shipped) on {sample_rows} rows x {d}, the "
+                  f"{len(queries)}-query step, best of {reps}, scaled by n/{sample_rows}",
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    queries = the_queries(D_FULL)
+    if not O.RefTPAc.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference TPAc library oracle/_ref not built"}))
+        return 0
+    sample = 1 << 25
+    t = O.generate(sample, D_FULL, 1, 0)
+    ref = O.RefTPAc(t)
+    del t
+    ref.init()
+    for _ in range(args.warmup):
+        ref.query(2, 16, queries[0][2], queries[0][3])
+    times = []
+    for _ in range(args.steps):
+        tot = 0.0
+        for k, q, w, a in queries:
+            tot += ref.query(2, k, w, a)[3]
+        times.append(tot * (N_FULL / sample))
+    ref.close()
+    ms = statistics.mean(times)
+    qps = len(queries) * 1000.0 / ms
+    cores = int(O.RefTPAc.lib().ref_threads_constant())
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "single-query exact top-k, n=2^28 x d=16, 16 queries/step", "n": N_FULL, "d": D_FULL},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "host_cpus": os.cpu_count(),
+                         "kind": "reference",
+                         "sample": f"TPAc::findTopKthreads on {sample} rows x {D_FULL}, scaled by n/{sample}"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_FULL)
+    ap.add_argument("--d", type=int, default=D_FULL)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import topk_b200 as T
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    n, d = args.n, args.d
+    queries = the_queries(d)
+    table = T.Table(n, d, device=local)
+    table.generate(T.DIST_INDEPENDENT, 0)
+    table.normalize()
+    stream = torch.cuda.current_stream()
+    kmax = max(KS)
+    out_ids = torch.empty(kmax, dtype=torch.int64, device="cuda")
+    out_sc = torch.empty(kmax, dtype=torch.float32, device="cuda")
+
+    def run_step(events=None):
+        for j, (k, q, w, a) in enumerate(queries):
+            if events is not None:
+                events[j][0].record(stream)
+            table.query_device(k, w, a, out_ids.data_ptr(), out_sc.data_ptr(), 0, stream.cuda_stream)
+            if events is not None:
+                events[j][1].record(stream)
+
+    for _ in range(args.warmup):
+        run_step()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in queries] for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for s in range(args.steps):
+        run_step(per_launch[s])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    if dist:
+        tt = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+
+    # per-launch durations -> roofline of the fused scan kernel
+    bytes_by_q, time_by_q = {}, {}
+    for s in range(args.steps):
+        for j, (k, q, w, a) in enumerate(queries):
+            ms = per_launch[s][j][0].elapsed_time(per_launch[s][j][1])
+            bytes_by_q[q] = bytes_by_q.get(q, 0.0) + 4.0 * n * q
+            time_by_q[q] = time_by_q.get(q, 0.0) + ms
+    tot_bytes = sum(bytes_by_q.values())
+    tot_ms = sum(time_by_q.values())
+    achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic()
+    launches = args.steps * len(queries)
+    traffic_per_launch = None
+    if traffic and all(q in traffic for q in QS):
+        traffic_per_launch = sum(traffic[q] * (n / N_FULL) for (_, q, _, _) in queries) / len(queries)
+
+    # e2e: the host-buffer C-ABI call, host wall time per step
+    if dist:
+        dist.barrier()
+    e2e_times = []
+    for s in range(max(3, args.steps // 2)):
+        torch.cuda.synchronize()
+        a0 = time.perf_counter()
+        for k, q, w, a in queries:
+            table.query(k, w, a)
+        e2e_times.append(time.perf_counter() - a0)
+    e2e_ms = statistics.median(e2e_times) * 1e3
+    if dist:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    h2d = sum(len(a) * 5 for (_, _, _, a) in queries)  # weights[attr] + attr ids, in the launch parameters
+    d2h = sum(64 + 12 * k for (k, _, _, _) in queries)  # header + ids (u64) + scores (f32)
+
+    ms_per_step = elapsed_ms / args.steps
+    value = world * len(queries) * 1000.0 / ms_per_step
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded independent U[0,1) table generated on the device, normalised; U(0,1] weights",
+        "config": {
+            "workload": "single-query exact top-k (fused scan+select), n=2^28 x d=16 column-major FP32, "
+                        "16 queries/step: q in {2,4,8,16} (last q attributes) x k in {16,64,256,1024}",
+            "n": n, "d": d, "queries_per_step": len(queries),
+            "l2": "inputs larger than L2 (16 GiB table per query scan), no flush needed",
+            "parallelism": f"replica x{world}",
+        },
+        "scan_gbs": achieved,
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind,
+            "traffic": traffic_per_launch,
+            "per_q": {str(q): {"gbs": bytes_by_q[q] / (time_by_q[q] * 1e-3) / 1e9,
+                               "ms_per_launch": time_by_q[q] / (args.steps * len(KS))} for q in QS},
+        },
+        "e2e": {"value": world * len(queries) * 1000.0 / e2e_ms, "unit": "queries/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "timing": "host wall clock per step, median"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline and n == N_FULL:
+        try:
+            result["cpu_baseline"] = cpu_baseline(n, d, queries)
+        except Exception as e:  # the baseline is reported, never the product
+            result["cpu_baseline"] = {"error": str(e)}
+    table.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,166 @@
+/*
+ * topk_b200 - C ABI of the B200 (sm_100a) exact top-k linear-aggregation engine.
+ *
+ * One handle holds one n x d FP32 table, column-major, resident in HBM (the
+ * device copy of AA::cdata).  Queries return the k object ids with the largest
+ * weighted sums over a subset of attributes, bit-exact with the reference's
+ * strict-FP32 TPAc path.  Everything in these signatures is plain C: pointers,
+ * sizes and int status codes.
+ *
+ * Reference interfaces replaced (paths inside the TopK project):
+ *   AA<T,Z>::AA(n,d), get_cdata()            cpu/AA.h:66, :77      -> topk_create, topk_upload_colmajor
+ *   TPAc::init() -> normalize_transpose       cpu/TPAc.h:28-32,
+ *                                             common/common.h:30-61 -> topk_normalize
+ *   File<T>::gen(data, type)                  input/File.h:335-354  -> topk_generate
+ *   TPAc::findTopKscalar/simd/threads         cpu/TPAc.h:35,118,257 -> topk_query
+ *   TPAc::findTopKsimdMQ + MQ loop            cpu/TPAc.h:210-254,
+ *                                             validation/bench_cpu.h:198-232 -> topk_query_batch
+ *   AA::get_res(), get_thres()                cpu/AA.h:71,73        -> ids/scores/threshold outputs
+ *   AA::~AA()                                 cpu/AA.h:147-150      -> topk_destroy
+ *
+ * Semantics (same meaning as the reference's arguments):
+ *   weights  - indexed by ATTRIBUTE ID, length >= d (cpu/TPAc.h:135 weights[attr[m]]).
+ *   attr     - qq attribute ids; the score is s = 0; for m in 0..qq-1:
+ *              s = s + x[attr[m]] * weights[attr[m]]  (one rounding per op, no FMA).
+ *   result   - min(k, rows) tuples ASCENDING by score, like the reference's min-heap
+ *              drain (cpu/TPAc.h:198-203); threshold = the k-th best score
+ *              (cpu/TPAc.h:199).  Ties are ranked by lower id first, so among equal
+ *              scores the ascending output lists the higher id first.
+ *   NaN scores rank below every number.
+ *
+ * Errors: every call returns TOPK_OK or a TOPK_ERR_* code; topk_last_error()
+ * gives a message for the calling thread.  (The reference prints and exit(1)s;
+ * the C++ drop-in wrapper keeps that behaviour on top of these codes.)
+ *
+ * Threading: topk_query and topk_query_batch are safe to call concurrently on one
+ * handle (each call takes its own scratch context and stream from a pool), which
+ * is what the reference's findTopKsimdMQ callers do (validation/bench_cpu.h:204-212).
+ * topk_query_device uses the handle's primary context: callers serialise it.
+ */
+#ifndef TOPK_B200_H
+#define TOPK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOPK_OK 0
+#define TOPK_ERR_ARG 1         /* bad argument (k == 0, qq == 0, attr >= d, null pointer, ...) */
+#define TOPK_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define TOPK_ERR_OOM 3         /* device or pinned allocation failed */
+#define TOPK_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define TOPK_ERR_UNSUPPORTED 5 /* valid request outside this build's limits (e.g. k > TOPK_MAX_K) */
+#define TOPK_ERR_STATE 6       /* call out of order (e.g. query before any table data) */
+
+#define TOPK_MAX_K 4096u   /* largest k of the fused scan + select path */
+#define TOPK_MAX_Q 64u     /* largest qq per query */
+#define TOPK_MAX_D 255u    /* attr ids are uint8_t in the reference (cpu/TPAc.h:19) */
+
+/* Distribution codes of topk_generate, numbered like File<T>::gen
+ * (input/File.h:345-352); 3 mixes them by object id modulo 3. */
+#define TOPK_DIST_CORRELATED 0
+#define TOPK_DIST_INDEPENDENT 1
+#define TOPK_DIST_ANTICORRELATED 2
+#define TOPK_DIST_MIXED 3
+
+typedef struct topk_table_s *topk_table_t;
+
+/* Create a handle for an n x d table on CUDA device `device` and allocate its
+ * device copy (column stride rounded up to 64 rows).  Replaces AA(n,d). */
+int topk_create(uint64_t n, uint32_t d, int device, topk_table_t *out);
+
+/* Free the device table and every scratch context.  Replaces ~AA(). */
+int topk_destroy(topk_table_t h);
+
+/* Copy a host column-major table (column m at host + m*ld_host, ld_host >= n)
+ * into the device copy.  Replaces filling get_cdata(). */
+int topk_upload_colmajor(topk_table_t h, const float *host, uint64_t ld_host);
+
+/* Fill the device table with this engine's seeded synthetic distribution
+ * (bit-identical to the oracle's generator).  Replaces File<T>::gen. */
+int topk_generate(topk_table_t h, int dist, uint64_t seed);
+
+/* normalize_transpose on the device copy: per-attribute min/max, then
+ * v = (v - min) / (max - min), IEEE division.  Replaces TPAc::init().
+ * mins/maxs (length d, may be NULL) receive the values used. */
+int topk_normalize(topk_table_t h, float *mins, float *maxs);
+
+/* Copy the device table back (column-major, host stride ld_host >= n). */
+int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host);
+
+/* Exact top-k over all n objects with host inputs and host outputs (synchronous).
+ * ids/scores must hold min(k, n) entries; count/threshold may be NULL.
+ * Replaces findTopKscalar / findTopKsimd / findTopKthreads + get_res/get_thres. */
+int topk_query(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
+               uint64_t *ids, float *scores, uint64_t *count, float *threshold);
+
+/* Same over rows [row_begin, row_end) only (one shard of the objects).
+ * Ids stay global.  No reference counterpart: it is the per-shard step of an
+ * object-sharded query. */
+int topk_query_range(topk_table_t h, uint64_t row_begin, uint64_t row_end, uint64_t k, uint32_t qq,
+                     const float *weights, const uint8_t *attr, uint64_t *ids, float *scores,
+                     uint64_t *count, float *threshold);
+
+/* Asynchronous form with DEVICE outputs on a caller stream (cudaStream_t passed
+ * as void*; NULL = the handle's own stream).  d_ids/d_scores hold min(k, n)
+ * entries; d_threshold (may be NULL) receives the k-th score.  Uses the handle's
+ * primary scratch: calls on one handle must not overlap.  Same results as
+ * topk_query. */
+int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weights,
+                      const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_threshold,
+                      void *stream);
+
+/* A batch of independent queries with host inputs/outputs (synchronous).
+ * Query j uses ks[j], qqs[j], weights + j*wstride (indexed by attribute id),
+ * attrs + j*astride.  Outputs: ids/scores + j*kstride (kstride >= max k),
+ * counts[j], thresholds[j] (either may be NULL).  Replaces the multi-query
+ * findTopKsimdMQ loop, and unlike it keeps every result. */
+int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs,
+                     const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride,
+                     uint64_t *ids, float *scores, uint64_t kstride, uint64_t *counts,
+                     float *thresholds);
+
+/* Verification entry (no reference counterpart): copy the full rows of `count`
+ * objects to host memory, out[j*d + m] = attribute m of object ids[j]. */
+int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out);
+
+/* Verification entry (no reference counterpart): with a plain kernel independent
+ * of the fused scan, count objects in rows [row_begin, row_end) whose
+ * reference-order score is >= thr and > thr.  For a correct top-k over all rows,
+ * count_gt < k <= count_ge at thr = the k-th score. */
+int topk_count_ge(topk_table_t h, uint64_t row_begin, uint64_t row_end, uint32_t qq, const float *weights,
+                  const uint8_t *attr, float thr, uint64_t *count_ge, uint64_t *count_gt);
+
+/* Test entry (no reference counterpart): mode 1 makes the next fused scans wait,
+ * before any copy is issued, on a barrier that nothing completes, so the bounded
+ * wait runs out and the call returns TOPK_ERR_TIMEOUT; 0 turns it off.  Host-side
+ * fault injection: no GPU fault, the context stays usable. */
+int topk_set_fault_injection(topk_table_t h, int mode);
+
+/* Device-side scan statistics of the last topk_query* on this thread:
+ * candidates kept by the fused select and the number of block reductions. */
+int topk_last_stats(topk_table_t h, uint64_t *candidates, uint64_t *reductions);
+
+/* Bound (in polling iterations) on every device-side wait; 0 restores the default.
+ * A wait that runs out makes the call return TOPK_ERR_TIMEOUT. */
+int topk_set_wait_limit(topk_table_t h, uint64_t iterations);
+
+/* Table shape and device stride. */
+int topk_shape(topk_table_t h, uint64_t *n, uint32_t *d, uint64_t *ld);
+
+/* Message for the last error on the calling thread ("" if none). */
+const char *topk_last_error(void);
+
+/* Name of a status code. */
+const char *topk_status_name(int status);
+
+/* Library version string. */
+const char *topk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOPK_B200_H */

@@ -1,0 +1,70 @@
+"""Build recipe for the CPU checker (TEST INFRASTRUCTURE ONLY).
+
+Two products:
+  * oracle/_build/liboracle.so  - the C restatement (topk_oracle.c), strict FP flags.
+  * oracle/_ref/libref_tpac.so  - the reference's own TPAc (cpu/TPAc.h, cpu/AA.h,
+    common/common.h, time/Time.h) compiled from where its sources lie, through the
+    forwarding shim ref_tpac_shim.cpp.  Built only when the reference tree is present
+    (TOPK_REFERENCE, default /root/reference); the .so then travels with the repo.
+
+Strict flags for both: -O3 -ffp-contract=off, never -ffast-math.  The reference's
+own Makefile:60 adds -ffast-math, which changes the normalised table and the
+scores; the strict build is the one whose scalar/SIMD/threads paths agree.
+-march=x86-64-v3 (AVX2) keeps the .so runnable on any AVX2 host.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(BUILD, "liboracle.so")
+REF_SO = os.path.join(REF_OUT, "libref_tpac.so")
+
+
+def reference_root():
+    return os.environ.get("TOPK_REFERENCE", "/root/reference")
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs if os.path.exists(s))
+
+
+def build_oracle(verbose=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = [os.path.join(HERE, "topk_oracle.c"), os.path.join(HERE, "topk_oracle.h")]
+    if force or _stale(ORACLE_SO, srcs):
+        _run(["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
+              "-std=c11", srcs[0], "-o", ORACLE_SO, "-lm"], verbose)
+    return ORACLE_SO
+
+
+def build_ref(verbose=False, force=False):
+    """Compile the reference TPAc through the shim. Returns the .so path or None."""
+    root = reference_root()
+    hdrs = [os.path.join(root, p) for p in ("cpu/TPAc.h", "cpu/AA.h", "common/common.h", "time/Time.h")]
+    if not all(os.path.exists(h) for h in hdrs):
+        return REF_SO if os.path.exists(REF_SO) else None
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_tpac_shim.cpp")
+    if force or _stale(REF_SO, [shim] + hdrs):
+        _run(["g++", "-std=c++14", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math",
+              "-fopenmp", "-fPIC", "-shared", "-w",
+              "-I", root, "-I", os.path.join(HERE, "stub"), shim, "-o", REF_SO], verbose)
+    return REF_SO
+
+
+if __name__ == "__main__":
+    v = "-v" in sys.argv
+    print(build_oracle(v, force="-f" in sys.argv))
+    print(build_ref(v, force="-f" in sys.argv))

@@ -1,0 +1,1 @@
+/* Empty stand-in: the reference AA.h includes this boost header but uses nothing from it. */

@@ -1,0 +1,72 @@
+"""CPU: the C-ABI library loads, exports every declared symbol, fails cleanly.
+
+No compute is attempted here (there is no GPU on this machine).
+"""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import topk_b200 as T
+from topk_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "topk_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(topk_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_expected_entries():
+    syms = declared_symbols()
+    for s in ("topk_create", "topk_destroy", "topk_upload_colmajor", "topk_normalize", "topk_query",
+              "topk_query_batch", "topk_query_device", "topk_generate"):
+        assert s in syms
+    # the Python binding types every declared entry
+    assert sorted(n for n, _, _ in _lib.SIGNATURES) == syms
+
+
+def test_library_exports_every_declared_symbol():
+    L = T.load()
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+    assert L.topk_version().startswith(b"topk_b200")
+
+
+def test_status_names():
+    assert _lib.status_name(0) == "TOPK_OK"
+    assert _lib.status_name(4) == "TOPK_ERR_TIMEOUT"
+    assert _lib.status_name(99) == "TOPK_ERR_UNKNOWN"
+
+
+def test_create_argument_errors_without_gpu():
+    L = T.load()
+    h = C.c_void_p()
+    assert L.topk_create(0, 8, 0, C.byref(h)) == _lib.ERR_ARG
+    assert L.topk_create(16, 0, 0, C.byref(h)) == _lib.ERR_ARG
+    assert L.topk_create(16, 300, 0, C.byref(h)) == _lib.ERR_ARG
+    assert L.topk_create(1 << 33, 4, 0, C.byref(h)) == _lib.ERR_UNSUPPORTED
+    assert b"n and d" in L.topk_last_error() or L.topk_last_error()
+
+
+def test_null_handle_calls_fail_cleanly():
+    L = T.load()
+    import numpy as np
+    w = np.ones(4, np.float32)
+    a = np.zeros(2, np.uint8)
+    ids = np.zeros(4, np.uint64)
+    sc = np.zeros(4, np.float32)
+    assert L.topk_query(None, 4, 2, w, a, ids, sc, None, None) == _lib.ERR_ARG
+    assert L.topk_destroy(None) == _lib.OK
+    assert L.topk_shape(None, None, None, None) == _lib.ERR_ARG
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") == "__never__", reason="")
+def test_create_without_gpu_reports_cuda_error(gpu_available):
+    if gpu_available:
+        pytest.skip("a GPU is present")
+    with pytest.raises(T.TopKError) as ei:
+        T.Table(1024, 4)
+    assert ei.value.status == _lib.ERR_CUDA

@@ -1,0 +1,13 @@
+"""topk_b200: exact top-k linear aggregation on B200 (sm_100a).
+
+Drop-in for the TPAc path of avionicscode/TopK: the C ABI is include/topk_b200.h
+(libtopk_b200.so, built by `python -m topk_b200.build`); this package is its
+Python face, mirroring the reference's AA / TPAc algorithm-class API.
+"""
+from ._lib import (DIST_ANTICORRELATED, DIST_CORRELATED, DIST_INDEPENDENT, DIST_MIXED, MAX_D, MAX_K, MAX_Q,
+                   TopKError, load)
+from .table import Table
+from .tpac import AA, TPAc
+
+__all__ = ["Table", "AA", "TPAc", "TopKError", "load", "MAX_K", "MAX_Q", "MAX_D", "DIST_CORRELATED",
+           "DIST_INDEPENDENT", "DIST_ANTICORRELATED", "DIST_MIXED"]

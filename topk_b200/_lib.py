@@ -1,0 +1,99 @@
+"""ctypes binding of libtopk_b200.so (the C ABI declared in include/topk_b200.h).
+
+The library is the only compute path: if it is missing, importing this module
+raises, and there is no CPU fallback anywhere in the package.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libtopk_b200.so")
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_OOM = 3
+ERR_TIMEOUT = 4
+ERR_UNSUPPORTED = 5
+ERR_STATE = 6
+
+MAX_K = 4096
+MAX_Q = 64
+MAX_D = 255
+
+DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
+
+
+class TopKError(RuntimeError):
+    """A TOPK_ERR_* status from the C ABI."""
+
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__(f"{status_name(status)}: {message}")
+
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_H = C.c_void_p
+
+# (name, restype, argtypes) for every entry of include/topk_b200.h
+SIGNATURES = [
+    ("topk_create", C.c_int, [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
+    ("topk_destroy", C.c_int, [_H]),
+    ("topk_upload_colmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_generate", C.c_int, [_H, C.c_int, C.c_uint64]),
+    ("topk_normalize", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("topk_download_colmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_query", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, _u64p, _f32p,
+                             C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
+    ("topk_query_range", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, _f32p, _u8p, _u64p, _f32p,
+                                   C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
+    ("topk_query_device", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]),
+    ("topk_query_batch", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _u64p, _f32p,
+                                   C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("topk_gather_rows", C.c_int, [_H, _u64p, C.c_uint64, _f32p]),
+    ("topk_count_ge", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_float,
+                                C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("topk_set_fault_injection", C.c_int, [_H, C.c_int]),
+    ("topk_last_stats", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("topk_set_wait_limit", C.c_int, [_H, C.c_uint64]),
+    ("topk_shape", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    ("topk_last_error", C.c_char_p, []),
+    ("topk_status_name", C.c_char_p, [C.c_int]),
+    ("topk_version", C.c_char_p, []),
+]
+
+_lib = None
+
+
+def load():
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libtopk_b200.so not found at {LIB_PATH}: build it with `python -m topk_b200.build` "
+            "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def status_name(st):
+    return load().topk_status_name(st).decode()
+
+
+def check(st):
+    if st != OK:
+        raise TopKError(st, load().topk_last_error().decode())
+    return st

@@ -1,0 +1,565 @@
+// Host runtime behind the C ABI (include/topk_b200.h).
+//
+// A handle owns the device copy of the table (column-major, stride ld = n rounded
+// up to 64 rows so every column starts 256-byte aligned, which the bulk copies
+// need) and a pool of query contexts.  A context is one stream, one device
+// scratch block for the fused scan, one device result block and a pinned host
+// mirror of it, so a synchronous query costs one kernel launch, one
+// device-to-host copy and one stream synchronisation.  Concurrent callers (the
+// reference's findTopKsimdMQ threads, validation/bench_cpu.h:204-212) each take
+// their own context from the pool.
+#include "../../include/topk_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "topk_internal.h"
+
+using namespace topk;
+
+namespace {
+
+thread_local std::string g_last_error;
+thread_local uint64_t g_last_cands = 0, g_last_reductions = 0;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  if (e == cudaErrorMemoryAllocation) return fail(TOPK_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return fail(TOPK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                    \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+// Switch to the handle's device for the duration of a call.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Result block layout (device and pinned host mirror): header, ids[k], scores[k].
+struct ResultHeader {
+  uint32_t count;
+  float threshold;
+  uint32_t stats[2];  // candidates in the final select, block-selects
+  uint32_t pad[12];
+};
+constexpr size_t kHdr = sizeof(ResultHeader);  // 64 bytes
+size_t result_bytes(uint32_t k) { return kHdr + (size_t)k * 8 + (size_t)k * 4; }
+
+struct Ctx {
+  cudaStream_t stream = nullptr;
+  ScanScratch *scratch = nullptr;
+  uint2 *gcand = nullptr;
+  uint32_t gcand_cap = 0;
+  unsigned char *d_res = nullptr;  // device result block (kMaxK capacity)
+  unsigned char *h_res = nullptr;  // pinned mirror
+  unsigned long long *d_count2 = nullptr;
+  uint64_t *d_ids_scratch = nullptr;  // gather ids
+  float *d_rows = nullptr;
+  size_t rows_cap = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+struct topk_table_s {
+  int device = 0;
+  uint64_t n = 0, ld = 0;
+  uint32_t d = 0;
+  float *table = nullptr;
+  bool has_data = false;
+  int num_sms = 148;
+  size_t smem_optin = 0;
+  uint64_t wait_limit = 1ull << 26;
+  int fault_mode = 0;
+  uint32_t *d_minmax = nullptr;
+  float *d_norm = nullptr;  // mins[d], ranges[d]
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Ctx *> ctxs;
+  Ctx *primary = nullptr;
+};
+
+namespace {
+
+constexpr size_t kMaxContexts = 64;
+
+int ctx_create(topk_table_t h, Ctx **out) {
+  Ctx *c = new Ctx();
+  auto bail = [&](cudaError_t e, const char *what) {
+    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaFree(c->scratch);
+    cudaFree(c->gcand);
+    cudaFree(c->d_res);
+    cudaFree(c->d_count2);
+    if (c->h_res) cudaFreeHost(c->h_res);
+    delete c;
+    return cuda_fail(e, what);
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  if ((e = cudaMalloc(&c->scratch, sizeof(ScanScratch))) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMemset(c->scratch, 0, sizeof(ScanScratch))) != cudaSuccess) return bail(e, "scratch memset");
+  c->gcand_cap = (uint32_t)h->num_sms * kMaxK;  // grid <= num_sms CTAs, each appends <= k entries
+  if ((e = cudaMalloc(&c->gcand, (size_t)c->gcand_cap * sizeof(uint2))) != cudaSuccess) return bail(e, "gcand");
+  if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
+  if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
+  if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK), cudaHostAllocDefault)) != cudaSuccess)
+    return bail(e, "pinned result");
+  *out = c;
+  return TOPK_OK;
+}
+
+void ctx_free(Ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  cudaFree(c->scratch);
+  cudaFree(c->gcand);
+  cudaFree(c->d_res);
+  cudaFree(c->d_count2);
+  cudaFree(c->d_ids_scratch);
+  cudaFree(c->d_rows);
+  if (c->h_res) cudaFreeHost(c->h_res);
+  delete c;
+}
+
+// Take a free context (creating one up to kMaxContexts, else wait for one).
+int ctx_acquire(topk_table_t h, Ctx **out) {
+  std::unique_lock<std::mutex> lk(h->mu);
+  for (;;) {
+    for (Ctx *c : h->ctxs)
+      if (!c->busy) { c->busy = true; *out = c; return TOPK_OK; }
+    if (h->ctxs.size() < kMaxContexts) {
+      Ctx *c = nullptr;
+      int st = ctx_create(h, &c);
+      if (st != TOPK_OK) return st;
+      c->busy = true;
+      h->ctxs.push_back(c);
+      *out = c;
+      return TOPK_OK;
+    }
+    h->cv.wait(lk);
+  }
+}
+
+void ctx_release(topk_table_t h, Ctx *c) {
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    c->busy = false;
+  }
+  h->cv.notify_one();
+}
+
+struct CtxLease {
+  topk_table_t h;
+  Ctx *c = nullptr;
+  int status;
+  explicit CtxLease(topk_table_t hh) : h(hh) { status = ctx_acquire(h, &c); }
+  ~CtxLease() { if (c) ctx_release(h, c); }
+};
+
+int check_query(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data: call topk_upload_colmajor or topk_generate first");
+  if (k == 0) return fail(TOPK_ERR_ARG, "k must be >= 1");
+  if (k > kMaxK) return fail(TOPK_ERR_UNSUPPORTED, "k=%llu exceeds TOPK_MAX_K=%u", (unsigned long long)k, kMaxK);
+  if (qq == 0) return fail(TOPK_ERR_ARG, "qq must be >= 1");
+  if (qq > kMaxQ) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u exceeds TOPK_MAX_Q=%u", qq, kMaxQ);
+  if (!weights || !attr) return fail(TOPK_ERR_ARG, "null weights or attr");
+  for (uint32_t m = 0; m < qq; m++)
+    if (attr[m] >= h->d) return fail(TOPK_ERR_ARG, "attr[%u]=%u out of range (d=%u)", m, attr[m], h->d);
+  return TOPK_OK;
+}
+
+// Enqueue one fused scan over rows [r0, r1) writing into the given outputs.
+int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint64_t r1, uint64_t k, uint32_t qq,
+                 const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_thr,
+                 uint32_t *d_count, uint32_t *d_stats = nullptr) {
+  const uint64_t rows = r1 - r0;
+  ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin);
+  if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)k);
+  ScanParams p{};
+  p.table = h->table;
+  p.ld = h->ld;
+  p.row_begin = r0;
+  p.row_end = r1;
+  p.tile_begin = r0 & ~3ull;
+  p.tile_end = (r1 + 3) & ~3ull;
+  const uint64_t span = p.tile_end - p.tile_begin;
+  const uint64_t tiles = (span + pl.tile - 1) / pl.tile;
+  p.num_tiles = (uint32_t)tiles;
+  if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;
+  p.qq = qq;
+  p.k = (uint32_t)k;
+  p.cap = pl.cap;
+  p.stages = pl.stages;
+  p.gcand_cap = c->gcand_cap;
+  if ((uint64_t)pl.grid * k > c->gcand_cap) return fail(TOPK_ERR_UNSUPPORTED, "candidate list too small");
+  p.wait_limit = h->wait_limit;
+  p.fault_mode = (uint32_t)h->fault_mode;
+  p.scratch = c->scratch;
+  p.gcand = c->gcand;
+  p.out_ids = d_ids;
+  p.out_scores = d_scores;
+  p.out_threshold = d_thr;
+  p.out_count = d_count;
+  p.out_stats = d_stats;
+  for (uint32_t m = 0; m < qq; m++) {
+    p.attr[m] = attr[m];
+    p.w[m] = weights[attr[m]];
+  }
+  CK(launch_scan(pl, p, stream));
+  return TOPK_OK;
+}
+
+// Synchronous query into host buffers through a leased context.
+int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_t qq, const float *weights,
+                   const uint8_t *attr, uint64_t *ids, float *scores, uint64_t *count, float *threshold) {
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (r1 > h->n || r0 > r1) return fail(TOPK_ERR_ARG, "row range [%llu, %llu) outside [0, %llu)",
+                                        (unsigned long long)r0, (unsigned long long)r1, (unsigned long long)h->n);
+  const uint64_t kk = std::min<uint64_t>(k, r1 - r0);
+  if (kk == 0) {
+    if (count) *count = 0;
+    if (threshold) *threshold = 0.0f;
+    return TOPK_OK;
+  }
+  if (!ids || !scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  CtxLease lease(h);
+  if (lease.status != TOPK_OK) return lease.status;
+  Ctx *c = lease.c;
+  unsigned char *dr = c->d_res;
+  ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
+  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
+  float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
+  // a sentinel count tells a completed scan from one that left early
+  CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), c->stream));
+  st = enqueue_scan(h, c, c->stream, r0, r1, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+                    dh->stats);
+  if (st != TOPK_OK) return st;
+  const size_t bytes = kHdr + kk * 12;
+  CK(cudaMemcpyAsync(c->h_res, dr, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
+  if (hh->count != (uint32_t)kk) {
+    ScanScratch s{};
+    cudaMemcpy(&s, c->scratch, sizeof(s), cudaMemcpyDeviceToHost);
+    cudaMemset(c->scratch, 0, sizeof(ScanScratch));
+    if (s.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
+    return fail(TOPK_ERR_CUDA, "scan did not complete (count %u, expected %llu, error 0x%x)", hh->count,
+                (unsigned long long)kk, s.error);
+  }
+  std::memcpy(ids, c->h_res + kHdr, kk * 8);
+  std::memcpy(scores, c->h_res + kHdr + kk * 8, kk * 4);
+  if (count) *count = kk;
+  if (threshold) *threshold = hh->threshold;
+  g_last_cands = hh->stats[0];
+  g_last_reductions = hh->stats[1];
+  return TOPK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *topk_version(void) { return "topk_b200 0.1 (sm_100a)"; }
+
+const char *topk_last_error(void) { return g_last_error.c_str(); }
+
+const char *topk_status_name(int s) {
+  switch (s) {
+    case TOPK_OK: return "TOPK_OK";
+    case TOPK_ERR_ARG: return "TOPK_ERR_ARG";
+    case TOPK_ERR_CUDA: return "TOPK_ERR_CUDA";
+    case TOPK_ERR_OOM: return "TOPK_ERR_OOM";
+    case TOPK_ERR_TIMEOUT: return "TOPK_ERR_TIMEOUT";
+    case TOPK_ERR_UNSUPPORTED: return "TOPK_ERR_UNSUPPORTED";
+    case TOPK_ERR_STATE: return "TOPK_ERR_STATE";
+    default: return "TOPK_ERR_UNKNOWN";
+  }
+}
+
+int topk_create(uint64_t n, uint32_t d, int device, topk_table_t *out) {
+  g_last_error.clear();
+  if (!out) return fail(TOPK_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (n == 0 || d == 0) return fail(TOPK_ERR_ARG, "n and d must be >= 1");
+  if (d > TOPK_MAX_D) return fail(TOPK_ERR_ARG, "d=%u exceeds %u", d, TOPK_MAX_D);
+  if (n >= 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "n must be < 2^32 - 1 (32-bit ids on the device)");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(TOPK_ERR_ARG, "device %d not present (%d devices)", device, ndev);
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  topk_table_t h = new topk_table_s();
+  h->device = device;
+  h->n = n;
+  h->d = d;
+  h->ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  h->num_sms = v > 0 ? v : 148;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  h->smem_optin = v > 0 ? (size_t)v : 48 * 1024;
+  cudaError_t e = scan_set_attributes(h->smem_optin);
+  if (e == cudaSuccess) e = cudaMalloc(&h->table, h->ld * d * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(h->table, 0, h->ld * d * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_minmax, (size_t)d * kMinmaxWords * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_norm, (size_t)2 * d * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaFree(h->table);
+    cudaFree(h->d_minmax);
+    cudaFree(h->d_norm);
+    delete h;
+    return cuda_fail(e, "topk_create");
+  }
+  int st = ctx_create(h, &h->primary);
+  if (st != TOPK_OK) {
+    cudaFree(h->table);
+    cudaFree(h->d_minmax);
+    cudaFree(h->d_norm);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return TOPK_OK;
+}
+
+int topk_destroy(topk_table_t h) {
+  if (!h) return TOPK_OK;
+  DeviceGuard dg(h->device);
+  for (Ctx *c : h->ctxs) ctx_free(c);
+  ctx_free(h->primary);
+  cudaFree(h->table);
+  cudaFree(h->d_minmax);
+  cudaFree(h->d_norm);
+  delete h;
+  return TOPK_OK;
+}
+
+int topk_shape(topk_table_t h, uint64_t *n, uint32_t *d, uint64_t *ld) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (n) *n = h->n;
+  if (d) *d = h->d;
+  if (ld) *ld = h->ld;
+  return TOPK_OK;
+}
+
+int topk_set_wait_limit(topk_table_t h, uint64_t it) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  h->wait_limit = it ? it : (1ull << 26);
+  return TOPK_OK;
+}
+
+int topk_upload_colmajor(topk_table_t h, const float *host, uint64_t ld_host) {
+  if (!h || !host) return fail(TOPK_ERR_ARG, "null argument");
+  if (ld_host < h->n) return fail(TOPK_ERR_ARG, "ld_host=%llu < n=%llu", (unsigned long long)ld_host, (unsigned long long)h->n);
+  DeviceGuard dg(h->device);
+  CK(cudaMemcpy2D(h->table, h->ld * sizeof(float), host, ld_host * sizeof(float), h->n * sizeof(float), h->d,
+                  cudaMemcpyHostToDevice));
+  h->has_data = true;
+  return TOPK_OK;
+}
+
+int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host) {
+  if (!h || !host) return fail(TOPK_ERR_ARG, "null argument");
+  if (ld_host < h->n) return fail(TOPK_ERR_ARG, "ld_host < n");
+  DeviceGuard dg(h->device);
+  CK(cudaMemcpy2D(host, ld_host * sizeof(float), h->table, h->ld * sizeof(float), h->n * sizeof(float), h->d,
+                  cudaMemcpyDeviceToHost));
+  return TOPK_OK;
+}
+
+int topk_generate(topk_table_t h, int dist, uint64_t seed) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (dist < 0 || dist > 3) return fail(TOPK_ERR_ARG, "dist must be 0..3");
+  if (h->d > 64) return fail(TOPK_ERR_UNSUPPORTED, "generator supports d <= 64");
+  DeviceGuard dg(h->device);
+  CK(launch_generate(h->table, h->ld, h->d, h->n, dist, seed, h->primary->stream));
+  CK(cudaStreamSynchronize(h->primary->stream));
+  h->has_data = true;
+  return TOPK_OK;
+}
+
+int topk_normalize(topk_table_t h, float *mins, float *maxs) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  DeviceGuard dg(h->device);
+  cudaStream_t s = h->primary->stream;
+  CK(launch_minmax(h->table, h->ld, h->d, h->n, h->d_minmax, s));
+  std::vector<uint32_t> w((size_t)h->d * kMinmaxWords);
+  CK(cudaMemcpyAsync(w.data(), h->d_minmax, w.size() * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<float> host(2 * (size_t)h->d);
+  for (uint32_t m = 0; m < h->d; m++) {
+    const uint32_t *c = &w[(size_t)m * kMinmaxWords];
+    auto k2f = [](uint32_t k) {
+      uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+      float f;
+      std::memcpy(&f, &u, 4);
+      return f;
+    };
+    float mx = k2f(c[0]);
+    float mn = k2f(c[1]);
+    if (c[1] == 0x80000000u) {  // minimum is zero: sign of the first zero in the column
+      uint64_t pz = (uint64_t)c[2] | ((uint64_t)c[3] << 32);
+      uint64_t nz = (uint64_t)c[4] | ((uint64_t)c[5] << 32);
+      mn = (nz < pz) ? -0.0f : 0.0f;
+    }
+    volatile float vmx = mx, vmn = mn;
+    float range = vmx - vmn;  // _mm = _max - _min (common/common.h:50)
+    host[m] = mn;
+    host[h->d + m] = range;
+    if (mins) mins[m] = mn;
+    if (maxs) maxs[m] = mx;
+  }
+  CK(cudaMemcpyAsync(h->d_norm, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s));
+  CK(launch_normalize(h->table, h->ld, h->d, h->n, h->d_norm, h->d_norm + h->d, s));
+  CK(cudaStreamSynchronize(s));
+  return TOPK_OK;
+}
+
+int topk_query(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, uint64_t *ids,
+               float *scores, uint64_t *count, float *threshold) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  return run_query_sync(h, 0, h->n, k, qq, weights, attr, ids, scores, count, threshold);
+}
+
+int topk_query_range(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_t qq, const float *weights,
+                     const uint8_t *attr, uint64_t *ids, float *scores, uint64_t *count, float *threshold) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  return run_query_sync(h, r0, r1, k, qq, weights, attr, ids, scores, count, threshold);
+}
+
+int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
+                      uint64_t *d_ids, float *d_scores, float *d_threshold, void *stream) {
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (!d_ids || !d_scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  DeviceGuard dg(h->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->primary->stream;
+  return enqueue_scan(h, h->primary, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, d_threshold, nullptr);
+}
+
+int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+                     uint64_t wstride, const uint8_t *attrs, uint64_t astride, uint64_t *ids, float *scores,
+                     uint64_t kstride, uint64_t *counts, float *thresholds) {
+  g_last_error.clear();
+  if (!h || (nq && (!ks || !qqs || !weights || !attrs || !ids || !scores)))
+    return fail(TOPK_ERR_ARG, "null argument");
+  if (wstride < h->d) return fail(TOPK_ERR_ARG, "wstride < d");
+  for (uint64_t j = 0; j < nq; j++) {
+    if (kstride < std::min<uint64_t>(ks[j], h->n)) return fail(TOPK_ERR_ARG, "kstride < k of query %llu", (unsigned long long)j);
+    if (qqs[j] > astride) return fail(TOPK_ERR_ARG, "astride < qq of query %llu", (unsigned long long)j);
+    int st = check_query(h, ks[j], qqs[j], weights + j * wstride, attrs + j * astride);
+    if (st != TOPK_OK) return st;
+  }
+  for (uint64_t j = 0; j < nq; j++) {
+    uint64_t c = 0;
+    float th = 0;
+    int st = run_query_sync(h, 0, h->n, ks[j], qqs[j], weights + j * wstride, attrs + j * astride, ids + j * kstride,
+                            scores + j * kstride, &c, &th);
+    if (st != TOPK_OK) return st;
+    if (counts) counts[j] = c;
+    if (thresholds) thresholds[j] = th;
+  }
+  return TOPK_OK;
+}
+
+int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out) {
+  if (!h || (count && (!ids || !out))) return fail(TOPK_ERR_ARG, "null argument");
+  for (uint64_t j = 0; j < count; j++)
+    if (ids[j] >= h->n) return fail(TOPK_ERR_ARG, "id %llu out of range", (unsigned long long)ids[j]);
+  if (count == 0) return TOPK_OK;
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  if (lease.status != TOPK_OK) return lease.status;
+  Ctx *c = lease.c;
+  const size_t need = (size_t)count * h->d;
+  if (c->rows_cap < need) {
+    cudaFree(c->d_rows);
+    cudaFree(c->d_ids_scratch);
+    c->d_rows = nullptr;
+    c->d_ids_scratch = nullptr;
+    c->rows_cap = 0;
+    CK(cudaMalloc(&c->d_rows, need * sizeof(float)));
+    CK(cudaMalloc(&c->d_ids_scratch, (size_t)count * sizeof(uint64_t) + need));  // ids fit: need >= count
+    c->rows_cap = need;
+  }
+  CK(cudaMemcpyAsync(c->d_ids_scratch, ids, count * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_gather(h->table, h->ld, h->d, c->d_ids_scratch, count, c->d_rows, c->stream));
+  CK(cudaMemcpyAsync(out, c->d_rows, need * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TOPK_OK;
+}
+
+int topk_count_ge(topk_table_t h, uint64_t r0, uint64_t r1, uint32_t qq, const float *weights, const uint8_t *attr,
+                  float thr, uint64_t *ge, uint64_t *gt) {
+  int st = check_query(h, 1, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (r1 > h->n || r0 > r1) return fail(TOPK_ERR_ARG, "row range outside the table");
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  if (lease.status != TOPK_OK) return lease.status;
+  Ctx *c = lease.c;
+  float w[kMaxQ];
+  for (uint32_t m = 0; m < qq; m++) w[m] = weights[attr[m]];
+  CK(launch_count(h->table, h->ld, r0, r1, qq, attr, w, thr, c->d_count2, c->stream));
+  unsigned long long r[2];
+  CK(cudaMemcpyAsync(r, c->d_count2, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (ge) *ge = r[0];
+  if (gt) *gt = r[1];
+  return TOPK_OK;
+}
+
+int topk_set_fault_injection(topk_table_t h, int mode) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (mode < 0 || mode > 1) return fail(TOPK_ERR_ARG, "mode must be 0 or 1");
+  h->fault_mode = mode;
+  return TOPK_OK;
+}
+
+int topk_last_stats(topk_table_t h, uint64_t *cands, uint64_t *reds) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (cands) *cands = g_last_cands;
+  if (reds) *reds = g_last_reductions;
+  return TOPK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+"""Python handle over the C ABI: one n x d FP32 table resident on one GPU."""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+def _weights(w, d):
+    w = np.ascontiguousarray(w, np.float32).reshape(-1)
+    if len(w) < d:
+        raise ValueError(f"weights are indexed by attribute id and need length >= d={d}, got {len(w)}")
+    return w
+
+
+def _attr(a):
+    return np.ascontiguousarray(a, np.uint8).reshape(-1)
+
+
+class Table:
+    """Device-resident column-major table (the device copy of AA::cdata).
+
+    Entry points map one-to-one onto include/topk_b200.h.
+    """
+
+    def __init__(self, n, d, device=0):
+        L = _lib.load()
+        h = C.c_void_p()
+        check(L.topk_create(int(n), int(d), int(device), C.byref(h)))
+        self._h = h
+        self.n, self.d, self.device = int(n), int(d), int(device)
+        ld = C.c_uint64()
+        check(L.topk_shape(self._h, None, None, C.byref(ld)))
+        self.ld = ld.value
+
+    # -- data ---------------------------------------------------------------
+    def upload(self, table):
+        """table: (d, ld_host) float32, column m in row m (column-major host layout)."""
+        t = np.ascontiguousarray(table, np.float32)
+        if t.ndim != 2 or t.shape[0] != self.d or t.shape[1] < self.n:
+            raise ValueError(f"expected a ({self.d}, >= {self.n}) array, got {t.shape}")
+        check(_lib.load().topk_upload_colmajor(self._h, t.reshape(-1), t.shape[1]))
+
+    def generate(self, dist, seed):
+        check(_lib.load().topk_generate(self._h, int(dist), int(seed)))
+
+    def normalize(self):
+        mins = np.empty(self.d, np.float32)
+        maxs = np.empty(self.d, np.float32)
+        check(_lib.load().topk_normalize(self._h, mins.ctypes.data, maxs.ctypes.data))
+        return mins, maxs
+
+    def download(self):
+        out = np.empty((self.d, self.n), np.float32)
+        check(_lib.load().topk_download_colmajor(self._h, out.reshape(-1), self.n))
+        return out
+
+    def gather_rows(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = np.empty((len(ids), self.d), np.float32)
+        check(_lib.load().topk_gather_rows(self._h, ids, len(ids), out.reshape(-1)))
+        return out
+
+    # -- queries ------------------------------------------------------------
+    def query(self, k, weights, attr, row_begin=None, row_end=None):
+        """Exact top-k; returns (ids uint64, scores float32, threshold) ascending by score."""
+        L = _lib.load()
+        w, a = _weights(weights, self.d), _attr(attr)
+        r0 = 0 if row_begin is None else int(row_begin)
+        r1 = self.n if row_end is None else int(row_end)
+        cap = max(1, min(int(k), max(r1 - r0, 0)))
+        ids = np.empty(cap, np.uint64)
+        sc = np.empty(cap, np.float32)
+        cnt = C.c_uint64()
+        th = C.c_float()
+        if row_begin is None and row_end is None:
+            check(L.topk_query(self._h, int(k), len(a), w, a, ids, sc, C.byref(cnt), C.byref(th)))
+        else:
+            check(L.topk_query_range(self._h, r0, r1, int(k), len(a), w, a, ids, sc, C.byref(cnt), C.byref(th)))
+        c = cnt.value
+        return ids[:c], sc[:c], th.value
+
+    def query_device(self, k, weights, attr, d_ids, d_scores, d_threshold=0, stream=0):
+        """Asynchronous query writing into device pointers (ints) on a stream (int handle)."""
+        w, a = _weights(weights, self.d), _attr(attr)
+        check(_lib.load().topk_query_device(self._h, int(k), len(a), w, a, C.c_void_p(d_ids), C.c_void_p(d_scores),
+                                            C.c_void_p(d_threshold or None), C.c_void_p(stream or None)))
+
+    def query_batch(self, ks, weights, attrs, qqs=None):
+        """ks: (nq,), weights: (nq, >=d), attrs: (nq, astride) with qqs[j] valid ids each."""
+        L = _lib.load()
+        ks = np.ascontiguousarray(ks, np.uint64)
+        nq = len(ks)
+        W = np.ascontiguousarray(weights, np.float32).reshape(nq, -1)
+        A = np.ascontiguousarray(attrs, np.uint8).reshape(nq, -1)
+        qqs = np.full(nq, A.shape[1], np.uint32) if qqs is None else np.ascontiguousarray(qqs, np.uint32)
+        kstride = int(max(1, min(int(ks.max()) if nq else 1, self.n)))
+        ids = np.zeros((nq, kstride), np.uint64)
+        sc = np.zeros((nq, kstride), np.float32)
+        counts = np.zeros(nq, np.uint64)
+        ths = np.zeros(nq, np.float32)
+        check(L.topk_query_batch(self._h, nq, ks, qqs, W.reshape(-1), W.shape[1], A.reshape(-1), A.shape[1],
+                                 ids.reshape(-1), sc.reshape(-1), kstride, counts.ctypes.data, ths.ctypes.data))
+        return ids, sc, counts, ths
+
+    def count_ge(self, weights, attr, thr, row_begin=0, row_end=None):
+        w, a = _weights(weights, self.d), _attr(attr)
+        r1 = self.n if row_end is None else int(row_end)
+        ge, gt = C.c_uint64(), C.c_uint64()
+        check(_lib.load().topk_count_ge(self._h, int(row_begin), r1, len(a), w, a, float(thr), C.byref(ge),
+                                        C.byref(gt)))
+        return ge.value, gt.value
+
+    def set_fault_injection(self, mode):
+        check(_lib.load().topk_set_fault_injection(self._h, int(mode)))
+
+    def last_stats(self):
+        c, r = C.c_uint64(), C.c_uint64()
+        check(_lib.load().topk_last_stats(self._h, C.byref(c), C.byref(r)))
+        return c.value, r.value
+
+    def set_wait_limit(self, iterations):
+        check(_lib.load().topk_set_wait_limit(self._h, int(iterations)))
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().topk_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

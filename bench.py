@@ -232,7 +232,10 @@ def main():
     table = T.Table(n, d, device=local)
     table.generate(T.DIST_INDEPENDENT, 0)
     table.normalize()
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: its handle is passed to the C ABI and the CUDA events are
+    # recorded on it, so they bracket exactly the launched kernels.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     kmax = max(KS)
     out_ids = torch.empty(kmax, dtype=torch.int64, device="cuda")
     out_sc = torch.empty(kmax, dtype=torch.float32, device="cuda")

@@ -9,7 +9,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libtopk_b200.so")
+# TOPK_B200_LIB selects another build of the same ABI (e.g. the bounds-checking one).
+LIB_PATH = os.environ.get("TOPK_B200_LIB") or os.path.join(_HERE, "_lib", "libtopk_b200.so")
 
 OK = 0
 ERR_ARG = 1

@@ -45,25 +45,30 @@ def headers():
                   glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
-def build(verbose=False, force=False, ptxas_verbose=False):
+def build(verbose=False, force=False, ptxas_verbose=False, check=False):
+    """check=True builds libtopk_b200_check.so with -DTOPK_BOUNDS_CHECK (kernels record
+    the first failed bounds/alignment/phase check in their scratch and skip the access)."""
+    lib = LIB.replace(".so", "_check.so") if check else LIB
+    objdir = OBJDIR + ("_check" if check else "")
     os.makedirs(LIBDIR, exist_ok=True)
-    os.makedirs(OBJDIR, exist_ok=True)
+    os.makedirs(objdir, exist_ok=True)
     hdr_t = max((os.path.getmtime(h) for h in headers()), default=0)
     objs = []
     for src in sources():
-        obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         stale = force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_t)
         if not stale:
             continue
-        cmd = [NVCC] + COMMON + ARCH + ["-c", src, "-o", obj]
+        cmd = [NVCC] + COMMON + ARCH + (["-DTOPK_BOUNDS_CHECK"] if check else []) + ["-c", src, "-o", obj]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if ptxas_verbose else []
         _run(cmd, verbose or ptxas_verbose)
-    if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lpthread", "-ldl", "-lrt"], verbose)
-    return LIB
+    if force or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", lib] + objs + ["-lpthread", "-ldl", "-lrt"], verbose)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_verbose="--ptxas" in sys.argv))
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_verbose="--ptxas" in sys.argv,
+                check="--check" in sys.argv))

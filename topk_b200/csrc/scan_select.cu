@@ -52,6 +52,34 @@ struct SmemCtl {
 constexpr int kCtlBytes = 256;
 constexpr int kHistBytes = 256 * 4;
 
+// TOPK_BOUNDS_CHECK: record the first failed check in scratch->diag and tell the
+// caller to skip the guarded access.  Compiled out of the product build.
+#ifdef TOPK_BOUNDS_CHECK
+__device__ __forceinline__ bool check(bool ok, ScanScratch *s, uint32_t code, uint32_t i, uint32_t a, uint32_t b) {
+  if (!ok && atomicCAS(&s->diag[0], 0u, code) == 0u) {
+    s->diag[1] = blockIdx.x;
+    s->diag[2] = i;
+    s->diag[3] = a;
+    s->diag[4] = b;
+  }
+  return ok;
+}
+__device__ __forceinline__ bool mbar_test_parity(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+#define TOPK_CHECK(cond, code, i, a, b) check((cond), p.scratch, (code), (i), (a), (b))
+#else
+#define TOPK_CHECK(cond, code, i, a, b) true
+#endif
+
 // Source of candidate entries for the radix select: shared or global memory.
 struct SmemSrc {
   const uint2 *p;
@@ -252,10 +280,22 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_select_kernel(const __gr
     const uint64_t left = p.tile_end - base;
     const uint32_t objs = left < TILE ? (uint32_t)left : TILE;
     const uint32_t bytes = objs * 4u;
+#ifdef TOPK_BOUNDS_CHECK
+    if (i >= S && !TOPK_CHECK(mbar_test_parity(&full[s], ((i - S) / S) & 1u), kDiagPhase, i, s, 0)) return;
+#endif
     mbar_arrive_expect_tx(&full[s], bytes * qq);
-    for (uint32_t m = 0; m < qq; ++m)
-      bulk_g2s(stage + ((size_t)s * qq + m) * TILE, p.table + (uint64_t)p.attr[m] * p.ld + base, bytes,
-               &full[s]);
+    for (uint32_t m = 0; m < qq; ++m) {
+      float *dst = stage + ((size_t)s * qq + m) * TILE;
+      const float *src = p.table + (uint64_t)p.attr[m] * p.ld + base;
+      if (!TOPK_CHECK(objs > 0 && (bytes & 15u) == 0 && ((uintptr_t)dst & 15u) == 0 &&
+                          (const unsigned char *)dst + bytes <= (const unsigned char *)cand,
+                      kDiagCopyShape, i, m, bytes))
+        continue;
+      if (!TOPK_CHECK(((uintptr_t)src & 15u) == 0 && base + objs <= p.ld && p.attr[m] < 255, kDiagCopySource, i,
+                      m, (uint32_t)base))
+        continue;
+      bulk_g2s(dst, src, bytes, &full[s]);
+    }
   };
 
   if (p.fault_mode == 1) {
@@ -306,16 +346,27 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_select_kernel(const __gr
       if ((tid & 31) >= o) incl += y;
     }
     const uint32_t wtotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    // Buffer fill after this warp's append.  The warp that appends last in a tile
+    // sees the tile's final count, so OR-voting "after > cap - TILE" at the barrier
+    // below gives every thread the same reduce decision.  (Reading ctl->count after
+    // the barrier would not: a fast warp may already be appending the next tile.)
+    uint32_t after = 0;
     if (wtotal) {
       uint32_t base = 0;
       if ((tid & 31) == 31) base = atomicAdd(&ctl->count, wtotal);
-      base = __shfl_sync(0xFFFFFFFFu, base, 31) + incl - npass;
+      base = __shfl_sync(0xFFFFFFFFu, base, 31);
+      after = base + wtotal;
+      base += incl - npass;
 #pragma unroll
       for (int v = 0; v < VEC; ++v)
-        if (pass_mask & (1u << v)) cand[base++] = make_uint2(keys[v], (uint32_t)(row0 + v));
+        if (pass_mask & (1u << v)) {
+          if (TOPK_CHECK(base < p.cap, kDiagAppend, i, base, p.cap)) cand[base] = make_uint2(keys[v], (uint32_t)(row0 + v));
+          ++base;
+        }
     }
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
+        TOPK_CHECK(false, kDiagWait, i, s, (i / S) & 1u);
         atomicOr(&p.scratch->error, 1u);
         // let this CTA's own copies still in flight land (bounded) before leaving
         for (uint32_t j = i; j < i + S && j < my_tiles; ++j)
@@ -324,7 +375,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_select_kernel(const __gr
       return;
     }
     if (tid == 0 && i + S < my_tiles) issue(i + S);
-    if (ctl->count > p.cap - TILE) {
+    if (__syncthreads_or(after > p.cap - TILE)) {
       if (tid == 0) ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
       __syncthreads();
       const uint32_t min_key = max(ctl->thr_g, 0u);

@@ -278,9 +278,11 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
     ScanScratch s{};
     cudaMemcpy(&s, c->scratch, sizeof(s), cudaMemcpyDeviceToHost);
     cudaMemset(c->scratch, 0, sizeof(ScanScratch));
-    if (s.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
-    return fail(TOPK_ERR_CUDA, "scan did not complete (count %u, expected %llu, error 0x%x)", hh->count,
-                (unsigned long long)kk, s.error);
+    if (s.error & 1u)
+      return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls); diag %u block %u tile %u [%u %u]",
+                  (unsigned long long)h->wait_limit, s.diag[0], s.diag[1], s.diag[2], s.diag[3], s.diag[4]);
+    return fail(TOPK_ERR_CUDA, "scan did not complete (count %u, expected %llu, error 0x%x); diag %u block %u tile %u [%u %u]",
+                hh->count, (unsigned long long)kk, s.error, s.diag[0], s.diag[1], s.diag[2], s.diag[3], s.diag[4]);
   }
   std::memcpy(ids, c->h_res + kHdr, kk * 8);
   std::memcpy(scores, c->h_res + kHdr + kk * 8, kk * 4);

@@ -21,7 +21,21 @@ struct ScanScratch {
   uint32_t acc_reductions;  // CTA block-selects during this scan
   uint32_t last_cands;      // candidates seen by the final select of the last scan
   uint32_t last_reductions; // block-selects of the last scan
-  uint32_t pad[9];
+  // Diagnostics of a TOPK_BOUNDS_CHECK build: first failed check (code, block,
+  // tile, two values); the access it guarded was skipped.
+  uint32_t diag[5];
+  uint32_t pad[4];
+};
+
+// TOPK_BOUNDS_CHECK codes
+enum : uint32_t {
+  kDiagCopyShape = 1,   // bulk copy size/alignment/destination out of range
+  kDiagCopySource = 2,  // bulk copy source outside the table
+  kDiagPhase = 3,       // stage barrier re-armed before its previous phase completed
+  kDiagAppend = 4,      // candidate append past capacity
+  kDiagCompact = 5,     // compaction write past capacity
+  kDiagWait = 6,        // a stage wait gave up
+  kDiagOutput = 7,      // output index out of range
 };
 
 struct ScanParams {

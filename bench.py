@@ -276,12 +276,13 @@ def main():
         elapsed_ms = float(tt.item())
 
     # per-launch durations -> roofline of the fused scan kernel
-    bytes_by_q, time_by_q = {}, {}
+    bytes_by_q, time_by_q, time_by_qk = {}, {}, {}
     for s in range(args.steps):
         for j, (k, q, w, a) in enumerate(queries):
             ms = per_launch[s][j][0].elapsed_time(per_launch[s][j][1])
             bytes_by_q[q] = bytes_by_q.get(q, 0.0) + 4.0 * n * q
             time_by_q[q] = time_by_q.get(q, 0.0) + ms
+            time_by_qk[f"q{q}_k{k}"] = time_by_qk.get(f"q{q}_k{k}", 0.0) + ms / args.steps
     tot_bytes = sum(bytes_by_q.values())
     tot_ms = sum(time_by_q.values())
     achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
@@ -339,6 +340,7 @@ def main():
             "traffic": traffic_per_launch,
             "per_q": {str(q): {"gbs": bytes_by_q[q] / (time_by_q[q] * 1e-3) / 1e9,
                                "ms_per_launch": time_by_q[q] / (args.steps * len(KS))} for q in QS},
+            "ms_per_query": {key: round(v, 4) for key, v in time_by_qk.items()},
         },
         "e2e": {"value": world * len(queries) * 1000.0 / e2e_ms, "unit": "queries/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -134,6 +134,10 @@ int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float 
 int topk_count_ge(topk_table_t h, uint64_t row_begin, uint64_t row_end, uint32_t qq, const float *weights,
                   const uint8_t *attr, float thr, uint64_t *count_ge, uint64_t *count_gt);
 
+/* Tuning entry (no reference counterpart): the most CTAs of the fused scan per SM
+ * (0 = as many as fit, up to 8).  Results do not depend on it. */
+int topk_set_scan_tuning(topk_table_t h, uint32_t max_ctas_per_sm);
+
 /* Test entry (no reference counterpart): mode 1 makes the next fused scans wait,
  * before any copy is issued, on a barrier that nothing completes, so the bounded
  * wait runs out and the call returns TOPK_ERR_TIMEOUT; 0 turns it off.  Host-side

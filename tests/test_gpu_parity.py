@@ -332,3 +332,24 @@ def test_scan_stats_reported():
         cands, reds = t.last_stats()
         assert 64 <= cands <= 148 * 4 * 4096
         assert reds >= 0
+
+
+def test_scan_tuning_does_not_change_results():
+    """The CTAs-per-SM cap (grid size, merge-tree shape) is a performance knob only."""
+    n, d = (1 << 20) + 12, 16
+    rng = np.random.default_rng(9)
+    with T.Table(n, d) as t:
+        t.generate(3, 12)
+        t.normalize()
+        tn = t.download()
+        w, a = H.random_query(rng, d)
+        want = O.topk_numpy(tn, 200, w, a)
+        for ctas in (1, 2, 3, 8, 0):
+            t.set_scan_tuning(ctas)
+            for q in (1, 2, 5, 12, 16, 17):
+                aq = (np.arange(q) % d).astype(np.uint8)  # q = 17 repeats attribute 0
+                H.assert_same_result(t.query(77, w, aq), O.topk_numpy(tn, 77, w, aq))
+            H.assert_same_result(t.query(200, w, a), want)
+            H.assert_same_result(t.query(4096, w, a), O.topk_numpy(tn, 4096, w, a))
+        with pytest.raises(T.TopKError):
+            t.set_scan_tuning(9)

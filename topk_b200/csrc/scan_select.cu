@@ -5,24 +5,25 @@
 //     s = 0; for m in attr order: s = s + x[attr[m]] * w[attr[m]]   (RN mul, RN add)
 // and the same result (the k best by score; ties here go to the lower id).
 //
-// Design, per persistent CTA (256 threads, one or more per SM):
-//   * Only the qq queried columns are streamed.  For each tile of TILE objects the
-//     elected thread issues one cp.async.bulk (TMA engine) copy per column into a
-//     multi-stage shared-memory ring, completing on an mbarrier; the ring keeps
-//     several tiles in flight per SM, which is what saturates HBM.
-//   * Threads read their objects from shared memory with 128/64/32-bit loads and
-//     score them; an object passes if its key >= the running threshold.  Passing
-//     objects go to a shared candidate buffer (warp-aggregated append).
-//   * When the buffer nears capacity the CTA selects its top-k by an 8-bit radix
-//     select on the 64-bit (key, ~id) word, keeps those k, raises its local
-//     threshold and publishes its k-th key with atomicMax to a global word that
-//     every CTA folds into its own filter.  Any CTA's k-th best lower-bounds the
-//     global k-th best, so nothing that can win is dropped.
-//   * At the end each CTA appends its survivors to a global list; the last CTA to
-//     finish selects the final top-k from it, sorts (bitonic) and writes the
-//     result, then zeroes the scratch for the next query.
-// Every mbarrier wait is bounded; a wait that runs out sets scratch->error and the
-// CTA leaves uniformly.
+// Persistent CTAs of 256 threads, several per SM:
+//   * Each tile is 1024 objects (4 per thread).  A thread issues one 128-bit
+//     streaming load (ld.global.cs) per queried column for its 4 objects, all of
+//     them before the first multiply, so each warp keeps q x 512 bytes in flight and
+//     an SM with several CTAs keeps far more than the ~45 KB that HBM3e latency
+//     needs.  Only the queried columns are read.  (A TMA bulk-copy ring with a
+//     producer warp was measured on this GPU at 2.6-4.9 TB/s against 3.1-5.9 TB/s
+//     for plain loads, so the scan uses plain loads.)
+//   * An object passes if its score is >= the running threshold; passing objects
+//     go to a shared candidate buffer (warp-aggregated append).  When the buffer
+//     nears capacity (a barrier vote, so every thread decides alike) the CTA keeps
+//     its top-k by an 8-bit radix select on the 64-bit (key, ~id) word, raises its
+//     own threshold and publishes its k-th key with atomicMax to a global word that
+//     every CTA folds into its filter.  Any CTA's k-th best lower-bounds the global
+//     k-th best, so nothing that can win is dropped.
+//   * End: a merge tree with fan-in G.  Each CTA writes its survivors to a slot; the
+//     last CTA of each group of G slots (per-group arrival counter) merges them to k
+//     entries in shared memory and moves up; the root sorts (bitonic) and writes the
+//     result.  Counters are put back to zero for the next query.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -34,23 +35,34 @@ namespace topk {
 namespace {
 
 struct SmemCtl {
-  uint32_t count;       // entries in cand[]
-  uint32_t thr_local;   // min key that can still enter (k-th local key + 1)
-  uint32_t thr_g;       // copy of the global threshold
-  uint32_t kept_min;    // min key among kept entries (select result)
+  uint32_t count;      // entries in the current candidate buffer
+  uint32_t cur;        // which of the two candidate buffers is current
+  uint32_t thr_local;  // min key that can still enter (k-th CTA key + 1)
+  uint32_t thr_g;      // CTA copy of the global threshold
+  uint32_t kept_min;   // min key among kept entries (select result)
   uint32_t digit, above, eq, valid;
-  uint32_t wcount;      // compaction write cursor
-  uint32_t is_last;
+  uint32_t wcount;     // compaction / append cursor
   uint32_t reductions;
-  uint32_t timed_out;
-  uint32_t base;        // global append base
+  uint32_t is_last;
+  uint32_t red_g;      // threshold snapshot shared by the block
   uint32_t pad[3];
 };
 
-// shared layout: [0,64) stage barriers, [64,72) test barrier, [128,192) SmemCtl,
-// then the radix histogram, the stage ring and the candidate buffer.
-constexpr int kCtlBytes = 256;
-constexpr int kHistBytes = 256 * 4;
+// shared layout
+constexpr int kOffCtl = 0;        // SmemCtl (64 B)
+constexpr int kOffMinMax = 64;    // two u64: min / max composite of a select
+constexpr int kOffNever = 80;     // test barrier (u64)
+constexpr int kOffHist = 128;     // 256-bin radix histogram
+constexpr int kOffWsm = 1152;     // weights of the runtime-q path (kMaxQ floats)
+constexpr int kOffCand = kScanSmemFixed;
+static_assert(kOffWsm + 4 * (int)kMaxQ <= kScanSmemFixed, "fixed shared block");
+static_assert(sizeof(SmemCtl) == 64, "control block layout");
+static_assert(kScanThreads == 256, "one histogram bin per thread");
+
+constexpr int kVec = 4;                      // objects per thread per tile
+constexpr uint32_t kTile = kScanThreads * kVec;
+
+__device__ __forceinline__ void bsync() { __syncthreads(); }
 
 // TOPK_BOUNDS_CHECK: record the first failed check in scratch->diag and tell the
 // caller to skip the guarded access.  Compiled out of the product build.
@@ -64,71 +76,103 @@ __device__ __forceinline__ bool check(bool ok, ScanScratch *s, uint32_t code, ui
   }
   return ok;
 }
-__device__ __forceinline__ bool mbar_test_parity(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n"
-      " mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
 #define TOPK_CHECK(cond, code, i, a, b) check((cond), p.scratch, (code), (i), (a), (b))
 #else
-#define TOPK_CHECK(cond, code, i, a, b) true
+#define TOPK_CHECK(cond, code, i, a, b) (true)
 #endif
 
-// Source of candidate entries for the radix select: shared or global memory.
+// Source of candidate entries for the radix select.
 struct SmemSrc {
   const uint2 *p;
   __device__ uint2 operator()(uint32_t j) const { return p[j]; }
 };
-struct GlobalSrc {
-  const uint2 *p;
-  __device__ uint2 operator()(uint32_t j) const { return __ldcg(p + j); }
-};
 
-// Block-wide radix select over `count` entries of `src` that have key >= min_key:
-// finds (prefix, mask) such that exactly `need` valid entries satisfy
+// Block-wide radix select over `count` entries of `src` with key >= min_key: finds
+// (prefix, mask) such that exactly `need` valid entries satisfy
 // (composite & mask) >= prefix.  Requires need <= number of valid entries.
+// Digits are taken from the highest bit where the valid entries differ (min/max of
+// the composites first), 8 bits at a time; histogram updates are aggregated per
+// warp with __match_any_sync, because candidates crowd into few bins.
 template <class Src>
 __device__ void block_radix_select(const Src &src, uint32_t count, uint32_t min_key, uint32_t need,
-                                   uint32_t *hist, SmemCtl *ctl, uint64_t &prefix_out,
+                                   uint32_t *hist, SmemCtl *ctl, unsigned long long *mm, uint64_t &prefix_out,
                                    uint64_t &mask_out) {
-  const int tid = threadIdx.x;
-  uint64_t prefix = 0, mask = 0;
-  for (int shift = 56; shift >= 0; shift -= 8) {
-    hist[tid] = 0;  // kScanThreads == 256 bins
-    __syncthreads();
-    for (uint32_t j = tid; j < count; j += kScanThreads) {
-      uint2 e = src(j);
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  if (t == 0) {
+    mm[0] = ~0ull;
+    mm[1] = 0ull;
+  }
+  bsync();
+  {
+    unsigned long long lo = ~0ull, hi = 0ull;
+    for (uint32_t j = t; j < count; j += kScanThreads) {
+      const uint2 e = src(j);
       if (e.x < min_key) continue;
-      uint64_t c = composite(e.x, e.y);
-      if ((c & mask) == prefix) atomicAdd(&hist[(uint32_t)(c >> shift) & 255u], 1u);
+      const unsigned long long c = composite(e.x, e.y);
+      lo = c < lo ? c : lo;
+      hi = c > hi ? c : hi;
     }
-    __syncthreads();
-    if (tid < 32) {
-      // lane l owns bins [255-8l-7, 255-8l], visited from high to low.
-      const int hi = 255 - 8 * tid;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long a = __shfl_xor_sync(0xFFFFFFFFu, lo, o);
+      const unsigned long long b = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+      lo = a < lo ? a : lo;
+      hi = b > hi ? b : hi;
+    }
+    if (lane == 0) {
+      atomicMin(&mm[0], lo);
+      atomicMax(&mm[1], hi);
+    }
+  }
+  bsync();
+  const uint64_t cmin = mm[0], cmax = mm[1];
+  const uint64_t diff = cmin ^ cmax;
+  int hib = diff ? 63 - __clzll((long long)diff) : -1;  // highest differing bit
+  uint64_t mask = hib >= 63 ? 0ull : (~0ull << (hib + 1));
+  uint64_t prefix = cmin & mask;
+  while (hib >= 0) {
+    const int lob = hib >= 7 ? hib - 7 : 0;
+    const uint32_t dmask = (1u << (hib - lob + 1)) - 1u;
+    hist[t] = 0;
+    bsync();
+    for (uint32_t base = 0; base < count; base += kScanThreads) {  // uniform trip count
+      const uint32_t j = base + t;
+      uint32_t bin = 0xFFFFFFFFu;
+      if (j < count) {
+        const uint2 e = src(j);
+        if (e.x >= min_key) {
+          const uint64_t c = composite(e.x, e.y);
+          if ((c & mask) == prefix) bin = (uint32_t)(c >> lob) & dmask;
+        }
+      }
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+      if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+    }
+    bsync();
+    if (t < 32) {
+      // lane l owns bins [255-8l-7, 255-8l], visited from high to low
+      const int top = 255 - 8 * t;
       uint32_t local[8];
       uint32_t s = 0;
 #pragma unroll
-      for (int b = 0; b < 8; ++b) { local[b] = hist[hi - b]; s += local[b]; }
+      for (int b = 0; b < 8; ++b) {
+        local[b] = hist[top - b];
+        s += local[b];
+      }
       uint32_t incl = s;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (tid >= o) incl += v;
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (t >= o) incl += v;
       }
-      uint32_t excl = incl - s;
+      const uint32_t excl = incl - s;
       if (excl < need && need <= incl) {
         uint32_t run = excl;
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
           if (run + local[b] >= need) {
-            ctl->digit = (uint32_t)(hi - b);
+            ctl->digit = (uint32_t)(top - b);
             ctl->above = run;
             ctl->eq = local[b];
             break;
@@ -137,423 +181,457 @@ __device__ void block_radix_select(const Src &src, uint32_t count, uint32_t min_
         }
       }
     }
-    __syncthreads();
+    bsync();
     const uint32_t digit = ctl->digit, above = ctl->above, eq = ctl->eq;
-    __syncthreads();  // everyone read ctl before it is rewritten next pass
+    bsync();  // everyone has read ctl before the next pass rewrites it
     need -= above;
-    prefix |= (uint64_t)digit << shift;
-    mask |= (uint64_t)0xFFu << shift;
+    prefix |= (uint64_t)digit << lob;
+    mask |= (uint64_t)dmask << lob;
     if (eq == need) break;
+    hib = lob - 1;
   }
   prefix_out = prefix;
   mask_out = mask;
 }
 
-// Reduce the shared candidate buffer to its best k valid entries (in place).
-// Valid = key >= min_key.  Updates ctl->count; returns true and sets
-// ctl->kept_min when exactly k entries remain (the CTA then knows a k-th key).
-template <int R>
-__device__ bool block_reduce(uint2 *cand, uint32_t k, uint32_t min_key, uint32_t *hist, SmemCtl *ctl) {
-  const int tid = threadIdx.x;
-  const uint32_t count = ctl->count;
-  // count valid entries
+// Keep the best k entries with key >= min_key of src[0..count), written to dst
+// (out of place).  Returns the number kept; ctl->kept_min gets their min key.
+__device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, uint32_t k, uint32_t min_key,
+                                 uint32_t *hist, SmemCtl *ctl, unsigned long long *mm) {
+  const int t = threadIdx.x;
   uint32_t v = 0;
-  for (uint32_t j = tid; j < count; j += kScanThreads) v += (cand[j].x >= min_key);
+  for (uint32_t j = t; j < count; j += kScanThreads) v += (src[j].x >= min_key);
   v = warp_sum_u32(v);
-  if (tid == 0) { ctl->valid = 0; ctl->wcount = 0; ctl->kept_min = 0xFFFFFFFFu; }
-  __syncthreads();
-  if ((tid & 31) == 0) atomicAdd(&ctl->valid, v);
-  __syncthreads();
+  if (t == 0) {
+    ctl->valid = 0;
+    ctl->wcount = 0;
+    ctl->kept_min = 0xFFFFFFFFu;
+  }
+  bsync();
+  if ((t & 31) == 0) atomicAdd(&ctl->valid, v);
+  bsync();
   const uint32_t valid = ctl->valid;
   uint64_t prefix = 0, mask = 0;
   const bool select = valid > k;
-  if (select) block_radix_select(SmemSrc{cand}, count, min_key, k, hist, ctl, prefix, mask);
-  // compaction: pull my entries into registers, then write the kept ones back
-  uint2 mine[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    uint32_t j = tid + r * kScanThreads;
-    mine[r] = (j < count) ? cand[j] : make_uint2(0u, 0xFFFFFFFFu);
-  }
-  __syncthreads();
+  if (select) block_radix_select(SmemSrc{src}, count, min_key, k, hist, ctl, mm, prefix, mask);
   uint32_t kmin = 0xFFFFFFFFu;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    uint32_t j = tid + r * kScanThreads;
-    bool keep = j < count && mine[r].x >= min_key &&
-                (!select || (composite(mine[r].x, mine[r].y) & mask) >= prefix);
-    unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
-    uint32_t base = 0;
-    if ((tid & 31) == 0 && bal) base = atomicAdd(&ctl->wcount, (uint32_t)__popc(bal));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  for (uint32_t base = 0; base < count; base += kScanThreads) {  // uniform trip count
+    const uint32_t j = base + t;
+    uint2 e = make_uint2(0u, 0u);
+    bool keep = false;
+    if (j < count) {
+      e = src[j];
+      keep = e.x >= min_key && (!select || (composite(e.x, e.y) & mask) >= prefix);
+    }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+    uint32_t pos = 0;
+    if ((t & 31) == 0 && bal) pos = atomicAdd(&ctl->wcount, (uint32_t)__popc(bal));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
     if (keep) {
-      cand[base + __popc(bal & ((1u << (tid & 31)) - 1u))] = mine[r];
-      kmin = min(kmin, mine[r].x);
+      dst[pos + __popc(bal & ((1u << (t & 31)) - 1u))] = e;
+      kmin = min(kmin, e.x);
     }
   }
   kmin = warp_min_u32(kmin);
-  if ((tid & 31) == 0) atomicMin(&ctl->kept_min, kmin);
-  __syncthreads();
-  if (tid == 0) ctl->count = ctl->wcount;
-  __syncthreads();
-  return ctl->count == k;
+  if ((t & 31) == 0) atomicMin(&ctl->kept_min, kmin);
+  bsync();
+  const uint32_t kept = ctl->wcount;
+  bsync();  // every thread has its copy before thread 0 may reset wcount
+  return kept;
 }
 
-// Sort cand[0..n) descending by composite (bitonic, padded to a power of two).
-__device__ void block_sort_desc(uint2 *cand, uint32_t n, uint32_t pcap) {
-  const int tid = threadIdx.x;
+// Sort a[0..n) descending by composite (bitonic, padded to a power of two; the
+// caller guarantees room for the padding).
+__device__ void block_sort_desc(uint2 *a, uint32_t n) {
+  const int t = threadIdx.x;
   uint32_t P = 1;
   while (P < n) P <<= 1;
-  (void)pcap;
-  for (uint32_t j = n + tid; j < P; j += kScanThreads) cand[j] = make_uint2(0u, 0xFFFFFFFFu);
-  __syncthreads();
+  for (uint32_t j = n + t; j < P; j += kScanThreads) a[j] = make_uint2(0u, 0xFFFFFFFFu);
+  bsync();
   for (uint32_t size = 2; size <= P; size <<= 1) {
     for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-      for (uint32_t i = tid; i < P / 2; i += kScanThreads) {
-        uint32_t lo = 2 * i - (i & (stride - 1));
-        uint32_t hi = lo + stride;
-        bool desc = (lo & size) == 0;
-        uint2 a = cand[lo], b = cand[hi];
-        uint64_t ca = composite(a.x, a.y), cb = composite(b.x, b.y);
-        if (desc ? (ca < cb) : (ca > cb)) { cand[lo] = b; cand[hi] = a; }
+      for (uint32_t i = t; i < P / 2; i += kScanThreads) {
+        const uint32_t lo = 2 * i - (i & (stride - 1));
+        const uint32_t hi = lo + stride;
+        const bool desc = (lo & size) == 0;
+        const uint2 x = a[lo], y = a[hi];
+        const uint64_t cx = composite(x.x, x.y), cy = composite(y.x, y.y);
+        if (desc ? (cx < cy) : (cx > cy)) {
+          a[lo] = y;
+          a[hi] = x;
+        }
       }
-      __syncthreads();
+      bsync();
     }
   }
 }
 
-template <int VEC>
-struct VecLoad;
-template <>
-struct VecLoad<1> {
-  __device__ static void load(const float *p, float *x) { x[0] = p[0]; }
-};
-template <>
-struct VecLoad<2> {
-  __device__ static void load(const float *p, float *x) {
-    float2 v = *reinterpret_cast<const float2 *>(p);
-    x[0] = v.x; x[1] = v.y;
-  }
-};
-template <>
-struct VecLoad<4> {
-  __device__ static void load(const float *p, float *x) {
-    float4 v = *reinterpret_cast<const float4 *>(p);
-    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
-  }
-};
+// Lowest float whose key is >= thr, for thr > 0: keys 1..key(-inf) are the
+// negative-NaN patterns no score maps to, so they all mean "any number".
+__device__ __forceinline__ float thr_float(uint32_t thr) {
+  return thr <= 0x007FFFFFu ? __int_as_float(0xFF800000) : key2f(thr);
+}
 
-// R = max candidate entries per thread in block_reduce (cap / 256).
-template <int VEC, int R>
-__global__ void __launch_bounds__(kScanThreads, 1) scan_select_kernel(const __grid_constant__ ScanParams p) {
-  constexpr uint32_t TILE = kScanThreads * VEC;
-  extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *never = reinterpret_cast<uint64_t *>(smem + 64);
-  SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + 128);
-  uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kCtlBytes);
-  float *stage = reinterpret_cast<float *>(smem + kCtlBytes + kHistBytes);
-  uint2 *cand = reinterpret_cast<uint2 *>(stage + (size_t)p.stages * p.qq * TILE);
+__device__ __forceinline__ float4 ld_stream(const float *p) { return __ldcs(reinterpret_cast<const float4 *>(p)); }
 
-  const int tid = threadIdx.x;
-  const uint32_t qq = p.qq;
-  const uint32_t S = p.stages;
+// Scores of this thread's 4 objects at rows [row0, row0+4) of one tile, reference
+// order.  QQ > 0: compile-time attribute count, every load issued before the first
+// multiply, weights as constant-bank operands.  QQ == 0: runtime count, weights
+// from shared memory.  `guard`: partial tile, load only below tile_end.
+template <int QQ>
+__device__ __forceinline__ float4 score4(const ScanParams &p, const float *wsm, uint32_t qq, uint64_t row0,
+                                         bool guard) {
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+  const bool inb = !guard || row0 < p.tile_end;  // tile_end <= ld, multiple of 4
+  if constexpr (QQ > 0) {
+    float4 x[QQ];
+#pragma unroll
+    for (int m = 0; m < QQ; ++m)
+      x[m] = inb ? ld_stream(p.table + (uint64_t)p.attr[m] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < QQ; ++m) {
+      const float w = p.w[m];
+      a0 = __fadd_rn(a0, __fmul_rn(x[m].x, w));
+      a1 = __fadd_rn(a1, __fmul_rn(x[m].y, w));
+      a2 = __fadd_rn(a2, __fmul_rn(x[m].z, w));
+      a3 = __fadd_rn(a3, __fmul_rn(x[m].w, w));
+    }
+  } else {
+    uint32_t m = 0;
+    for (; m + 4 <= qq; m += 4) {  // four loads in flight at a time
+      float4 x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        x[u] = inb ? ld_stream(p.table + (uint64_t)p.attr[m + u] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float w = wsm[m + u];
+        a0 = __fadd_rn(a0, __fmul_rn(x[u].x, w));
+        a1 = __fadd_rn(a1, __fmul_rn(x[u].y, w));
+        a2 = __fadd_rn(a2, __fmul_rn(x[u].z, w));
+        a3 = __fadd_rn(a3, __fmul_rn(x[u].w, w));
+      }
+    }
+    for (; m < qq; ++m) {
+      const float4 x = inb ? ld_stream(p.table + (uint64_t)p.attr[m] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float w = wsm[m];
+      a0 = __fadd_rn(a0, __fmul_rn(x.x, w));
+      a1 = __fadd_rn(a1, __fmul_rn(x.y, w));
+      a2 = __fadd_rn(a2, __fmul_rn(x.z, w));
+      a3 = __fadd_rn(a3, __fmul_rn(x.w, w));
+    }
+  }
+  return make_float4(a0, a1, a2, a3);
+}
+
+// QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).
+template <int QQ>
+__global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_constant__ ScanParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + kOffCtl);
+  unsigned long long *mm = reinterpret_cast<unsigned long long *>(smem + kOffMinMax);
+  uint64_t *never = reinterpret_cast<uint64_t *>(smem + kOffNever);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffHist);
+  float *wsm = reinterpret_cast<float *>(smem + kOffWsm);
+  uint2 *cand0 = reinterpret_cast<uint2 *>(smem + kOffCand);  // two buffers of cap entries
+  uint2 *mbuf = cand0;                                         // merge area (reuses both)
+
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  const uint32_t qq = QQ > 0 ? (uint32_t)QQ : p.qq;
+  const uint32_t cap = p.cap;
   const uint32_t my_tiles =
       blockIdx.x < p.num_tiles ? (p.num_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-  if (tid == 0) {
-    for (uint32_t s = 0; s < S; ++s) mbar_init(&full[s], 1);
+  if (QQ == 0 && t < (int)kMaxQ && t < (int)qq) wsm[t] = p.w[t];
+  if (t == 0) {
     mbar_init(never, 1);
     fence_barrier_init();
     ctl->count = 0;
+    ctl->cur = 0;
     ctl->thr_local = 0;
     ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
     ctl->reductions = 0;
-    ctl->timed_out = 0;
   }
-  __syncthreads();
-
-  auto issue = [&](uint32_t i) {
-    const uint32_t s = i % S;
-    const uint64_t t = blockIdx.x + (uint64_t)i * gridDim.x;
-    const uint64_t base = p.tile_begin + t * TILE;
-    const uint64_t left = p.tile_end - base;
-    const uint32_t objs = left < TILE ? (uint32_t)left : TILE;
-    const uint32_t bytes = objs * 4u;
-#ifdef TOPK_BOUNDS_CHECK
-    if (i >= S && !TOPK_CHECK(mbar_test_parity(&full[s], ((i - S) / S) & 1u), kDiagPhase, i, s, 0)) return;
-#endif
-    mbar_arrive_expect_tx(&full[s], bytes * qq);
-    for (uint32_t m = 0; m < qq; ++m) {
-      float *dst = stage + ((size_t)s * qq + m) * TILE;
-      const float *src = p.table + (uint64_t)p.attr[m] * p.ld + base;
-      if (!TOPK_CHECK(objs > 0 && (bytes & 15u) == 0 && ((uintptr_t)dst & 15u) == 0 &&
-                          (const unsigned char *)dst + bytes <= (const unsigned char *)cand,
-                      kDiagCopyShape, i, m, bytes))
-        continue;
-      if (!TOPK_CHECK(((uintptr_t)src & 15u) == 0 && base + objs <= p.ld && p.attr[m] < 255, kDiagCopySource, i,
-                      m, (uint32_t)base))
-        continue;
-      bulk_g2s(dst, src, bytes, &full[s]);
-    }
-  };
+  bsync();
 
   if (p.fault_mode == 1) {
-    // Test hook: wait, before any copy is in flight, on a barrier that nothing
-    // arrives on.  The bounded wait runs out and the scan reports a timeout.
+    // Test hook: wait on a barrier that nothing arrives on.  The bounded wait runs
+    // out and the scan reports a timeout; nothing else is in flight.
     const bool ok = mbar_wait_bounded(never, 0, p.wait_limit);
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(&p.scratch->error, 1u);
+      if (t == 0) atomicOr(&p.scratch->error, 1u);
       return;
     }
   }
 
-  if (tid == 0)
-    for (uint32_t i = 0; i < S && i < my_tiles; ++i) issue(i);
-
+  uint32_t g_pending = 0;  // thread 0's in-flight copy of the global threshold
   for (uint32_t i = 0; i < my_tiles; ++i) {
-    const uint32_t s = i % S;
-    const bool ok = mbar_wait_bounded(&full[s], (i / S) & 1u, p.wait_limit);
-    const uint64_t t = blockIdx.x + (uint64_t)i * gridDim.x;
-    const uint64_t row0 = p.tile_begin + t * TILE + (uint64_t)tid * VEC;
-    const uint32_t thr = max(ctl->thr_local, *reinterpret_cast<volatile uint32_t *>(&ctl->thr_g));
+    const uint64_t tile0 = p.tile_begin + (blockIdx.x + (uint64_t)i * gridDim.x) * kTile;
+    const uint64_t row0 = tile0 + (uint64_t)t * kVec;
+    const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
+    const uint32_t thr = max(ctl->thr_local, ctl->thr_g);
+    const float4 s = score4<QQ>(p, wsm, qq, row0, !interior);
 
-    float acc[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = 0.0f;
-    const float *col = stage + (size_t)s * qq * TILE + tid * VEC;
-    for (uint32_t m = 0; m < qq; ++m) {
-      float x[VEC];
-      VecLoad<VEC>::load(col + (size_t)m * TILE, x);
-      const float w = p.w[m];
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) acc[v] = __fadd_rn(acc[v], __fmul_rn(x[v], w));
-    }
-    // filter and append
-    uint32_t keys[VEC];
+    // key(score) >= thr  <=>  thr == 0 (everything, NaN included) or score >= thr_float(thr)
+    const bool take_all = thr == 0u;
+    const float thr_f = thr_float(thr);
+    const float sv[4] = {s.x, s.y, s.z, s.w};
     unsigned pass_mask = 0;
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) {
-      keys[v] = f2key(acc[v]);
-      const uint64_t row = row0 + v;
-      if (row >= p.row_begin && row < p.row_end && keys[v] >= thr) pass_mask |= 1u << v;
+    for (int v = 0; v < 4; ++v) {
+      bool pv = take_all || sv[v] >= thr_f;
+      if (!interior) pv = pv && row0 + v >= p.row_begin && row0 + v < p.row_end;
+      pass_mask |= (unsigned)pv << v;
     }
-    uint32_t npass = __popc(pass_mask);
-    uint32_t incl = npass;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if ((tid & 31) >= o) incl += y;
-    }
-    const uint32_t wtotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    // Buffer fill after this warp's append.  The warp that appends last in a tile
+    // `after` = fill after this warp's append.  The warp that appends last in a tile
     // sees the tile's final count, so OR-voting "after > cap - TILE" at the barrier
-    // below gives every thread the same reduce decision.  (Reading ctl->count after
-    // the barrier would not: a fast warp may already be appending the next tile.)
+    // gives every thread the same reduce decision.  (Reading ctl->count after a
+    // barrier would not: a fast warp may already be appending the next tile.)
     uint32_t after = 0;
-    if (wtotal) {
+    if (__ballot_sync(0xFFFFFFFFu, pass_mask != 0u)) {  // warp-uniform: some lane passed
+      uint2 *cand = cand0 + (size_t)ctl->cur * cap;
+      const uint32_t npass = __popc(pass_mask);
+      uint32_t incl = npass;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const uint32_t wtotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
       uint32_t base = 0;
-      if ((tid & 31) == 31) base = atomicAdd(&ctl->count, wtotal);
+      if (lane == 31) base = atomicAdd(&ctl->count, wtotal);
       base = __shfl_sync(0xFFFFFFFFu, base, 31);
       after = base + wtotal;
       base += incl - npass;
 #pragma unroll
-      for (int v = 0; v < VEC; ++v)
+      for (int v = 0; v < 4; ++v)
         if (pass_mask & (1u << v)) {
-          if (TOPK_CHECK(base < p.cap, kDiagAppend, i, base, p.cap)) cand[base] = make_uint2(keys[v], (uint32_t)(row0 + v));
+          if (TOPK_CHECK(base < cap, kDiagAppend, i, base, cap))
+            cand[base] = make_uint2(f2key(sv[v]), (uint32_t)(row0 + v));
           ++base;
         }
     }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        TOPK_CHECK(false, kDiagWait, i, s, (i / S) & 1u);
-        atomicOr(&p.scratch->error, 1u);
-        // let this CTA's own copies still in flight land (bounded) before leaving
-        for (uint32_t j = i; j < i + S && j < my_tiles; ++j)
-          mbar_wait_bounded(&full[j % S], (j / S) & 1u, p.wait_limit);
-      }
-      return;
-    }
-    if (tid == 0 && i + S < my_tiles) issue(i + S);
-    if (__syncthreads_or(after > p.cap - TILE)) {
-      if (tid == 0) ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
-      __syncthreads();
-      const uint32_t min_key = max(ctl->thr_g, 0u);
-      if (block_reduce<R>(cand, p.k, min_key, hist, ctl)) {
-        if (tid == 0) {
-          const uint32_t kth = ctl->kept_min;
-          ctl->thr_local = kth + 1u;
-          atomicMax(&p.scratch->g_thr, kth);
+    if (__syncthreads_or(after > cap - kTile)) {
+      if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
+      bsync();
+      const uint32_t c = ctl->cur;
+      const uint32_t kept = block_reduce(cand0 + (size_t)c * cap, ctl->count, cand0 + (size_t)(c ^ 1u) * cap, p.k,
+                                         ctl->red_g, hist, ctl, mm);
+      if (t == 0) {
+        ctl->cur = c ^ 1u;
+        ctl->count = kept;
+        ctl->reductions++;
+        if (kept == p.k) {  // the CTA knows a k-th key
+          ctl->thr_local = ctl->kept_min + 1u;
+          atomicMax(&p.scratch->g_thr, ctl->kept_min);
         }
       }
-      if (tid == 0) ctl->reductions++;
-      __syncthreads();
-    } else if (tid == 0) {
-      ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
+      bsync();
+    }
+    // Thread 0 loads the global threshold every 8 tiles and publishes it to the CTA
+    // 7 tiles later, so the L2 round trip is never waited on.
+    if (t == 0) {
+      if ((i & 7u) == 7u) ctl->thr_g = max(ctl->thr_g, g_pending);
+      if ((i & 7u) == 0u) g_pending = ld_volatile_u32(&p.scratch->g_thr);
     }
   }
 
-  // ---- end of scan: reduce to <= k, append survivors to the global list ----
-  __syncthreads();
-  if (tid == 0) ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
-  __syncthreads();
+  // ---- end of scan: reduce to <= k ----
+  bsync();
+  if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
+  bsync();
   if (ctl->count > p.k) {
-    if (block_reduce<R>(cand, p.k, ctl->thr_g, hist, ctl)) {
-      if (tid == 0) atomicMax(&p.scratch->g_thr, ctl->kept_min);
+    const uint32_t c = ctl->cur;
+    const uint32_t kept = block_reduce(cand0 + (size_t)c * cap, ctl->count, cand0 + (size_t)(c ^ 1u) * cap, p.k,
+                                       ctl->red_g, hist, ctl, mm);
+    if (t == 0) {
+      ctl->cur = c ^ 1u;
+      ctl->count = kept;
+      ctl->reductions++;
+      if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->kept_min);
     }
-    if (tid == 0) ctl->reductions++;
-    __syncthreads();
+    bsync();
   }
-  if (tid == 0) {
-    ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
-    ctl->wcount = 0;
-  }
-  __syncthreads();
-  {
-    const uint32_t g = ctl->thr_g;
-    const uint32_t count = ctl->count;
-    uint32_t v = 0;
-    for (uint32_t j = tid; j < count; j += kScanThreads) v += cand[j].x >= g;
-    v = warp_sum_u32(v);
-    if ((tid & 31) == 0 && v) atomicAdd(&ctl->wcount, v);
-    __syncthreads();
-    if (tid == 0) {
-      ctl->base = ctl->wcount ? atomicAdd(&p.scratch->cand_count, ctl->wcount) : 0u;
+  if (t == 0 && ctl->reductions) atomicAdd(&p.scratch->acc_reductions, ctl->reductions);
+
+  // ---- merge tree ----
+  const uint32_t k = p.k;
+  uint2 *res = cand0 + (size_t)ctl->cur * cap;
+  uint32_t res_n = ctl->count;
+  uint32_t level = 0, slot = blockIdx.x, merged = res_n;
+  uint2 *outb = mbuf + (size_t)p.fanin * k;
+  while (p.nslots[level] > 1) {
+    // publish my result into slot (level, slot), filtered by the current threshold
+    if (t == 0) {
+      ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       ctl->wcount = 0;
-      if (ctl->reductions) atomicAdd(&p.scratch->acc_reductions, ctl->reductions);
     }
-    __syncthreads();
-    const uint32_t base = ctl->base;
-    for (uint32_t j = tid; j < count; j += kScanThreads) {
-      const uint2 e = cand[j];
-      if (e.x >= g) {
-        const uint32_t slot = base + atomicAdd(&ctl->wcount, 1u);
-        if (slot < p.gcand_cap) p.gcand[slot] = e;
-        else atomicOr(&p.scratch->error, 2u);  // list sized too small (host bug)
+    bsync();
+    {
+      const uint32_t g = ctl->red_g;
+      uint2 *dst = p.slots + (size_t)(p.slot_off[level] + slot) * k;
+      for (uint32_t j = t; j < res_n; j += kScanThreads) {
+        const uint2 e = res[j];
+        if (e.x >= g) dst[atomicAdd(&ctl->wcount, 1u)] = e;  // <= res_n <= k entries
       }
     }
-  }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) ctl->is_last = (atomicAdd(&p.scratch->done, 1u) == gridDim.x - 1) ? 1u : 0u;
-  __syncthreads();
-  if (!ctl->is_last) return;
-  __threadfence();
-
-  // ---- last CTA: final select over the global list ----
-  if (tid == 0) {
-    ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
-    ctl->base = min(ld_volatile_u32(&p.scratch->cand_count), p.gcand_cap);
-    ctl->valid = 0;
-    ctl->wcount = 0;
-  }
-  __syncthreads();
-  const uint32_t g = ctl->thr_g;
-  const uint32_t total = ctl->base;
-  {
-    uint32_t v = 0;
-    for (uint32_t j = tid; j < total; j += kScanThreads) v += __ldcg(&p.gcand[j]).x >= g;
-    v = warp_sum_u32(v);
-    if ((tid & 31) == 0 && v) atomicAdd(&ctl->valid, v);
-  }
-  __syncthreads();
-  const uint32_t valid = ctl->valid;
-  const uint32_t kk = min(valid, p.k);
-  uint64_t prefix = 0, mask = 0;
-  const bool select = valid > kk;
-  if (select) block_radix_select(GlobalSrc{p.gcand}, total, g, kk, hist, ctl, prefix, mask);
-  __syncthreads();
-  if (tid == 0) ctl->wcount = 0;
-  __syncthreads();
-  for (uint32_t j = tid; j < total; j += kScanThreads) {
-    uint2 e = __ldcg(&p.gcand[j]);
-    bool keep = e.x >= g && (!select || (composite(e.x, e.y) & mask) >= prefix);
-    if (keep) {
-      const uint32_t slot = atomicAdd(&ctl->wcount, 1u);
-      if (slot < p.cap) cand[slot] = e;  // exactly kk <= k <= cap are kept
+    __threadfence();  // each writer makes its slot entries visible device-wide
+    bsync();
+    const uint32_t grp = slot / p.fanin;
+    const uint32_t first = grp * p.fanin;
+    const uint32_t gsize = min(p.fanin, p.nslots[level] - first);
+    if (t == 0) {
+      p.slot_count[p.slot_off[level] + slot] = ctl->wcount;
+      __threadfence();
+      const uint32_t arrived = atomicAdd(&p.done[p.done_off[level] + grp], 1u);
+      ctl->is_last = (arrived == gsize - 1u) ? 1u : 0u;
+      if (ctl->is_last) p.done[p.done_off[level] + grp] = 0u;  // every arrival is in: reset
     }
+    bsync();
+    if (!ctl->is_last) return;
+    __threadfence();
+    // the last arrival merges the group's slots
+    if (t == 0) {
+      ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
+      ctl->wcount = 0;
+    }
+    bsync();
+    {
+      const uint32_t g = ctl->red_g;
+      const uint32_t lim = p.fanin * k;
+      (void)lim;
+      for (uint32_t si = 0; si < gsize; ++si) {
+        const uint32_t so = p.slot_off[level] + first + si;
+        const uint32_t cnt = __ldcg(&p.slot_count[so]);
+        const uint2 *src = p.slots + (size_t)so * k;
+        for (uint32_t j = t; j < cnt; j += kScanThreads) {
+          const uint2 e = __ldcg(src + j);
+          if (e.x >= g) {
+            const uint32_t pos = atomicAdd(&ctl->wcount, 1u);
+            if (TOPK_CHECK(pos < lim, kDiagMerge, level, pos, lim)) mbuf[pos] = e;
+          }
+        }
+      }
+    }
+    bsync();
+    const uint32_t loaded = min(ctl->wcount, p.fanin * k);
+    bsync();  // every thread has `loaded` before block_reduce resets wcount
+    merged = loaded;
+    res_n = block_reduce(mbuf, loaded, outb, k, 0u, hist, ctl, mm);
+    res = outb;
+    level += 1;
+    slot = grp;
   }
-  __syncthreads();
-  block_sort_desc(cand, kk, p.cap);
-  for (uint32_t r = tid; r < kk; r += kScanThreads) {
-    const uint2 e = cand[r];
-    const uint32_t pos = kk - 1 - r;  // ascending output
+
+  // ---- root: sort and write the result (res has room for the padding) ----
+  block_sort_desc(res, res_n);
+  for (uint32_t r = t; r < res_n; r += kScanThreads) {
+    const uint2 e = res[r];
+    const uint32_t pos = res_n - 1 - r;  // ascending output
     p.out_ids[pos] = (uint64_t)e.y;
     p.out_scores[pos] = key2f(e.x);
   }
-  if (tid == 0) {
-    if (p.out_threshold) *p.out_threshold = kk ? key2f(cand[kk - 1].x) : 0.0f;
-    if (p.out_count) *p.out_count = kk;
-    p.scratch->last_cands = total;
-    p.scratch->last_reductions = ld_volatile_u32(&p.scratch->acc_reductions);
+  if (t == 0) {
+    if (p.out_threshold) *p.out_threshold = res_n ? key2f(res[res_n - 1].x) : 0.0f;
+    if (p.out_count) *p.out_count = res_n;
+    const uint32_t reds = ld_volatile_u32(&p.scratch->acc_reductions);
+    p.scratch->last_cands = merged;
+    p.scratch->last_reductions = reds;
     if (p.out_stats) {
-      p.out_stats[0] = total;
-      p.out_stats[1] = p.scratch->last_reductions;
+      p.out_stats[0] = merged;
+      p.out_stats[1] = reds;
     }
     p.scratch->acc_reductions = 0;
     p.scratch->g_thr = 0;
-    p.scratch->cand_count = 0;
-    p.scratch->done = 0;
     __threadfence();
   }
 }
 
-template <int VEC, int R>
-cudaError_t set_attr_one(size_t smem_optin) {
-  return cudaFuncSetAttribute(scan_select_kernel<VEC, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem_optin);
-}
+using ScanKernel = void (*)(ScanParams);
+
+// [q] for q = 1..16; [0] is the runtime-q kernel used for q > 16
+const ScanKernel kKernels[17] = {
+    scan_select_kernel<0>,  scan_select_kernel<1>,  scan_select_kernel<2>,  scan_select_kernel<3>,
+    scan_select_kernel<4>,  scan_select_kernel<5>,  scan_select_kernel<6>,  scan_select_kernel<7>,
+    scan_select_kernel<8>,  scan_select_kernel<9>,  scan_select_kernel<10>, scan_select_kernel<11>,
+    scan_select_kernel<12>, scan_select_kernel<13>, scan_select_kernel<14>, scan_select_kernel<15>,
+    scan_select_kernel<16>};
+
+ScanKernel kernel_for(uint32_t qq) { return kKernels[qq <= 16 ? qq : 0]; }
 
 }  // namespace
 
 cudaError_t scan_set_attributes(size_t smem_optin) {
-  cudaError_t e;
-#define TOPK_SET(V, R) \
-  if ((e = set_attr_one<V, R>(smem_optin)) != cudaSuccess) return e;
-  TOPK_SET(1, 8) TOPK_SET(1, 24) TOPK_SET(2, 8) TOPK_SET(2, 24) TOPK_SET(4, 16) TOPK_SET(4, 24)
-#undef TOPK_SET
+  for (ScanKernel f : kKernels) {
+    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(f),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_optin);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 
-ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin) {
+ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin, uint32_t max_ctas_per_sm) {
   ScanPlan pl{};
-  pl.vec = qq <= 8 ? 4 : (qq <= 16 ? 2 : 1);
-  pl.tile = kScanThreads * pl.vec;
+  pl.tile = kTile;
   uint32_t P = 1;
   while (P < k) P <<= 1;
-  uint32_t cap = k + 2 * pl.tile;
+  // after a select the buffer holds <= k entries; one tile adds <= kTile, and a select
+  // runs once the fill exceeds cap - kTile
+  uint32_t cap = k + kTile + kTile / 2;
   if (cap < P) cap = P;
   if (cap < 2048) cap = 2048;
   cap = (cap + kScanThreads - 1) / kScanThreads * kScanThreads;
   pl.cap = cap;
-  const size_t fixed = kCtlBytes + kHistBytes + (size_t)cap * 8;
-  const size_t stage_bytes = (size_t)qq * pl.tile * 4;
-  size_t budget = smem_optin > fixed ? smem_optin - fixed : 0;
-  uint32_t S = (uint32_t)(budget / stage_bytes);
-  if (S > 8) S = 8;
-  pl.stages = S;
-  pl.smem = fixed + (size_t)S * stage_bytes;
-  const uint64_t tiles = (rows + 3 + pl.tile) / pl.tile;
-  uint64_t grid = (uint64_t)num_sms;
+  // the merge reuses the two candidate buffers: fan-in G needs G*k + P entries
+  uint32_t mcap = 2 * cap;
+  uint32_t G = (mcap - P) / k;
+  if (G > 8) G = 8;
+  if (G < 2) {
+    G = 2;
+    mcap = 2 * k + P;
+  }
+  pl.fanin = G;
+  pl.mcap = mcap;
+  pl.smem = kScanSmemFixed + (size_t)mcap * 8;
+  pl.stages = pl.smem <= smem_optin ? 1u : 0u;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reinterpret_cast<const void *>(kernel_for(qq)),
+                                                    kScanThreads, pl.smem) != cudaSuccess || occ < 1)
+    occ = 1;
+  if (max_ctas_per_sm >= 1 && (uint32_t)occ > max_ctas_per_sm) occ = (int)max_ctas_per_sm;
+  pl.ctas_per_sm = occ;
+  const uint64_t tiles = (rows + 3 + kTile) / kTile;
+  uint64_t grid = (uint64_t)num_sms * (uint64_t)occ;
   if (grid > tiles) grid = tiles;
   if (grid < 1) grid = 1;
   pl.grid = (int)grid;
   return pl;
 }
 
-cudaError_t launch_scan(const ScanPlan &pl, const ScanParams &p, cudaStream_t stream) {
-  const uint32_t R = (pl.cap + kScanThreads - 1) / kScanThreads;
-  dim3 grid(pl.grid), block(kScanThreads);
-  if (pl.vec == 1) {
-    if (R <= 8) scan_select_kernel<1, 8><<<grid, block, pl.smem, stream>>>(p);
-    else scan_select_kernel<1, 24><<<grid, block, pl.smem, stream>>>(p);
-  } else if (pl.vec == 2) {
-    if (R <= 8) scan_select_kernel<2, 8><<<grid, block, pl.smem, stream>>>(p);
-    else scan_select_kernel<2, 24><<<grid, block, pl.smem, stream>>>(p);
-  } else {
-    if (R <= 16) scan_select_kernel<4, 16><<<grid, block, pl.smem, stream>>>(p);
-    else scan_select_kernel<4, 24><<<grid, block, pl.smem, stream>>>(p);
+void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *total_slots, uint32_t *total_groups) {
+  uint32_t l = 0, soff = 0, doff = 0;
+  p.nslots[0] = grid;
+  while (p.nslots[l] > 1 && l + 1 < (uint32_t)kMaxLevels) {
+    const uint32_t groups = (p.nslots[l] + fanin - 1) / fanin;
+    p.slot_off[l] = soff;
+    p.done_off[l] = doff;
+    soff += p.nslots[l];
+    doff += groups;
+    p.nslots[l + 1] = groups;
+    ++l;
   }
+  p.slot_off[l] = soff;
+  p.done_off[l] = doff;
+  p.levels = l;
+  p.fanin = fanin;
+  *total_slots = soff;
+  *total_groups = doff;
+}
+
+cudaError_t launch_scan(const ScanPlan &pl, const ScanParams &p, cudaStream_t stream) {
+  if (pl.stages < 1) return cudaErrorInvalidValue;
+  kernel_for(p.qq)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
   return cudaGetLastError();
 }
 

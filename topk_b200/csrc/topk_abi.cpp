@@ -77,9 +77,15 @@ size_t result_bytes(uint32_t k) { return kHdr + (size_t)k * 8 + (size_t)k * 4; }
 
 struct Ctx {
   cudaStream_t stream = nullptr;
+  // Device scratch of the fused scan, one allocation:
+  //   ScanScratch | done[max_groups] | slot_count[max_slots] | pad | slots[max_slots * kMaxK]
   ScanScratch *scratch = nullptr;
-  uint2 *gcand = nullptr;
-  uint32_t gcand_cap = 0;
+  uint32_t *done = nullptr;
+  uint32_t *slot_count = nullptr;
+  uint2 *slots = nullptr;
+  uint32_t max_slots = 0, max_groups = 0;
+  size_t slot_entries = 0;  // capacity of `slots`
+  size_t meta_bytes = 0;    // bytes that must be zero between queries (header + done)
   unsigned char *d_res = nullptr;  // device result block (kMaxK capacity)
   unsigned char *h_res = nullptr;  // pinned mirror
   unsigned long long *d_count2 = nullptr;
@@ -101,6 +107,7 @@ struct topk_table_s {
   size_t smem_optin = 0;
   uint64_t wait_limit = 1ull << 26;
   int fault_mode = 0;
+  uint32_t max_ctas_per_sm = 0;  // 0 = as many as fit
   uint32_t *d_minmax = nullptr;
   float *d_norm = nullptr;  // mins[d], ranges[d]
   std::mutex mu;
@@ -118,7 +125,6 @@ int ctx_create(topk_table_t h, Ctx **out) {
   auto bail = [&](cudaError_t e, const char *what) {
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaFree(c->scratch);
-    cudaFree(c->gcand);
     cudaFree(c->d_res);
     cudaFree(c->d_count2);
     if (c->h_res) cudaFreeHost(c->h_res);
@@ -127,10 +133,24 @@ int ctx_create(topk_table_t h, Ctx **out) {
   };
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
-  if ((e = cudaMalloc(&c->scratch, sizeof(ScanScratch))) != cudaSuccess) return bail(e, "scratch");
-  if ((e = cudaMemset(c->scratch, 0, sizeof(ScanScratch))) != cudaSuccess) return bail(e, "scratch memset");
-  c->gcand_cap = (uint32_t)h->num_sms * kMaxK;  // grid <= num_sms CTAs, each appends <= k entries
-  if ((e = cudaMalloc(&c->gcand, (size_t)c->gcand_cap * sizeof(uint2))) != cudaSuccess) return bail(e, "gcand");
+  // grid <= num_sms * 8 CTAs (256 threads each); with fan-in >= 2 each tree level has
+  // at most half the slots of the one below, rounded up, so slots <= 2 * grid + levels
+  // and groups <= grid + levels.  Slot entries (slots * k) have their own budget: the
+  // planner keeps grid * k within it (large k means few CTAs per SM anyway).
+  const uint32_t max_grid = (uint32_t)h->num_sms * 8u;
+  c->max_slots = 2u * max_grid + (uint32_t)kMaxLevels;
+  c->max_groups = max_grid + (uint32_t)kMaxLevels;
+  c->slot_entries = (size_t)4 * (size_t)h->num_sms * kMaxK;
+  c->meta_bytes = sizeof(ScanScratch) + (size_t)c->max_groups * 4;
+  const size_t slots_off = (c->meta_bytes + (size_t)c->max_slots * 4 + 255) / 256 * 256;
+  const size_t bytes = slots_off + c->slot_entries * sizeof(uint2);
+  unsigned char *blk = nullptr;
+  if ((e = cudaMalloc(&blk, bytes)) != cudaSuccess) return bail(e, "scan scratch");
+  c->scratch = reinterpret_cast<ScanScratch *>(blk);
+  c->done = reinterpret_cast<uint32_t *>(blk + sizeof(ScanScratch));
+  c->slot_count = reinterpret_cast<uint32_t *>(blk + c->meta_bytes);
+  c->slots = reinterpret_cast<uint2 *>(blk + slots_off);
+  if ((e = cudaMemset(blk, 0, slots_off)) != cudaSuccess) return bail(e, "scratch memset");
   if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
   if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
   if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK), cudaHostAllocDefault)) != cudaSuccess)
@@ -144,7 +164,6 @@ void ctx_free(Ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaFree(c->scratch);
-  cudaFree(c->gcand);
   cudaFree(c->d_res);
   cudaFree(c->d_count2);
   cudaFree(c->d_ids_scratch);
@@ -206,8 +225,12 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
                  const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_thr,
                  uint32_t *d_count, uint32_t *d_stats = nullptr) {
   const uint64_t rows = r1 - r0;
-  ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin);
+  ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin, h->max_ctas_per_sm);
   if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)k);
+  // keep the merge tree's slot entries (< (2 * grid + levels) * k) within the context budget
+  const uint64_t max_grid_k = (c->slot_entries / k - (uint64_t)kMaxLevels) / 2;
+  if ((uint64_t)pl.grid > max_grid_k) pl.grid = (int)max_grid_k;
+  if ((uint64_t)pl.grid > c->max_groups - (uint64_t)kMaxLevels) pl.grid = (int)(c->max_groups - kMaxLevels);
   ScanParams p{};
   p.table = h->table;
   p.ld = h->ld;
@@ -222,13 +245,18 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   p.qq = qq;
   p.k = (uint32_t)k;
   p.cap = pl.cap;
-  p.stages = pl.stages;
-  p.gcand_cap = c->gcand_cap;
-  if ((uint64_t)pl.grid * k > c->gcand_cap) return fail(TOPK_ERR_UNSUPPORTED, "candidate list too small");
+  p.mcap = pl.mcap;
+  uint32_t tree_slots = 0, tree_groups = 0;
+  plan_merge_tree(p, (uint32_t)pl.grid, pl.fanin, &tree_slots, &tree_groups);
+  if (tree_slots > c->max_slots || tree_groups > c->max_groups || p.nslots[p.levels] != 1 ||
+      (size_t)tree_slots * k > c->slot_entries)
+    return fail(TOPK_ERR_UNSUPPORTED, "merge tree of %d CTAs does not fit the scratch", pl.grid);
   p.wait_limit = h->wait_limit;
   p.fault_mode = (uint32_t)h->fault_mode;
   p.scratch = c->scratch;
-  p.gcand = c->gcand;
+  p.slots = c->slots;
+  p.slot_count = c->slot_count;
+  p.done = c->done;
   p.out_ids = d_ids;
   p.out_scores = d_scores;
   p.out_threshold = d_thr;
@@ -277,7 +305,7 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
   if (hh->count != (uint32_t)kk) {
     ScanScratch s{};
     cudaMemcpy(&s, c->scratch, sizeof(s), cudaMemcpyDeviceToHost);
-    cudaMemset(c->scratch, 0, sizeof(ScanScratch));
+    cudaMemset(c->scratch, 0, c->meta_bytes);  // threshold, counters and group arrivals
     if (s.error & 1u)
       return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls); diag %u block %u tile %u [%u %u]",
                   (unsigned long long)h->wait_limit, s.diag[0], s.diag[1], s.diag[2], s.diag[3], s.diag[4]);
@@ -547,6 +575,13 @@ int topk_count_ge(topk_table_t h, uint64_t r0, uint64_t r1, uint32_t qq, const f
   CK(cudaStreamSynchronize(c->stream));
   if (ge) *ge = r[0];
   if (gt) *gt = r[1];
+  return TOPK_OK;
+}
+
+int topk_set_scan_tuning(topk_table_t h, uint32_t max_ctas_per_sm) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (max_ctas_per_sm > 8) return fail(TOPK_ERR_ARG, "max_ctas_per_sm must be 0..8");
+  h->max_ctas_per_sm = max_ctas_per_sm;
   return TOPK_OK;
 }
 

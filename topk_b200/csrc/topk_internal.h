@@ -10,21 +10,21 @@ constexpr int kScanThreads = 256;     // threads per scan CTA
 constexpr uint32_t kMaxQ = 64;        // attributes per query
 constexpr uint32_t kMaxK = 4096;      // largest k of the fused path
 constexpr uint32_t kLdAlign = 64;     // device column stride alignment (rows)
+constexpr int kMaxLevels = 12;        // merge-tree levels (fan-in >= 2, <= 4096 CTAs)
+constexpr int kScanSmemFixed = 1536;  // barriers, control block, radix histogram, weights
 
 // Device-side per-context scratch of the fused scan.  Zero between queries:
-// the last CTA of each scan puts it back.
+// the kernel puts every counter back before it ends.
 struct ScanScratch {
-  uint32_t g_thr;        // running global threshold key (objects below it cannot win)
-  uint32_t done;         // CTAs finished
-  uint32_t cand_count;   // candidates appended to the global list
-  uint32_t error;        // nonzero after a device wait gave up (bit 0: stage wait)
+  uint32_t g_thr;           // running global threshold key (objects below it cannot win)
+  uint32_t error;           // nonzero after a device wait gave up (bit 0: stage wait)
   uint32_t acc_reductions;  // CTA block-selects during this scan
-  uint32_t last_cands;      // candidates seen by the final select of the last scan
+  uint32_t last_cands;      // entries merged at the root of the last scan
   uint32_t last_reductions; // block-selects of the last scan
   // Diagnostics of a TOPK_BOUNDS_CHECK build: first failed check (code, block,
   // tile, two values); the access it guarded was skipped.
   uint32_t diag[5];
-  uint32_t pad[4];
+  uint32_t pad[6];
 };
 
 // TOPK_BOUNDS_CHECK codes
@@ -36,6 +36,7 @@ enum : uint32_t {
   kDiagCompact = 5,     // compaction write past capacity
   kDiagWait = 6,        // a stage wait gave up
   kDiagOutput = 7,      // output index out of range
+  kDiagMerge = 8,       // merge load past capacity
 };
 
 struct ScanParams {
@@ -48,52 +49,65 @@ struct ScanParams {
   uint32_t num_tiles;
   uint32_t qq;
   uint32_t k;
-  uint32_t cap;         // shared-memory candidate capacity (entries)
-  uint32_t stages;      // copy pipeline depth
-  uint32_t gcand_cap;   // entries of the global candidate list
+  uint32_t cap;         // entries of each of the two shared candidate buffers
+  uint32_t mcap;        // shared entries available to the merge (both buffers reused)
+  uint32_t fanin;       // merge-tree fan-in G
+  uint32_t levels;      // merge-tree levels below the root (level l has nslots[l] slots)
+  uint32_t nslots[kMaxLevels];
+  uint32_t slot_off[kMaxLevels];  // first slot of level l in `slots` (slot = k entries)
+  uint32_t done_off[kMaxLevels];  // first group counter of level l in `done`
   uint64_t wait_limit;  // polls per bounded wait
   uint32_t fault_mode;  // 1: wait on a barrier nothing completes (timeout test)
   ScanScratch *scratch;
-  uint2 *gcand;         // global candidate list (key, id)
+  uint2 *slots;         // merge-tree slots, k entries each (key, id)
+  uint32_t *slot_count; // entries per slot
+  uint32_t *done;       // per-group arrival counters (zero between queries)
   uint64_t *out_ids;    // min(k, rows) ids, ascending by score
   float *out_scores;
   float *out_threshold; // may be null
   uint32_t *out_count;  // may be null
-  uint32_t *out_stats;  // may be null: [0] candidates in the final select, [1] block-selects
+  uint32_t *out_stats;  // may be null: [0] entries merged at the root, [1] block-selects
   uint8_t attr[kMaxQ];
   float w[kMaxQ];       // weights[attr[m]], gathered on the host
 };
 
 struct ScanPlan {
-  int vec;           // objects per thread per tile (1, 2 or 4)
   uint32_t tile;     // objects per tile
-  uint32_t stages;
+  uint32_t stages;   // 1 when the request fits in shared memory, else 0
   uint32_t cap;
+  uint32_t mcap;
+  uint32_t fanin;
+  int ctas_per_sm;
   size_t smem;       // dynamic shared memory bytes
   int grid;
 };
 
-// Plan a launch for qq attributes and top-k over `rows` rows.
-ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin);
+// Plan a launch for qq attributes and top-k over `rows` rows (max_ctas_per_sm 0 =
+// as many as fit).  stages == 0 means the request does not fit.
+ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin,
+                   uint32_t max_ctas_per_sm = 0);
+// Fill the merge-tree fields of p for `grid` CTAs; returns slots and group
+// counters needed (entries = slots * k).
+void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *total_slots, uint32_t *total_groups);
 cudaError_t launch_scan(const ScanPlan &plan, const ScanParams &p, cudaStream_t stream);
 cudaError_t scan_set_attributes(size_t smem_optin);
 
 // Table kernels.
 cudaError_t launch_generate(float *table, uint64_t ld, uint32_t d, uint64_t n, int dist, uint64_t seed,
                             cudaStream_t stream);
-// Per-column min/max with std::min/std::max semantics; mm[0..d) = max, mm[d..2d) = min.
+// Per-column min/max with std::min/std::max semantics.
 cudaError_t launch_minmax(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint32_t *work,
                           cudaStream_t stream);
 cudaError_t launch_normalize(float *table, uint64_t ld, uint32_t d, uint64_t n, const float *mins,
                              const float *ranges, cudaStream_t stream);
 // work layout for launch_minmax (uint32 words): per column
-//   [0] max key, [1] min key, [2] first +0 index (lo), [3] first -0 index (lo),
-//   plus [4],[5] hi words of those indices; 8 words per column.
+//   [0] max key, [1] min key, [2..3] first +0 index, [4..5] first -0 index; 8 words per column.
 constexpr int kMinmaxWords = 8;
 
-// Plain reference-order count of objects with score >= thr and > thr (verification).
-cudaError_t launch_count(const float *table, uint64_t ld, uint64_t r0, uint64_t r1, uint32_t qq, const uint8_t *attr,
-                         const float *w, float thr, unsigned long long *out2, cudaStream_t stream);
+// Plain reference-order count of objects in [r0, r1) with score >= thr and > thr.
+cudaError_t launch_count(const float *table, uint64_t ld, uint64_t r0, uint64_t r1, uint32_t qq,
+                         const uint8_t *attr, const float *w, float thr, unsigned long long *out2,
+                         cudaStream_t stream);
 // Gather full rows for a list of ids: out[j*d + m] = table[m*ld + ids[j]].
 cudaError_t launch_gather(const float *table, uint64_t ld, uint32_t d, const uint64_t *ids, uint64_t cnt,
                           float *out, cudaStream_t stream);

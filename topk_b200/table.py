@@ -112,6 +112,9 @@ class Table:
                                         C.byref(gt)))
         return ge.value, gt.value
 
+    def set_scan_tuning(self, max_ctas_per_sm=0):
+        check(_lib.load().topk_set_scan_tuning(self._h, int(max_ctas_per_sm)))
+
     def set_fault_injection(self, mode):
         check(_lib.load().topk_set_fault_injection(self._h, int(mode)))
 

@@ -1,0 +1,106 @@
+// Drop-in check in the reference's own terms: the reference's TPAc<float,uint64_t>
+// (cpu/TPAc.h, on the CPU) and TPAcGPU<float,uint64_t> (include/topk_b200/TPAcGPU.h,
+// on the GPU) load the same table through get_cdata(), run init(), and answer the
+// harness's queries (validation/bench_cpu.h:171-195: k doubling, last-q attribute
+// sets); results must agree: same k-th score, same score multiset, same ids above it.
+//
+// Built by topk_b200/build.py when the reference tree is available (it compiles the
+// reference headers); run by tests/test_gpu_dropin.py.  Usage:
+//     tpac_dropin_demo <n> <d> <seed>
+#define MQTHREADS 64
+#define STATS_EFF false
+#define IMP 1
+#define LD 1
+#define WORKLOAD 1024
+#define NUM_DIMS 16
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <queue>
+#include <sstream>
+#include <vector>
+
+#include "time/Time.h"
+#include "cpu/TPAc.h"
+#include "topk_b200/TPAcGPU.h"
+
+// Deterministic U[0,1) table (xorshift64*), column-major.
+static void fill(float *data, uint64_t n, uint64_t d, uint64_t seed) {
+  uint64_t x = seed * 0x9E3779B97F4A7C15ull + 1;
+  for (uint64_t m = 0; m < d; m++)
+    for (uint64_t i = 0; i < n; i++) {
+      x ^= x >> 12;
+      x ^= x << 25;
+      x ^= x >> 27;
+      data[m * n + i] = (float)((x * 0x2545F4914F6CDD1Dull) >> 40) * (1.0f / 16777216.0f);
+    }
+}
+
+int main(int argc, char **argv) {
+  const uint64_t n = argc > 1 ? strtoull(argv[1], nullptr, 10) : (1u << 20);
+  const uint64_t d = argc > 2 ? strtoull(argv[2], nullptr, 10) : 8;
+  const uint64_t seed = argc > 3 ? strtoull(argv[3], nullptr, 10) : 1;
+
+  TPAc<float, uint64_t> ref(n, d);
+  TPAcGPU<float, uint64_t> gpu(n, d);
+  ref.get_cdata() = static_cast<float *>(aligned_alloc(64, sizeof(float) * n * d));
+  gpu.get_cdata() = static_cast<float *>(aligned_alloc(64, sizeof(float) * n * d));
+  fill(ref.get_cdata(), n, d, seed);
+  std::memcpy(gpu.get_cdata(), ref.get_cdata(), sizeof(float) * n * d);
+
+  std::ostringstream sink;  // the reference prints a line per query
+  std::streambuf *old = std::cout.rdbuf(sink.rdbuf());
+  ref.init();
+  gpu.init();
+  std::cout.rdbuf(old);
+  if (std::memcmp(ref.get_cdata(), gpu.get_cdata(), sizeof(float) * n * d) != 0) {
+    std::printf("normalize MISMATCH\n");
+    return 1;
+  }
+  std::printf("normalize ok\n");
+
+  std::vector<float> weights(d);
+  for (uint64_t m = 0; m < d; m++) weights[m] = 0.1f * (float)(m + 1);
+  int bad = 0;
+  for (uint64_t k = 16; k <= 1024; k *= 4) {
+    for (uint64_t q = 2; q <= d; q += 2) {
+      std::vector<uint8_t> attr(q);
+      for (uint64_t m = 0; m < q; m++) attr[m] = (uint8_t)(d - q + m);  // last q (QM == 0)
+      old = std::cout.rdbuf(sink.rdbuf());
+      ref.findTopKsimd(k, (uint8_t)q, weights.data(), attr.data());
+      gpu.findTopKsimd(k, (uint8_t)q, weights.data(), attr.data());
+      std::cout.rdbuf(old);
+      std::vector<tuple_<float, uint64_t>> a = ref.get_res(), b = gpu.get_res();
+      bool ok = a.size() == b.size() && ref.get_thres() == gpu.get_thres();
+      std::vector<float> sa, sb;
+      std::vector<uint64_t> ia, ib;
+      for (auto &e : a) {
+        sa.push_back(e.score);
+        if (e.score > ref.get_thres()) ia.push_back(e.tid);
+      }
+      for (auto &e : b) {
+        sb.push_back(e.score);
+        if (e.score > gpu.get_thres()) ib.push_back(e.tid);
+      }
+      std::sort(sa.begin(), sa.end());
+      std::sort(sb.begin(), sb.end());
+      std::sort(ia.begin(), ia.end());
+      std::sort(ib.begin(), ib.end());
+      ok = ok && sa == sb && ia == ib;
+      std::printf("k=%llu q=%llu threshold=%.9g %s\n", (unsigned long long)k, (unsigned long long)q,
+                  (double)gpu.get_thres(), ok ? "ok" : "MISMATCH");
+      bad += ok ? 0 : 1;
+    }
+  }
+  // the multi-query entry from several threads, as validation/bench_cpu.h:204-212 does
+  std::vector<uint8_t> attr4 = {(uint8_t)(d - 4), (uint8_t)(d - 3), (uint8_t)(d - 2), (uint8_t)(d - 1)};
+#pragma omp parallel num_threads(8)
+  for (int j = 0; j < 4; j++) gpu.findTopKsimdMQ(64, 4, weights.data(), attr4.data(), (uint32_t)omp_get_thread_num());
+  std::printf("%s\n", bad ? "FAIL" : "PASS");
+  return bad ? 1 : 0;
+}

@@ -113,6 +113,26 @@ int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
                       const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_threshold,
                       void *stream);
 
+/* The same exact top-k as topk_query_device, for callers that must not allocate GPU
+ * memory: no handle, no cudaMalloc/cudaFree, nothing from an allocating library.
+ * It serves host applications that own the whole device memory budget and hand it
+ * out through their own pool, and latency-critical paths that cannot pay for
+ * cudaMalloc/cudaFree (both synchronise the device).  No counterpart in the
+ * reference.  The caller passes a column-major table it owns (d_table, 16-byte
+ * aligned, column m at d_table + m*ld, ld >= n and a multiple of 4, n < 2^32 - 1),
+ * the query (host weights indexed by attribute id, host attr), and device outputs
+ * for min(k, n) ids / scores (d_threshold may be NULL); work is enqueued on
+ * `stream` (a cudaStream_t, NULL = the legacy default stream).  The scan's scratch
+ * is a fixed array compiled into the library (about 2.7 MB on each GPU that loads
+ * it, held until the process exits): k is limited to 1024 (TOPK_ERR_UNSUPPORTED
+ * above), and calls whose work overlaps on the GPU share that array and race, so
+ * serialise them.  The first call on each device performs a one-time set-up on
+ * that device; make it before capturing work on that device.  Errors: the usual
+ * status codes, message from topk_last_error(). */
+int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld, uint32_t d, uint64_t k, uint32_t qq,
+                       const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores,
+                       float *d_threshold, void *stream);
+
 /* A batch of independent queries with host inputs/outputs (synchronous).
  * Query j uses ks[j], qqs[j], weights + j*wstride (indexed by attribute id),
  * attrs + j*astride.  Outputs: ids/scores + j*kstride (kstride >= max k),

@@ -97,6 +97,8 @@ struct Ctx {
 
 }  // namespace
 
+void topk::set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 struct topk_table_s {
   int device = 0;
   uint64_t n = 0, ld = 0;

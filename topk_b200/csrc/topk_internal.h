@@ -92,6 +92,9 @@ void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *tot
 cudaError_t launch_scan(const ScanPlan &plan, const ScanParams &p, cudaStream_t stream);
 cudaError_t scan_set_attributes(size_t smem_optin);
 
+// Set the calling thread's message returned by topk_last_error().
+void set_last_error(const char *msg);
+
 // Table kernels.
 cudaError_t launch_generate(float *table, uint64_t ld, uint32_t d, uint64_t n, int dist, uint64_t seed,
                             cudaStream_t stream);

@@ -164,6 +164,19 @@ int topk_set_scan_tuning(topk_table_t h, uint32_t max_ctas_per_sm);
  * fault injection: no GPU fault, the context stays usable. */
 int topk_set_fault_injection(topk_table_t h, int mode);
 
+/* Methods of topk_query_batch (no reference counterpart; results are identical). */
+#define TOPK_BATCH_AUTO 0  /* the fastest available (today: TOPK_BATCH_FP32) */
+#define TOPK_BATCH_LOOP 1  /* one fused single-query scan per query */
+#define TOPK_BATCH_FP32 2  /* batched plain FP32: each table tile scored for 64 queries */
+
+/* Choose the method of topk_query_batch on this handle. */
+int topk_set_batch_method(topk_table_t h, int method);
+
+/* Statistics of the handle's last topk_query_batch: device time of the batched
+ * kernels (CUDA events; 0 for the loop method), queries answered again by the
+ * single-query scan after a candidate overflow, filter candidates (0 for FP32). */
+int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks, uint64_t *candidates);
+
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */
 int topk_last_stats(topk_table_t h, uint64_t *candidates, uint64_t *reductions);

@@ -1,0 +1,340 @@
+// Batched exact top-k: many independent queries over one resident table.
+//
+// Replaces the reference's multi-query loop (validation/bench_cpu.h:198-232 calling
+// TPAc::findTopKsimdMQ, cpu/TPAc.h:210-254), which scans the whole table once per
+// query; here every table tile read from HBM is scored for a whole group of queries.
+// Arithmetic and tie rule per query are those of the single-query path.
+//
+// Schedule (host-driven, kernels below):
+//   bootstrap   each query's exact top-k over the first S0 rows -> best[], and its
+//               threshold thr = k-th key + 1 (later rows have larger ids, so an
+//               object must beat the k-th strictly);
+//   chunks      rows [S0, n) in chunks that double in size; per chunk a scorer
+//               appends (key, id) of every object with key >= thr to the query's
+//               candidate region, then a reduce merges best[] and the candidates
+//               into the new top-k and raises thr.  Doubling keeps the expected
+//               candidates per query per chunk near k*ln 2;
+//   finish      sort each best[] and write the results ascending by score.
+// A query whose candidate region overflows in some chunk (possible only on
+// adversarial orders) is flagged; the host answers it with the single-query scan.
+//
+// Two scorers share this schedule: the plain FP32 one here (exact keys), and the
+// BF16 tensor-core filter (bf16_filter.cu), whose candidates carry approximate
+// keys that the reduce rescoring makes exact.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "batch_internal.h"
+#include "block_select.cuh"
+#include "device_common.cuh"
+
+namespace topk {
+
+namespace {
+
+constexpr int kBT = 256;  // threads per block of the batched kernels
+
+struct BatchShared {
+  SelShared sel;
+  uint32_t qq, k;
+  uint32_t pad[2];
+};
+
+__device__ __forceinline__ float score_row(const float *table, uint64_t ld, uint64_t row, const uint8_t *attr,
+                                           const float *w, uint32_t qq) {
+  float s = 0.0f;
+  for (uint32_t m = 0; m < qq; ++m) s = __fadd_rn(s, __fmul_rn(__ldg(table + (uint64_t)attr[m] * ld + row), w[m]));
+  return s;
+}
+
+// ---------------------------------------------------------------- bootstrap
+// One block per query: exact top-k of rows [0, rows).  Shared: entries[rows] and
+// best[k] (dynamic), histogram, select state, the query's attr/weights.
+__global__ void __launch_bounds__(kBT) batch_bootstrap_kernel(const float *__restrict__ table, uint64_t ld,
+                                                              uint32_t rows, const BatchQuery *__restrict__ qs,
+                                                              BatchState *__restrict__ st, uint2 *__restrict__ best) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  BatchShared *sh = reinterpret_cast<BatchShared *>(smem);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(smem + 128);
+  uint8_t *attr = smem + 1152;
+  float *w = reinterpret_cast<float *>(smem + 1184);
+  uint2 *ent = reinterpret_cast<uint2 *>(smem + 1408);
+  const BatchQuery &q = qs[blockIdx.x];
+  const int t = threadIdx.x;
+  if (t < (int)kBatchMaxQ) {
+    attr[t] = q.attr[t];
+    w[t] = q.w[t];
+  }
+  if (t == 0) {
+    sh->qq = q.qq;
+    sh->k = q.k;
+  }
+  __syncthreads();
+  const uint32_t qq = sh->qq, k = sh->k;
+  uint2 *out = ent + rows;
+  for (uint32_t i = t; i < rows; i += kBT) ent[i] = make_uint2(f2key(score_row(table, ld, i, attr, w, qq)), i);
+  __syncthreads();
+  const uint32_t kept = block_reduce<kBT>(ent, rows, out, k, 0u, hist, &sh->sel);
+  uint2 *dst = best + q.best_off;
+  for (uint32_t j = t; j < kept; j += kBT) dst[j] = out[j];
+  if (t == 0) {
+    BatchState s{};
+    s.cnt = kept;
+    s.thr = (kept == k) ? sh->sel.kept_min + 1u : 0u;
+    st[blockIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------- FP32 scorer
+// Block (query group g, tile): rows [row0, row0 + OPT*256) of the chunk, all d
+// columns staged in shared memory once, scored for the group's queries.
+template <int OPT>
+__global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__restrict__ table, uint64_t ld,
+                                                               uint32_t d, uint64_t r0, uint64_t r1,
+                                                               const BatchQuery *__restrict__ qs, uint32_t nq,
+                                                               BatchState *__restrict__ st,
+                                                               uint2 *__restrict__ cand) {
+  constexpr uint32_t TO = kBT * OPT;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *xs = reinterpret_cast<float *>(smem);                       // d x TO
+  uint8_t *gattr = smem + (size_t)d * TO * 4;                        // kBatchGroup x kBatchMaxQ
+  float *gw = reinterpret_cast<float *>(gattr + kBatchGroup * kBatchMaxQ);  // kBatchGroup x kBatchMaxQ
+  uint32_t *gthr = reinterpret_cast<uint32_t *>(gw + kBatchGroup * kBatchMaxQ);
+  uint32_t *gqq = gthr + kBatchGroup;
+
+  const int t = threadIdx.x;
+  // block -> (query group, tile), groups fastest: the blocks of one tile run together
+  // and its second and later reads come from L2
+  const uint32_t ngroups = (nq + kBatchGroup - 1) / kBatchGroup;
+  const uint32_t q0 = (blockIdx.x % ngroups) * kBatchGroup;
+  const uint64_t tile = blockIdx.x / ngroups;
+  const uint32_t nqg = min(kBatchGroup, nq - q0);
+  const uint64_t base = r0 + tile * TO;
+  const uint32_t valid = (uint32_t)min((uint64_t)TO, r1 - base);
+  // stage the tile (rows beyond r1 read as 0 and are never appended)
+  for (uint32_t m = 0; m < d; ++m) {
+    const float *col = table + (uint64_t)m * ld + base;
+    for (uint32_t i = t; i < TO; i += kBT) xs[m * TO + i] = i < valid ? __ldcs(col + i) : 0.0f;
+  }
+  for (uint32_t j = t; j < nqg * kBatchMaxQ; j += kBT) {
+    const uint32_t qj = j / kBatchMaxQ, m = j % kBatchMaxQ;
+    gattr[j] = qs[q0 + qj].attr[m];
+    gw[j] = qs[q0 + qj].w[m];
+  }
+  for (uint32_t j = t; j < nqg; j += kBT) {
+    gthr[j] = st[q0 + j].thr;
+    gqq[j] = qs[q0 + j].qq;
+  }
+  __syncthreads();
+
+  const int lane = t & 31;
+  for (uint32_t j = 0; j < nqg; ++j) {
+    const uint32_t qq = gqq[j];
+    const uint8_t *a = gattr + j * kBatchMaxQ;
+    const float *w = gw + j * kBatchMaxQ;
+    float acc[OPT];
+#pragma unroll
+    for (int v = 0; v < OPT; ++v) acc[v] = 0.0f;
+    for (uint32_t m = 0; m < qq; ++m) {
+      const float *row = xs + (uint32_t)a[m] * TO + t * OPT;
+      const float wm = w[m];
+      if constexpr (OPT == 4) {
+        const float4 x = *reinterpret_cast<const float4 *>(row);
+        acc[0] = __fadd_rn(acc[0], __fmul_rn(x.x, wm));
+        acc[1] = __fadd_rn(acc[1], __fmul_rn(x.y, wm));
+        acc[2] = __fadd_rn(acc[2], __fmul_rn(x.z, wm));
+        acc[3] = __fadd_rn(acc[3], __fmul_rn(x.w, wm));
+      } else {
+#pragma unroll
+        for (int v = 0; v < OPT; ++v) acc[v] = __fadd_rn(acc[v], __fmul_rn(row[v], wm));
+      }
+    }
+    const uint32_t thr = gthr[j];
+    const bool take_all = thr == 0u;
+    const float thr_f = thr_float(thr);
+    unsigned pass = 0;
+#pragma unroll
+    for (int v = 0; v < OPT; ++v)
+      pass |= (unsigned)((take_all || acc[v] >= thr_f) && (uint32_t)(t * OPT + v) < valid) << v;
+    if (__ballot_sync(0xFFFFFFFFu, pass != 0u)) {  // warp-uniform
+      const uint32_t np = __popc(pass);
+      uint32_t incl = np;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const uint32_t wtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      const BatchQuery &q = qs[q0 + j];
+      uint32_t pos = 0;
+      if (lane == 31) pos = atomicAdd(&st[q0 + j].ccount, wtot);
+      pos = __shfl_sync(0xFFFFFFFFu, pos, 31) + incl - np;
+#pragma unroll
+      for (int v = 0; v < OPT; ++v)
+        if (pass & (1u << v)) {
+          if (pos < q.cand_cap) cand[q.cand_off + pos] = make_uint2(f2key(acc[v]), (uint32_t)(base + t * OPT + v));
+          ++pos;
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- reduce
+// One block per query: merge best[] with the chunk's candidates (rescoring them
+// exactly first when they carry approximate keys) into the new top-k.
+__global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restrict__ table, uint64_t ld,
+                                                           const BatchQuery *__restrict__ qs,
+                                                           BatchState *__restrict__ st, uint2 *__restrict__ best,
+                                                           const uint2 *__restrict__ cand, int rescore) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  BatchShared *sh = reinterpret_cast<BatchShared *>(smem);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(smem + 128);
+  uint8_t *attr = smem + 1152;
+  float *w = reinterpret_cast<float *>(smem + 1184);
+  uint2 *ent = reinterpret_cast<uint2 *>(smem + 1408);
+  const BatchQuery &q = qs[blockIdx.x];
+  BatchState &s = st[blockIdx.x];
+  const int t = threadIdx.x;
+  if (t < (int)kBatchMaxQ) {
+    attr[t] = q.attr[t];
+    w[t] = q.w[t];
+  }
+  if (t == 0) {
+    sh->qq = q.qq;
+    sh->k = q.k;
+  }
+  __syncthreads();
+  const uint32_t qq = sh->qq, k = sh->k;
+  const uint32_t cnt = s.cnt;
+  const uint32_t thr = s.thr;
+  const uint32_t nc_raw = s.ccount;
+  const uint32_t nc = min(nc_raw, q.cand_cap);
+  const uint32_t total = cnt + nc;
+  uint2 *out = ent + cnt + q.cand_cap;
+  const uint2 *b = best + q.best_off;
+  const uint2 *c = cand + q.cand_off;
+  for (uint32_t j = t; j < cnt; j += kBT) ent[j] = b[j];
+  for (uint32_t j = t; j < nc; j += kBT) {
+    uint2 e = c[j];
+    if (rescore) e.x = f2key(score_row(table, ld, e.y, attr, w, qq));  // exact key in reference order
+    ent[cnt + j] = e;
+  }
+  __syncthreads();
+  // candidates below thr (an approximate filter lets a few in) cannot beat the k-th
+  uint32_t kept;
+  if (cnt == k) {
+    // best[] is a full top-k: new entries must reach thr; merge the two sets
+    for (uint32_t j = cnt + t; j < total; j += kBT)
+      if (ent[j].x < thr) ent[j] = make_uint2(0u, 0xFFFFFFFFu);  // below every real entry
+    __syncthreads();
+  }
+  kept = block_reduce<kBT>(ent, total, out, k, 0u, hist, &sh->sel);
+  uint2 *dst = best + q.best_off;
+  for (uint32_t j = t; j < kept; j += kBT) dst[j] = out[j];
+  if (t == 0) {
+    BatchState ns = s;
+    ns.cnt = kept;
+    if (kept == k) ns.thr = max(thr, sh->sel.kept_min + 1u);
+    if (nc_raw > q.cand_cap) ns.flags |= 1u;
+    ns.ccount = 0;
+    s = ns;
+  }
+}
+
+// ---------------------------------------------------------------- finish
+// One block per query: sort best[] and write the result ascending by score.
+__global__ void __launch_bounds__(kBT) batch_finish_kernel(const BatchQuery *__restrict__ qs,
+                                                           const BatchState *__restrict__ st,
+                                                           const uint2 *__restrict__ best, uint64_t *out_ids,
+                                                           float *out_scores, uint64_t kstride, uint32_t *out_count,
+                                                           float *out_thr) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint2 *a = reinterpret_cast<uint2 *>(smem);
+  const BatchQuery &q = qs[blockIdx.x];
+  const uint32_t cnt = st[blockIdx.x].cnt;
+  const int t = threadIdx.x;
+  for (uint32_t j = t; j < cnt; j += kBT) a[j] = best[q.best_off + j];
+  __syncthreads();
+  block_sort_desc<kBT>(a, cnt);
+  uint64_t *ids = out_ids + (uint64_t)blockIdx.x * kstride;
+  float *sc = out_scores + (uint64_t)blockIdx.x * kstride;
+  for (uint32_t r = t; r < cnt; r += kBT) {
+    const uint2 e = a[r];
+    ids[cnt - 1 - r] = e.y;
+    sc[cnt - 1 - r] = key2f(e.x);
+  }
+  if (t == 0) {
+    out_count[blockIdx.x] = cnt;
+    out_thr[blockIdx.x] = cnt ? key2f(a[cnt - 1].x) : 0.0f;
+  }
+}
+
+constexpr size_t kQueryShared = 1408;  // select state, histogram, attr, weights
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+size_t batch_bootstrap_smem(uint32_t rows, uint32_t kmax) { return kQueryShared + (size_t)(rows + kmax) * 8; }
+
+cudaError_t launch_batch_bootstrap(const float *table, uint64_t ld, uint32_t rows, uint32_t kmax,
+                                   const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *best, cudaStream_t s) {
+  const size_t smem = batch_bootstrap_smem(rows, kmax);
+  cudaError_t e = cudaFuncSetAttribute(batch_bootstrap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  batch_bootstrap_kernel<<<nq, kBT, smem, s>>>(table, ld, rows, qs, st, best);
+  return cudaGetLastError();
+}
+
+size_t batch_score_smem(uint32_t d) {
+  const uint32_t to = (d <= 16 ? 4u : 1u) * kBT;
+  return (size_t)d * to * 4 + kBatchGroup * kBatchMaxQ * 5 + kBatchGroup * 8;
+}
+
+cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
+                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, cudaStream_t s) {
+  const size_t smem = batch_score_smem(d);
+  const uint32_t opt = d <= 16 ? 4u : 1u;
+  const uint64_t to = (uint64_t)opt * kBT;
+  const uint64_t blocks = (uint64_t)((nq + kBatchGroup - 1) / kBatchGroup) * ((r1 - r0 + to - 1) / to);
+  if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  const dim3 grid((unsigned)blocks);
+  cudaError_t e;
+  if (opt == 4) {
+    if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+      return e;
+    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand);
+  } else {
+    if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+      return e;
+    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand);
+  }
+  return cudaGetLastError();
+}
+
+size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax) { return kQueryShared + (size_t)(2 * kmax + capmax) * 8; }
+
+cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
+                                uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,
+                                cudaStream_t s) {
+  const size_t smem = batch_reduce_smem(kmax, capmax);
+  cudaError_t e = cudaFuncSetAttribute(batch_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  batch_reduce_kernel<<<nq, kBT, smem, s>>>(table, ld, qs, st, best, cand, rescore ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
+                                uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
+                                uint32_t *out_count, float *out_thr, cudaStream_t s) {
+  uint32_t P = 1;
+  while (P < kmax) P <<= 1;
+  const size_t smem = (size_t)P * 8;
+  cudaError_t e = cudaFuncSetAttribute(batch_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  batch_finish_kernel<<<nq, kBT, smem, s>>>(qs, st, best, out_ids, out_scores, kstride, out_count, out_thr);
+  return cudaGetLastError();
+}
+
+}  // namespace topk

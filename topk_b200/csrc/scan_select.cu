@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "block_select.cuh"
 #include "device_common.cuh"
 #include "topk_internal.h"
 
@@ -39,24 +40,21 @@ struct SmemCtl {
   uint32_t cur;        // which of the two candidate buffers is current
   uint32_t thr_local;  // min key that can still enter (k-th CTA key + 1)
   uint32_t thr_g;      // CTA copy of the global threshold
-  uint32_t kept_min;   // min key among kept entries (select result)
-  uint32_t digit, above, eq, valid;
-  uint32_t wcount;     // compaction / append cursor
   uint32_t reductions;
   uint32_t is_last;
   uint32_t red_g;      // threshold snapshot shared by the block
-  uint32_t pad[3];
+  uint32_t pad;
+  SelShared sel;       // state of the block-wide selects
 };
 
 // shared layout
-constexpr int kOffCtl = 0;        // SmemCtl (64 B)
-constexpr int kOffMinMax = 64;    // two u64: min / max composite of a select
-constexpr int kOffNever = 80;     // test barrier (u64)
+constexpr int kOffCtl = 0;        // SmemCtl (80 B)
+constexpr int kOffNever = 96;     // test barrier (u64)
 constexpr int kOffHist = 128;     // 256-bin radix histogram
 constexpr int kOffWsm = 1152;     // weights of the runtime-q path (kMaxQ floats)
 constexpr int kOffCand = kScanSmemFixed;
 static_assert(kOffWsm + 4 * (int)kMaxQ <= kScanSmemFixed, "fixed shared block");
-static_assert(sizeof(SmemCtl) == 64, "control block layout");
+static_assert(sizeof(SmemCtl) <= kOffNever, "control block layout");
 static_assert(kScanThreads == 256, "one histogram bin per thread");
 
 constexpr int kVec = 4;                      // objects per thread per tile
@@ -80,197 +78,6 @@ __device__ __forceinline__ bool check(bool ok, ScanScratch *s, uint32_t code, ui
 #else
 #define TOPK_CHECK(cond, code, i, a, b) (true)
 #endif
-
-// Source of candidate entries for the radix select.
-struct SmemSrc {
-  const uint2 *p;
-  __device__ uint2 operator()(uint32_t j) const { return p[j]; }
-};
-
-// Block-wide radix select over `count` entries of `src` with key >= min_key: finds
-// (prefix, mask) such that exactly `need` valid entries satisfy
-// (composite & mask) >= prefix.  Requires need <= number of valid entries.
-// Digits are taken from the highest bit where the valid entries differ (min/max of
-// the composites first), 8 bits at a time; histogram updates are aggregated per
-// warp with __match_any_sync, because candidates crowd into few bins.
-template <class Src>
-__device__ void block_radix_select(const Src &src, uint32_t count, uint32_t min_key, uint32_t need,
-                                   uint32_t *hist, SmemCtl *ctl, unsigned long long *mm, uint64_t &prefix_out,
-                                   uint64_t &mask_out) {
-  const int t = threadIdx.x;
-  const int lane = t & 31;
-  if (t == 0) {
-    mm[0] = ~0ull;
-    mm[1] = 0ull;
-  }
-  bsync();
-  {
-    unsigned long long lo = ~0ull, hi = 0ull;
-    for (uint32_t j = t; j < count; j += kScanThreads) {
-      const uint2 e = src(j);
-      if (e.x < min_key) continue;
-      const unsigned long long c = composite(e.x, e.y);
-      lo = c < lo ? c : lo;
-      hi = c > hi ? c : hi;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long a = __shfl_xor_sync(0xFFFFFFFFu, lo, o);
-      const unsigned long long b = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
-      lo = a < lo ? a : lo;
-      hi = b > hi ? b : hi;
-    }
-    if (lane == 0) {
-      atomicMin(&mm[0], lo);
-      atomicMax(&mm[1], hi);
-    }
-  }
-  bsync();
-  const uint64_t cmin = mm[0], cmax = mm[1];
-  const uint64_t diff = cmin ^ cmax;
-  int hib = diff ? 63 - __clzll((long long)diff) : -1;  // highest differing bit
-  uint64_t mask = hib >= 63 ? 0ull : (~0ull << (hib + 1));
-  uint64_t prefix = cmin & mask;
-  while (hib >= 0) {
-    const int lob = hib >= 7 ? hib - 7 : 0;
-    const uint32_t dmask = (1u << (hib - lob + 1)) - 1u;
-    hist[t] = 0;
-    bsync();
-    for (uint32_t base = 0; base < count; base += kScanThreads) {  // uniform trip count
-      const uint32_t j = base + t;
-      uint32_t bin = 0xFFFFFFFFu;
-      if (j < count) {
-        const uint2 e = src(j);
-        if (e.x >= min_key) {
-          const uint64_t c = composite(e.x, e.y);
-          if ((c & mask) == prefix) bin = (uint32_t)(c >> lob) & dmask;
-        }
-      }
-      const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
-      if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
-    }
-    bsync();
-    if (t < 32) {
-      // lane l owns bins [255-8l-7, 255-8l], visited from high to low
-      const int top = 255 - 8 * t;
-      uint32_t local[8];
-      uint32_t s = 0;
-#pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        local[b] = hist[top - b];
-        s += local[b];
-      }
-      uint32_t incl = s;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (t >= o) incl += v;
-      }
-      const uint32_t excl = incl - s;
-      if (excl < need && need <= incl) {
-        uint32_t run = excl;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          if (run + local[b] >= need) {
-            ctl->digit = (uint32_t)(top - b);
-            ctl->above = run;
-            ctl->eq = local[b];
-            break;
-          }
-          run += local[b];
-        }
-      }
-    }
-    bsync();
-    const uint32_t digit = ctl->digit, above = ctl->above, eq = ctl->eq;
-    bsync();  // everyone has read ctl before the next pass rewrites it
-    need -= above;
-    prefix |= (uint64_t)digit << lob;
-    mask |= (uint64_t)dmask << lob;
-    if (eq == need) break;
-    hib = lob - 1;
-  }
-  prefix_out = prefix;
-  mask_out = mask;
-}
-
-// Keep the best k entries with key >= min_key of src[0..count), written to dst
-// (out of place).  Returns the number kept; ctl->kept_min gets their min key.
-__device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, uint32_t k, uint32_t min_key,
-                                 uint32_t *hist, SmemCtl *ctl, unsigned long long *mm) {
-  const int t = threadIdx.x;
-  uint32_t v = 0;
-  for (uint32_t j = t; j < count; j += kScanThreads) v += (src[j].x >= min_key);
-  v = warp_sum_u32(v);
-  if (t == 0) {
-    ctl->valid = 0;
-    ctl->wcount = 0;
-    ctl->kept_min = 0xFFFFFFFFu;
-  }
-  bsync();
-  if ((t & 31) == 0) atomicAdd(&ctl->valid, v);
-  bsync();
-  const uint32_t valid = ctl->valid;
-  uint64_t prefix = 0, mask = 0;
-  const bool select = valid > k;
-  if (select) block_radix_select(SmemSrc{src}, count, min_key, k, hist, ctl, mm, prefix, mask);
-  uint32_t kmin = 0xFFFFFFFFu;
-  for (uint32_t base = 0; base < count; base += kScanThreads) {  // uniform trip count
-    const uint32_t j = base + t;
-    uint2 e = make_uint2(0u, 0u);
-    bool keep = false;
-    if (j < count) {
-      e = src[j];
-      keep = e.x >= min_key && (!select || (composite(e.x, e.y) & mask) >= prefix);
-    }
-    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
-    uint32_t pos = 0;
-    if ((t & 31) == 0 && bal) pos = atomicAdd(&ctl->wcount, (uint32_t)__popc(bal));
-    pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-    if (keep) {
-      dst[pos + __popc(bal & ((1u << (t & 31)) - 1u))] = e;
-      kmin = min(kmin, e.x);
-    }
-  }
-  kmin = warp_min_u32(kmin);
-  if ((t & 31) == 0) atomicMin(&ctl->kept_min, kmin);
-  bsync();
-  const uint32_t kept = ctl->wcount;
-  bsync();  // every thread has its copy before thread 0 may reset wcount
-  return kept;
-}
-
-// Sort a[0..n) descending by composite (bitonic, padded to a power of two; the
-// caller guarantees room for the padding).
-__device__ void block_sort_desc(uint2 *a, uint32_t n) {
-  const int t = threadIdx.x;
-  uint32_t P = 1;
-  while (P < n) P <<= 1;
-  for (uint32_t j = n + t; j < P; j += kScanThreads) a[j] = make_uint2(0u, 0xFFFFFFFFu);
-  bsync();
-  for (uint32_t size = 2; size <= P; size <<= 1) {
-    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-      for (uint32_t i = t; i < P / 2; i += kScanThreads) {
-        const uint32_t lo = 2 * i - (i & (stride - 1));
-        const uint32_t hi = lo + stride;
-        const bool desc = (lo & size) == 0;
-        const uint2 x = a[lo], y = a[hi];
-        const uint64_t cx = composite(x.x, x.y), cy = composite(y.x, y.y);
-        if (desc ? (cx < cy) : (cx > cy)) {
-          a[lo] = y;
-          a[hi] = x;
-        }
-      }
-      bsync();
-    }
-  }
-}
-
-// Lowest float whose key is >= thr, for thr > 0: keys 1..key(-inf) are the
-// negative-NaN patterns no score maps to, so they all mean "any number".
-__device__ __forceinline__ float thr_float(uint32_t thr) {
-  return thr <= 0x007FFFFFu ? __int_as_float(0xFF800000) : key2f(thr);
-}
 
 __device__ __forceinline__ float4 ld_stream(const float *p) { return __ldcs(reinterpret_cast<const float4 *>(p)); }
 
@@ -329,7 +136,6 @@ template <int QQ>
 __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + kOffCtl);
-  unsigned long long *mm = reinterpret_cast<unsigned long long *>(smem + kOffMinMax);
   uint64_t *never = reinterpret_cast<uint64_t *>(smem + kOffNever);
   uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffHist);
   float *wsm = reinterpret_cast<float *>(smem + kOffWsm);
@@ -416,15 +222,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
       if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       bsync();
       const uint32_t c = ctl->cur;
-      const uint32_t kept = block_reduce(cand0 + (size_t)c * cap, ctl->count, cand0 + (size_t)(c ^ 1u) * cap, p.k,
-                                         ctl->red_g, hist, ctl, mm);
+      const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
+                                                       cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
       if (t == 0) {
         ctl->cur = c ^ 1u;
         ctl->count = kept;
         ctl->reductions++;
         if (kept == p.k) {  // the CTA knows a k-th key
-          ctl->thr_local = ctl->kept_min + 1u;
-          atomicMax(&p.scratch->g_thr, ctl->kept_min);
+          ctl->thr_local = ctl->sel.kept_min + 1u;
+          atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
         }
       }
       bsync();
@@ -443,13 +249,13 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   bsync();
   if (ctl->count > p.k) {
     const uint32_t c = ctl->cur;
-    const uint32_t kept = block_reduce(cand0 + (size_t)c * cap, ctl->count, cand0 + (size_t)(c ^ 1u) * cap, p.k,
-                                       ctl->red_g, hist, ctl, mm);
+    const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
+                                                     cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
     if (t == 0) {
       ctl->cur = c ^ 1u;
       ctl->count = kept;
       ctl->reductions++;
-      if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->kept_min);
+      if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
     }
     bsync();
   }
@@ -465,7 +271,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     // publish my result into slot (level, slot), filtered by the current threshold
     if (t == 0) {
       ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
-      ctl->wcount = 0;
+      ctl->sel.wcount = 0;
     }
     bsync();
     {
@@ -473,7 +279,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
       uint2 *dst = p.slots + (size_t)(p.slot_off[level] + slot) * k;
       for (uint32_t j = t; j < res_n; j += kScanThreads) {
         const uint2 e = res[j];
-        if (e.x >= g) dst[atomicAdd(&ctl->wcount, 1u)] = e;  // <= res_n <= k entries
+        if (e.x >= g) dst[atomicAdd(&ctl->sel.wcount, 1u)] = e;  // <= res_n <= k entries
       }
     }
     __threadfence();  // each writer makes its slot entries visible device-wide
@@ -482,7 +288,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     const uint32_t first = grp * p.fanin;
     const uint32_t gsize = min(p.fanin, p.nslots[level] - first);
     if (t == 0) {
-      p.slot_count[p.slot_off[level] + slot] = ctl->wcount;
+      p.slot_count[p.slot_off[level] + slot] = ctl->sel.wcount;
       __threadfence();
       const uint32_t arrived = atomicAdd(&p.done[p.done_off[level] + grp], 1u);
       ctl->is_last = (arrived == gsize - 1u) ? 1u : 0u;
@@ -494,7 +300,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     // the last arrival merges the group's slots
     if (t == 0) {
       ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
-      ctl->wcount = 0;
+      ctl->sel.wcount = 0;
     }
     bsync();
     {
@@ -508,24 +314,24 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
         for (uint32_t j = t; j < cnt; j += kScanThreads) {
           const uint2 e = __ldcg(src + j);
           if (e.x >= g) {
-            const uint32_t pos = atomicAdd(&ctl->wcount, 1u);
+            const uint32_t pos = atomicAdd(&ctl->sel.wcount, 1u);
             if (TOPK_CHECK(pos < lim, kDiagMerge, level, pos, lim)) mbuf[pos] = e;
           }
         }
       }
     }
     bsync();
-    const uint32_t loaded = min(ctl->wcount, p.fanin * k);
+    const uint32_t loaded = min(ctl->sel.wcount, p.fanin * k);
     bsync();  // every thread has `loaded` before block_reduce resets wcount
     merged = loaded;
-    res_n = block_reduce(mbuf, loaded, outb, k, 0u, hist, ctl, mm);
+    res_n = block_reduce<kScanThreads>(mbuf, loaded, outb, k, 0u, hist, &ctl->sel);
     res = outb;
     level += 1;
     slot = grp;
   }
 
   // ---- root: sort and write the result (res has room for the padding) ----
-  block_sort_desc(res, res_n);
+  block_sort_desc<kScanThreads>(res, res_n);
   for (uint32_t r = t; r < res_n; r += kScanThreads) {
     const uint2 e = res[r];
     const uint32_t pos = res_n - 1 - r;  // ascending output

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "batch_internal.h"
 #include "topk_internal.h"
 
 using namespace topk;
@@ -116,6 +117,17 @@ struct topk_table_s {
   std::condition_variable cv;
   std::vector<Ctx *> ctxs;
   Ctx *primary = nullptr;
+  // batched path: one batch at a time per handle, device buffers grow and are kept
+  std::mutex batch_mu;
+  int batch_method = TOPK_BATCH_AUTO;
+  struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+  };
+  DevBuf b_q, b_st, b_best, b_cand, b_ids, b_scores, b_count, b_thr;
+  cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
+  double last_batch_ms = 0;
+  uint64_t last_batch_fallbacks = 0, last_batch_cands = 0;
 };
 
 namespace {
@@ -323,6 +335,128 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
   return TOPK_OK;
 }
 
+// Grow a cached device buffer to at least `bytes`.
+int ensure(topk_table_s::DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes) return TOPK_OK;
+  cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  CK(cudaMalloc(&b.p, bytes));
+  b.bytes = bytes;
+  return TOPK_OK;
+}
+
+void free_batch_buffers(topk_table_t h) {
+  for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
+                                  &h->b_thr}) {
+    cudaFree(b->p);
+    b->p = nullptr;
+    b->bytes = 0;
+  }
+  if (h->b_ev0) cudaEventDestroy(h->b_ev0);
+  if (h->b_ev1) cudaEventDestroy(h->b_ev1);
+  h->b_ev0 = h->b_ev1 = nullptr;
+}
+
+// Batched exact top-k on the handle's primary stream (caller holds batch_mu):
+// bootstrap over the first rows, doubling chunks (score + reduce), finish.  Queries
+// flagged for a candidate overflow are answered again by the single-query scan.
+int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+              uint64_t wstride, const uint8_t *attrs, uint64_t astride, uint64_t *ids, float *scores,
+              uint64_t kstride, uint64_t *counts, float *thresholds) {
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::vector<BatchQuery> q(nq);
+  uint64_t best_total = 0, cand_total = 0;
+  uint32_t kmax = 1, capmax = 1;
+  for (uint64_t j = 0; j < nq; j++) {
+    BatchQuery &b = q[j];
+    std::memset(&b, 0, sizeof(b));
+    b.k = (uint32_t)std::min<uint64_t>(ks[j], h->n);
+    b.qq = qqs[j];
+    b.best_off = (uint32_t)best_total;
+    best_total += b.k;
+    b.cand_cap = 2 * b.k + 2048;
+    b.cand_off = (uint32_t)cand_total;
+    cand_total += b.cand_cap;
+    for (uint32_t m = 0; m < b.qq; m++) {
+      b.attr[m] = attrs[j * astride + m];
+      b.w[m] = weights[j * wstride + b.attr[m]];
+    }
+    kmax = std::max(kmax, b.k);
+    capmax = std::max(capmax, b.cand_cap);
+  }
+  if (best_total > 0xFFFFFFFFull || cand_total > 0xFFFFFFFFull)
+    return fail(TOPK_ERR_UNSUPPORTED, "batch too large: split it");
+  int st;
+  if ((st = ensure(h->b_q, nq * sizeof(BatchQuery))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_st, nq * sizeof(BatchState))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_best, best_total * sizeof(uint2))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_cand, cand_total * sizeof(uint2))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_ids, nq * kmax * sizeof(uint64_t))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_scores, nq * kmax * sizeof(float))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_count, nq * sizeof(uint32_t))) != TOPK_OK) return st;
+  if ((st = ensure(h->b_thr, nq * sizeof(float))) != TOPK_OK) return st;
+  if (!h->b_ev0) CK(cudaEventCreate(&h->b_ev0));
+  if (!h->b_ev1) CK(cudaEventCreate(&h->b_ev1));
+  BatchQuery *dq = static_cast<BatchQuery *>(h->b_q.p);
+  BatchState *dst = static_cast<BatchState *>(h->b_st.p);
+  uint2 *dbest = static_cast<uint2 *>(h->b_best.p);
+  uint2 *dcand = static_cast<uint2 *>(h->b_cand.p);
+  cudaStream_t s = h->primary->stream;
+  const uint32_t nqq = (uint32_t)nq;
+  CK(cudaMemcpyAsync(dq, q.data(), nq * sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(dst, 0, nq * sizeof(BatchState), s));
+  CK(cudaEventRecord(h->b_ev0, s));
+  const uint64_t boot = std::min<uint64_t>(h->n, kBatchBootRows);
+  CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
+  for (uint64_t r = boot, size = boot; r < h->n; size *= 2) {
+    const uint64_t e = std::min<uint64_t>(h->n, r + size);
+    CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, s));
+    CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, false, s));
+    r = e;
+  }
+  CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
+                         static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
+                         static_cast<float *>(h->b_thr.p), s));
+  CK(cudaEventRecord(h->b_ev1, s));
+  std::vector<uint64_t> hid(nq * kmax);
+  std::vector<float> hsc(nq * kmax), hth(nq);
+  std::vector<uint32_t> hcnt(nq);
+  std::vector<BatchState> hst(nq);
+  CK(cudaMemcpyAsync(hid.data(), h->b_ids.p, hid.size() * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hsc.data(), h->b_scores.p, hsc.size() * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hcnt.data(), h->b_count.p, nq * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hth.data(), h->b_thr.p, nq * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->b_ev0, h->b_ev1));
+  h->last_batch_ms = ms;
+  uint64_t fallbacks = 0;
+  for (uint64_t j = 0; j < nq; j++) {
+    if (hst[j].flags & 1u) {  // a candidate region overflowed: answer exactly with the scan
+      ++fallbacks;
+      uint64_t c = 0;
+      float th = 0;
+      st = run_query_sync(h, 0, h->n, ks[j], qqs[j], weights + j * wstride, attrs + j * astride, ids + j * kstride,
+                          scores + j * kstride, &c, &th);
+      if (st != TOPK_OK) return st;
+      if (counts) counts[j] = c;
+      if (thresholds) thresholds[j] = th;
+      continue;
+    }
+    const uint32_t c = hcnt[j];
+    std::memcpy(ids + j * kstride, &hid[j * kmax], (size_t)c * 8);
+    std::memcpy(scores + j * kstride, &hsc[j * kmax], (size_t)c * 4);
+    if (counts) counts[j] = c;
+    if (thresholds) thresholds[j] = hth[j];
+  }
+  h->last_batch_fallbacks = fallbacks;
+  h->last_batch_cands = 0;
+  return TOPK_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -395,6 +529,7 @@ int topk_destroy(topk_table_t h) {
   DeviceGuard dg(h->device);
   for (Ctx *c : h->ctxs) ctx_free(c);
   ctx_free(h->primary);
+  free_batch_buffers(h);
   cudaFree(h->table);
   cudaFree(h->d_minmax);
   cudaFree(h->d_norm);
@@ -515,12 +650,20 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
   if (!h || (nq && (!ks || !qqs || !weights || !attrs || !ids || !scores)))
     return fail(TOPK_ERR_ARG, "null argument");
   if (wstride < h->d) return fail(TOPK_ERR_ARG, "wstride < d");
+  bool batchable = h->d <= kBatchMaxD && nq > 0 && nq < 0x7FFFFFFFull;
   for (uint64_t j = 0; j < nq; j++) {
     if (kstride < std::min<uint64_t>(ks[j], h->n)) return fail(TOPK_ERR_ARG, "kstride < k of query %llu", (unsigned long long)j);
     if (qqs[j] > astride) return fail(TOPK_ERR_ARG, "astride < qq of query %llu", (unsigned long long)j);
     int st = check_query(h, ks[j], qqs[j], weights + j * wstride, attrs + j * astride);
     if (st != TOPK_OK) return st;
+    if (qqs[j] > kBatchMaxQ) batchable = false;
   }
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  if (h->batch_method != TOPK_BATCH_LOOP && batchable)
+    return run_batch(h, nq, ks, qqs, weights, wstride, attrs, astride, ids, scores, kstride, counts, thresholds);
+  h->last_batch_ms = 0;
+  h->last_batch_fallbacks = 0;
+  h->last_batch_cands = 0;
   for (uint64_t j = 0; j < nq; j++) {
     uint64_t c = 0;
     float th = 0;
@@ -530,6 +673,24 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
     if (counts) counts[j] = c;
     if (thresholds) thresholds[j] = th;
   }
+  return TOPK_OK;
+}
+
+int topk_set_batch_method(topk_table_t h, int method) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (method < TOPK_BATCH_AUTO || method > TOPK_BATCH_FP32)
+    return fail(TOPK_ERR_UNSUPPORTED, "batch method %d not available", method);
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  h->batch_method = method;
+  return TOPK_OK;
+}
+
+int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks, uint64_t *candidates) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  if (device_ms) *device_ms = h->last_batch_ms;
+  if (fallbacks) *fallbacks = h->last_batch_fallbacks;
+  if (candidates) *candidates = h->last_batch_cands;
   return TOPK_OK;
 }
 

@@ -165,17 +165,27 @@ int topk_set_scan_tuning(topk_table_t h, uint32_t max_ctas_per_sm);
 int topk_set_fault_injection(topk_table_t h, int mode);
 
 /* Methods of topk_query_batch (no reference counterpart; results are identical). */
-#define TOPK_BATCH_AUTO 0  /* the fastest available (today: TOPK_BATCH_FP32) */
+#define TOPK_BATCH_AUTO 0  /* TOPK_BATCH_BF16 where it applies, else TOPK_BATCH_FP32 */
 #define TOPK_BATCH_LOOP 1  /* one fused single-query scan per query */
 #define TOPK_BATCH_FP32 2  /* batched plain FP32: each table tile scored for 64 queries */
+#define TOPK_BATCH_BF16 3  /* BF16 tensor-core filter (tcgen05) with a per-query error
+                            * bound; candidates rescored exactly in FP32.  Applies to
+                            * d <= 16 with finite table values and weights of magnitude
+                            * <= 2^60; other batches run TOPK_BATCH_FP32 */
 
 /* Choose the method of topk_query_batch on this handle. */
 int topk_set_batch_method(topk_table_t h, int method);
 
 /* Statistics of the handle's last topk_query_batch: device time of the batched
  * kernels (CUDA events; 0 for the loop method), queries answered again by the
- * single-query scan after a candidate overflow, filter candidates (0 for FP32). */
+ * single-query scan after a candidate overflow, candidates appended by the
+ * scorer over all chunks. */
 int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks, uint64_t *candidates);
+
+/* More about the last topk_query_batch: the method that ran (TOPK_BATCH_*), and for
+ * TOPK_BATCH_BF16 the largest |filter score - exact score| / bound seen over the
+ * rescored candidates (must stay below 1; 0 for the other methods). */
+int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio);
 
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */

@@ -109,11 +109,11 @@ def scores(table, weights, attr, ids=None):
     for m in a:
         col = table[m] if ids is None else table[m][ids]
         p = (col * w[m]).astype(np.float32)
-        s = p.copy() if s is None else (s + p).astype(np.float32)
+        # the first term is 0 + p, not p: a -0 product (negative weight) becomes +0
+        s = (np.float32(0) + p).astype(np.float32) if s is None else (s + p).astype(np.float32)
     if s is None:
         n = table.shape[1] if ids is None else len(ids)
         s = np.zeros(n, np.float32)
-    # s = 0 + p for the first term is p exactly (no -0 arises from x*w with w > 0)
     return s
 
 

@@ -119,3 +119,140 @@ def test_batch_ties_and_wide_queries():
         W2 = W[:2].copy()
         A2 = np.tile(np.arange(d, dtype=np.uint8), (2, 1))
         check_batch(t, tn, ks[:2], W2, A2, np.array([40, 33], np.uint32))
+
+
+# ---------------------------------------------------------------- BF16 filter
+BF16 = 3
+
+
+def bf16_ran(t):
+    """The last batch ran the tensor-core filter, and every rescored candidate's
+    filter score was within half of its error bound."""
+    st = t.last_batch_stats()
+    assert st["method"] == BF16
+    assert 0.0 < st["max_err_ratio"] < 0.5, st
+    return st
+
+
+@pytest.mark.parametrize("n,dist,d", [((1 << 20) + 77, 1, 16), (300000, 0, 16), (250001, 2, 16),
+                                      ((1 << 19) + 5, 3, 16), (200003, 1, 8), (100000, 1, 3)])
+def test_batch_bf16_vs_oracle(n, dist, d):
+    rng = np.random.default_rng(n + d)
+    with T.Table(n, d) as t:
+        t.generate(dist, 7)
+        t.normalize()
+        tn = t.download()
+        t.set_batch_method(BF16)
+        ks, W, A, qqs = make_batch(rng, 150, d, 1024, qmax=min(16, d))
+        ks[:3] = [1, 1024, 4096]
+        ids, sc, counts, _ = check_batch(t, tn, ks, W, A, qqs)
+        st = bf16_ran(t)
+        assert st["fallbacks"] == 0
+        # FP32 scores against an FP64 evaluation of the same ids (reported, bounded)
+        worst = 0.0
+        for j in range(0, len(ks), 15):
+            c = int(counts[j])
+            a = A[j, : qqs[j]]
+            s64 = sum(tn[m][ids[j, :c].astype(np.int64)].astype(np.float64) * np.float64(W[j][m]) for m in a)
+            worst = max(worst, float(np.max(np.abs(sc[j, :c].astype(np.float64) - s64))))
+        print(f"max |score_fp32 - score_fp64| = {worst:.3e}")
+        assert worst < 16 * 2.0 ** -24 * 16
+
+
+def test_batch_bf16_matches_fp32_across_query_groups():
+    """2100 queries = 17 query tiles: two CTA query groups, a partial last tile."""
+    n, d = (1 << 18) + 3, 16
+    rng = np.random.default_rng(11)
+    with T.Table(n, d) as t:
+        t.generate(3, 2)
+        t.normalize()
+        tn = t.download()
+        ks, W, A, qqs = make_batch(rng, 2100, d, 1024)
+        t.set_batch_method(BF16)
+        a = t.query_batch(ks, W, A, qqs)
+        bf16_ran(t)
+        t.set_batch_method(FP32)
+        b = t.query_batch(ks, W, A, qqs)
+        assert t.last_batch_stats()["method"] == FP32
+        for x, y in zip(a, b):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
+        for j in rng.choice(len(ks), size=40, replace=False):
+            c = int(a[2][j])
+            want = O.topk_numpy(tn, int(ks[j]), W[j], A[j, : qqs[j]])
+            H.assert_same_result((a[0][j, :c], a[1][j, :c], a[3][j]), want)
+
+
+def test_batch_bf16_ties_negative_and_repeated_attributes():
+    n, d = 150001, 16
+    rng = np.random.default_rng(5)
+    raw = (np.floor(O.generate(n, d, 1, 8) * 16) / 16).astype(np.float32)  # coarse: many ties
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.set_batch_method(BF16)
+        nq = 60
+        W = rng.uniform(-1, 1, size=(nq, d)).astype(np.float32)
+        A = np.zeros((nq, 6), np.uint8)
+        qqs = np.zeros(nq, np.uint32)
+        for j in range(nq):
+            q = int(rng.integers(1, 7))
+            A[j, :q] = rng.integers(0, d, size=q)  # repeats allowed, any order
+            qqs[j] = q
+        ks = rng.integers(1, 2000, size=nq).astype(np.uint64)
+        ids, sc, counts, ths = t.query_batch(ks, W, A, qqs)
+        bf16_ran(t)
+        for j in range(nq):
+            c = int(counts[j])
+            want = O.topk(tn, int(ks[j]), W[j], A[j, : qqs[j]])
+            H.assert_same_result((ids[j, :c], sc[j, :c], ths[j]), want)
+
+
+def test_batch_bf16_not_applicable_runs_fp32():
+    rng = np.random.default_rng(6)
+    # wider than 16 attributes
+    with T.Table(70000, 20) as t:
+        t.generate(1, 3)
+        t.normalize()
+        tn = t.download()
+        t.set_batch_method(BF16)
+        ks, W, A, qqs = make_batch(rng, 20, 20, 500)
+        check_batch(t, tn, ks, W, A, qqs)
+        assert t.last_batch_stats()["method"] == FP32
+    # a value above 2^60 in the table, then a weight above 2^60
+    n, d = 70000, 8
+    raw = O.generate(n, d, 1, 4)
+    raw[3, 1234] = np.float32(1e30)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.set_batch_method(0)
+        ks, W, A, qqs = make_batch(rng, 20, d, 500, qmax=d)
+        check_batch(t, raw, ks, W, A, qqs)
+        assert t.last_batch_stats()["method"] == FP32
+        t.generate(1, 4)
+        tn = t.download()
+        check_batch(t, tn, ks, W, A, qqs)
+        assert t.last_batch_stats()["method"] == BF16  # the table changed: the split was rebuilt
+        W2 = W.copy()
+        W2[0, A[0, 0]] = np.float32(1e20)
+        check_batch(t, tn, ks, W2, A, qqs)
+        assert t.last_batch_stats()["method"] == FP32
+
+
+def test_batch_bf16_overflow_falls_back_exactly():
+    n, d = 400003, 3
+    raw = np.tile(np.linspace(0, 1, n, dtype=np.float32), (d, 1))
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.set_batch_method(BF16)
+        ks = np.array([5, 700, 4096], np.uint64)
+        W = np.ones((3, d), np.float32)
+        A = np.array([[0, 1, 2], [2, 0, 1], [1, 1, 1]], np.uint8)
+        qqs = np.array([3, 3, 3], np.uint32)
+        check_batch(t, tn, ks, W, A, qqs)
+        st = t.last_batch_stats()
+        assert st["method"] == BF16 and st["fallbacks"] >= 1

@@ -26,6 +26,9 @@ MAX_D = 255
 
 DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
 
+# topk_query_batch methods (TOPK_BATCH_* in include/topk_b200.h)
+BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16 = 0, 1, 2, 3
+
 
 class TopKError(RuntimeError):
     """A TOPK_ERR_* status from the C ABI."""
@@ -64,6 +67,7 @@ SIGNATURES = [
     ("topk_set_scan_tuning", C.c_int, [_H, C.c_uint32]),
     ("topk_set_batch_method", C.c_int, [_H, C.c_int]),
     ("topk_last_batch_stats", C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     ("topk_query_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, _f32p,
                                      _u8p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("topk_last_stats", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -1,0 +1,453 @@
+// BF16 tensor-core filter of the batched path (tcgen05 + TMEM, sm_100a).
+//
+// For every (query, object) pair of a chunk the filter computes an approximate
+// score on the 5th-generation tensor cores.  The objects whose approximate score
+// can still reach the query's threshold are rescored exactly in the reference
+// order (cpu/TPAc.h:135-150: s += x[attr[m]] * weights[attr[m]], FP32, no FMA)
+// and appended to the query's candidate region when the exact key reaches the
+// threshold, so batch_reduce_kernel (batch.cu) merges exact keys and the results
+// are bit-identical to the FP32 paths.  Rescoring before appending keeps the
+// regions as small as the FP32 scorer's even where many objects tie just below
+// the threshold (clipped, correlated data).
+//
+// Operands, both K-major without swizzle (core matrices of 8 rows x 16 bytes; the
+// K-adjacent core matrix 128 B further on, the next 8 rows 256 B further on):
+//   table  each object's 16 attributes split x = hi + lo (bf16 each, |x - hi - lo|
+//          <= 2^-16 |x|); tiles of 256 objects: hi 8 KB, then lo 8 KB;
+//   query  a 16-wide row a[m] = sum of weights[attr[j]] over the j with attr[j] = m,
+//          split the same way; tiles of 128 queries: hi 4 KB, then lo 4 KB.
+// One (query tile, object tile) pair is three MMAs M=128 N=256 K=16 into FP32 TMEM:
+//   D = Ahi.Bhi + Alo.Bhi + Ahi.Blo        (the lo.lo term lies inside the bound)
+// Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
+//   E = 2^-12 * sum_m |weights[attr[m]]| * max|column attr[m]|  (+ 2^-100 terms for
+//   subnormal flushing).  Split and product errors give 3.1*2^-16, 48 FP32
+//   accumulations 48*2^-22, the reference's own FP32 rounding 17*2^-24: about
+//   2^-14 in all; the factor 4 covers the tensor core's accumulation rounding,
+//   which is not specified.  An object with exact score >= the threshold float t
+//   has D >= t - E, so the cut t - E (rounded down) loses none.
+//
+// Roles of the 320 threads of a CTA (one CTA per SM: TMEM is allocated whole):
+//   warps 0-7  epilogue: warp w reads TMEM lanes 32*(w%4).. (one query per thread),
+//              columns 128*(w/4).. (half an object tile), compares with the
+//              query's cut, rescores survivors and appends candidates;
+//   warp 8     producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
+//              the CTA's query tiles once and object tiles into a 4-stage ring;
+//   warp 9     allocates the 512 TMEM columns; lane 0 issues the MMAs for two
+//              accumulators of 256 columns (double buffered against the epilogue).
+// Every mbarrier wait is bounded; a wait that runs out sets the CTA's abort flag,
+// every role leaves its loop, in-flight copies and MMAs are waited for (bounded),
+// TMEM is freed and the error word is set (the host reports TOPK_ERR_TIMEOUT).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "batch_internal.h"
+#include "block_select.cuh"
+#include "device_common.cuh"
+
+namespace topk {
+
+namespace {
+
+constexpr uint32_t kFTile = 256;        // objects per tile (MMA N)
+constexpr uint32_t kFTileBytes = 16384; // hi + lo of one object tile
+constexpr uint32_t kQTile = 128;        // queries per tile (MMA M)
+constexpr uint32_t kQTileBytes = 8192;  // hi + lo of one query tile
+constexpr uint32_t kStages = 4;
+constexpr uint32_t kEpiWarps = 8;
+constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kMaxQTPerCta = 16;
+constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
+
+// Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits
+// 7-9 = 1, 10-12 = 1), both K-major, N>>3 at bits 17-22, M>>4 at bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kFTile >> 3) << 17) | ((kQTile >> 4) << 24);
+
+// Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B (K-adjacent
+// core matrices), SBO 256 B (next 8 rows), version 1 (bit 46).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+#define TOPK_R8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), "=r"(v[i + 5]), \
+                   "=r"(v[i + 6]), "=r"(v[i + 7])
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : TOPK_R8(0), TOPK_R8(8), TOPK_R8(16), TOPK_R8(24)
+      : "r"(taddr));
+}
+#undef TOPK_R8
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float max3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Bounded wait that also gives up once another role of the CTA has aborted.
+__device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, uint64_t limit, volatile uint32_t *abort_flag) {
+  for (uint64_t it = 0; it < limit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63u) == 63u && *abort_flag) return false;
+  }
+  *abort_flag = 1u;
+  return false;
+}
+
+// A survivor of the approximate cut: score it exactly in the reference order
+// (cpu/TPAc.h:135-150), record the filter's error, append it if its exact key
+// reaches the threshold.  Rare, so kept out of line.
+__device__ __noinline__ void filter_survivor(const float *__restrict__ table, uint64_t ld,
+                                             const BatchQuery *__restrict__ qs, BatchState *__restrict__ st,
+                                             uint2 *__restrict__ cand, uint32_t q, uint32_t thr, float approx,
+                                             uint32_t id) {
+  const BatchQuery &bq = qs[q];
+  float s = 0.0f;
+  for (uint32_t m = 0; m < bq.qq; ++m)
+    s = __fadd_rn(s, __fmul_rn(__ldg(table + (uint64_t)bq.attr[m] * ld + id), bq.w[m]));
+  BatchState &b = st[q];
+  atomicAdd(&b.rescored, 1u);
+  const float ratio = fabsf(approx - s) / bq.err;
+  if (ratio == ratio) atomicMax(&b.errmax, __float_as_uint(ratio));
+  const uint32_t key = f2key(s);
+  if (key >= thr) {
+    const uint32_t pos = atomicAdd(&b.ccount, 1u);
+    if (pos < bq.cand_cap) cand[bq.cand_off + pos] = make_uint2(key, id);
+  }
+}
+
+struct FilterArgs {
+  const uint8_t *xbf;  // object tiles (kFTileBytes each)
+  const uint8_t *abf;  // query tiles (kQTileBytes each)
+  const float *table;  // the FP32 column-major table (exact rescoring)
+  uint64_t ld;
+  const BatchQuery *qs;
+  BatchState *st;
+  uint2 *cand;
+  uint64_t tile0, tile1;  // object tiles of the chunk
+  uint64_t r1;            // rows >= r1 are never appended
+  uint32_t nq, nqt;       // queries, query tiles
+  uint32_t qt_per_cta, ngroups, cpg;
+  uint32_t pad;
+  uint64_t wait_limit;
+  uint32_t *err;
+};
+
+__global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterArgs p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const uint32_t g = blockIdx.x % p.ngroups, c = blockIdx.x / p.ngroups;
+  const uint32_t QT = p.qt_per_cta;
+  const uint32_t qt0 = g * QT;
+  const uint32_t nqt = min(QT, p.nqt - qt0);
+  const uint64_t ntiles = p.tile1 - p.tile0;
+  const uint64_t per = (ntiles + p.cpg - 1) / p.cpg;
+  const uint64_t tb = p.tile0 + (uint64_t)c * per;
+  const uint64_t te = min(p.tile1, tb + per);
+  if (tb >= te) return;  // uniform over the block: no barrier or TMEM touched yet
+
+  unsigned char *sa = smem;
+  unsigned char *sb = smem + (size_t)QT * kQTileBytes;
+  float *scut = reinterpret_cast<float *>(sb + (size_t)kStages * kFTileBytes);
+  uint32_t *sthr = reinterpret_cast<uint32_t *>(scut + QT * kQTile);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sthr + QT * kQTile);
+  uint64_t *full = bars, *empty = bars + kStages, *accf = bars + 2 * kStages, *acce = accf + 2;
+  uint64_t *afull = acce + 2, *mdone = afull + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 1);
+  volatile uint32_t *abort_flag = tmem_slot + 1;
+
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t limit = p.wait_limit;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf + b, 1);
+      mbar_init(acce + b, kEpiWarps);
+    }
+    mbar_init(afull, 1);
+    mbar_init(mdone, 1);
+    *abort_flag = 0u;
+    fence_barrier_init();
+  }
+  // per-query cut: threshold float minus the bound, rounded down; +inf for rows
+  // past the last query, -inf while best[] is not full (every object is a candidate)
+  for (uint32_t j = threadIdx.x; j < QT * kQTile; j += kFThreads) {
+    const uint32_t q = qt0 * kQTile + j;
+    float cut = __int_as_float(0x7F800000);
+    uint32_t thr = 0xFFFFFFFFu;
+    if (j < nqt * kQTile && q < p.nq) {
+      thr = p.st[q].thr;
+      cut = thr == 0u ? __int_as_float(0xFF800000) : __fsub_rd(thr_float(thr), p.qs[q].err);
+    }
+    scut[j] = cut;
+    sthr[j] = thr;
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 8) {
+    // ---------------------------------------------------------------- producer
+    if (lane == 0) {
+      mbar_arrive_expect_tx(afull, nqt * kQTileBytes);
+      for (uint32_t i = 0; i < nqt; ++i)
+        bulk_g2s(sa + (size_t)i * kQTileBytes, p.abf + (size_t)(qt0 + i) * kQTileBytes, kQTileBytes, afull);
+      uint64_t it = 0;
+      for (uint64_t t = tb; t < te; ++t, ++it) {
+        const uint32_t s = (uint32_t)(it % kStages);
+        if (it >= kStages && !fwait(empty + s, (uint32_t)((it / kStages - 1) & 1), limit, abort_flag)) break;
+        mbar_arrive_expect_tx(full + s, kFTileBytes);
+        bulk_g2s(sb + (size_t)s * kFTileBytes, p.xbf + t * kFTileBytes, kFTileBytes, full + s);
+      }
+      // the CTA must not exit with copies in flight: wait for the last use of each stage
+      const uint64_t first = it > kStages ? it - kStages : 0;
+      for (uint64_t j = first; j < it; ++j)
+        if (!mbar_wait_bounded(full + (j % kStages), (uint32_t)((j / kStages) & 1), limit)) *abort_flag = 1u;
+      if (!mbar_wait_bounded(afull, 0, limit)) *abort_flag = 1u;
+    }
+  } else if (warp == 9) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      bool ok = fwait(afull, 0, limit, abort_flag);
+      uint64_t it = 0;
+      uint32_t seq = 0;
+      for (uint64_t t = tb; ok && t < te; ++t, ++it) {
+        const uint32_t s = (uint32_t)(it % kStages);
+        if (!fwait(full + s, (uint32_t)((it / kStages) & 1), limit, abort_flag)) break;
+        tc_fence_after();
+        const uint32_t bs = smem_u32(sb + (size_t)s * kFTileBytes);
+        const uint64_t bhi = smem_desc(bs), blo = smem_desc(bs + kFTileBytes / 2);
+        for (uint32_t i = 0; i < nqt; ++i, ++seq) {
+          const uint32_t buf = seq & 1u;
+          if (seq >= 2 && !fwait(acce + buf, ((seq >> 1) - 1) & 1u, limit, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t as = smem_u32(sa + (size_t)i * kQTileBytes);
+          const uint64_t ahi = smem_desc(as), alo = smem_desc(as + kQTileBytes / 2);
+          const uint32_t d = tmem + buf * kFTile;
+          tc_mma(d, ahi, bhi, 0u);
+          tc_mma(d, alo, bhi, 1u);
+          tc_mma(d, ahi, blo, 1u);
+          tc_commit(accf + buf);
+        }
+        if (!ok) break;
+        tc_commit(empty + s);  // the stage is free once these MMAs have read it
+      }
+      // TMEM is freed below: every issued MMA must have completed first
+      tc_commit(mdone);
+      if (!mbar_wait_bounded(mdone, 0, limit)) *abort_flag = 1u;
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    const uint32_t quarter = warp & 3u, half = warp >> 2;
+    const uint32_t row = quarter * 32u + lane;  // query row of the tile = TMEM lane
+    const uint32_t lane_addr = (quarter * 32u) << 16;
+    uint32_t seq = 0;
+    bool ok = true;
+    for (uint64_t t = tb; ok && t < te; ++t) {
+      const uint64_t id0 = t * kFTile + half * 128u;
+      for (uint32_t i = 0; i < nqt; ++i, ++seq) {
+        const uint32_t buf = seq & 1u;
+        ok = __all_sync(0xFFFFFFFFu, fwait(accf + buf, (seq >> 1) & 1u, limit, abort_flag));
+        if (!ok) break;
+        tc_fence_after();
+        uint32_t v[128];
+        const uint32_t ta = tmem + lane_addr + buf * kFTile + half * 128u;
+        tmem_ld32(ta, v);
+        tmem_ld32(ta + 32, v + 32);
+        tmem_ld32(ta + 64, v + 64);
+        tmem_ld32(ta + 96, v + 96);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce + buf);
+        const float cut = scut[i * kQTile + row];
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const uint32_t *u = v + cc * 32;
+          float m = max3(__uint_as_float(u[0]), __uint_as_float(u[1]), __uint_as_float(u[2]));
+#pragma unroll
+          for (int j = 3; j < 31; j += 2) m = max3(m, __uint_as_float(u[j]), __uint_as_float(u[j + 1]));
+          m = fmaxf(m, __uint_as_float(u[31]));
+          if (m >= cut) {
+            const uint32_t q = (qt0 + i) * kQTile + row;
+            const uint32_t thr = sthr[i * kQTile + row];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const float f = __uint_as_float(u[j]);
+              const uint64_t id = id0 + cc * 32 + j;
+              if (f >= cut && id < p.r1) filter_survivor(p.table, p.ld, p.qs, p.st, p.cand, q, thr, f, (uint32_t)id);
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // ---------------------------------------------------------------- teardown
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(p.err, 1u);
+}
+
+// ---------------------------------------------------------------- table split
+// One thread per object (grid-stride): reads its 16 attributes (columns >= d and
+// rows >= n are zero), writes hi and lo in the tiled core-matrix layout, and
+// keeps the largest |x| bit pattern per column (NaN and inf show as >= 0x7F800000).
+__global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict__ table, uint64_t ld, uint32_t d,
+                                                        uint64_t n, uint64_t nobj, uint8_t *__restrict__ xbf,
+                                                        uint32_t *__restrict__ absmax) {
+  uint32_t amax[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) amax[m] = 0u;
+  for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nobj; o += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t hi[8], lo[8];
+#pragma unroll
+    for (int m = 0; m < 16; m += 2) {
+      float x[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        x[e] = ((uint32_t)(m + e) < d && o < n) ? __ldg(table + (uint64_t)(m + e) * ld + o) : 0.0f;
+        amax[m + e] = max(amax[m + e], __float_as_uint(x[e]) & 0x7FFFFFFFu);
+      }
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(x[0]), h1 = __float2bfloat16_rn(x[1]);
+      const __nv_bfloat16 l0 = __float2bfloat16_rn(x[0] - __bfloat162float(h0));
+      const __nv_bfloat16 l1 = __float2bfloat16_rn(x[1] - __bfloat162float(h1));
+      hi[m / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      lo[m / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    const uint64_t t = o / kFTile;
+    const uint32_t r = (uint32_t)(o % kFTile);
+    uint8_t *base = xbf + t * kFTileBytes + (r >> 3) * 256u + (r & 7u) * 16u;
+    *reinterpret_cast<uint4 *>(base) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4 *>(base + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+    *reinterpret_cast<uint4 *>(base + kFTileBytes / 2) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    *reinterpret_cast<uint4 *>(base + kFTileBytes / 2 + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+  }
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    uint32_t a = amax[m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a = max(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
+    if ((threadIdx.x & 31) == 0 && (uint32_t)m < d) atomicMax(absmax + m, a);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+uint64_t bf16_table_bytes(uint64_t n) { return (n + kFTile - 1) / kFTile * kFTileBytes; }
+
+cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,
+                             int num_sms, cudaStream_t s) {
+  if (d > kBf16MaxD) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(absmax, 0, d * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  const uint64_t nobj = (n + kFTile - 1) / kFTile * kFTile;
+  const uint64_t blocks = std::min<uint64_t>((nobj + 255) / 256, (uint64_t)num_sms * 8);
+  bf16_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(table, ld, d, n, nobj, xbf, absmax);
+  return cudaGetLastError();
+}
+
+size_t bf16_query_bytes(uint32_t nq) { return (size_t)((nq + kQTile - 1) / kQTile) * kQTileBytes; }
+
+void bf16_pack_query(const float *a, uint32_t j, uint8_t *abf) {
+  auto f2bf = [](float f) -> uint16_t {  // round to nearest even (finite inputs)
+    uint32_t u;
+    __builtin_memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+  };
+  auto bf2f = [](uint16_t b) -> float {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    __builtin_memcpy(&f, &u, 4);
+    return f;
+  };
+  const uint32_t tile = j / kQTile, r = j % kQTile;
+  uint8_t *base = abf + (size_t)tile * kQTileBytes + (r >> 3) * 256u + (r & 7u) * 16u;
+  for (uint32_t m = 0; m < kBf16MaxD; ++m) {
+    const uint16_t h = f2bf(a[m]);
+    const volatile float res = a[m] - bf2f(h);  // exact: hi is within a factor 2 of a[m]
+    const uint16_t l = f2bf(res);
+    const size_t off = (m >> 3) * 128u + (m & 7u) * 2u;
+    __builtin_memcpy(base + off, &h, 2);
+    __builtin_memcpy(base + kQTileBytes / 2 + off, &l, 2);
+  }
+}
+
+cudaError_t launch_bf16_filter(const uint8_t *xbf, const uint8_t *abf, const float *table, uint64_t ld, uint64_t r0,
+                               uint64_t r1, const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, int num_sms,
+                               uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
+  if (r0 % kFTile) return cudaErrorInvalidValue;
+  FilterArgs p{};
+  p.xbf = xbf;
+  p.abf = abf;
+  p.table = table;
+  p.ld = ld;
+  p.qs = qs;
+  p.st = st;
+  p.cand = cand;
+  p.tile0 = r0 / kFTile;
+  p.tile1 = (r1 + kFTile - 1) / kFTile;
+  p.r1 = r1;
+  p.nq = nq;
+  p.nqt = (nq + kQTile - 1) / kQTile;
+  p.qt_per_cta = std::min<uint32_t>(p.nqt, kMaxQTPerCta);
+  p.ngroups = (p.nqt + p.qt_per_cta - 1) / p.qt_per_cta;
+  const uint64_t ntiles = p.tile1 - p.tile0;
+  p.cpg = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)std::max(1, num_sms / (int)p.ngroups)));
+  p.wait_limit = wait_limit;
+  p.err = err;
+  const size_t smem = std::max(kMinFilterSmem, (size_t)p.qt_per_cta * (kQTileBytes + kQTile * 8) +
+                                                   (size_t)kStages * kFTileBytes + 256);
+  cudaError_t e = cudaFuncSetAttribute(bf16_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t grid = (uint64_t)p.ngroups * p.cpg;
+  if (grid > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  bf16_filter_kernel<<<(unsigned)grid, kFThreads, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace topk

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -125,9 +126,16 @@ struct topk_table_s {
     size_t bytes = 0;
   };
   DevBuf b_q, b_st, b_best, b_cand, b_ids, b_scores, b_count, b_thr;
+  // BF16 filter: split copy of the table (rebuilt when the table changed), the
+  // per-column max |x| it was built from, the batch's query tiles and error word
+  DevBuf xbf, xbf_absmax, b_abf, b_err;
+  uint64_t data_version = 1, xbf_version = 0;
+  std::vector<float> absmax;
+  bool xbf_usable = false;
   cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
-  double last_batch_ms = 0;
+  double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0;
+  int last_batch_method = 0;
 };
 
 namespace {
@@ -348,7 +356,7 @@ int ensure(topk_table_s::DevBuf &b, size_t bytes) {
 
 void free_batch_buffers(topk_table_t h) {
   for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
-                                  &h->b_thr}) {
+                                  &h->b_thr, &h->xbf, &h->xbf_absmax, &h->b_abf, &h->b_err}) {
     cudaFree(b->p);
     b->p = nullptr;
     b->bytes = 0;
@@ -356,6 +364,60 @@ void free_batch_buffers(topk_table_t h) {
   if (h->b_ev0) cudaEventDestroy(h->b_ev0);
   if (h->b_ev1) cudaEventDestroy(h->b_ev1);
   h->b_ev0 = h->b_ev1 = nullptr;
+}
+
+// The device table is about to change: derived copies (the BF16 split) are stale.
+void table_changed(topk_table_t h) {
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  ++h->data_version;
+}
+
+// Largest magnitude the BF16 filter accepts in the table and the weights: products
+// and 48-term sums stay far from FP32 overflow, and bf16 rounding cannot overflow.
+constexpr float kBf16MaxAbs = 1.152921504606846976e18f;  // 2^60
+
+// Build (or reuse) the BF16 split of the table; caller holds batch_mu.  Sets
+// h->xbf_usable: false for tables wider than 16 or holding non-finite or huge values.
+int ensure_bf16_table(topk_table_t h, cudaStream_t s) {
+  if (h->xbf_version == h->data_version) return TOPK_OK;
+  h->xbf_usable = false;
+  if (h->d > kBf16MaxD) {
+    h->xbf_version = h->data_version;
+    return TOPK_OK;
+  }
+  int st;
+  if ((st = ensure(h->xbf, bf16_table_bytes(h->n))) != TOPK_OK) return st;
+  if ((st = ensure(h->xbf_absmax, (size_t)h->d * 4)) != TOPK_OK) return st;
+  CK(launch_bf16_pack(h->table, h->ld, h->d, h->n, static_cast<uint8_t *>(h->xbf.p),
+                      static_cast<uint32_t *>(h->xbf_absmax.p), h->num_sms, s));
+  std::vector<uint32_t> bits(h->d);
+  CK(cudaMemcpyAsync(bits.data(), h->xbf_absmax.p, (size_t)h->d * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  h->absmax.assign(h->d, 0.0f);
+  bool usable = true;
+  for (uint32_t m = 0; m < h->d; m++) {
+    float f;
+    std::memcpy(&f, &bits[m], 4);
+    if (!(f <= kBf16MaxAbs)) usable = false;  // also NaN / inf
+    h->absmax[m] = f;
+  }
+  h->xbf_usable = usable;
+  h->xbf_version = h->data_version;
+  return TOPK_OK;
+}
+
+// Per-query bound of the BF16 filter, rounded up to a float:
+// 2^-12 * sum_m |w_m| * absmax[attr_m] + 2^-100 * sum_m (|w_m| + absmax[attr_m]).
+float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
+  double rel = 0, tiny = 0;
+  for (uint32_t m = 0; m < b.qq; m++) {
+    rel += std::fabs((double)b.w[m]) * (double)absmax[b.attr[m]];
+    tiny += std::fabs((double)b.w[m]) + (double)absmax[b.attr[m]];
+  }
+  const double e = std::ldexp(rel, -12) + std::ldexp(tiny, -100);
+  float f = (float)e;
+  if ((double)f < e) f = std::nextafter(f, INFINITY);
+  return f;
 }
 
 // Batched exact top-k on the handle's primary stream (caller holds batch_mu):
@@ -389,6 +451,33 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (best_total > 0xFFFFFFFFull || cand_total > 0xFFFFFFFFull)
     return fail(TOPK_ERR_UNSUPPORTED, "batch too large: split it");
   int st;
+  cudaStream_t s = h->primary->stream;
+  // scorer: the BF16 tensor-core filter where the table and every weight allow it
+  bool use_bf16 = false;
+  if (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_BF16) {
+    if ((st = ensure_bf16_table(h, s)) != TOPK_OK) return st;
+    use_bf16 = h->xbf_usable && nq <= 0xFFFFFFFFull;
+    for (uint64_t j = 0; use_bf16 && j < nq; j++)
+      for (uint32_t m = 0; m < q[j].qq; m++)
+        if (!(std::fabs(q[j].w[m]) <= kBf16MaxAbs)) use_bf16 = false;
+  }
+  h->last_batch_method = use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
+  if (use_bf16) {
+    std::vector<uint8_t> habf(bf16_query_bytes((uint32_t)nq), 0);
+    for (uint64_t j = 0; j < nq; j++) {
+      double acc[kBf16MaxD] = {0};
+      for (uint32_t m = 0; m < q[j].qq; m++) acc[q[j].attr[m]] += (double)q[j].w[m];
+      float a[kBf16MaxD];
+      for (uint32_t m = 0; m < kBf16MaxD; m++) a[m] = (float)acc[m];
+      bf16_pack_query(a, (uint32_t)j, habf.data());
+      q[j].err = bf16_error_bound(q[j], h->absmax);
+    }
+    if ((st = ensure(h->b_abf, habf.size())) != TOPK_OK) return st;
+    if ((st = ensure(h->b_err, sizeof(uint32_t))) != TOPK_OK) return st;
+    CK(cudaMemcpyAsync(h->b_abf.p, habf.data(), habf.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h->b_err.p, 0, sizeof(uint32_t), s));
+    CK(cudaStreamSynchronize(s));  // habf is pageable and goes out of scope
+  }
   if ((st = ensure(h->b_q, nq * sizeof(BatchQuery))) != TOPK_OK) return st;
   if ((st = ensure(h->b_st, nq * sizeof(BatchState))) != TOPK_OK) return st;
   if ((st = ensure(h->b_best, best_total * sizeof(uint2))) != TOPK_OK) return st;
@@ -403,17 +492,22 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   BatchState *dst = static_cast<BatchState *>(h->b_st.p);
   uint2 *dbest = static_cast<uint2 *>(h->b_best.p);
   uint2 *dcand = static_cast<uint2 *>(h->b_cand.p);
-  cudaStream_t s = h->primary->stream;
   const uint32_t nqq = (uint32_t)nq;
   CK(cudaMemcpyAsync(dq, q.data(), nq * sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(dst, 0, nq * sizeof(BatchState), s));
   CK(cudaEventRecord(h->b_ev0, s));
   const uint64_t boot = std::min<uint64_t>(h->n, kBatchBootRows);
   CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
+  // chunk boundaries stay multiples of 256 rows (the filter's object tiles)
   for (uint64_t r = boot, size = boot; r < h->n; size *= 2) {
     const uint64_t e = std::min<uint64_t>(h->n, r + size);
-    CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, s));
-    CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, false, s));
+    if (use_bf16)
+      CK(launch_bf16_filter(static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf.p),
+                            h->table, h->ld, r, e, dq, nqq, dst, dcand, h->num_sms, h->wait_limit,
+                            static_cast<uint32_t *>(h->b_err.p), s));
+    else
+      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, s));
+    CK(launch_batch_reduce(dq, nqq, dst, dbest, dcand, kmax, capmax, s));
     r = e;
   }
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
@@ -429,11 +523,23 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   CK(cudaMemcpyAsync(hcnt.data(), h->b_count.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hth.data(), h->b_thr.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
+  uint32_t herr = 0;
+  if (use_bf16) CK(cudaMemcpyAsync(&herr, h->b_err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->b_ev0, h->b_ev1));
   h->last_batch_ms = ms;
-  uint64_t fallbacks = 0;
+  uint64_t fallbacks = 0, cands = 0;
+  float err_ratio = 0;
+  for (uint64_t j = 0; j < nq; j++) {
+    cands += hst[j].cands;
+    float r;
+    std::memcpy(&r, &hst[j].errmax, 4);
+    err_ratio = std::max(err_ratio, r);
+  }
+  h->last_batch_cands = cands;
+  h->last_batch_err_ratio = err_ratio;
   for (uint64_t j = 0; j < nq; j++) {
     if (hst[j].flags & 1u) {  // a candidate region overflowed: answer exactly with the scan
       ++fallbacks;
@@ -453,7 +559,6 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if (thresholds) thresholds[j] = hth[j];
   }
   h->last_batch_fallbacks = fallbacks;
-  h->last_batch_cands = 0;
   return TOPK_OK;
 }
 
@@ -555,6 +660,7 @@ int topk_upload_colmajor(topk_table_t h, const float *host, uint64_t ld_host) {
   if (!h || !host) return fail(TOPK_ERR_ARG, "null argument");
   if (ld_host < h->n) return fail(TOPK_ERR_ARG, "ld_host=%llu < n=%llu", (unsigned long long)ld_host, (unsigned long long)h->n);
   DeviceGuard dg(h->device);
+  table_changed(h);
   CK(cudaMemcpy2D(h->table, h->ld * sizeof(float), host, ld_host * sizeof(float), h->n * sizeof(float), h->d,
                   cudaMemcpyHostToDevice));
   h->has_data = true;
@@ -575,6 +681,7 @@ int topk_generate(topk_table_t h, int dist, uint64_t seed) {
   if (dist < 0 || dist > 3) return fail(TOPK_ERR_ARG, "dist must be 0..3");
   if (h->d > 64) return fail(TOPK_ERR_UNSUPPORTED, "generator supports d <= 64");
   DeviceGuard dg(h->device);
+  table_changed(h);
   CK(launch_generate(h->table, h->ld, h->d, h->n, dist, seed, h->primary->stream));
   CK(cudaStreamSynchronize(h->primary->stream));
   h->has_data = true;
@@ -614,6 +721,7 @@ int topk_normalize(topk_table_t h, float *mins, float *maxs) {
     if (maxs) maxs[m] = mx;
   }
   CK(cudaMemcpyAsync(h->d_norm, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s));
+  table_changed(h);
   CK(launch_normalize(h->table, h->ld, h->d, h->n, h->d_norm, h->d_norm + h->d, s));
   CK(cudaStreamSynchronize(s));
   return TOPK_OK;
@@ -664,6 +772,8 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
   h->last_batch_ms = 0;
   h->last_batch_fallbacks = 0;
   h->last_batch_cands = 0;
+  h->last_batch_err_ratio = 0;
+  h->last_batch_method = TOPK_BATCH_LOOP;
   for (uint64_t j = 0; j < nq; j++) {
     uint64_t c = 0;
     float th = 0;
@@ -678,7 +788,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
 
 int topk_set_batch_method(topk_table_t h, int method) {
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
-  if (method < TOPK_BATCH_AUTO || method > TOPK_BATCH_FP32)
+  if (method < TOPK_BATCH_AUTO || method > TOPK_BATCH_BF16)
     return fail(TOPK_ERR_UNSUPPORTED, "batch method %d not available", method);
   std::lock_guard<std::mutex> lk(h->batch_mu);
   h->batch_method = method;
@@ -691,6 +801,14 @@ int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks
   if (device_ms) *device_ms = h->last_batch_ms;
   if (fallbacks) *fallbacks = h->last_batch_fallbacks;
   if (candidates) *candidates = h->last_batch_cands;
+  return TOPK_OK;
+}
+
+int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  if (method) *method = h->last_batch_method;
+  if (max_err_ratio) *max_err_ratio = h->last_batch_err_ratio;
   return TOPK_OK;
 }
 

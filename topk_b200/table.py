@@ -113,13 +113,18 @@ class Table:
         return ge.value, gt.value
 
     def set_batch_method(self, method):
-        """0 auto, 1 loop of single-query scans, 2 batched FP32 (see include/topk_b200.h)."""
+        """0 auto, 1 loop of single-query scans, 2 batched FP32, 3 BF16 tensor-core
+        filter with exact rescoring (see include/topk_b200.h)."""
         check(_lib.load().topk_set_batch_method(self._h, int(method)))
 
     def last_batch_stats(self):
+        L = _lib.load()
         ms, fb, cand = C.c_double(), C.c_uint64(), C.c_uint64()
-        check(_lib.load().topk_last_batch_stats(self._h, C.byref(ms), C.byref(fb), C.byref(cand)))
-        return {"device_ms": ms.value, "fallbacks": fb.value, "candidates": cand.value}
+        check(L.topk_last_batch_stats(self._h, C.byref(ms), C.byref(fb), C.byref(cand)))
+        method, ratio = C.c_int(), C.c_double()
+        check(L.topk_last_batch_info(self._h, C.byref(method), C.byref(ratio)))
+        return {"device_ms": ms.value, "fallbacks": fb.value, "candidates": cand.value, "method": method.value,
+                "max_err_ratio": ratio.value}
 
     def set_scan_tuning(self, max_ctas_per_sm=0):
         check(_lib.load().topk_set_scan_tuning(self._h, int(max_ctas_per_sm)))

@@ -18,9 +18,9 @@
 // A query whose candidate region overflows in some chunk (possible only on
 // adversarial orders) is flagged; the host answers it with the single-query scan.
 //
-// Two scorers share this schedule: the plain FP32 one here, and the BF16
-// tensor-core filter (bf16_filter.cu), which rescores its survivors exactly before
-// appending them.  Either way the candidates carry exact keys.
+// Two scorers share this schedule: the plain FP32 one here (exact keys), and the
+// BF16 tensor-core filter (bf16_filter.cu), whose candidates carry approximate
+// keys that the reduce makes exact by rescoring them in the reference order.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -180,19 +180,34 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
 }
 
 // ---------------------------------------------------------------- reduce
-// One block per query: merge best[] with the chunk's candidates (exact keys, from
-// either scorer) into the new top-k.
-__global__ void __launch_bounds__(kBT) batch_reduce_kernel(const BatchQuery *__restrict__ qs,
+// One block per query: merge best[] with the chunk's candidates into the new
+// top-k.  Candidates of the BF16 filter carry approximate keys: with `rescore`
+// each is first scored exactly in the reference order (and the filter's error,
+// relative to its bound, recorded).
+__global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restrict__ table, uint64_t ld,
+                                                           const BatchQuery *__restrict__ qs,
                                                            BatchState *__restrict__ st, uint2 *__restrict__ best,
-                                                           const uint2 *__restrict__ cand) {
+                                                           const uint2 *__restrict__ cand, int rescore) {
   extern __shared__ __align__(16) unsigned char smem[];
   BatchShared *sh = reinterpret_cast<BatchShared *>(smem);
   uint32_t *hist = reinterpret_cast<uint32_t *>(smem + 128);
+  uint8_t *attr = smem + 1152;
+  float *w = reinterpret_cast<float *>(smem + 1184);
   uint2 *ent = reinterpret_cast<uint2 *>(smem + 1408);
   const BatchQuery &q = qs[blockIdx.x];
   BatchState &s = st[blockIdx.x];
   const int t = threadIdx.x;
-  const uint32_t k = q.k;
+  if (t < (int)kBatchMaxQ) {
+    attr[t] = q.attr[t];
+    w[t] = q.w[t];
+  }
+  if (t == 0) {
+    sh->qq = q.qq;
+    sh->k = q.k;
+    sh->pad[0] = 0u;  // largest |filter score - exact| / err of this chunk (FP32 bits)
+  }
+  __syncthreads();
+  const uint32_t qq = sh->qq, k = sh->k;
   const uint32_t cnt = s.cnt;
   const uint32_t thr = s.thr;
   const uint32_t nc_raw = s.ccount;
@@ -201,12 +216,22 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const BatchQuery *__r
   uint2 *out = ent + cnt + q.cand_cap;
   const uint2 *b = best + q.best_off;
   const uint2 *c = cand + q.cand_off;
+  const float err = q.err;
   for (uint32_t j = t; j < cnt; j += kBT) ent[j] = b[j];
-  for (uint32_t j = t; j < nc; j += kBT) ent[cnt + j] = c[j];
+  for (uint32_t j = t; j < nc; j += kBT) {
+    uint2 e = c[j];
+    if (rescore) {
+      const float exact = score_row(table, ld, e.y, attr, w, qq);
+      const float ratio = fabsf(key2f(e.x) - exact) / err;
+      if (ratio == ratio) atomicMax(&sh->pad[0], __float_as_uint(ratio));
+      e.x = f2key(exact);
+    }
+    ent[cnt + j] = e;
+  }
   __syncthreads();
   if (cnt == k) {
-    // best[] is a full top-k: new entries must reach thr (the scorers only append
-    // such entries; this keeps the merge correct whatever a scorer appends)
+    // best[] is a full top-k: new entries must reach thr (rescored filter
+    // candidates may not); merge the two sets
     for (uint32_t j = cnt + t; j < total; j += kBT)
       if (ent[j].x < thr) ent[j] = make_uint2(0u, 0xFFFFFFFFu);  // below every real entry
     __syncthreads();
@@ -220,6 +245,7 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const BatchQuery *__r
     if (kept == k) ns.thr = max(thr, sh->sel.kept_min + 1u);
     if (nc_raw > q.cand_cap) ns.flags |= 1u;
     ns.cands = (ns.cands + nc_raw < ns.cands) ? 0xFFFFFFFFu : ns.cands + nc_raw;
+    ns.errmax = max(ns.errmax, sh->pad[0]);
     ns.ccount = 0;
     s = ns;
   }
@@ -299,12 +325,13 @@ cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d,
 
 size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax) { return kQueryShared + (size_t)(2 * kmax + capmax) * 8; }
 
-cudaError_t launch_batch_reduce(const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *best, const uint2 *cand,
-                                uint32_t kmax, uint32_t capmax, cudaStream_t s) {
+cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
+                                uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,
+                                cudaStream_t s) {
   const size_t smem = batch_reduce_smem(kmax, capmax);
   cudaError_t e = cudaFuncSetAttribute(batch_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  batch_reduce_kernel<<<nq, kBT, smem, s>>>(qs, st, best, cand);
+  batch_reduce_kernel<<<nq, kBT, smem, s>>>(table, ld, qs, st, best, cand, rescore ? 1 : 0);
   return cudaGetLastError();
 }
 

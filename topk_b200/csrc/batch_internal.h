@@ -11,6 +11,7 @@ constexpr uint32_t kBatchGroup = 64;   // queries scored per staged table tile (
 constexpr uint32_t kBatchMaxD = 64;    // table width the FP32 scorer stages
 constexpr uint32_t kBatchBootRows = 8192;  // rows of the exact bootstrap
 constexpr uint32_t kBf16MaxD = 16;         // table width of the BF16 tensor-core filter (MMA K)
+constexpr uint32_t kBf16LogCap = 65536;    // survivor-log entries per filter CTA
 
 // Per-query descriptor (device, read-only during a batch).
 struct BatchQuery {
@@ -31,10 +32,8 @@ struct BatchState {
   uint32_t cnt;     // entries in best[]
   uint32_t ccount;  // candidates appended since the last reduce (may exceed the cap)
   uint32_t flags;   // bit 0: a candidate region overflowed (exact fallback needed)
-  uint32_t cands;     // candidates appended over the whole batch (saturating)
-  uint32_t errmax;    // BF16 filter: max |filter score - exact score| / err, FP32 bits
-  uint32_t rescored;  // BF16 filter: survivors of the approximate cut (rescored exactly)
-  uint32_t pad;
+  uint32_t cands;   // candidates appended over the whole batch (saturating)
+  uint32_t errmax;  // BF16 filter: max |filter score - exact score| / err, FP32 bits
 };
 
 size_t batch_bootstrap_smem(uint32_t rows, uint32_t kmax);
@@ -44,8 +43,9 @@ size_t batch_score_smem(uint32_t d);
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                     const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, cudaStream_t s);
 size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax);
-cudaError_t launch_batch_reduce(const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *best, const uint2 *cand,
-                                uint32_t kmax, uint32_t capmax, cudaStream_t s);
+cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
+                                uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,
+                                cudaStream_t s);
 // BF16 tensor-core filter (bf16_filter.cu).
 uint64_t bf16_table_bytes(uint64_t n);
 cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,
@@ -53,9 +53,19 @@ cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64
 size_t bf16_query_bytes(uint32_t nq);
 // Host: write query j's 16-wide row a[] (hi and lo) into the tiled query buffer.
 void bf16_pack_query(const float *a, uint32_t j, uint8_t *abf);
-cudaError_t launch_bf16_filter(const uint8_t *xbf, const uint8_t *abf, const float *table, uint64_t ld, uint64_t r0,
-                               uint64_t r1, const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, int num_sms,
-                               uint64_t wait_limit, uint32_t *err, cudaStream_t s);
+// Work split of one filter launch over rows [r0, r1): query tiles of 256 in groups
+// of up to 8 per CTA, the chunk's object tiles of 128 split among cpg CTAs per group.
+struct FilterPlan {
+  uint64_t tile0, tile1;
+  uint32_t nqt, qt_per_cta, ngroups, cpg;
+  uint64_t grid;
+};
+FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms);
+// r0 must be a multiple of 128; log/log_q hold grid * log_cap entries.
+cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
+                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint2 *log,
+                               uint16_t *log_q, uint32_t log_cap, uint64_t wait_limit, uint32_t *err,
+                               cudaStream_t s);
 cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
                                 uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
                                 uint32_t *out_count, float *out_thr, cudaStream_t s);

@@ -1,23 +1,21 @@
 // BF16 tensor-core filter of the batched path (tcgen05 + TMEM, sm_100a).
 //
 // For every (query, object) pair of a chunk the filter computes an approximate
-// score on the 5th-generation tensor cores.  The objects whose approximate score
-// can still reach the query's threshold are rescored exactly in the reference
-// order (cpu/TPAc.h:135-150: s += x[attr[m]] * weights[attr[m]], FP32, no FMA)
-// and appended to the query's candidate region when the exact key reaches the
-// threshold, so batch_reduce_kernel (batch.cu) merges exact keys and the results
-// are bit-identical to the FP32 paths.  Rescoring before appending keeps the
-// regions as small as the FP32 scorer's even where many objects tie just below
-// the threshold (clipped, correlated data).
+// score on the 5th-generation tensor cores and keeps, per query, the objects whose
+// approximate score can still reach the query's threshold.  batch_reduce_kernel
+// (batch.cu) rescoring those candidates in the reference order (cpu/TPAc.h:135-150:
+// s += x[attr[m]] * weights[attr[m]], FP32, no FMA) makes every kept key exact, so
+// the results are bit-identical to the FP32 paths.
 //
 // Operands, both K-major without swizzle (core matrices of 8 rows x 16 bytes; the
 // K-adjacent core matrix 128 B further on, the next 8 rows 256 B further on):
 //   table  each object's 16 attributes split x = hi + lo (bf16 each, |x - hi - lo|
-//          <= 2^-16 |x|); tiles of 256 objects: hi 8 KB, then lo 8 KB;
+//          <= 2^-16 |x|); tiles of 128 objects: hi 4 KB, then lo 4 KB  (MMA A, M=128);
 //   query  a 16-wide row a[m] = sum of weights[attr[j]] over the j with attr[j] = m,
-//          split the same way; tiles of 128 queries: hi 4 KB, then lo 4 KB.
-// One (query tile, object tile) pair is three MMAs M=128 N=256 K=16 into FP32 TMEM:
-//   D = Ahi.Bhi + Alo.Bhi + Ahi.Blo        (the lo.lo term lies inside the bound)
+//          split the same way; tiles of 256 queries: hi 8 KB, then lo 8 KB (MMA B, N=256).
+// One (object tile, query tile) pair is three MMAs M=128 N=256 K=16 into FP32 TMEM
+// (lane = object, column = query):
+//   D = Xhi.Ahi + Xlo.Ahi + Xhi.Alo        (the lo.lo term lies inside the bound)
 // Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
 //   E = 2^-12 * sum_m |weights[attr[m]]| * max|column attr[m]|  (+ 2^-100 terms for
 //   subnormal flushing).  Split and product errors give 3.1*2^-16, 48 FP32
@@ -26,14 +24,21 @@
 //   which is not specified.  An object with exact score >= the threshold float t
 //   has D >= t - E, so the cut t - E (rounded down) loses none.
 //
-// Roles of the 320 threads of a CTA (one CTA per SM: TMEM is allocated whole):
-//   warps 0-7  epilogue: warp w reads TMEM lanes 32*(w%4).. (one query per thread),
-//              columns 128*(w/4).. (half an object tile), compares with the
-//              query's cut, rescores survivors and appends candidates;
-//   warp 8     producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
-//              the CTA's query tiles once and object tiles into a 4-stage ring;
-//   warp 9     allocates the 512 TMEM columns; lane 0 issues the MMAs for two
+// Roles of the 576 threads of a CTA (one CTA per SM: TMEM is allocated whole):
+//   warps 0-15 epilogue: warp w reads TMEM lanes 32*(w%4).. (one object per
+//              thread), columns 64*(w/4).. (a quarter of a query tile);
+//              one compare per value against the column's cut and a warp vote;
+//              for the rare chunks with survivors a ballot per column gives the
+//              passing objects, appended with one shared atomic per column to the
+//              CTA's survivor log in global memory (no global atomic in the
+//              MMA pipeline);
+//   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
+//              the CTA's query tiles once and object tiles into a 6-stage ring;
+//   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs for two
 //              accumulators of 256 columns (double buffered against the epilogue).
+// After the last tile the whole CTA moves its log into the queries' candidate
+// regions (global atomics, many in flight).  A survivor that finds the log full
+// flags its query for the exact single-query fallback.
 // Every mbarrier wait is bounded; a wait that runs out sets the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (bounded),
 // TMEM is freed and the error word is set (the host reports TOPK_ERR_TIMEOUT).
@@ -51,20 +56,21 @@ namespace topk {
 
 namespace {
 
-constexpr uint32_t kFTile = 256;        // objects per tile (MMA N)
-constexpr uint32_t kFTileBytes = 16384; // hi + lo of one object tile
-constexpr uint32_t kQTile = 128;        // queries per tile (MMA M)
-constexpr uint32_t kQTileBytes = 8192;  // hi + lo of one query tile
-constexpr uint32_t kStages = 4;
-constexpr uint32_t kEpiWarps = 8;
+constexpr uint32_t kOTile = 128;        // objects per tile (MMA M, TMEM lanes)
+constexpr uint32_t kOTileBytes = 8192;  // hi + lo of one object tile
+constexpr uint32_t kQTile = 256;        // queries per tile (MMA N, TMEM columns)
+constexpr uint32_t kQTileBytes = 16384; // hi + lo of one query tile
+constexpr uint32_t kStages = 6;
+constexpr uint32_t kEpiWarps = 16;
+constexpr uint32_t kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kMaxQTPerCta = 16;
+constexpr uint32_t kMaxQTPerCta = 8;
 constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
 
 // Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits
 // 7-9 = 1, 10-12 = 1), both K-major, N>>3 at bits 17-22, M>>4 at bits 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kFTile >> 3) << 17) | ((kQTile >> 4) << 24);
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kQTile >> 3) << 17) | ((kOTile >> 4) << 24);
 
 // Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B (K-adjacent
 // core matrices), SBO 256 B (next 8 rows), version 1 (bit 46).
@@ -103,12 +109,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ float max3(float a, float b, float c) {
-  float r;
-  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-  return r;
-}
-
 // Bounded wait that also gives up once another role of the CTA has aborted.
 __device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, uint64_t limit, volatile uint32_t *abort_flag) {
   for (uint64_t it = 0; it < limit; ++it) {
@@ -119,41 +119,19 @@ __device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, uint64_t l
   return false;
 }
 
-// A survivor of the approximate cut: score it exactly in the reference order
-// (cpu/TPAc.h:135-150), record the filter's error, append it if its exact key
-// reaches the threshold.  Rare, so kept out of line.
-__device__ __noinline__ void filter_survivor(const float *__restrict__ table, uint64_t ld,
-                                             const BatchQuery *__restrict__ qs, BatchState *__restrict__ st,
-                                             uint2 *__restrict__ cand, uint32_t q, uint32_t thr, float approx,
-                                             uint32_t id) {
-  const BatchQuery &bq = qs[q];
-  float s = 0.0f;
-  for (uint32_t m = 0; m < bq.qq; ++m)
-    s = __fadd_rn(s, __fmul_rn(__ldg(table + (uint64_t)bq.attr[m] * ld + id), bq.w[m]));
-  BatchState &b = st[q];
-  atomicAdd(&b.rescored, 1u);
-  const float ratio = fabsf(approx - s) / bq.err;
-  if (ratio == ratio) atomicMax(&b.errmax, __float_as_uint(ratio));
-  const uint32_t key = f2key(s);
-  if (key >= thr) {
-    const uint32_t pos = atomicAdd(&b.ccount, 1u);
-    if (pos < bq.cand_cap) cand[bq.cand_off + pos] = make_uint2(key, id);
-  }
-}
-
 struct FilterArgs {
-  const uint8_t *xbf;  // object tiles (kFTileBytes each)
+  const uint8_t *xbf;  // object tiles (kOTileBytes each)
   const uint8_t *abf;  // query tiles (kQTileBytes each)
-  const float *table;  // the FP32 column-major table (exact rescoring)
-  uint64_t ld;
   const BatchQuery *qs;
   BatchState *st;
   uint2 *cand;
+  uint2 *log;          // per-CTA survivor logs: (key, id), log_cap entries each
+  uint16_t *log_q;     // query of each log entry, relative to the CTA's first query
+  uint32_t log_cap;
+  uint32_t nq, nqt;    // queries, query tiles
+  uint32_t qt_per_cta, ngroups, cpg;
   uint64_t tile0, tile1;  // object tiles of the chunk
   uint64_t r1;            // rows >= r1 are never appended
-  uint32_t nq, nqt;       // queries, query tiles
-  uint32_t qt_per_cta, ngroups, cpg;
-  uint32_t pad;
   uint64_t wait_limit;
   uint32_t *err;
 };
@@ -170,15 +148,19 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   const uint64_t te = min(p.tile1, tb + per);
   if (tb >= te) return;  // uniform over the block: no barrier or TMEM touched yet
 
-  unsigned char *sa = smem;
-  unsigned char *sb = smem + (size_t)QT * kQTileBytes;
-  float *scut = reinterpret_cast<float *>(sb + (size_t)kStages * kFTileBytes);
-  uint32_t *sthr = reinterpret_cast<uint32_t *>(scut + QT * kQTile);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sthr + QT * kQTile);
+  // shared layout: query tiles | object ring | cut[QT*256] | barriers and words
+  unsigned char *sq = smem;
+  unsigned char *so = smem + (size_t)QT * kQTileBytes;
+  float *scut = reinterpret_cast<float *>(so + (size_t)kStages * kOTileBytes);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(scut + QT * kQTile);
   uint64_t *full = bars, *empty = bars + kStages, *accf = bars + 2 * kStages, *acce = accf + 2;
-  uint64_t *afull = acce + 2, *mdone = afull + 1;
+  uint64_t *qfull = acce + 2, *mdone = qfull + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 1);
   volatile uint32_t *abort_flag = tmem_slot + 1;
+  uint32_t *log_n = tmem_slot + 2;
+  uint2 *log = p.log + (size_t)blockIdx.x * p.log_cap;
+  uint16_t *log_q = p.log_q + (size_t)blockIdx.x * p.log_cap;
+  const uint32_t q0 = qt0 * kQTile;  // first query of this CTA
 
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t limit = p.wait_limit;
@@ -191,25 +173,24 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
       mbar_init(accf + b, 1);
       mbar_init(acce + b, kEpiWarps);
     }
-    mbar_init(afull, 1);
+    mbar_init(qfull, 1);
     mbar_init(mdone, 1);
     *abort_flag = 0u;
+    *log_n = 0u;
     fence_barrier_init();
   }
-  // per-query cut: threshold float minus the bound, rounded down; +inf for rows
+  // per-query cut: threshold float minus the bound, rounded down; +inf for columns
   // past the last query, -inf while best[] is not full (every object is a candidate)
   for (uint32_t j = threadIdx.x; j < QT * kQTile; j += kFThreads) {
-    const uint32_t q = qt0 * kQTile + j;
+    const uint32_t q = q0 + j;
     float cut = __int_as_float(0x7F800000);
-    uint32_t thr = 0xFFFFFFFFu;
     if (j < nqt * kQTile && q < p.nq) {
-      thr = p.st[q].thr;
+      const uint32_t thr = p.st[q].thr;
       cut = thr == 0u ? __int_as_float(0xFF800000) : __fsub_rd(thr_float(thr), p.qs[q].err);
     }
     scut[j] = cut;
-    sthr[j] = thr;
   }
-  if (warp == 9) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols)
                  : "memory");
@@ -220,37 +201,37 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 8) {
+  if (warp == kProducerWarp) {
     // ---------------------------------------------------------------- producer
     if (lane == 0) {
-      mbar_arrive_expect_tx(afull, nqt * kQTileBytes);
+      mbar_arrive_expect_tx(qfull, nqt * kQTileBytes);
       for (uint32_t i = 0; i < nqt; ++i)
-        bulk_g2s(sa + (size_t)i * kQTileBytes, p.abf + (size_t)(qt0 + i) * kQTileBytes, kQTileBytes, afull);
+        bulk_g2s(sq + (size_t)i * kQTileBytes, p.abf + (size_t)(qt0 + i) * kQTileBytes, kQTileBytes, qfull);
       uint64_t it = 0;
       for (uint64_t t = tb; t < te; ++t, ++it) {
         const uint32_t s = (uint32_t)(it % kStages);
         if (it >= kStages && !fwait(empty + s, (uint32_t)((it / kStages - 1) & 1), limit, abort_flag)) break;
-        mbar_arrive_expect_tx(full + s, kFTileBytes);
-        bulk_g2s(sb + (size_t)s * kFTileBytes, p.xbf + t * kFTileBytes, kFTileBytes, full + s);
+        mbar_arrive_expect_tx(full + s, kOTileBytes);
+        bulk_g2s(so + (size_t)s * kOTileBytes, p.xbf + t * kOTileBytes, kOTileBytes, full + s);
       }
       // the CTA must not exit with copies in flight: wait for the last use of each stage
       const uint64_t first = it > kStages ? it - kStages : 0;
       for (uint64_t j = first; j < it; ++j)
         if (!mbar_wait_bounded(full + (j % kStages), (uint32_t)((j / kStages) & 1), limit)) *abort_flag = 1u;
-      if (!mbar_wait_bounded(afull, 0, limit)) *abort_flag = 1u;
+      if (!mbar_wait_bounded(qfull, 0, limit)) *abort_flag = 1u;
     }
-  } else if (warp == 9) {
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      bool ok = fwait(afull, 0, limit, abort_flag);
+      bool ok = fwait(qfull, 0, limit, abort_flag);
       uint64_t it = 0;
       uint32_t seq = 0;
       for (uint64_t t = tb; ok && t < te; ++t, ++it) {
         const uint32_t s = (uint32_t)(it % kStages);
         if (!fwait(full + s, (uint32_t)((it / kStages) & 1), limit, abort_flag)) break;
         tc_fence_after();
-        const uint32_t bs = smem_u32(sb + (size_t)s * kFTileBytes);
-        const uint64_t bhi = smem_desc(bs), blo = smem_desc(bs + kFTileBytes / 2);
+        const uint32_t os = smem_u32(so + (size_t)s * kOTileBytes);
+        const uint64_t xhi = smem_desc(os), xlo = smem_desc(os + kOTileBytes / 2);
         for (uint32_t i = 0; i < nqt; ++i, ++seq) {
           const uint32_t buf = seq & 1u;
           if (seq >= 2 && !fwait(acce + buf, ((seq >> 1) - 1) & 1u, limit, abort_flag)) {
@@ -258,12 +239,12 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
             break;
           }
           tc_fence_after();
-          const uint32_t as = smem_u32(sa + (size_t)i * kQTileBytes);
-          const uint64_t ahi = smem_desc(as), alo = smem_desc(as + kQTileBytes / 2);
-          const uint32_t d = tmem + buf * kFTile;
-          tc_mma(d, ahi, bhi, 0u);
-          tc_mma(d, alo, bhi, 1u);
-          tc_mma(d, ahi, blo, 1u);
+          const uint32_t qsa = smem_u32(sq + (size_t)i * kQTileBytes);
+          const uint64_t ahi = smem_desc(qsa), alo = smem_desc(qsa + kQTileBytes / 2);
+          const uint32_t d = tmem + buf * kQTile;
+          tc_mma(d, xhi, ahi, 0u);
+          tc_mma(d, xlo, ahi, 1u);
+          tc_mma(d, xhi, alo, 1u);
           tc_commit(accf + buf);
         }
         if (!ok) break;
@@ -275,47 +256,90 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    const uint32_t quarter = warp & 3u, half = warp >> 2;
-    const uint32_t row = quarter * 32u + lane;  // query row of the tile = TMEM lane
+    const uint32_t quarter = warp & 3u, part = warp >> 2;  // TMEM lanes 32*quarter.., columns 64*part..
     const uint32_t lane_addr = (quarter * 32u) << 16;
+    const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t seq = 0;
     bool ok = true;
     for (uint64_t t = tb; ok && t < te; ++t) {
-      const uint64_t id0 = t * kFTile + half * 128u;
+      const uint64_t obj = t * kOTile + quarter * 32u + lane;  // this thread's object
+      const bool valid = obj < p.r1;
       for (uint32_t i = 0; i < nqt; ++i, ++seq) {
         const uint32_t buf = seq & 1u;
         ok = __all_sync(0xFFFFFFFFu, fwait(accf + buf, (seq >> 1) & 1u, limit, abort_flag));
         if (!ok) break;
         tc_fence_after();
-        uint32_t v[128];
-        const uint32_t ta = tmem + lane_addr + buf * kFTile + half * 128u;
-        tmem_ld32(ta, v);
-        tmem_ld32(ta + 32, v + 32);
-        tmem_ld32(ta + 64, v + 64);
-        tmem_ld32(ta + 96, v + 96);
-        tmem_wait_ld();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(acce + buf);
-        const float cut = scut[i * kQTile + row];
+        const uint32_t col0 = i * kQTile + part * 64u;  // CTA-relative query of chunk 0, column 0
+        const uint32_t tcol = tmem + lane_addr + buf * kQTile + part * 64u;
+        // hot path: all 64 columns in one round trip, one compare per value
+        uint32_t hits;
+        {
+          uint32_t v[64];
+          tmem_ld32(tcol, v);
+          tmem_ld32(tcol + 32, v + 32);
+          tmem_wait_ld();
+          const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0);
+          uint32_t h = 0;
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          const uint32_t *u = v + cc * 32;
-          float m = max3(__uint_as_float(u[0]), __uint_as_float(u[1]), __uint_as_float(u[2]));
+          for (int k = 0; k < 16; ++k) {
+            const float4 x = c4[k];
+            const uint32_t a = (uint32_t)(__uint_as_float(v[4 * k]) >= x.x) |
+                               (uint32_t)(__uint_as_float(v[4 * k + 1]) >= x.y) |
+                               (uint32_t)(__uint_as_float(v[4 * k + 2]) >= x.z) |
+                               (uint32_t)(__uint_as_float(v[4 * k + 3]) >= x.w);
+            h |= a << (k >> 3);  // bit cc: chunk cc of 32 columns has a hit
+          }
+          hits = __reduce_or_sync(0xFFFFFFFFu, valid ? h : 0u);
+        }
+        if (hits == 0u) {  // common case: the accumulator is free right away
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(acce + buf);
+          continue;
+        }
+        // cold path: the chunks with a hit, read again (the accumulator is held until done)
+#pragma unroll 1
+        for (uint32_t cc = 0; cc < 2; ++cc) {
+          if (!(hits & (1u << cc))) continue;
+          uint32_t v[32];
+          tmem_ld32(tcol + cc * 32u, v);
+          tmem_wait_ld();
+          const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0 + cc * 32u);
+          float cut[32];
 #pragma unroll
-          for (int j = 3; j < 31; j += 2) m = max3(m, __uint_as_float(u[j]), __uint_as_float(u[j + 1]));
-          m = fmaxf(m, __uint_as_float(u[31]));
-          if (m >= cut) {
-            const uint32_t q = (qt0 + i) * kQTile + row;
-            const uint32_t thr = sthr[i * kQTile + row];
+          for (int k = 0; k < 8; ++k) {
+            const float4 x = c4[k];
+            cut[4 * k] = x.x;
+            cut[4 * k + 1] = x.y;
+            cut[4 * k + 2] = x.z;
+            cut[4 * k + 3] = x.w;
+          }
+          {
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-              const float f = __uint_as_float(u[j]);
-              const uint64_t id = id0 + cc * 32 + j;
-              if (f >= cut && id < p.r1) filter_survivor(p.table, p.ld, p.qs, p.st, p.cand, q, thr, f, (uint32_t)id);
+              const bool pass = valid && __uint_as_float(v[j]) >= cut[j];
+              const uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
+              if (b) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(log_n, __popc(b));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (pass) {
+                  const uint32_t e = base + __popc(b & lt_mask);
+                  const uint32_t ql = col0 + cc * 32u + j;
+                  if (e < p.log_cap) {
+                    log[e] = make_uint2(f2key(__uint_as_float(v[j])), (uint32_t)obj);
+                    log_q[e] = (uint16_t)ql;
+                  } else {
+                    atomicOr(&p.st[q0 + ql].flags, 1u);  // lost: the exact scan answers it
+                  }
+                }
+              }
             }
           }
         }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce + buf);
       }
     }
   }
@@ -323,12 +347,36 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   // ---------------------------------------------------------------- teardown
   tc_fence_before();
   __syncthreads();
-  if (warp == 9) {
+  if (warp == kMmaWarp) {
     __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
-  if (threadIdx.x == 0 && *abort_flag) atomicExch(p.err, 1u);
+  if (*abort_flag) {
+    if (threadIdx.x == 0) atomicExch(p.err, 1u);
+    return;
+  }
+  // the CTA's survivors into their queries' candidate regions (4 in flight a thread)
+  const uint32_t n = min(*log_n, p.log_cap);
+  for (uint32_t e0 = threadIdx.x; e0 < n; e0 += 4 * kFThreads) {
+    uint32_t pos[4], q[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t e = e0 + u * kFThreads;
+      if (e < n) {
+        q[u] = q0 + log_q[e];
+        pos[u] = atomicAdd(&p.st[q[u]].ccount, 1u);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t e = e0 + u * kFThreads;
+      if (e < n) {
+        const BatchQuery &bq = p.qs[q[u]];
+        if (pos[u] < bq.cand_cap) p.cand[bq.cand_off + pos[u]] = log[e];
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------- table split
@@ -357,13 +405,13 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict_
       hi[m / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
       lo[m / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
     }
-    const uint64_t t = o / kFTile;
-    const uint32_t r = (uint32_t)(o % kFTile);
-    uint8_t *base = xbf + t * kFTileBytes + (r >> 3) * 256u + (r & 7u) * 16u;
+    const uint64_t t = o / kOTile;
+    const uint32_t r = (uint32_t)(o % kOTile);
+    uint8_t *base = xbf + t * kOTileBytes + (r >> 3) * 256u + (r & 7u) * 16u;
     *reinterpret_cast<uint4 *>(base) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4 *>(base + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-    *reinterpret_cast<uint4 *>(base + kFTileBytes / 2) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    *reinterpret_cast<uint4 *>(base + kFTileBytes / 2 + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+    *reinterpret_cast<uint4 *>(base + kOTileBytes / 2) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    *reinterpret_cast<uint4 *>(base + kOTileBytes / 2 + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
   }
 #pragma unroll
   for (int m = 0; m < 16; ++m) {
@@ -377,14 +425,19 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict_
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-uint64_t bf16_table_bytes(uint64_t n) { return (n + kFTile - 1) / kFTile * kFTileBytes; }
+// query tiles | object ring | cuts | barriers and words
+size_t filter_smem_bytes(uint32_t qt) {
+  return (size_t)qt * (kQTileBytes + kQTile * 4) + (size_t)kStages * kOTileBytes + 256;
+}
+
+uint64_t bf16_table_bytes(uint64_t n) { return (n + kOTile - 1) / kOTile * kOTileBytes; }
 
 cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,
                              int num_sms, cudaStream_t s) {
   if (d > kBf16MaxD) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(absmax, 0, d * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  const uint64_t nobj = (n + kFTile - 1) / kFTile * kFTile;
+  const uint64_t nobj = (n + kOTile - 1) / kOTile * kOTile;
   const uint64_t blocks = std::min<uint64_t>((nobj + 255) / 256, (uint64_t)num_sms * 8);
   bf16_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(table, ld, d, n, nobj, xbf, absmax);
   return cudaGetLastError();
@@ -417,36 +470,47 @@ void bf16_pack_query(const float *a, uint32_t j, uint8_t *abf) {
   }
 }
 
-cudaError_t launch_bf16_filter(const uint8_t *xbf, const uint8_t *abf, const float *table, uint64_t ld, uint64_t r0,
-                               uint64_t r1, const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, int num_sms,
-                               uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
-  if (r0 % kFTile) return cudaErrorInvalidValue;
+FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms) {
+  FilterPlan f{};
+  f.tile0 = r0 / kOTile;
+  f.tile1 = (r1 + kOTile - 1) / kOTile;
+  f.nqt = (nq + kQTile - 1) / kQTile;
+  f.qt_per_cta = std::min<uint32_t>(f.nqt, kMaxQTPerCta);
+  f.ngroups = (f.nqt + f.qt_per_cta - 1) / f.qt_per_cta;
+  const uint64_t ntiles = f.tile1 - f.tile0;
+  f.cpg = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)std::max(1, num_sms / (int)f.ngroups)));
+  f.grid = (uint64_t)f.ngroups * f.cpg;
+  return f;
+}
+
+cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
+                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint2 *log,
+                               uint16_t *log_q, uint32_t log_cap, uint64_t wait_limit, uint32_t *err,
+                               cudaStream_t s) {
+  if (r0 % kOTile || f.grid == 0 || f.grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
   FilterArgs p{};
   p.xbf = xbf;
   p.abf = abf;
-  p.table = table;
-  p.ld = ld;
   p.qs = qs;
   p.st = st;
   p.cand = cand;
-  p.tile0 = r0 / kFTile;
-  p.tile1 = (r1 + kFTile - 1) / kFTile;
-  p.r1 = r1;
+  p.log = log;
+  p.log_q = log_q;
+  p.log_cap = log_cap;
   p.nq = nq;
-  p.nqt = (nq + kQTile - 1) / kQTile;
-  p.qt_per_cta = std::min<uint32_t>(p.nqt, kMaxQTPerCta);
-  p.ngroups = (p.nqt + p.qt_per_cta - 1) / p.qt_per_cta;
-  const uint64_t ntiles = p.tile1 - p.tile0;
-  p.cpg = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)std::max(1, num_sms / (int)p.ngroups)));
+  p.nqt = f.nqt;
+  p.qt_per_cta = f.qt_per_cta;
+  p.ngroups = f.ngroups;
+  p.cpg = f.cpg;
+  p.tile0 = f.tile0;
+  p.tile1 = f.tile1;
+  p.r1 = r1;
   p.wait_limit = wait_limit;
   p.err = err;
-  const size_t smem = std::max(kMinFilterSmem, (size_t)p.qt_per_cta * (kQTileBytes + kQTile * 8) +
-                                                   (size_t)kStages * kFTileBytes + 256);
+  const size_t smem = std::max(kMinFilterSmem, filter_smem_bytes(f.qt_per_cta));
   cudaError_t e = cudaFuncSetAttribute(bf16_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const uint64_t grid = (uint64_t)p.ngroups * p.cpg;
-  if (grid > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
-  bf16_filter_kernel<<<(unsigned)grid, kFThreads, smem, s>>>(p);
+  bf16_filter_kernel<<<(unsigned)f.grid, kFThreads, smem, s>>>(p);
   return cudaGetLastError();
 }
 

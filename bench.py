@@ -15,6 +15,10 @@ flush is needed between queries.
           launch time (per-launch CUDA events), against MEASURED_PEAKS.json hbm_gbs.
   cpu_baseline  the reference's TPAc::findTopKthreads (compiled strict into
           oracle/_ref) on this host, timed on a 2^25-row sample, scaled to n.
+  batched  the multi-query workload: 4096 queries (attribute subsets of size
+          U{2..16}, k U{1..1024}) over a 2^26 x 16 table, plain batched FP32
+          against the BF16 tensor-core filter with exact rescoring; identical
+          results checked, speed-up and the filter's tensor roofline reported.
 
 Multi-GPU (torchrun): every rank holds its own replica and runs the same query
 steps (weak scaling, no collective on the data path); time = max over ranks.
@@ -41,6 +45,8 @@ N_FULL = 1 << 28
 D_FULL = 16
 QS = (2, 4, 8, 16)
 KS = (16, 64, 256, 1024)
+BATCH_N = 1 << 26  # batched workload: 4096 queries over a 2^26 x 16 table
+BATCH_Q = 4096
 
 
 def weights_u01(d, seed):
@@ -200,6 +206,77 @@ def run_reference(args):
     return 0
 
 
+def batch_queries(nq, d, seed=3):
+    """The batched workload's queries: random attribute subsets of size U{2..16}
+    (ascending), weights U(0,1] on the 2^-24 grid, k U{1..1024}; seeded."""
+    rng = np.random.default_rng(seed)
+    W = ((rng.integers(0, 1 << 24, size=(nq, d)) + 1) * 2.0 ** -24).astype(np.float32)
+    A = np.zeros((nq, 16), np.uint8)
+    qqs = np.zeros(nq, np.uint32)
+    for j in range(nq):
+        q = int(rng.integers(2, 17))
+        A[j, :q] = np.sort(rng.choice(d, size=q, replace=False))
+        qqs[j] = q
+    ks = rng.integers(1, 1025, size=nq).astype(np.uint64)
+    return ks, W, A, qqs
+
+
+def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
+    """Batched workload: nq queries over an n x 16 independent table, plain batched
+    FP32 against the BF16 tensor-core filter (same results, checked); device time of
+    the batch kernels (CUDA events inside topk_query_batch), max over ranks."""
+    ks, W, A, qqs = batch_queries(nq, d)
+    t = T.Table(n, d, device=device)
+    t.generate(T.DIST_INDEPENDENT, 0)
+    t.normalize()
+    out = {}
+    res = {}
+    for name, method, r in (("fp32", T.BATCH_FP32, 1), ("bf16", T.BATCH_BF16, reps)):
+        t.set_batch_method(method)
+        res[name] = t.query_batch(ks, W, A, qqs)  # warm-up (and the BF16 table split)
+        ms, walls = [], []
+        for _ in range(r):
+            w0 = time.perf_counter()
+            t.query_batch(ks, W, A, qqs)
+            walls.append(time.perf_counter() - w0)
+            ms.append(t.last_batch_stats()["device_ms"])
+        st = t.last_batch_stats()
+        dev = statistics.median(ms)
+        wall = statistics.median(walls) * 1e3
+        if dist:
+            tt = torch.tensor([dev, wall], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dev, wall = float(tt[0].item()), float(tt[1].item())
+        out[name] = {"device_ms": dev, "queries_per_s": nq * 1000.0 / dev, "e2e_ms": wall,
+                     "e2e_queries_per_s": nq * 1000.0 / wall, "fallbacks": st["fallbacks"],
+                     "candidates": st["candidates"], "method_ran": st["method"]}
+        if name == "bf16":
+            out[name]["max_err_ratio"] = st["max_err_ratio"]
+    t.close()
+    same = all(np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
+               for x, y in zip(res["fp32"], res["bf16"]))
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    tf_peak = float(peaks.get("bf16_tflops", 1590.0))
+    flops = 2.0 * nq * 16 * n  # the dense Q x 16 by 16 x n contraction
+    tf = flops / (out["bf16"]["device_ms"] * 1e-3) / 1e12
+    out.update({
+        "workload": f"{nq} queries, n={n} x 16 FP32 independent, |attrs| U{{2..16}}, k U{{1..1024}}, "
+                    "weights U(0,1]",
+        "identical_results": same,
+        "speedup_bf16_vs_fp32": out["fp32"]["device_ms"] / out["bf16"]["device_ms"],
+        "roofline_bf16": {"bound": "tensor", "achieved": tf, "peak": tf_peak, "unit": "TFLOP/s",
+                          "frac": tf / tf_peak,
+                          "note": "dense-contraction flops 2*Q*16*n over the whole batch's device time; "
+                                  "the filter issues 3 BF16 MMA passes (hi/lo split) per tile"},
+    })
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -209,6 +286,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_FULL)
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-n", type=int, default=BATCH_N)
+    ap.add_argument("--batched-q", type=int, default=BATCH_Q)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -354,6 +434,8 @@ def main():
         except Exception as e:  # the baseline is reported, never the product
             result["cpu_baseline"] = {"error": str(e)}
     table.close()
+    if not args.no_batched:
+        result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -143,6 +143,31 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
                      uint64_t *ids, float *scores, uint64_t kstride, uint64_t *counts,
                      float *thresholds);
 
+/* Build a partitioned copy of the current table for pruned queries: the rows
+ * reordered (Morton order of the attribute values) into partitions of part_rows
+ * consecutive rows (a power of two in [1024, 2^24]), each with its per-attribute
+ * min, max and mean, computed on the device.  Replaces the index build of
+ * VTA::init / PTA::init (cpu/VTA.h:74-158, cpu/PTA.h:88-267).  Needs about
+ * 4*(d+1)*n more bytes of device memory; rebuild after the table changes. */
+int topk_build_partitions(topk_table_t h, uint32_t part_rows);
+
+/* The partitions: count, rows each, and (arrays of num_parts*d, row p*d + m for
+ * partition p, attribute m; any may be NULL) per-attribute min, max and mean. */
+int topk_partition_info(topk_table_t h, uint32_t *num_parts, uint32_t *part_rows, float *mins, float *maxs,
+                        float *means);
+
+/* Exact top-k like topk_query, scanning only the partitions whose bound
+ * sum_m weights[attr[m]] * (weight >= 0 ? max : min) can reach the threshold
+ * (the stop rule of VTA/PTA::findTopK*, cpu/VTA.h:210-216, cpu/PTA.h:337-340).
+ * cut: a predicted lower bound of the k-th score (e.g. from the learned model),
+ * or NaN for none.  With a cut, one scan of the partitions reaching it; the
+ * answer is accepted only if at least min(k, n) objects score >= cut, else the
+ * plain two-round pruned method runs.  Results identical to topk_query.
+ * stats (may be NULL): [0] partitions scanned, [1] partitions, [2] 1 if the cut
+ * was accepted, [3] scans launched. */
+int topk_query_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
+                      uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats);
+
 /* Verification entry (no reference counterpart): copy the full rows of `count`
  * objects to host memory, out[j*d + m] = attribute m of object ids[j]. */
 int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out);

@@ -1,0 +1,121 @@
+"""GPU: the partitioned copy and pruned exact queries against the oracle.
+
+The reference prunes with per-block bounds and stops once the k-th score reaches
+the bound of the rest (cpu/VTA.h:210-216, cpu/PTA.h:337-340); here whole
+partitions are skipped by the same rule.  Results must equal the plain exact
+top-k bit for bit, with or without a predicted cut.
+"""
+import numpy as np
+import pytest
+
+import topk_b200 as T
+from oracle import oracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def part_table(n, d, dist, seed, rows):
+    t = T.Table(n, d)
+    t.generate(dist, seed)
+    t.normalize()
+    t.build_partitions(rows)
+    return t
+
+
+def test_partition_stats_cover_the_table():
+    n, d = 300001, 8
+    with part_table(n, d, 2, 3, 4096) as t:
+        tn = t.download()
+        R, mins, maxs, means = t.partition_info()
+        assert R == 4096 and mins.shape == ((n + R - 1) // R, d)
+        assert np.all(mins <= means) and np.all(means <= maxs)
+        # every row lies in exactly one partition: extremes and sums agree with the table
+        assert np.array_equal(mins.min(axis=0), tn.min(axis=1))
+        assert np.array_equal(maxs.max(axis=0), tn.max(axis=1))
+        counts = np.full(len(means), R, np.float64)
+        counts[-1] = n - R * (len(means) - 1)
+        sums = (means.astype(np.float64) * counts[:, None]).sum(axis=0)
+        assert np.allclose(sums, tn.astype(np.float64).sum(axis=1), rtol=1e-5)
+
+
+@pytest.mark.parametrize("dist", [2, 1, 0, 3])
+def test_pruned_matches_oracle(dist):
+    n, d = (1 << 20) + 333, 8
+    rng = np.random.default_rng(dist)
+    with part_table(n, d, dist, 7, 8192) as t:
+        tn = t.download()
+        scanned = []
+        for j in range(24):
+            w, a = H.random_query(rng, d)
+            k = int(rng.choice([1, 16, 100, 1024, 4096]))
+            ids, sc, th, st = t.query_pruned(k, w, a)
+            H.assert_same_result((ids, sc, th), O.topk_numpy(tn, k, w, a))
+            assert st[1] == (n + 8191) // 8192 and st[2] == 0
+            scanned.append(st[0] / st[1])
+        print(f"dist {dist}: mean fraction of partitions scanned {np.mean(scanned):.3f}")
+        if dist == 2:  # the Morton order localises anticorrelated data: most partitions are skipped
+            assert np.mean(scanned) < 0.6
+
+
+def test_pruned_with_cut_accepts_or_falls_back_exactly():
+    n, d = 400000, 8
+    rng = np.random.default_rng(9)
+    with part_table(n, d, 2, 1, 4096) as t:
+        tn = t.download()
+        for j in range(12):
+            w, a = H.random_query(rng, d)
+            k = int(rng.integers(1, 1025))
+            want = O.topk_numpy(tn, k, w, a)
+            kth = float(want[2])
+            # a cut at or below the k-th score is accepted: one scan, fewer partitions
+            ids, sc, th, st = t.query_pruned(k, w, a, cut=np.nextafter(np.float32(kth), np.float32(-np.inf)))
+            H.assert_same_result((ids, sc, th), want)
+            assert st[2] == 1 and st[3] == 1
+            ids, sc, th, st = t.query_pruned(k, w, a, cut=kth)  # exactly the k-th: still enough objects
+            H.assert_same_result((ids, sc, th), want)
+            assert st[2] == 1
+            # a cut above the k-th score leaves fewer than k objects: the plain method answers
+            ids, sc, th, st = t.query_pruned(k, w, a, cut=kth + 0.05)
+            H.assert_same_result((ids, sc, th), want)
+            assert st[2] == 0
+
+
+def test_pruned_negative_weights_ties_and_small_tables():
+    rng = np.random.default_rng(4)
+    n, d = 150000, 6
+    raw = (np.floor(O.generate(n, d, 2, 5) * 8) / 8).astype(np.float32)  # coarse: many ties
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.build_partitions(2048)
+        for j in range(16):
+            w = rng.uniform(-1, 1, size=d).astype(np.float32)
+            q = int(rng.integers(1, 7))
+            a = rng.integers(0, d, size=q).astype(np.uint8)  # repeats allowed
+            k = int(rng.integers(1, 3000))
+            ids, sc, th, st = t.query_pruned(k, w, a)
+            H.assert_same_result((ids, sc, th), O.topk(tn, k, w, a))
+    for n in (1, 1000, 1025, 5000):
+        with part_table(n, 3, 1, n, 1024) as t:
+            tn = t.download()
+            w, a = H.random_query(rng, 3)
+            for k in (1, 7, min(n + 5, T.MAX_K)):
+                ids, sc, th, st = t.query_pruned(k, w, a)
+                H.assert_same_result((ids, sc, th), O.topk_numpy(tn, k, w, a))
+
+
+def test_pruned_needs_current_partitions():
+    with T.Table(5000, 4) as t:
+        t.generate(1, 1)
+        with pytest.raises(T.TopKError):
+            t.query_pruned(5, np.ones(4, np.float32), np.array([0, 1], np.uint8))
+        t.build_partitions(1024)
+        t.query_pruned(5, np.ones(4, np.float32), np.array([0, 1], np.uint8))
+        t.normalize()  # the table changed: the partitions are stale
+        with pytest.raises(T.TopKError):
+            t.query_pruned(5, np.ones(4, np.float32), np.array([0, 1], np.uint8))
+        with pytest.raises(T.TopKError):
+            t.build_partitions(1000)  # not a power of two

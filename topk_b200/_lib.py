@@ -60,6 +60,11 @@ SIGNATURES = [
                                     C.c_void_p]),
     ("topk_query_batch", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _u64p, _f32p,
                                    C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("topk_build_partitions", C.c_int, [_H, C.c_uint32]),
+    ("topk_partition_info", C.c_int, [_H, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
+    ("topk_query_pruned", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_float, _u64p, _f32p,
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_float), _u64p]),
     ("topk_gather_rows", C.c_int, [_H, _u64p, C.c_uint64, _f32p]),
     ("topk_count_ge", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_float,
                                 C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

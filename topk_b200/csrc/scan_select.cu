@@ -156,7 +156,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     ctl->count = 0;
     ctl->cur = 0;
     ctl->thr_local = 0;
-    ctl->thr_g = ld_volatile_u32(&p.scratch->g_thr);
+    if (p.thr_seed) atomicMax(&p.scratch->g_thr, p.thr_seed);  // every later read includes it
+    ctl->thr_g = max(ld_volatile_u32(&p.scratch->g_thr), p.thr_seed);
     ctl->reductions = 0;
   }
   bsync();
@@ -172,8 +173,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   }
 
   uint32_t g_pending = 0;  // thread 0's in-flight copy of the global threshold
+  // partition mode: the partition of the next tile is loaded one tile ahead
+  const uint32_t pmask = (1u << p.part_shift) - 1u;
+  uint32_t part_next = (p.part_list && my_tiles) ? __ldg(p.part_list + (blockIdx.x >> p.part_shift)) : 0u;
   for (uint32_t i = 0; i < my_tiles; ++i) {
-    const uint64_t tile0 = p.tile_begin + (blockIdx.x + (uint64_t)i * gridDim.x) * kTile;
+    const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
+    uint64_t tile0;
+    if (p.part_list) {
+      tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
+      if (i + 1 < my_tiles) part_next = __ldg(p.part_list + ((tix + gridDim.x) >> p.part_shift));
+    } else {
+      tile0 = p.tile_begin + tix * kTile;
+    }
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
     const uint32_t thr = max(ctl->thr_local, ctl->thr_g);
@@ -214,7 +225,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
       for (int v = 0; v < 4; ++v)
         if (pass_mask & (1u << v)) {
           if (TOPK_CHECK(base < cap, kDiagAppend, i, base, cap))
-            cand[base] = make_uint2(f2key(sv[v]), (uint32_t)(row0 + v));
+            cand[base] = make_uint2(f2key(sv[v]), p.row_ids ? __ldg(p.row_ids + row0 + v) : (uint32_t)(row0 + v));
           ++base;
         }
     }

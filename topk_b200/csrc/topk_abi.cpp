@@ -94,6 +94,8 @@ struct Ctx {
   uint64_t *d_ids_scratch = nullptr;  // gather ids
   float *d_rows = nullptr;
   size_t rows_cap = 0;
+  uint32_t *d_plist = nullptr;  // partition list of a pruned scan
+  size_t plist_cap = 0;
   bool busy = false;
 };
 
@@ -132,6 +134,14 @@ struct topk_table_s {
   uint64_t data_version = 1, xbf_version = 0;
   std::vector<float> absmax;
   bool xbf_usable = false;
+  // partitioned copy for pruned queries (topk_build_partitions): rows reordered,
+  // original ids, per-partition [P][d] min / max / mean (device and host copies)
+  float *ptable = nullptr;
+  uint32_t *pids = nullptr;
+  float *pstats = nullptr;
+  uint32_t part_log2 = 0, num_parts = 0;
+  uint64_t part_version = 0;
+  std::vector<float> pmin, pmax, pmean;
   cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
   double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0;
@@ -190,6 +200,7 @@ void ctx_free(Ctx *c) {
   cudaFree(c->d_count2);
   cudaFree(c->d_ids_scratch);
   cudaFree(c->d_rows);
+  cudaFree(c->d_plist);
   if (c->h_res) cudaFreeHost(c->h_res);
   delete c;
 }
@@ -242,11 +253,19 @@ int check_query(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, c
   return TOPK_OK;
 }
 
-// Enqueue one fused scan over rows [r0, r1) writing into the given outputs.
+// A scan over a list of partitions of the partitioned copy, with a threshold seed.
+struct PartScan {
+  const uint32_t *d_list;  // partition numbers (device)
+  uint32_t count;
+  uint32_t seed;           // objects need key >= seed (0: none)
+};
+
+// Enqueue one fused scan over rows [r0, r1) (or over the partitions of `ps`)
+// writing into the given outputs.
 int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint64_t r1, uint64_t k, uint32_t qq,
                  const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_thr,
-                 uint32_t *d_count, uint32_t *d_stats = nullptr) {
-  const uint64_t rows = r1 - r0;
+                 uint32_t *d_count, uint32_t *d_stats = nullptr, const PartScan *ps = nullptr) {
+  const uint64_t rows = ps ? ((uint64_t)ps->count << h->part_log2) : r1 - r0;
   ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin, h->max_ctas_per_sm);
   if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)k);
   // keep the merge tree's slot entries (< (2 * grid + levels) * k) within the context budget
@@ -261,7 +280,25 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   p.tile_begin = r0 & ~3ull;
   p.tile_end = (r1 + 3) & ~3ull;
   const uint64_t span = p.tile_end - p.tile_begin;
-  const uint64_t tiles = (span + pl.tile - 1) / pl.tile;
+  uint64_t tiles = (span + pl.tile - 1) / pl.tile;
+  if (ps) {  // tiles of the listed partitions of the reordered copy, original ids
+    uint32_t tile_log2 = 0;
+    while ((1u << tile_log2) < pl.tile) ++tile_log2;
+    if ((1u << tile_log2) != pl.tile || h->part_log2 < tile_log2)
+      return fail(TOPK_ERR_STATE, "partition rows 2^%u below the scan tile %u", h->part_log2, pl.tile);
+    p.table = h->ptable;
+    p.row_begin = 0;
+    p.row_end = h->n;
+    p.tile_begin = 0;
+    p.tile_end = (h->n + 3) & ~3ull;
+    p.part_list = ps->d_list;
+    p.part_shift = h->part_log2 - tile_log2;
+    p.part_rows_log2 = h->part_log2;
+    p.row_ids = h->pids;
+    p.thr_seed = ps->seed;
+    tiles = (uint64_t)ps->count << p.part_shift;
+    if (tiles > 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "too many tiles");
+  }
   p.num_tiles = (uint32_t)tiles;
   if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;
   p.qq = qq;
@@ -340,6 +377,187 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
   if (threshold) *threshold = hh->threshold;
   g_last_cands = hh->stats[0];
   g_last_reductions = hh->stats[1];
+  return TOPK_OK;
+}
+
+// ---------------------------------------------------------------- pruned queries
+uint32_t host_f2key(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if (f != f) return 0u;
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// A result as (key, id) pairs.
+struct HostResult {
+  std::vector<uint32_t> key;
+  std::vector<uint64_t> id;
+  std::vector<float> score;
+  float threshold = 0.0f;
+};
+
+// One fused scan over a list of partitions with a threshold seed; synchronous.
+// Fewer than min(k, n) results means fewer objects reached the seed.
+int scan_partitions(topk_table_t h, Ctx *c, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
+                    const std::vector<uint32_t> &list, uint32_t seed, HostResult *out) {
+  out->key.clear();
+  out->id.clear();
+  out->score.clear();
+  if (list.empty()) return TOPK_OK;
+  if (c->plist_cap < list.size()) {
+    cudaFree(c->d_plist);
+    c->d_plist = nullptr;
+    c->plist_cap = 0;
+    CK(cudaMalloc(&c->d_plist, h->num_parts * sizeof(uint32_t)));
+    c->plist_cap = h->num_parts;
+  }
+  const uint64_t kk = std::min<uint64_t>(k, h->n);
+  unsigned char *dr = c->d_res;
+  ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
+  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
+  float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
+  CK(cudaMemcpyAsync(c->d_plist, list.data(), list.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), c->stream));
+  PartScan ps{c->d_plist, (uint32_t)list.size(), seed};
+  int st = enqueue_scan(h, c, c->stream, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+                        dh->stats, &ps);
+  if (st != TOPK_OK) return st;
+  CK(cudaMemcpyAsync(c->h_res, dr, kHdr + kk * 12, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
+  if (hh->count > kk) {
+    ScanScratch sc{};
+    cudaMemcpy(&sc, c->scratch, sizeof(sc), cudaMemcpyDeviceToHost);
+    cudaMemset(c->scratch, 0, c->meta_bytes);
+    if (sc.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
+    return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
+  }
+  const uint32_t cnt = hh->count;
+  out->id.assign(reinterpret_cast<const uint64_t *>(c->h_res + kHdr), reinterpret_cast<const uint64_t *>(c->h_res + kHdr) + cnt);
+  const float *sc = reinterpret_cast<const float *>(c->h_res + kHdr + kk * 8);
+  out->score.assign(sc, sc + cnt);
+  for (uint32_t j = 0; j < cnt; j++) out->key.push_back(host_f2key(sc[j]));
+  out->threshold = hh->threshold;
+  return TOPK_OK;
+}
+
+// Upper bound of every reference-order FP32 score in partition p: the bound in
+// double over the partition's extremes, plus the FP32 rounding of qq products and
+// qq additions (each within 2^-24 relative of the running magnitude), rounded up.
+float partition_bound(topk_table_t h, uint32_t p, uint32_t qq, const float *weights, const uint8_t *attr) {
+  double ub = 0.0, mag = 0.0;
+  for (uint32_t m = 0; m < qq; m++) {
+    const double w = weights[attr[m]];
+    const size_t o = (size_t)p * h->d + attr[m];
+    const double x = w >= 0.0 ? h->pmax[o] : h->pmin[o];
+    ub += w * x;
+    mag += std::fabs(w * x);
+  }
+  const double b = ub + mag * std::ldexp((double)(2 * qq + 2), -24) + 1e-37;
+  if (!(b == b) || b > 3.0e38) return INFINITY;
+  float f = (float)b;
+  if ((double)f < b) f = std::nextafter(f, INFINITY);
+  return f;
+}
+
+// Exact top-k over the partitioned copy, scanning only partitions whose bound can
+// reach the threshold.  With a finite `cut` (a predicted lower bound of the k-th
+// score): one scan of the partitions with bound >= cut, seeded with cut, accepted
+// when it returns min(k, n) objects (then every object of the true top-k scored
+// >= cut and was scanned); otherwise, and without a cut, two rounds: the
+// highest-bound partitions give an exact k-th score t1 of a subset (a lower bound
+// of the true k-th), then the other partitions with bound >= t1, seeded with t1;
+// the union's top-k is the answer.  stats: partitions scanned, partitions,
+// cut accepted (1/0), scans.
+int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
+               uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats) {
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (!h->ptable || h->part_version != h->data_version)
+    return fail(TOPK_ERR_STATE, "no partitions for the current table: call topk_build_partitions");
+  const uint64_t kk = std::min<uint64_t>(k, h->n);
+  if (!ids || !scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  CtxLease lease(h);
+  if (lease.status != TOPK_OK) return lease.status;
+  Ctx *c = lease.c;
+  const uint32_t P = h->num_parts;
+  std::vector<float> ub(P);
+  for (uint32_t p = 0; p < P; p++) ub[p] = partition_bound(h, p, qq, weights, attr);
+  uint64_t scanned = 0, scans = 0, accepted = 0;
+  HostResult res;
+  bool done = false;
+  if (std::isfinite(cut)) {
+    std::vector<uint32_t> list;
+    for (uint32_t p = 0; p < P; p++)
+      if (ub[p] >= cut) list.push_back(p);
+    if ((st = scan_partitions(h, c, k, qq, weights, attr, list, host_f2key(cut), &res)) != TOPK_OK) return st;
+    scanned += list.size();
+    scans++;
+    if (res.id.size() == kk) {
+      done = true;
+      accepted = 1;
+    }
+  }
+  if (!done) {
+    std::vector<uint32_t> order(P);
+    for (uint32_t p = 0; p < P; p++) order[p] = p;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return ub[a] > ub[b]; });
+    // round 1: enough highest-bound partitions for k objects, and at least 1/32 of them
+    const uint64_t R = 1ull << h->part_log2;
+    uint32_t m1 = (uint32_t)std::min<uint64_t>(P, std::max<uint64_t>((kk + R - 1) / R + 1, (P + 31) / 32));
+    std::vector<uint32_t> l1(order.begin(), order.begin() + m1);
+    HostResult r1;
+    if ((st = scan_partitions(h, c, k, qq, weights, attr, l1, 0u, &r1)) != TOPK_OK) return st;
+    scanned += m1;
+    scans++;
+    if (r1.id.size() < kk) {  // the first round held fewer than k rows: scan everything else too
+      std::vector<uint32_t> rest(order.begin() + m1, order.end());
+      HostResult r2;
+      if ((st = scan_partitions(h, c, k, qq, weights, attr, rest, 0u, &r2)) != TOPK_OK) return st;
+      scanned += rest.size();
+      scans++;
+      res = r1;
+      res.key.insert(res.key.end(), r2.key.begin(), r2.key.end());
+      res.id.insert(res.id.end(), r2.id.begin(), r2.id.end());
+      res.score.insert(res.score.end(), r2.score.begin(), r2.score.end());
+    } else {
+      // k-th key of the first round; compared as keys, so a NaN k-th score (key 0,
+      // below every number) keeps every partition
+      const uint32_t t1 = host_f2key(r1.threshold);
+      std::vector<uint32_t> l2;
+      for (uint32_t j = m1; j < P; j++)
+        if (host_f2key(ub[order[j]]) >= t1) l2.push_back(order[j]);
+      HostResult r2;
+      if ((st = scan_partitions(h, c, k, qq, weights, attr, l2, t1, &r2)) != TOPK_OK) return st;
+      scanned += l2.size();
+      scans += l2.empty() ? 0 : 1;
+      res = r1;
+      res.key.insert(res.key.end(), r2.key.begin(), r2.key.end());
+      res.id.insert(res.id.end(), r2.id.begin(), r2.id.end());
+      res.score.insert(res.score.end(), r2.score.begin(), r2.score.end());
+    }
+  }
+  // top kk of the union by (key desc, id asc), written ascending like topk_query
+  std::vector<uint32_t> idx(res.id.size());
+  for (uint32_t j = 0; j < idx.size(); j++) idx[j] = j;
+  std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+    return res.key[a] != res.key[b] ? res.key[a] > res.key[b] : res.id[a] < res.id[b];
+  });
+  const uint64_t cnt = std::min<uint64_t>(kk, idx.size());
+  for (uint64_t r = 0; r < cnt; r++) {
+    ids[cnt - 1 - r] = res.id[idx[r]];
+    scores[cnt - 1 - r] = res.score[idx[r]];
+  }
+  if (count) *count = cnt;
+  if (threshold) *threshold = cnt ? res.score[idx[cnt - 1]] : 0.0f;
+  if (stats) {
+    stats[0] = scanned;
+    stats[1] = P;
+    stats[2] = accepted;
+    stats[3] = scans;
+  }
   return TOPK_OK;
 }
 
@@ -647,6 +865,9 @@ int topk_destroy(topk_table_t h) {
   for (Ctx *c : h->ctxs) ctx_free(c);
   ctx_free(h->primary);
   free_batch_buffers(h);
+  cudaFree(h->ptable);
+  cudaFree(h->pids);
+  cudaFree(h->pstats);
   cudaFree(h->table);
   cudaFree(h->d_minmax);
   cudaFree(h->d_norm);
@@ -822,6 +1043,104 @@ int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio) {
   if (method) *method = h->last_batch_method;
   if (max_err_ratio) *max_err_ratio = h->last_batch_err_ratio;
   return TOPK_OK;
+}
+
+int topk_build_partitions(topk_table_t h, uint32_t part_rows) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  if (part_rows < 1024 || part_rows > (1u << 24) || (part_rows & (part_rows - 1)))
+    return fail(TOPK_ERR_ARG, "part_rows must be a power of two in [1024, 2^24]");
+  uint32_t lg = 0;
+  while ((1u << lg) < part_rows) ++lg;
+  const uint64_t P = (h->n + part_rows - 1) / part_rows;
+  if (P > (1u << 22)) return fail(TOPK_ERR_UNSUPPORTED, "more than 2^22 partitions");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  cudaStream_t s = h->primary->stream;
+  // column extremes: the Morton code quantises each attribute over [min, max]
+  CK(launch_minmax(h->table, h->ld, h->d, h->n, h->d_minmax, s));
+  std::vector<uint32_t> w((size_t)h->d * kMinmaxWords);
+  CK(cudaMemcpyAsync(w.data(), h->d_minmax, w.size() * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint32_t dims = std::min<uint32_t>(h->d, 16u);
+  const uint32_t bits = std::max<uint32_t>(1u, 16u / dims);
+  std::vector<float> lo_scale(2 * (size_t)h->d, 0.0f);
+  for (uint32_t m = 0; m < h->d; m++) {
+    auto k2f = [](uint32_t k) {
+      uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+      float f;
+      std::memcpy(&f, &u, 4);
+      return f;
+    };
+    const float mx = k2f(w[(size_t)m * kMinmaxWords]), mn = k2f(w[(size_t)m * kMinmaxWords + 1]);
+    const double range = (double)mx - (double)mn;
+    lo_scale[m] = std::isfinite(mn) ? mn : 0.0f;
+    lo_scale[h->d + m] = (range > 0 && std::isfinite(range)) ? (float)(std::ldexp(1.0, (int)bits) / range) : 0.0f;
+  }
+  // release an older copy first (its memory may be needed)
+  cudaFree(h->ptable);
+  cudaFree(h->pids);
+  cudaFree(h->pstats);
+  h->ptable = nullptr;
+  h->pids = nullptr;
+  h->pstats = nullptr;
+  h->num_parts = 0;
+  uint16_t *keys = nullptr;
+  uint32_t *hist = nullptr;
+  float *dls = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(keys);
+    cudaFree(hist);
+    cudaFree(dls);
+  };
+  cudaError_t e = cudaMalloc(&keys, h->n * sizeof(uint16_t));
+  if (e == cudaSuccess) e = cudaMalloc(&hist, (1u << 16) * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&dls, lo_scale.size() * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&h->pids, h->n * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&h->ptable, h->ld * h->d * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&h->pstats, 3 * P * h->d * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ptable, 0, h->ld * h->d * sizeof(float), s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dls, lo_scale.data(), lo_scale.size() * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = launch_partition_build(h->table, h->ld, h->d, h->n, dls, dls + h->d, bits, keys, hist, h->pids, h->ptable,
+                               h->num_sms, s);
+  float *pmin = h->pstats, *pmax = h->pstats + P * h->d, *pmean = h->pstats + 2 * P * h->d;
+  if (e == cudaSuccess) e = launch_partition_stats(h->ptable, h->ld, h->d, h->n, lg, (uint32_t)P, pmin, pmax, pmean, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cleanup();
+  if (e != cudaSuccess) return cuda_fail(e, "topk_build_partitions");
+  h->pmin.resize(P * h->d);
+  h->pmax.resize(P * h->d);
+  h->pmean.resize(P * h->d);
+  CK(cudaMemcpy(h->pmin.data(), pmin, P * h->d * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h->pmax.data(), pmax, P * h->d * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h->pmean.data(), pmean, P * h->d * 4, cudaMemcpyDeviceToHost));
+  h->part_log2 = lg;
+  h->num_parts = (uint32_t)P;
+  h->part_version = h->data_version;
+  return TOPK_OK;
+}
+
+int topk_partition_info(topk_table_t h, uint32_t *num_parts, uint32_t *part_rows, float *mins, float *maxs,
+                        float *means) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->ptable || h->part_version != h->data_version)
+    return fail(TOPK_ERR_STATE, "no partitions for the current table: call topk_build_partitions");
+  const size_t cnt = (size_t)h->num_parts * h->d;
+  if (num_parts) *num_parts = h->num_parts;
+  if (part_rows) *part_rows = 1u << h->part_log2;
+  if (mins) std::memcpy(mins, h->pmin.data(), cnt * 4);
+  if (maxs) std::memcpy(maxs, h->pmax.data(), cnt * 4);
+  if (means) std::memcpy(means, h->pmean.data(), cnt * 4);
+  return TOPK_OK;
+}
+
+int topk_query_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
+                      uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  return run_pruned(h, k, qq, weights, attr, cut, ids, scores, count, threshold, stats);
 }
 
 int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out) {

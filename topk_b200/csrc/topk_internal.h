@@ -67,6 +67,14 @@ struct ScanParams {
   float *out_threshold; // may be null
   uint32_t *out_count;  // may be null
   uint32_t *out_stats;  // may be null: [0] entries merged at the root, [1] block-selects
+  // Partition mode (part_list != null): tile t covers rows
+  //   part_list[t >> part_shift] << part_rows_log2  +  (t & ((1 << part_shift) - 1)) * tile
+  // instead of tile_begin + t * tile; rows stay within [row_begin, row_end).
+  const uint32_t *part_list;
+  uint32_t part_shift;      // log2(tiles per partition)
+  uint32_t part_rows_log2;  // log2(rows per partition)
+  const uint32_t *row_ids;  // may be null: id of each row (a reordered table's original ids)
+  uint32_t thr_seed;        // objects need key >= thr_seed from the start (0: none)
   uint8_t attr[kMaxQ];
   float w[kMaxQ];       // weights[attr[m]], gathered on the host
 };
@@ -114,5 +122,15 @@ cudaError_t launch_count(const float *table, uint64_t ld, uint64_t r0, uint64_t 
 // Gather full rows for a list of ids: out[j*d + m] = table[m*ld + ids[j]].
 cudaError_t launch_gather(const float *table, uint64_t ld, uint32_t d, const uint64_t *ids, uint64_t cnt,
                           float *out, cudaStream_t stream);
+
+// Partitioned copy (partition.cu): Morton-ordered counting sort of the rows into
+// ptable (same stride), perm[row] = original id.  lo/scale: per attribute (device),
+// scale = 2^bits / (max - min).  keys: n entries; hist: 2^16 entries.
+cudaError_t launch_partition_build(const float *table, uint64_t ld, uint32_t d, uint64_t n, const float *lo,
+                                   const float *scale, uint32_t bits, uint16_t *keys, uint32_t *hist,
+                                   uint32_t *perm, float *ptable, int num_sms, cudaStream_t s);
+// Per-partition min / max / mean of each attribute, [num_parts][d] each.
+cudaError_t launch_partition_stats(const float *ptable, uint64_t ld, uint32_t d, uint64_t n, uint32_t rows_log2,
+                                   uint32_t num_parts, float *mins, float *maxs, float *means, cudaStream_t s);
 
 }  // namespace topk

@@ -104,6 +104,37 @@ class Table:
                                  ids.reshape(-1), sc.reshape(-1), kstride, counts.ctypes.data, ths.ctypes.data))
         return ids, sc, counts, ths
 
+    # -- partitions and pruned queries -------------------------------------
+    def build_partitions(self, part_rows=1 << 16):
+        check(_lib.load().topk_build_partitions(self._h, int(part_rows)))
+
+    def partition_info(self):
+        """(part_rows, mins, maxs, means) with arrays of shape (num_parts, d)."""
+        L = _lib.load()
+        P, R = C.c_uint32(), C.c_uint32()
+        check(L.topk_partition_info(self._h, C.byref(P), C.byref(R), None, None, None))
+        mins = np.empty((P.value, self.d), np.float32)
+        maxs = np.empty_like(mins)
+        means = np.empty_like(mins)
+        check(L.topk_partition_info(self._h, None, None, mins.ctypes.data, maxs.ctypes.data, means.ctypes.data))
+        return R.value, mins, maxs, means
+
+    def query_pruned(self, k, weights, attr, cut=float("nan")):
+        """Exact top-k scanning only partitions that can reach the threshold;
+        returns (ids, scores, threshold, stats) with stats = (partitions scanned,
+        partitions, cut accepted, scans)."""
+        w, a = _weights(weights, self.d), _attr(attr)
+        cap = max(1, min(int(k), self.n))
+        ids = np.empty(cap, np.uint64)
+        sc = np.empty(cap, np.float32)
+        st = np.zeros(4, np.uint64)
+        cnt = C.c_uint64()
+        th = C.c_float()
+        check(_lib.load().topk_query_pruned(self._h, int(k), len(a), w, a, float(cut), ids, sc, C.byref(cnt),
+                                            C.byref(th), st))
+        c = cnt.value
+        return ids[:c], sc[:c], th.value, tuple(int(x) for x in st)
+
     def count_ge(self, weights, attr, thr, row_begin=0, row_end=None):
         w, a = _weights(weights, self.d), _attr(attr)
         r1 = self.n if row_end is None else int(row_end)

@@ -168,6 +168,67 @@ int topk_partition_info(topk_table_t h, uint32_t *num_parts, uint32_t *part_rows
 int topk_query_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
                       uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats);
 
+/* ---- Learned k-th-score model (no reference counterpart) ------------------------
+ * An MLP in_dim -> 64 -> 64 -> 1 (ReLU, FP32) predicting u = qq * ln(gap / S) of a
+ * query, gap = (largest partition bound) - (k-th score), S = sum_m
+ * |weights[attr[m]]|, from in_dim = 2d + 18 features: the query's weight per
+ * attribute / S, ln of those (0 where not queried), log2(k) / 10, qq / 16, the 1st,
+ * 2nd, 4th .. 128th largest partition bound / S and the same ranks of the partition
+ * mean scores / S (needs d <= 23).  The cut of a prediction
+ * is largest bound - S * exp((u + margin) / qq).  Parameters are one FP32 array:
+ * W1[64][in_dim] b1[64] W2[64][64] b2[64] w3[64] b3.  Training and inference run
+ * in this library's own kernels.  The cut is only a starting threshold: the
+ * pruned and batched queries accept it when enough objects reach it, so results
+ * never depend on the model. */
+#define TOPK_MLP_HIDDEN 64u
+#define TOPK_MLP_MAX_IN 64u
+
+/* Number of parameters of the model for in_dim inputs. */
+uint64_t topk_mlp_param_count(uint32_t in_dim);
+
+/* Mean squared error over one batch (<= 128 samples, X row-major batch x in_dim)
+ * and its gradient with respect to every parameter, computed on CUDA device
+ * `device`; no update.  For checking the training kernels against a reference. */
+int topk_mlp_grad(int device, uint32_t in_dim, const float *params, const float *X, const float *y, uint32_t batch,
+                  float *grad, float *loss);
+
+/* Predictions for n samples. */
+int topk_mlp_predict(int device, uint32_t in_dim, const float *params, const float *X, uint64_t n, float *out);
+
+/* Train in place with Adam (lr, batch <= 128) for `epochs` passes over n samples
+ * in a seeded order; epoch_loss (may be NULL) receives each epoch's mean loss. */
+int topk_mlp_train(int device, uint32_t in_dim, float *params, const float *X, const float *y, uint64_t n,
+                   uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *epoch_loss);
+
+/* Features of nq queries (layout of topk_query_batch's arguments) from the current
+ * partitions: X receives nq rows of 2d + 18 values; scale (may be NULL) receives S. */
+int topk_query_features(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+                        uint64_t wstride, const uint8_t *attrs, uint64_t astride, float *X, float *scale);
+
+/* Install (params != NULL) or remove the handle's model and its margin (in units
+ * of u, see above). */
+int topk_set_learned_model(topk_table_t h, const float *params, float margin);
+
+/* Copy the handle's model out (params may be NULL). */
+int topk_get_learned_model(topk_table_t h, float *params, float *margin);
+
+/* Fit the handle's model: n_train + n_val random queries (attribute subsets of
+ * size U{qmin..qmax}, weights U(0,1], k log-uniform in [kmin, kmax], seeded),
+ * labelled with their exact k-th scores by topk_query_batch, features on the
+ * device, `epochs` of Adam on the device, then the margin = the (1 - miss_rate)
+ * quantile of (target - prediction) over the n_val held-out queries.
+ * report (may be NULL, 6 values): last epoch's loss, held-out RMSE, margin,
+ * held-out miss rate at that margin, labelling seconds, training seconds. */
+int topk_learned_fit(topk_table_t h, uint64_t n_train, uint64_t n_val, uint32_t kmin, uint32_t kmax, uint32_t qmin,
+                     uint32_t qmax, uint32_t epochs, float miss_rate, uint64_t seed, double *report);
+
+/* Exact top-k through the model: features and the MLP forward in one kernel give
+ * the cut, then topk_query_pruned(cut).  Same results as
+ * topk_query; stats as topk_query_pruned; cut_out (may be NULL) receives the cut. */
+int topk_query_learned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
+                       uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats,
+                       float *cut_out);
+
 /* Verification entry (no reference counterpart): copy the full rows of `count`
  * objects to host memory, out[j*d + m] = attribute m of object ids[j]. */
 int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out);
@@ -190,13 +251,21 @@ int topk_set_scan_tuning(topk_table_t h, uint32_t max_ctas_per_sm);
 int topk_set_fault_injection(topk_table_t h, int mode);
 
 /* Methods of topk_query_batch (no reference counterpart; results are identical). */
-#define TOPK_BATCH_AUTO 0  /* TOPK_BATCH_BF16 where it applies, else TOPK_BATCH_FP32 */
+#define TOPK_BATCH_AUTO 0  /* TOPK_BATCH_LEARNED with a fitted model, else TOPK_BATCH_BF16
+                            * where it applies, else TOPK_BATCH_FP32 */
 #define TOPK_BATCH_LOOP 1  /* one fused single-query scan per query */
 #define TOPK_BATCH_FP32 2  /* batched plain FP32: each table tile scored for 64 queries */
 #define TOPK_BATCH_BF16 3  /* BF16 tensor-core filter (tcgen05) with a per-query error
                             * bound; candidates rescored exactly in FP32.  Applies to
                             * d <= 16 with finite table values and weights of magnitude
                             * <= 2^60; other batches run TOPK_BATCH_FP32 */
+#define TOPK_BATCH_LEARNED 4 /* TOPK_BATCH_BF16 (or FP32) whose per-query threshold starts
+                              * at the learned cut (prediction - margin) * S instead of a
+                              * bootstrap over the first rows; a query left with fewer
+                              * than k objects at or above its cut runs again without it.
+                              * Needs a model on the current partitions
+                              * (topk_learned_fit / topk_set_learned_model); without one
+                              * it runs as TOPK_BATCH_BF16 */
 
 /* Choose the method of topk_query_batch on this handle. */
 int topk_set_batch_method(topk_table_t h, int method);
@@ -207,10 +276,11 @@ int topk_set_batch_method(topk_table_t h, int method);
  * scorer over all chunks. */
 int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks, uint64_t *candidates);
 
-/* More about the last topk_query_batch: the method that ran (TOPK_BATCH_*), and for
- * TOPK_BATCH_BF16 the largest |filter score - exact score| / bound seen over the
- * rescored candidates (must stay below 1; 0 for the other methods). */
-int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio);
+/* More about the last topk_query_batch: the method that ran (TOPK_BATCH_*), for the
+ * BF16 filter the largest |filter score - exact score| / bound seen over the
+ * rescored candidates (must stay below 1; 0 for the other methods), and the
+ * queries whose learned start was too high (answered again without it). */
+int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uint64_t *learned_misses);
 
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */

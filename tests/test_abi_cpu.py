@@ -16,7 +16,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 def declared_symbols():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(topk_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|uint64_t|const char \*)\s*(topk_\w+)\s*\(", src, re.M)))
 
 
 def test_header_declares_expected_entries():

@@ -27,7 +27,7 @@ MAX_D = 255
 DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
 
 # topk_query_batch methods (TOPK_BATCH_* in include/topk_b200.h)
-BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16 = 0, 1, 2, 3
+BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16, BATCH_LEARNED = 0, 1, 2, 3, 4
 
 
 class TopKError(RuntimeError):
@@ -65,6 +65,19 @@ SIGNATURES = [
                                       C.c_void_p]),
     ("topk_query_pruned", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_float, _u64p, _f32p,
                                     C.POINTER(C.c_uint64), C.POINTER(C.c_float), _u64p]),
+    ("topk_mlp_param_count", C.c_uint64, [C.c_uint32]),
+    ("topk_mlp_grad", C.c_int, [C.c_int, C.c_uint32, _f32p, _f32p, _f32p, C.c_uint32, _f32p, C.POINTER(C.c_float)]),
+    ("topk_mlp_predict", C.c_int, [C.c_int, C.c_uint32, _f32p, _f32p, C.c_uint64, _f32p]),
+    ("topk_mlp_train", C.c_int, [C.c_int, C.c_uint32, _f32p, _f32p, _f32p, C.c_uint64, C.c_uint32, C.c_uint32,
+                                 C.c_float, C.c_uint64, C.c_void_p]),
+    ("topk_query_features", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _f32p,
+                                      C.c_void_p]),
+    ("topk_set_learned_model", C.c_int, [_H, C.c_void_p, C.c_float]),
+    ("topk_get_learned_model", C.c_int, [_H, C.c_void_p, C.POINTER(C.c_float)]),
+    ("topk_learned_fit", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                   C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
+    ("topk_query_learned", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, _u64p, _f32p, C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_float), _u64p, C.POINTER(C.c_float)]),
     ("topk_gather_rows", C.c_int, [_H, _u64p, C.c_uint64, _f32p]),
     ("topk_count_ge", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_float,
                                 C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
@@ -72,7 +85,7 @@ SIGNATURES = [
     ("topk_set_scan_tuning", C.c_int, [_H, C.c_uint32]),
     ("topk_set_batch_method", C.c_int, [_H, C.c_int]),
     ("topk_last_batch_stats", C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
-    ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("topk_query_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, _f32p,
                                      _u8p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("topk_last_stats", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
   }
   __syncthreads();
   const uint32_t qq = sh->qq, k = sh->k;
-  const uint32_t cnt = s.cnt;
+  const uint32_t cnt = min(s.cnt, k);
   const uint32_t thr = s.thr;
   const uint32_t nc_raw = s.ccount;
   const uint32_t nc = min(nc_raw, q.cand_cap);
@@ -229,14 +229,18 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
     ent[cnt + j] = e;
   }
   __syncthreads();
-  if (cnt == k) {
-    // best[] is a full top-k: new entries must reach thr (rescored filter
-    // candidates may not); merge the two sets
+  if (thr != 0u) {
+    // new entries must reach thr: the k-th key + 1 once best[] is full, or a
+    // predicted starting threshold (rescored filter candidates may not reach it)
     for (uint32_t j = cnt + t; j < total; j += kBT)
       if (ent[j].x < thr) ent[j] = make_uint2(0u, 0xFFFFFFFFu);  // below every real entry
     __syncthreads();
   }
-  const uint32_t kept = block_reduce<kBT>(ent, total, out, k, 0u, hist, &sh->sel);
+  // Entries replaced above carry key 0 and one id, so they share one composite; the
+  // select needs distinct composites at its k-th boundary.  Without a learned start
+  // best[] is full whenever they exist and they stay below it; with one, the seed
+  // (>= 1) as the minimum key leaves them out (and whatever lies below the start).
+  const uint32_t kept = block_reduce<kBT>(ent, total, out, k, s.seed, hist, &sh->sel);
   uint2 *dst = best + q.best_off;
   for (uint32_t j = t; j < kept; j += kBT) dst[j] = out[j];
   if (t == 0) {
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(kBT) batch_finish_kernel(const BatchQuery *__r
   extern __shared__ __align__(16) unsigned char smem[];
   uint2 *a = reinterpret_cast<uint2 *>(smem);
   const BatchQuery &q = qs[blockIdx.x];
-  const uint32_t cnt = st[blockIdx.x].cnt;
+  const uint32_t cnt = min(st[blockIdx.x].cnt, q.k);
   const int t = threadIdx.x;
   for (uint32_t j = t; j < cnt; j += kBT) a[j] = best[q.best_off + j];
   __syncthreads();

@@ -34,6 +34,8 @@ struct BatchState {
   uint32_t flags;   // bit 0: a candidate region overflowed (exact fallback needed)
   uint32_t cands;   // candidates appended over the whole batch (saturating)
   uint32_t errmax;  // BF16 filter: max |filter score - exact score| / err, FP32 bits
+  uint32_t seed;    // learned start: every kept entry needs key >= seed (0: none)
+  uint32_t pad;
 };
 
 size_t batch_bootstrap_smem(uint32_t rows, uint32_t kmax);
@@ -66,6 +68,32 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
                                const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint2 *log,
                                uint16_t *log_q, uint32_t log_cap, uint64_t wait_limit, uint32_t *err,
                                cudaStream_t s);
+// Learned k-th-score model (mlp.cu): in -> 64 -> 64 -> 1 ReLU MLP, features of
+// feature_dim(d) values per query from the partition statistics ([P][d] each).
+constexpr uint32_t kHid = 64;
+constexpr uint32_t kMlpMaxIn = 64;
+constexpr uint32_t kMaxFeatureParts = 16384;
+__host__ __device__ constexpr uint32_t feature_dim(uint32_t d) { return 2 * d + 18; }
+__host__ __device__ constexpr uint32_t feature_bound_col(uint32_t d) { return 2 * d + 2; }  // largest bound / S
+uint32_t mlp_param_count(uint32_t F);
+cudaError_t launch_mlp_grad(const float *params, const float *X, const float *y, uint32_t B, uint32_t F, float *grad,
+                            float *loss, cudaStream_t s);
+cudaError_t launch_mlp_train(float *params, float *m, float *v, const float *X, const float *y, uint64_t N, uint32_t F,
+                             uint32_t B, uint32_t epochs, const uint64_t *mul, const uint64_t *add, float lr,
+                             float *epoch_loss, cudaStream_t s);
+cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, uint32_t F, float *out, int num_sms,
+                               cudaStream_t s);
+cudaError_t launch_features(const float *pmin, const float *pmax, const float *pmean, uint32_t P, uint32_t d,
+                            const BatchQuery *qs, uint32_t nq, float *X, const float *params, float *pred,
+                            cudaStream_t s);
+// The learned cut: largest bound - S * exp((u + margin) / qq), u the model's output
+// (b1s: the largest partition bound / S, a feature).
+__host__ __device__ inline float learned_cut(float u, float b1s, float S, float qq, float margin) {
+  return (b1s - expf((u + margin) / qq)) * S;
+}
+// Start each query's state at its learned cut (pred: model outputs; X: features).
+cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
+                                BatchState *st, uint32_t nq, cudaStream_t s);
 cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
                                 uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
                                 uint32_t *out_count, float *out_thr, cudaStream_t s);

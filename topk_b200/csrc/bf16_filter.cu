@@ -109,6 +109,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// 1 if any of the 8 values reaches its cut (v[i] >= c[i]), or acc was already 1: one
+// predicate carried through the compares.
+__device__ __forceinline__ uint32_t any_ge8(uint32_t acc, const uint32_t *v, float4 c0, float4 c1) {
+  uint32_t r;
+  asm("{\n .reg .pred p;\n setp.ne.u32 p, %1, 0;\n"
+      " setp.ge.or.f32 p, %2, %10, p;\n setp.ge.or.f32 p, %3, %11, p;\n"
+      " setp.ge.or.f32 p, %4, %12, p;\n setp.ge.or.f32 p, %5, %13, p;\n"
+      " setp.ge.or.f32 p, %6, %14, p;\n setp.ge.or.f32 p, %7, %15, p;\n"
+      " setp.ge.or.f32 p, %8, %16, p;\n setp.ge.or.f32 p, %9, %17, p;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"(acc), "f"(__uint_as_float(v[0])), "f"(__uint_as_float(v[1])), "f"(__uint_as_float(v[2])),
+        "f"(__uint_as_float(v[3])), "f"(__uint_as_float(v[4])), "f"(__uint_as_float(v[5])),
+        "f"(__uint_as_float(v[6])), "f"(__uint_as_float(v[7])), "f"(c0.x), "f"(c0.y), "f"(c0.z), "f"(c0.w),
+        "f"(c1.x), "f"(c1.y), "f"(c1.z), "f"(c1.w));
+  return r;
+}
+
 // Bounded wait that also gives up once another role of the CTA has aborted.
 __device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, uint64_t limit, volatile uint32_t *abort_flag) {
   for (uint64_t it = 0; it < limit; ++it) {
@@ -271,75 +289,60 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         tc_fence_after();
         const uint32_t col0 = i * kQTile + part * 64u;  // CTA-relative query of chunk 0, column 0
         const uint32_t tcol = tmem + lane_addr + buf * kQTile + part * 64u;
-        // hot path: all 64 columns in one round trip, one compare per value
-        uint32_t hits;
+        // all 64 columns in one round trip; the accumulator is free as soon as they
+        // are in registers, and everything below works on the registers
+        uint32_t v[64];
+        tmem_ld32(tcol, v);
+        tmem_ld32(tcol + 32, v + 32);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce + buf);
+        // hot path: one compare per value against the column's cut, carried in a predicate
+        uint32_t h = 0;
         {
-          uint32_t v[64];
-          tmem_ld32(tcol, v);
-          tmem_ld32(tcol + 32, v + 32);
-          tmem_wait_ld();
           const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0);
-          uint32_t h = 0;
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const float4 x = c4[k];
-            const uint32_t a = (uint32_t)(__uint_as_float(v[4 * k]) >= x.x) |
-                               (uint32_t)(__uint_as_float(v[4 * k + 1]) >= x.y) |
-                               (uint32_t)(__uint_as_float(v[4 * k + 2]) >= x.z) |
-                               (uint32_t)(__uint_as_float(v[4 * k + 3]) >= x.w);
-            h |= a << (k >> 3);  // bit cc: chunk cc of 32 columns has a hit
+          for (int cc = 0; cc < 2; ++cc) {
+            uint32_t a = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a = any_ge8(a, v + cc * 32 + k * 8, c4[cc * 8 + 2 * k], c4[cc * 8 + 2 * k + 1]);
+            h |= a << cc;  // bit cc: chunk cc of 32 columns has a hit
           }
-          hits = __reduce_or_sync(0xFFFFFFFFu, valid ? h : 0u);
         }
-        if (hits == 0u) {  // common case: the accumulator is free right away
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(acce + buf);
-          continue;
-        }
-        // cold path: the chunks with a hit, read again (the accumulator is held until done)
+        const uint32_t hits = __reduce_or_sync(0xFFFFFFFFu, valid ? h : 0u);
+        if (hits == 0u) continue;  // common case
+        // cold path: per column of a chunk with a hit, a warp ballot gives the passing
+        // objects, appended with one shared atomic
 #pragma unroll 1
         for (uint32_t cc = 0; cc < 2; ++cc) {
           if (!(hits & (1u << cc))) continue;
-          uint32_t v[32];
-          tmem_ld32(tcol + cc * 32u, v);
-          tmem_wait_ld();
-          const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0 + cc * 32u);
-          float cut[32];
+          uint32_t u[32];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const float4 x = c4[k];
-            cut[4 * k] = x.x;
-            cut[4 * k + 1] = x.y;
-            cut[4 * k + 2] = x.z;
-            cut[4 * k + 3] = x.w;
-          }
-          {
+          for (int j = 0; j < 32; ++j) u[j] = cc ? v[32 + j] : v[j];
+          const float *cut = scut + col0 + cc * 32u;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const bool pass = valid && __uint_as_float(v[j]) >= cut[j];
-              const uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
-              if (b) {
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(log_n, __popc(b));
-                base = __shfl_sync(0xFFFFFFFFu, base, 0);
-                if (pass) {
-                  const uint32_t e = base + __popc(b & lt_mask);
-                  const uint32_t ql = col0 + cc * 32u + j;
-                  if (e < p.log_cap) {
-                    log[e] = make_uint2(f2key(__uint_as_float(v[j])), (uint32_t)obj);
-                    log_q[e] = (uint16_t)ql;
-                  } else {
-                    atomicOr(&p.st[q0 + ql].flags, 1u);  // lost: the exact scan answers it
-                  }
+          for (int j = 0; j < 32; ++j) {
+            const float x = __uint_as_float(u[j]);
+            const bool pass = valid && x >= cut[j];
+            const uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
+            if (b) {
+              uint32_t base = 0;
+              if (lane == 0) base = atomicAdd(log_n, __popc(b));
+              base = __shfl_sync(0xFFFFFFFFu, base, 0);
+              if (pass) {
+                const uint32_t e = base + __popc(b & lt_mask);
+                const uint32_t ql = col0 + cc * 32u + j;
+                if (e < p.log_cap) {
+                  log[e] = make_uint2(f2key(x), (uint32_t)obj);
+                  log_q[e] = (uint16_t)ql;
+                } else {
+                  atomicOr(&p.st[q0 + ql].flags, 1u);  // lost: the exact scan answers it
                 }
               }
             }
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(acce + buf);
       }
     }
   }

@@ -1,0 +1,444 @@
+// Learned k-th-score model: features from the partition statistics, and a small
+// MLP (in -> 64 -> 64 -> 1, ReLU, FP32) trained and served by the kernels here.
+//
+// No reference counterpart: the reference's pruning only uses exact bounds
+// (cpu/VTA.h:210-216, cpu/PTA.h:337-340).  The model predicts a query's k-th score
+// so that a pruned scan can start from a high threshold; the scan's own count
+// decides whether the prediction may be used (topk_abi.cpp), so exactness never
+// depends on the model.
+//
+// Features of a query (F = 2d + 18 values), with S = sum_m |weights[attr[m]]|:
+//   [0, d)        the weight on each attribute (summed over repeats) / S
+//   [d, 2d)       ln(|that| ) for the queried attributes, 0 for the others
+//   2d            log2(k) / 10
+//   2d+1          qq / 16
+//   2d+2..2d+9    the 1st, 2nd, 4th, ..., 128th largest partition bound / S, bound =
+//                 sum_m w_m * (w_m >= 0 ? max : min) over the partition's values
+//   2d+10..2d+17  the same ranks of the partition mean scores sum_m w_m * mean / S
+// Target: u = qq * ln(gap / S) with gap = (largest bound - k-th score), at least
+// 1e-9 S.  Near the top of a sum of qq attributes the number of objects within g of
+// the largest bound grows about like g^qq, so an error e in u scales the objects
+// above the predicted cut by about e^e whatever qq is.  Cut from a prediction u:
+//   cut = largest bound - S * exp((u + margin) / qq).
+//
+// Parameters, one flat FP32 array: W1[64][F] b1[64] W2[64][64] b2[64] w3[64] b3.
+// Training: one block runs every step (forward, backward, Adam) with the
+// parameters and gradients in shared memory and the Adam moments in global memory;
+// each epoch visits the samples in the order (a*i + c) mod N, gcd(a, N) = 1.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "batch_internal.h"
+#include "device_common.cuh"
+
+namespace topk {
+
+uint32_t mlp_param_count(uint32_t F) { return kHid * F + kHid + kHid * kHid + kHid + kHid + 1; }
+
+namespace {
+
+__device__ __forceinline__ uint32_t param_count(uint32_t F) { return kHid * F + kHid + kHid * kHid + kHid + kHid + 1; }
+
+constexpr int kMT = 256;        // threads of the training / gradient block
+constexpr uint32_t kMB = 128;   // largest batch of one step
+
+struct Net {
+  float *W1, *b1, *W2, *b2, *w3, *b3;
+};
+
+__device__ __forceinline__ Net net_at(float *base, uint32_t F) {
+  Net n;
+  n.W1 = base;
+  n.b1 = n.W1 + kHid * F;
+  n.W2 = n.b1 + kHid;
+  n.b2 = n.W2 + kHid * kHid;
+  n.w3 = n.b2 + kHid;
+  n.b3 = n.w3 + kHid;
+  return n;
+}
+
+// Forward and backward of one batch (MSE loss); adds the gradient into g (each
+// element owned by one thread) and the batch's mean squared error into *loss.
+// X [B][F], y [B], H1/H2 [B][64], dy [B] in shared memory; ends with a barrier.
+__device__ void batch_grad(const Net &p, const Net &g, const float *X, const float *y, uint32_t B, uint32_t F,
+                           float *H1, float *H2, float *dy, float *loss) {
+  const int t = threadIdx.x;
+  for (uint32_t e = t; e < B * kHid; e += kMT) {
+    const uint32_t i = e / kHid, j = e % kHid;
+    float s = p.b1[j];
+    for (uint32_t f = 0; f < F; ++f) s = fmaf(p.W1[j * F + f], X[i * F + f], s);
+    H1[e] = fmaxf(s, 0.0f);
+  }
+  __syncthreads();
+  for (uint32_t e = t; e < B * kHid; e += kMT) {
+    const uint32_t i = e / kHid, j = e % kHid;
+    float s = p.b2[j];
+    for (uint32_t l = 0; l < kHid; ++l) s = fmaf(p.W2[j * kHid + l], H1[i * kHid + l], s);
+    H2[e] = fmaxf(s, 0.0f);
+  }
+  __syncthreads();
+  for (uint32_t i = t; i < B; i += kMT) {
+    float s = p.b3[0];
+    for (uint32_t j = 0; j < kHid; ++j) s = fmaf(p.w3[j], H2[i * kHid + j], s);
+    const float r = s - y[i];
+    dy[i] = 2.0f * r / (float)B;
+    atomicAdd(loss, r * r / (float)B);
+  }
+  __syncthreads();
+  for (uint32_t j = t; j < kHid; j += kMT) {
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s = fmaf(dy[i], H2[i * kHid + j], s);
+    g.w3[j] += s;
+  }
+  if (t == 0) {
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s += dy[i];
+    g.b3[0] += s;
+  }
+  __syncthreads();
+  for (uint32_t e = t; e < B * kHid; e += kMT) {  // D2 = dy * w3 where the unit was active
+    const uint32_t i = e / kHid, j = e % kHid;
+    H2[e] = H2[e] > 0.0f ? dy[i] * p.w3[j] : 0.0f;
+  }
+  __syncthreads();
+  for (uint32_t e = t; e < kHid * kHid; e += kMT) {
+    const uint32_t j = e / kHid, l = e % kHid;
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s = fmaf(H2[i * kHid + j], H1[i * kHid + l], s);
+    g.W2[e] += s;
+  }
+  for (uint32_t j = t; j < kHid; j += kMT) {
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s += H2[i * kHid + j];
+    g.b2[j] += s;
+  }
+  __syncthreads();
+  constexpr uint32_t kPer = kMB * kHid / kMT;  // outputs of D1 per thread
+  float d1[kPer];
+#pragma unroll
+  for (uint32_t r = 0; r < kPer; ++r) {
+    const uint32_t e = t + r * kMT;
+    d1[r] = 0.0f;
+    if (e < B * kHid) {
+      const uint32_t i = e / kHid, l = e % kHid;
+      float s = 0.0f;
+      for (uint32_t j = 0; j < kHid; ++j) s = fmaf(H2[i * kHid + j], p.W2[j * kHid + l], s);
+      d1[r] = H1[e] > 0.0f ? s : 0.0f;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < kPer; ++r) {
+    const uint32_t e = t + r * kMT;
+    if (e < B * kHid) H1[e] = d1[r];
+  }
+  __syncthreads();
+  for (uint32_t e = t; e < kHid * F; e += kMT) {
+    const uint32_t j = e / F, f = e % F;
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s = fmaf(H1[i * kHid + j], X[i * F + f], s);
+    g.W1[e] += s;
+  }
+  for (uint32_t j = t; j < kHid; j += kMT) {
+    float s = 0.0f;
+    for (uint32_t i = 0; i < B; ++i) s += H1[i * kHid + j];
+    g.b1[j] += s;
+  }
+  __syncthreads();
+}
+
+// Shared layout of the single-block kernels: params | grad | X[kMB][F] | y | dy | H1 | H2 | loss
+size_t mlp_smem(uint32_t F) {
+  const size_t P = mlp_param_count(F);
+  return (2 * P + (size_t)kMB * F + 2 * kMB + 2 * (size_t)kMB * kHid + 4) * sizeof(float);
+}
+
+struct MlpShared {
+  float *params, *grad, *X, *y, *dy, *H1, *H2, *loss;
+};
+
+__device__ MlpShared mlp_shared(unsigned char *smem, uint32_t F) {
+  const uint32_t P = param_count(F);
+  MlpShared s;
+  s.params = reinterpret_cast<float *>(smem);
+  s.grad = s.params + P;
+  s.X = s.grad + P;
+  s.y = s.X + kMB * F;
+  s.dy = s.y + kMB;
+  s.H1 = s.dy + kMB;
+  s.H2 = s.H1 + kMB * kHid;
+  s.loss = s.H2 + kMB * kHid;
+  return s;
+}
+
+// One batch: gradient and loss at the given parameters, no update.
+__global__ void __launch_bounds__(kMT) mlp_grad_kernel(const float *__restrict__ params, const float *__restrict__ X,
+                                                       const float *__restrict__ y, uint32_t B, uint32_t F,
+                                                       float *__restrict__ grad, float *__restrict__ loss) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpShared s = mlp_shared(smem, F);
+  const uint32_t P = param_count(F);
+  for (uint32_t e = threadIdx.x; e < P; e += kMT) {
+    s.params[e] = params[e];
+    s.grad[e] = 0.0f;
+  }
+  for (uint32_t e = threadIdx.x; e < B * F; e += kMT) s.X[e] = X[e];
+  for (uint32_t e = threadIdx.x; e < B; e += kMT) s.y[e] = y[e];
+  if (threadIdx.x == 0) *s.loss = 0.0f;
+  __syncthreads();
+  batch_grad(net_at(s.params, F), net_at(s.grad, F), s.X, s.y, B, F, s.H1, s.H2, s.dy, s.loss);
+  for (uint32_t e = threadIdx.x; e < P; e += kMT) grad[e] = s.grad[e];
+  if (threadIdx.x == 0) *loss = *s.loss;
+}
+
+// Training: epochs x floor(N / B) Adam steps in one block.  mul/add: per-epoch
+// visiting order (mul coprime with N).  m, v: Adam moments (zeroed by the caller).
+// epoch_loss[e]: mean batch loss of epoch e.
+__global__ void __launch_bounds__(kMT) mlp_train_kernel(float *__restrict__ params, float *__restrict__ m,
+                                                        float *__restrict__ v, const float *__restrict__ X,
+                                                        const float *__restrict__ y, uint64_t N, uint32_t F,
+                                                        uint32_t B, uint32_t epochs, const uint64_t *__restrict__ mul,
+                                                        const uint64_t *__restrict__ add, float lr,
+                                                        float *__restrict__ epoch_loss) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpShared s = mlp_shared(smem, F);
+  const uint32_t P = param_count(F);
+  for (uint32_t e = threadIdx.x; e < P; e += kMT) s.params[e] = params[e];
+  const Net pn = net_at(s.params, F), gn = net_at(s.grad, F);
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  float b1t = 1.0f, b2t = 1.0f;
+  const uint64_t steps = N / B;
+  for (uint32_t ep = 0; ep < epochs; ++ep) {
+    if (threadIdx.x == 0) *s.loss = 0.0f;
+    for (uint64_t st = 0; st < steps; ++st) {
+      __syncthreads();
+      for (uint32_t e = threadIdx.x; e < P; e += kMT) s.grad[e] = 0.0f;
+      for (uint32_t e = threadIdx.x; e < B * F; e += kMT) {
+        const uint32_t i = e / F, f = e % F;
+        const uint64_t idx = (mul[ep] * (st * B + i) + add[ep]) % N;
+        s.X[e] = X[idx * F + f];
+        if (f == 0) s.y[i] = y[idx];
+      }
+      __syncthreads();
+      batch_grad(pn, gn, s.X, s.y, B, F, s.H1, s.H2, s.dy, s.loss);
+      b1t *= b1;
+      b2t *= b2;
+      const float c1 = 1.0f / (1.0f - b1t), c2 = 1.0f / (1.0f - b2t);
+      for (uint32_t e = threadIdx.x; e < P; e += kMT) {
+        const float gr = s.grad[e];
+        const float mm = b1 * m[e] + (1.0f - b1) * gr;
+        const float vv = b2 * v[e] + (1.0f - b2) * gr * gr;
+        m[e] = mm;
+        v[e] = vv;
+        s.params[e] -= lr * (mm * c1) / (sqrtf(vv * c2) + eps);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) epoch_loss[ep] = steps ? *s.loss / (float)steps : 0.0f;
+  }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < P; e += kMT) params[e] = s.params[e];
+}
+
+// Inference: one thread per sample, parameters in shared memory, the hidden
+// activations in a per-thread shared slice.
+__global__ void __launch_bounds__(128) mlp_predict_kernel(const float *__restrict__ params, const float *__restrict__ X,
+                                                          uint64_t N, uint32_t F, float *__restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *sp = reinterpret_cast<float *>(smem);
+  const uint32_t P = param_count(F);
+  float *h = sp + P + threadIdx.x * (2 * kHid);
+  for (uint32_t e = threadIdx.x; e < P; e += blockDim.x) sp[e] = params[e];
+  __syncthreads();
+  const Net p = net_at(sp, F);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float *x = X + i * F;
+    for (uint32_t j = 0; j < kHid; ++j) {
+      float s = p.b1[j];
+      for (uint32_t f = 0; f < F; ++f) s = fmaf(p.W1[j * F + f], x[f], s);
+      h[j] = fmaxf(s, 0.0f);
+    }
+    for (uint32_t j = 0; j < kHid; ++j) {
+      float s = p.b2[j];
+      for (uint32_t l = 0; l < kHid; ++l) s = fmaf(p.W2[j * kHid + l], h[l], s);
+      h[kHid + j] = fmaxf(s, 0.0f);
+    }
+    float s = p.b3[0];
+    for (uint32_t j = 0; j < kHid; ++j) s = fmaf(p.w3[j], h[kHid + j], s);
+    out[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------- features
+// Bitonic sort of n (a power of two) floats in shared memory, descending.
+__device__ void sort_desc(float *a, uint32_t n) {
+  for (uint32_t size = 2; size <= n; size <<= 1)
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < n / 2; i += blockDim.x) {
+        const uint32_t lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
+        const bool desc = (lo & size) == 0;
+        const float x = a[lo], y2 = a[hi];
+        if ((x < y2) == desc) {
+          a[lo] = y2;
+          a[hi] = x;
+        }
+      }
+    }
+  __syncthreads();
+}
+
+// One block per query: the F features (and, with params, the model's prediction
+// of k-th score / S, the MLP forward in the same block).
+__global__ void __launch_bounds__(256) features_kernel(const float *__restrict__ pmin, const float *__restrict__ pmax,
+                                                       const float *__restrict__ pmean, uint32_t P, uint32_t Ppad,
+                                                       uint32_t d, const BatchQuery *__restrict__ qs,
+                                                       float *__restrict__ X, const float *__restrict__ params,
+                                                       float *__restrict__ pred) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *bnd = reinterpret_cast<float *>(smem);
+  float *mu = bnd + Ppad;
+  float *feat = mu + Ppad;          // kMlpMaxIn
+  float *h = feat + kMlpMaxIn;      // 2 * kHid
+  __shared__ float S;
+  const BatchQuery &q = qs[blockIdx.x];
+  const uint32_t F = feature_dim(d);
+  if (threadIdx.x == 0) {
+    float s = 0.0f;
+    for (uint32_t m = 0; m < q.qq; ++m) s += fabsf(q.w[m]);
+    S = s > 0.0f ? s : 1.0f;
+  }
+  for (uint32_t p = threadIdx.x; p < Ppad; p += blockDim.x) {
+    float b = __int_as_float(0xFF800000), u = b;
+    if (p < P) {
+      b = 0.0f;
+      u = 0.0f;
+      for (uint32_t m = 0; m < q.qq; ++m) {
+        const size_t o = (size_t)p * d + q.attr[m];
+        const float w = q.w[m];
+        b += w * (w >= 0.0f ? pmax[o] : pmin[o]);
+        u += w * pmean[o];
+      }
+    }
+    bnd[p] = b;
+    mu[p] = u;
+  }
+  for (uint32_t m = threadIdx.x; m < kMlpMaxIn; m += blockDim.x) feat[m] = 0.0f;
+  __syncthreads();
+  sort_desc(bnd, Ppad);
+  sort_desc(mu, Ppad);
+  if (threadIdx.x == 0) {
+    const float inv = 1.0f / S;
+    for (uint32_t m = 0; m < q.qq; ++m) feat[q.attr[m]] += q.w[m] * inv;
+    for (uint32_t m = 0; m < d; ++m) feat[d + m] = feat[m] != 0.0f ? logf(fabsf(feat[m])) : 0.0f;
+    feat[2 * d] = log2f((float)q.k) * 0.1f;
+    feat[2 * d + 1] = (float)q.qq * (1.0f / 16.0f);
+    for (uint32_t r = 0; r < 8; ++r) {
+      const uint32_t at = min((1u << r), P) - 1u;
+      feat[2 * d + 2 + r] = bnd[at] * inv;
+      feat[2 * d + 10 + r] = mu[at] * inv;
+    }
+  }
+  __syncthreads();
+  for (uint32_t f = threadIdx.x; f < F; f += blockDim.x) X[(size_t)blockIdx.x * F + f] = feat[f];
+  if (!params) return;
+  const Net p = net_at(const_cast<float *>(params), F);
+  if (threadIdx.x < kHid) {
+    const uint32_t j = threadIdx.x;
+    float s = p.b1[j];
+    for (uint32_t f = 0; f < F; ++f) s = fmaf(p.W1[j * F + f], feat[f], s);
+    h[j] = fmaxf(s, 0.0f);
+  }
+  __syncthreads();
+  if (threadIdx.x < kHid) {
+    const uint32_t j = threadIdx.x;
+    float s = p.b2[j];
+    for (uint32_t l = 0; l < kHid; ++l) s = fmaf(p.W2[j * kHid + l], h[l], s);
+    h[kHid + j] = fmaxf(s, 0.0f);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float s = p.b3[0];
+    for (uint32_t j = 0; j < kHid; ++j) s = fmaf(p.w3[j], h[kHid + j], s);
+    pred[blockIdx.x] = s;
+  }
+}
+
+// Each query's batched state starts at its learned cut (no start when the cut is
+// not a finite number), nothing kept yet.  X: the features (row stride F, the
+// largest bound / S at column bcol).
+__global__ void learned_seed_kernel(const float *__restrict__ pred, const float *__restrict__ X, uint32_t F,
+                                    uint32_t bcol, const BatchQuery *__restrict__ qs, float margin,
+                                    BatchState *__restrict__ st, uint32_t nq) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nq) return;
+  const BatchQuery &q = qs[j];
+  float S = 0.0f;
+  for (uint32_t m = 0; m < q.qq; ++m) S += fabsf(q.w[m]);
+  if (S == 0.0f) S = 1.0f;
+  const float cut = learned_cut(pred[j], X[(size_t)j * F + bcol], S, (float)q.qq, margin);
+  BatchState s{};
+  s.thr = isfinite(cut) ? f2key(cut) : 0u;  // a finite float's key is >= 0x007FFFFF
+  s.seed = s.thr;
+  st[j] = s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
+                                BatchState *st, uint32_t nq, cudaStream_t s) {
+  if (nq)
+    learned_seed_kernel<<<(nq + 255) / 256, 256, 0, s>>>(pred, X, feature_dim(d), feature_bound_col(d), qs, margin, st,
+                                                         nq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_grad(const float *params, const float *X, const float *y, uint32_t B, uint32_t F, float *grad,
+                            float *loss, cudaStream_t s) {
+  if (B == 0 || B > kMB || F == 0 || F > kMlpMaxIn) return cudaErrorInvalidValue;
+  const size_t smem = mlp_smem(F);
+  cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  mlp_grad_kernel<<<1, kMT, smem, s>>>(params, X, y, B, F, grad, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_train(float *params, float *m, float *v, const float *X, const float *y, uint64_t N, uint32_t F,
+                             uint32_t B, uint32_t epochs, const uint64_t *mul, const uint64_t *add, float lr,
+                             float *epoch_loss, cudaStream_t s) {
+  if (B == 0 || B > kMB || F == 0 || F > kMlpMaxIn) return cudaErrorInvalidValue;
+  const size_t smem = mlp_smem(F);
+  cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  mlp_train_kernel<<<1, kMT, smem, s>>>(params, m, v, X, y, N, F, B, epochs, mul, add, lr, epoch_loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, uint32_t F, float *out, int num_sms,
+                               cudaStream_t s) {
+  if (F == 0 || F > kMlpMaxIn) return cudaErrorInvalidValue;
+  const size_t smem = ((size_t)mlp_param_count(F) + 128 * 2 * kHid) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t blocks = std::min<uint64_t>((N + 127) / 128, (uint64_t)num_sms * 4);
+  if (blocks) mlp_predict_kernel<<<(unsigned)blocks, 128, smem, s>>>(params, X, N, F, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_features(const float *pmin, const float *pmax, const float *pmean, uint32_t P, uint32_t d,
+                            const BatchQuery *qs, uint32_t nq, float *X, const float *params, float *pred,
+                            cudaStream_t s) {
+  if (feature_dim(d) > kMlpMaxIn || P == 0 || P > kMaxFeatureParts) return cudaErrorInvalidValue;
+  uint32_t Ppad = 1;
+  while (Ppad < P) Ppad <<= 1;
+  const size_t smem = (2 * (size_t)Ppad + kMlpMaxIn + 2 * kHid) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (nq) features_kernel<<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+  return cudaGetLastError();
+}
+
+}  // namespace topk

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <condition_variable>
 #include <cstdarg>
@@ -130,7 +131,7 @@ struct topk_table_s {
   DevBuf b_q, b_st, b_best, b_cand, b_ids, b_scores, b_count, b_thr;
   // BF16 filter: split copy of the table (rebuilt when the table changed), the
   // per-column max |x| it was built from, the batch's query tiles and error word
-  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logq;
+  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logq, b_feat, b_pred;
   uint64_t data_version = 1, xbf_version = 0;
   std::vector<float> absmax;
   bool xbf_usable = false;
@@ -142,9 +143,17 @@ struct topk_table_s {
   uint32_t part_log2 = 0, num_parts = 0;
   uint64_t part_version = 0;
   std::vector<float> pmin, pmax, pmean;
+  // learned k-th-score model (topk_set_learned_model / topk_learned_fit): device
+  // parameters, calibrated margin (in units of S = sum |w|), one query's buffers
+  std::mutex learned_mu;
+  float *mlp = nullptr;
+  float mlp_margin = 0.0f;
+  uint64_t mlp_part_version = 0;
+  BatchQuery *lq_query = nullptr;
+  float *lq_out = nullptr;  // features (kMlpMaxIn) then the prediction
   cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
   double last_batch_ms = 0, last_batch_err_ratio = 0;
-  uint64_t last_batch_fallbacks = 0, last_batch_cands = 0;
+  uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
   int last_batch_method = 0;
 };
 
@@ -575,7 +584,7 @@ int ensure(topk_table_s::DevBuf &b, size_t bytes) {
 void free_batch_buffers(topk_table_t h) {
   for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
                                   &h->b_thr, &h->xbf, &h->xbf_absmax, &h->b_abf, &h->b_err, &h->b_log,
-                                  &h->b_logq}) {
+                                  &h->b_logq, &h->b_feat, &h->b_pred}) {
     cudaFree(b->p);
     b->p = nullptr;
     b->bytes = 0;
@@ -642,9 +651,12 @@ float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
 // Batched exact top-k on the handle's primary stream (caller holds batch_mu):
 // bootstrap over the first rows, doubling chunks (score + reduce), finish.  Queries
 // flagged for a candidate overflow are answered again by the single-query scan.
+// With the learned start, each query's threshold begins at its predicted cut
+// instead (no bootstrap); a query left with fewer than k objects at or above its
+// cut is answered again by a batch without the learned start.
 int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
               uint64_t wstride, const uint8_t *attrs, uint64_t astride, uint64_t *ids, float *scores,
-              uint64_t kstride, uint64_t *counts, float *thresholds) {
+              uint64_t kstride, uint64_t *counts, float *thresholds, bool allow_learned = true) {
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   std::vector<BatchQuery> q(nq);
@@ -673,14 +685,22 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   cudaStream_t s = h->primary->stream;
   // scorer: the BF16 tensor-core filter where the table and every weight allow it
   bool use_bf16 = false;
-  if (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_BF16) {
+  if (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_BF16 ||
+      h->batch_method == TOPK_BATCH_LEARNED) {
     if ((st = ensure_bf16_table(h, s)) != TOPK_OK) return st;
     use_bf16 = h->xbf_usable && nq <= 0xFFFFFFFFull;
     for (uint64_t j = 0; use_bf16 && j < nq; j++)
       for (uint32_t m = 0; m < q[j].qq; m++)
         if (!(std::fabs(q[j].w[m]) <= kBf16MaxAbs)) use_bf16 = false;
   }
-  h->last_batch_method = use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
+  // learned start: a model fitted on the current partitions
+  bool use_learned = false;
+  if (allow_learned && (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_LEARNED)) {
+    std::lock_guard<std::mutex> lk(h->learned_mu);
+    use_learned = h->mlp && h->mlp_part_version == h->part_version && h->part_version == h->data_version &&
+                  feature_dim(h->d) <= kMlpMaxIn && h->num_parts <= kMaxFeatureParts && nq <= 0x7FFFFFFFull;
+  }
+  h->last_batch_method = use_learned ? TOPK_BATCH_LEARNED : use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
   const uint32_t nqq_all = (uint32_t)nq;
   uint64_t log_ctas = 0;
   if (use_bf16) {
@@ -721,11 +741,28 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   const uint32_t nqq = (uint32_t)nq;
   CK(cudaMemcpyAsync(dq, q.data(), nq * sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(dst, 0, nq * sizeof(BatchState), s));
+  if (use_learned) {
+    if ((st = ensure(h->b_feat, nq * feature_dim(h->d) * sizeof(float))) != TOPK_OK) return st;
+    if ((st = ensure(h->b_pred, nq * sizeof(float))) != TOPK_OK) return st;
+  }
   CK(cudaEventRecord(h->b_ev0, s));
   const uint64_t boot = std::min<uint64_t>(h->n, kBatchBootRows);
-  CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
+  uint64_t r_start = boot;
+  if (use_learned) {
+    // features and the model in one kernel, then each query's threshold starts at
+    // its cut (prediction - margin) * S; no bootstrap
+    std::lock_guard<std::mutex> lk(h->learned_mu);
+    const size_t P = h->num_parts, d = h->d;
+    CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, dq, nqq,
+                       static_cast<float *>(h->b_feat.p), h->mlp, static_cast<float *>(h->b_pred.p), s));
+    CK(launch_learned_seed(static_cast<const float *>(h->b_pred.p), static_cast<const float *>(h->b_feat.p), h->d, dq,
+                           h->mlp_margin, dst, nqq, s));
+    r_start = 0;
+  } else {
+    CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
+  }
   // chunk boundaries stay multiples of 128 rows (the filter's object tiles)
-  for (uint64_t r = boot, size = boot; r < h->n; size *= 2) {
+  for (uint64_t r = r_start, size = kBatchBootRows; r < h->n; size *= 2) {
     const uint64_t e = std::min<uint64_t>(h->n, r + size);
     if (use_bf16) {
       const FilterPlan fp = plan_bf16_filter(nqq, r, e, h->num_sms);
@@ -770,6 +807,48 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   }
   h->last_batch_cands = cands;
   h->last_batch_err_ratio = err_ratio;
+  // learned start too high (fewer than k objects reached the cut): answer those
+  // queries again with a batch that starts from the bootstrap
+  std::vector<uint64_t> miss;
+  if (use_learned)
+    for (uint64_t j = 0; j < nq; j++)
+      if (!(hst[j].flags & 1u) && hcnt[j] < q[j].k) miss.push_back(j);
+  h->last_batch_learned_misses = miss.size();
+  if (!miss.empty()) {
+    const uint64_t nm = miss.size();
+    std::vector<uint64_t> mk(nm), mcnt(nm);
+    std::vector<uint32_t> mqq(nm);
+    std::vector<float> mw(nm * wstride), mth(nm);
+    std::vector<uint8_t> ma(nm * astride);
+    for (uint64_t i = 0; i < nm; i++) {
+      const uint64_t j = miss[i];
+      mk[i] = ks[j];
+      mqq[i] = qqs[j];
+      std::memcpy(&mw[i * wstride], weights + j * wstride, wstride * 4);
+      std::memcpy(&ma[i * astride], attrs + j * astride, astride);
+    }
+    std::vector<uint64_t> mids(nm * kmax);
+    std::vector<float> msc(nm * kmax);
+    const double ms0 = ms;
+    const uint64_t cands0 = cands;
+    st = run_batch(h, nm, mk.data(), mqq.data(), mw.data(), wstride, ma.data(), astride, mids.data(), msc.data(),
+                   kmax, mcnt.data(), mth.data(), false);
+    if (st != TOPK_OK) return st;
+    for (uint64_t i = 0; i < nm; i++) {  // these results replace the batch's own below
+      const uint64_t j = miss[i];
+      hcnt[j] = (uint32_t)mcnt[i];
+      hth[j] = mth[i];
+      std::memcpy(&hid[j * kmax], &mids[i * kmax], mcnt[i] * 8);
+      std::memcpy(&hsc[j * kmax], &msc[i * kmax], mcnt[i] * 4);
+      hst[j].flags = 0;  // the rerun already answered overflows of its own
+    }
+    h->last_batch_ms += ms0;
+    h->last_batch_cands += cands0;
+    h->last_batch_err_ratio = std::max<double>(h->last_batch_err_ratio, err_ratio);
+    h->last_batch_learned_misses = nm;
+    h->last_batch_method = TOPK_BATCH_LEARNED;
+  }
+  uint64_t fallbacks_rerun = miss.empty() ? 0 : h->last_batch_fallbacks;
   for (uint64_t j = 0; j < nq; j++) {
     if (hst[j].flags & 1u) {  // a candidate region overflowed: answer exactly with the scan
       ++fallbacks;
@@ -788,7 +867,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if (counts) counts[j] = c;
     if (thresholds) thresholds[j] = hth[j];
   }
-  h->last_batch_fallbacks = fallbacks;
+  h->last_batch_fallbacks = fallbacks + fallbacks_rerun;
   return TOPK_OK;
 }
 
@@ -865,6 +944,9 @@ int topk_destroy(topk_table_t h) {
   for (Ctx *c : h->ctxs) ctx_free(c);
   ctx_free(h->primary);
   free_batch_buffers(h);
+  cudaFree(h->mlp);
+  cudaFree(h->lq_query);
+  cudaFree(h->lq_out);
   cudaFree(h->ptable);
   cudaFree(h->pids);
   cudaFree(h->pstats);
@@ -1006,6 +1088,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
   h->last_batch_fallbacks = 0;
   h->last_batch_cands = 0;
   h->last_batch_err_ratio = 0;
+  h->last_batch_learned_misses = 0;
   h->last_batch_method = TOPK_BATCH_LOOP;
   for (uint64_t j = 0; j < nq; j++) {
     uint64_t c = 0;
@@ -1021,7 +1104,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
 
 int topk_set_batch_method(topk_table_t h, int method) {
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
-  if (method < TOPK_BATCH_AUTO || method > TOPK_BATCH_BF16)
+  if (method < TOPK_BATCH_AUTO || method > TOPK_BATCH_LEARNED)
     return fail(TOPK_ERR_UNSUPPORTED, "batch method %d not available", method);
   std::lock_guard<std::mutex> lk(h->batch_mu);
   h->batch_method = method;
@@ -1037,11 +1120,12 @@ int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks
   return TOPK_OK;
 }
 
-int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio) {
+int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uint64_t *learned_misses) {
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   std::lock_guard<std::mutex> lk(h->batch_mu);
   if (method) *method = h->last_batch_method;
   if (max_err_ratio) *max_err_ratio = h->last_batch_err_ratio;
+  if (learned_misses) *learned_misses = h->last_batch_learned_misses;
   return TOPK_OK;
 }
 
@@ -1142,6 +1226,427 @@ int topk_query_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   return run_pruned(h, k, qq, weights, attr, cut, ids, scores, count, threshold, stats);
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- learned model
+extern "C" uint64_t topk_mlp_param_count(uint32_t in_dim) { return mlp_param_count(in_dim); }
+
+namespace {
+
+// Device buffers of one standalone model call, freed on scope exit.
+struct DevScope {
+  std::vector<void *> ptrs;
+  ~DevScope() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  cudaError_t alloc(T **p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes ? bytes : 4);
+    if (e == cudaSuccess) ptrs.push_back(*p);
+    return e;
+  }
+};
+
+int check_mlp_dims(uint32_t in_dim) {
+  if (in_dim == 0 || in_dim > kMlpMaxIn) return fail(TOPK_ERR_ARG, "in_dim must be in [1, %u]", kMlpMaxIn);
+  return TOPK_OK;
+}
+
+uint64_t splitmix(uint64_t &x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+uint64_t gcd64(uint64_t a, uint64_t b) {
+  while (b) {
+    const uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Pack host queries into BatchQuery records (k clamped to n).
+std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs,
+                                     const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride) {
+  std::vector<BatchQuery> q(nq);
+  for (uint64_t j = 0; j < nq; j++) {
+    BatchQuery &b = q[j];
+    std::memset(&b, 0, sizeof(b));
+    b.k = (uint32_t)std::min<uint64_t>(ks[j], h->n);
+    b.qq = qqs[j];
+    for (uint32_t m = 0; m < b.qq; m++) {
+      b.attr[m] = attrs[j * astride + m];
+      b.w[m] = weights[j * wstride + b.attr[m]];
+    }
+  }
+  return q;
+}
+
+float query_scale(const BatchQuery &b) {
+  float s = 0.0f;
+  for (uint32_t m = 0; m < b.qq; m++) s += std::fabs(b.w[m]);
+  return s > 0.0f ? s : 1.0f;
+}
+
+// Training target of a query: qq * ln(gap / S), gap = largest bound - k-th score,
+// at least 1e-9 S (the largest bound bounds every score, so gap >= 0 up to rounding).
+float learned_target(float kth, float b1s, float S, uint32_t qq) {
+  const double g = std::max((double)b1s - (double)kth / (double)S, 1e-9);
+  return (float)((double)qq * std::log(g));
+}
+
+int check_features_ready(topk_table_t h) {
+  if (!h->ptable || h->part_version != h->data_version)
+    return fail(TOPK_ERR_STATE, "no partitions for the current table: call topk_build_partitions");
+  if (feature_dim(h->d) > kMlpMaxIn)
+    return fail(TOPK_ERR_UNSUPPORTED, "the learned model supports d <= %u", (kMlpMaxIn - 18) / 2);
+  if (h->num_parts > kMaxFeatureParts)
+    return fail(TOPK_ERR_UNSUPPORTED, "the features support at most %u partitions", kMaxFeatureParts);
+  return TOPK_OK;
+}
+
+// Features of packed queries on the device: X (device, nq x feature_dim(d)).
+int device_features(topk_table_t h, const BatchQuery *dq, uint32_t nq, float *dX, cudaStream_t s) {
+  const size_t P = h->num_parts, d = h->d;
+  CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, dq, nq, dX, nullptr,
+                     nullptr, s));
+  return TOPK_OK;
+}
+
+}  // namespace
+
+extern "C" int topk_mlp_grad(int device, uint32_t in_dim, const float *params, const float *X, const float *y, uint32_t batch,
+                  float *grad, float *loss) {
+  g_last_error.clear();
+  int st = check_mlp_dims(in_dim);
+  if (st != TOPK_OK) return st;
+  if (!params || !X || !y || !grad) return fail(TOPK_ERR_ARG, "null argument");
+  if (batch == 0 || batch > 128) return fail(TOPK_ERR_ARG, "batch must be in [1, 128]");
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  const size_t P = mlp_param_count(in_dim);
+  DevScope ds;
+  float *dp, *dX, *dy, *dg2, *dl;
+  CK(ds.alloc(&dp, P * 4));
+  CK(ds.alloc(&dX, (size_t)batch * in_dim * 4));
+  CK(ds.alloc(&dy, batch * 4));
+  CK(ds.alloc(&dg2, P * 4));
+  CK(ds.alloc(&dl, 4));
+  CK(cudaMemcpy(dp, params, P * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dX, X, (size_t)batch * in_dim * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y, batch * 4, cudaMemcpyHostToDevice));
+  CK(launch_mlp_grad(dp, dX, dy, batch, in_dim, dg2, dl, 0));
+  CK(cudaMemcpy(grad, dg2, P * 4, cudaMemcpyDeviceToHost));
+  float l = 0;
+  CK(cudaMemcpy(&l, dl, 4, cudaMemcpyDeviceToHost));
+  if (loss) *loss = l;
+  return TOPK_OK;
+}
+
+extern "C" int topk_mlp_predict(int device, uint32_t in_dim, const float *params, const float *X, uint64_t n, float *out) {
+  g_last_error.clear();
+  int st = check_mlp_dims(in_dim);
+  if (st != TOPK_OK) return st;
+  if (!params || (n && (!X || !out))) return fail(TOPK_ERR_ARG, "null argument");
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const size_t P = mlp_param_count(in_dim);
+  DevScope ds;
+  float *dp, *dX, *dout;
+  CK(ds.alloc(&dp, P * 4));
+  CK(ds.alloc(&dX, n * in_dim * 4));
+  CK(ds.alloc(&dout, n * 4));
+  CK(cudaMemcpy(dp, params, P * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dX, X, n * in_dim * 4, cudaMemcpyHostToDevice));
+  CK(launch_mlp_predict(dp, dX, n, in_dim, dout, sms, 0));
+  CK(cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost));
+  return TOPK_OK;
+}
+
+namespace {
+
+// Adam training on the device; params (device) in/out, X/y device.
+int device_train(uint32_t in_dim, float *dp, const float *dX, const float *dy, uint64_t n, uint32_t epochs,
+                 uint32_t batch, float lr, uint64_t seed, float *epoch_loss) {
+  const size_t P = mlp_param_count(in_dim);
+  std::vector<uint64_t> mul(std::max<uint32_t>(epochs, 1)), add(mul.size());
+  uint64_t x = seed;
+  for (uint32_t e = 0; e < epochs; e++) {
+    uint64_t a;
+    do {
+      a = (splitmix(x) % n) | 1u;
+    } while (gcd64(a, n) != 1);
+    mul[e] = a;
+    add[e] = splitmix(x) % n;
+  }
+  DevScope ds;
+  float *dm, *dv, *dl;
+  uint64_t *dmul, *dadd;
+  CK(ds.alloc(&dm, P * 4));
+  CK(ds.alloc(&dv, P * 4));
+  CK(ds.alloc(&dl, mul.size() * 4));
+  CK(ds.alloc(&dmul, mul.size() * 8));
+  CK(ds.alloc(&dadd, mul.size() * 8));
+  CK(cudaMemset(dm, 0, P * 4));
+  CK(cudaMemset(dv, 0, P * 4));
+  CK(cudaMemcpy(dmul, mul.data(), mul.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dadd, add.data(), add.size() * 8, cudaMemcpyHostToDevice));
+  CK(launch_mlp_train(dp, dm, dv, dX, dy, n, in_dim, batch, epochs, dmul, dadd, lr, dl, 0));
+  CK(cudaDeviceSynchronize());
+  if (epoch_loss) CK(cudaMemcpy(epoch_loss, dl, (size_t)epochs * 4, cudaMemcpyDeviceToHost));
+  return TOPK_OK;
+}
+
+}  // namespace
+
+extern "C" int topk_mlp_train(int device, uint32_t in_dim, float *params, const float *X, const float *y, uint64_t n,
+                   uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *epoch_loss) {
+  g_last_error.clear();
+  int st = check_mlp_dims(in_dim);
+  if (st != TOPK_OK) return st;
+  if (!params || !X || !y) return fail(TOPK_ERR_ARG, "null argument");
+  if (batch == 0 || batch > 128) return fail(TOPK_ERR_ARG, "batch must be in [1, 128]");
+  if (n < batch || n >= (1ull << 31)) return fail(TOPK_ERR_ARG, "n must be in [batch, 2^31)");
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  const size_t P = mlp_param_count(in_dim);
+  DevScope ds;
+  float *dp, *dX, *dy;
+  CK(ds.alloc(&dp, P * 4));
+  CK(ds.alloc(&dX, n * in_dim * 4));
+  CK(ds.alloc(&dy, n * 4));
+  CK(cudaMemcpy(dp, params, P * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dX, X, n * in_dim * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y, n * 4, cudaMemcpyHostToDevice));
+  if ((st = device_train(in_dim, dp, dX, dy, n, epochs, batch, lr, seed, epoch_loss)) != TOPK_OK) return st;
+  CK(cudaMemcpy(params, dp, P * 4, cudaMemcpyDeviceToHost));
+  return TOPK_OK;
+}
+
+extern "C" int topk_query_features(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+                        uint64_t wstride, const uint8_t *attrs, uint64_t astride, float *X, float *scale) {
+  g_last_error.clear();
+  if (!h || (nq && (!ks || !qqs || !weights || !attrs || !X))) return fail(TOPK_ERR_ARG, "null argument");
+  int st = check_features_ready(h);
+  if (st != TOPK_OK) return st;
+  if (nq >= (1ull << 31)) return fail(TOPK_ERR_ARG, "too many queries");
+  for (uint64_t j = 0; j < nq; j++) {
+    if ((st = check_query(h, ks[j], qqs[j], weights + j * wstride, attrs + j * astride)) != TOPK_OK) return st;
+    if (qqs[j] > kBatchMaxQ) return fail(TOPK_ERR_UNSUPPORTED, "features support qq <= %u", kBatchMaxQ);
+  }
+  if (nq == 0) return TOPK_OK;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::vector<BatchQuery> q = pack_queries(h, nq, ks, qqs, weights, wstride, attrs, astride);
+  const uint32_t F = feature_dim(h->d);
+  DevScope ds;
+  BatchQuery *dq;
+  float *dX;
+  CK(ds.alloc(&dq, nq * sizeof(BatchQuery)));
+  CK(ds.alloc(&dX, nq * F * 4));
+  CK(cudaMemcpy(dq, q.data(), nq * sizeof(BatchQuery), cudaMemcpyHostToDevice));
+  if ((st = device_features(h, dq, (uint32_t)nq, dX, 0)) != TOPK_OK) return st;
+  CK(cudaMemcpy(X, dX, nq * F * 4, cudaMemcpyDeviceToHost));
+  if (scale)
+    for (uint64_t j = 0; j < nq; j++) scale[j] = query_scale(q[j]);
+  return TOPK_OK;
+}
+
+extern "C" int topk_set_learned_model(topk_table_t h, const float *params, float margin) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->learned_mu);
+  DeviceGuard dg(h->device);
+  if (!params) {
+    cudaFree(h->mlp);
+    h->mlp = nullptr;
+    return TOPK_OK;
+  }
+  int st = check_features_ready(h);
+  if (st != TOPK_OK) return st;
+  if (!std::isfinite(margin)) return fail(TOPK_ERR_ARG, "margin must be finite");
+  const size_t P = mlp_param_count(feature_dim(h->d));
+  if (!h->mlp) CK(cudaMalloc(&h->mlp, P * 4));
+  if (!h->lq_query) CK(cudaMalloc(&h->lq_query, sizeof(BatchQuery)));
+  if (!h->lq_out) CK(cudaMalloc(&h->lq_out, (kMlpMaxIn + 1) * 4));
+  CK(cudaMemcpy(h->mlp, params, P * 4, cudaMemcpyHostToDevice));
+  h->mlp_margin = margin;
+  h->mlp_part_version = h->part_version;
+  return TOPK_OK;
+}
+
+extern "C" int topk_learned_fit(topk_table_t h, uint64_t n_train, uint64_t n_val, uint32_t kmin, uint32_t kmax, uint32_t qmin,
+                     uint32_t qmax, uint32_t epochs, float miss_rate, uint64_t seed, double *report) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  int st = check_features_ready(h);
+  if (st != TOPK_OK) return st;
+  if (n_train < 128 || n_train + n_val >= (1ull << 31) || n_val == 0)
+    return fail(TOPK_ERR_ARG, "need n_train >= 128 and n_val >= 1");
+  if (kmin == 0 || kmin > kmax || kmax > kMaxK) return fail(TOPK_ERR_ARG, "need 1 <= kmin <= kmax <= %u", kMaxK);
+  if (qmin == 0 || qmin > qmax || qmax > std::min<uint32_t>(h->d, kBatchMaxQ))
+    return fail(TOPK_ERR_ARG, "need 1 <= qmin <= qmax <= min(d, %u)", kBatchMaxQ);
+  if (!(miss_rate > 0.0f && miss_rate < 1.0f)) return fail(TOPK_ERR_ARG, "miss_rate must be in (0, 1)");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  const uint32_t d = h->d, F = feature_dim(d);
+  const uint64_t N = n_train + n_val;
+  // random queries: qq uniform in [qmin, qmax] distinct attributes (ascending),
+  // weights U(0,1] on the 2^-24 grid, k log-uniform in [kmin, kmax]
+  std::vector<uint64_t> ks(N);
+  std::vector<uint32_t> qqs(N);
+  std::vector<float> W(N * d, 0.0f);
+  std::vector<uint8_t> A(N * d, 0);
+  uint64_t x = seed ^ 0x5EED0F7E11ull;
+  for (uint64_t j = 0; j < N; j++) {
+    const uint32_t q = qmin + (uint32_t)(splitmix(x) % (qmax - qmin + 1));
+    std::vector<uint8_t> perm(d);
+    for (uint32_t m = 0; m < d; m++) perm[m] = (uint8_t)m;
+    for (uint32_t m = 0; m < q; m++) std::swap(perm[m], perm[m + splitmix(x) % (d - m)]);
+    std::sort(perm.begin(), perm.begin() + q);
+    for (uint32_t m = 0; m < q; m++) A[j * d + m] = perm[m];
+    for (uint32_t m = 0; m < d; m++) W[j * d + m] = (float)((splitmix(x) >> 40) + 1) * 0x1p-24f;
+    const double u = (double)(splitmix(x) >> 11) * 0x1p-53;
+    const double lk = std::log((double)kmin) + u * (std::log((double)kmax + 1.0) - std::log((double)kmin));
+    ks[j] = std::min<uint64_t>(kmax, std::max<uint64_t>(kmin, (uint64_t)std::exp(lk)));
+    qqs[j] = q;
+  }
+  // exact labels: the k-th score of every query, by the batched exact path
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<float> kth(N);
+  {
+    std::lock_guard<std::mutex> lk(h->batch_mu);
+    const uint64_t chunk = 4096;
+    std::vector<uint64_t> ids(chunk * kmax), cnt(chunk);
+    std::vector<float> sc(chunk * kmax);
+    for (uint64_t j0 = 0; j0 < N; j0 += chunk) {
+      const uint64_t c = std::min(chunk, N - j0);
+      st = run_batch(h, c, &ks[j0], &qqs[j0], &W[j0 * d], d, &A[j0 * d], d, ids.data(), sc.data(), kmax, cnt.data(),
+                     &kth[j0]);
+      if (st != TOPK_OK) return st;
+    }
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  // features, then targets u = qq * ln(gap / S), gap = largest bound - k-th score
+  std::vector<BatchQuery> q = pack_queries(h, N, ks.data(), qqs.data(), W.data(), d, A.data(), d);
+  std::vector<float> y(N);
+  const size_t P = mlp_param_count(F);
+  DevScope ds;
+  BatchQuery *dq;
+  float *dX, *dy, *dp, *dpred;
+  CK(ds.alloc(&dq, N * sizeof(BatchQuery)));
+  CK(ds.alloc(&dX, N * F * 4));
+  CK(ds.alloc(&dy, N * 4));
+  CK(ds.alloc(&dp, P * 4));
+  CK(ds.alloc(&dpred, n_val * 4));
+  CK(cudaMemcpy(dq, q.data(), N * sizeof(BatchQuery), cudaMemcpyHostToDevice));
+  if ((st = device_features(h, dq, (uint32_t)N, dX, 0)) != TOPK_OK) return st;
+  {
+    std::vector<float> b1s(N);
+    CK(cudaMemcpy2D(b1s.data(), 4, dX + feature_bound_col(d), (size_t)F * 4, 4, N, cudaMemcpyDeviceToHost));
+    for (uint64_t j = 0; j < N; j++) y[j] = learned_target(kth[j], b1s[j], query_scale(q[j]), q[j].qq);
+  }
+  CK(cudaMemcpy(dy, y.data(), N * 4, cudaMemcpyHostToDevice));
+  // initial parameters: uniform +-sqrt(6 / fan_in) weights, zero biases, b3 = mean target
+  std::vector<float> params(P, 0.0f);
+  {
+    uint64_t r = seed * 0x2545F4914F6CDD1Dull + 1;
+    auto uni = [&](double lim) { return (float)(((double)(splitmix(r) >> 11) * 0x1p-53 * 2.0 - 1.0) * lim); };
+    size_t o = 0;
+    for (uint32_t i = 0; i < kHid * F; i++) params[o++] = uni(std::sqrt(6.0 / F));
+    o += kHid;
+    for (uint32_t i = 0; i < kHid * kHid; i++) params[o++] = uni(std::sqrt(6.0 / kHid));
+    o += kHid;
+    for (uint32_t i = 0; i < kHid; i++) params[o++] = uni(std::sqrt(6.0 / kHid));
+    double mean = 0;
+    for (uint64_t j = 0; j < n_train; j++) mean += y[j];
+    params[o] = (float)(mean / (double)n_train);
+  }
+  CK(cudaMemcpy(dp, params.data(), P * 4, cudaMemcpyHostToDevice));
+  std::vector<float> eloss(std::max<uint32_t>(epochs, 1), 0.0f);
+  if ((st = device_train(F, dp, dX, dy, n_train, epochs, 128, 1e-3f, seed, eloss.data())) != TOPK_OK) return st;
+  auto t2 = std::chrono::steady_clock::now();
+  // calibrate the margin on the held-out queries: the (1 - miss_rate) quantile of
+  // target - prediction, so that the cut lies at or below the k-th score for that share
+  int sms = h->num_sms;
+  CK(launch_mlp_predict(dp, dX + n_train * F, n_val, F, dpred, sms, 0));
+  std::vector<float> pred(n_val);
+  CK(cudaMemcpy(pred.data(), dpred, n_val * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(params.data(), dp, P * 4, cudaMemcpyDeviceToHost));
+  std::vector<double> res(n_val);
+  double se = 0;
+  for (uint64_t j = 0; j < n_val; j++) {
+    res[j] = (double)y[n_train + j] - (double)pred[j];  // the cut is below the k-th score iff res <= margin
+    se += res[j] * res[j];
+  }
+  std::vector<double> sorted = res;
+  std::sort(sorted.begin(), sorted.end());
+  const uint64_t qi = std::min<uint64_t>(n_val - 1, (uint64_t)std::ceil((1.0 - miss_rate) * (double)n_val));
+  const float margin = (float)sorted[qi];
+  uint64_t miss = 0;
+  for (uint64_t j = 0; j < n_val; j++) miss += res[j] > margin;
+  if ((st = topk_set_learned_model(h, params.data(), margin)) != TOPK_OK) return st;
+  if (report) {
+    report[0] = epochs ? eloss[epochs - 1] : 0.0;
+    report[1] = std::sqrt(se / (double)n_val);
+    report[2] = margin;
+    report[3] = (double)miss / (double)n_val;
+    report[4] = std::chrono::duration<double>(t1 - t0).count();
+    report[5] = std::chrono::duration<double>(t2 - t1).count();
+  }
+  return TOPK_OK;
+}
+
+extern "C" int topk_get_learned_model(topk_table_t h, float *params, float *margin) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->learned_mu);
+  if (!h->mlp) return fail(TOPK_ERR_STATE, "no learned model");
+  if (params) CK(cudaMemcpy(params, h->mlp, mlp_param_count(feature_dim(h->d)) * 4, cudaMemcpyDeviceToHost));
+  if (margin) *margin = h->mlp_margin;
+  return TOPK_OK;
+}
+
+extern "C" int topk_query_learned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
+                       uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats,
+                       float *cut_out) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (qq > kBatchMaxQ) return fail(TOPK_ERR_UNSUPPORTED, "the learned path supports qq <= %u", kBatchMaxQ);
+  float cut = NAN;
+  {
+    std::lock_guard<std::mutex> lk(h->learned_mu);
+    if (!h->mlp || h->mlp_part_version != h->part_version || h->part_version != h->data_version)
+      return fail(TOPK_ERR_STATE, "no learned model for the current partitions");
+    DeviceGuard dg(h->device);
+    if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+    const uint64_t k1 = k;
+    std::vector<BatchQuery> q = pack_queries(h, 1, &k1, &qq, weights, 0, attr, 0);
+    const size_t P = h->num_parts, d = h->d;
+    cudaStream_t s = h->primary->stream;
+    CK(cudaMemcpyAsync(h->lq_query, q.data(), sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
+    CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, h->lq_query, 1,
+                       h->lq_out, h->mlp, h->lq_out + kMlpMaxIn, s));
+    float out[kMlpMaxIn + 1];
+    CK(cudaMemcpyAsync(out, h->lq_out, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const float c =
+        learned_cut(out[kMlpMaxIn], out[feature_bound_col(h->d)], query_scale(q[0]), (float)qq, h->mlp_margin);
+    if (std::isfinite(c)) cut = c;
+  }
+  if (cut_out) *cut_out = cut;
+  return run_pruned(h, k, qq, weights, attr, cut, ids, scores, count, threshold, stats);
+}
+
+extern "C" {
 
 int topk_gather_rows(topk_table_t h, const uint64_t *ids, uint64_t count, float *out) {
   if (!h || (count && (!ids || !out))) return fail(TOPK_ERR_ARG, "null argument");

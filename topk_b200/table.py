@@ -135,6 +135,53 @@ class Table:
         c = cnt.value
         return ids[:c], sc[:c], th.value, tuple(int(x) for x in st)
 
+    # -- learned k-th-score model ------------------------------------------
+    def query_features(self, ks, weights, attrs, qqs=None):
+        """(X, S): 2d + 18 features per query from the current partitions, and S."""
+        ks = np.ascontiguousarray(ks, np.uint64)
+        nq = len(ks)
+        W = np.ascontiguousarray(weights, np.float32).reshape(nq, -1)
+        A = np.ascontiguousarray(attrs, np.uint8).reshape(nq, -1)
+        qqs = np.full(nq, A.shape[1], np.uint32) if qqs is None else np.ascontiguousarray(qqs, np.uint32)
+        X = np.zeros((nq, 2 * self.d + 18), np.float32)
+        S = np.zeros(nq, np.float32)
+        check(_lib.load().topk_query_features(self._h, nq, ks, qqs, W.reshape(-1), W.shape[1], A.reshape(-1),
+                                              A.shape[1], X.reshape(-1), S.ctypes.data))
+        return X, S
+
+    def set_learned_model(self, params, margin):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        check(_lib.load().topk_set_learned_model(self._h, None if p is None else p.ctypes.data, float(margin)))
+
+    def get_learned_model(self):
+        from . import learned
+        p = np.empty(learned.param_count(2 * self.d + 18), np.float32)
+        m = C.c_float()
+        check(_lib.load().topk_get_learned_model(self._h, p.ctypes.data, C.byref(m)))
+        return p, m.value
+
+    def learned_fit(self, n_train, n_val, kmin=16, kmax=1024, qmin=2, qmax=None, epochs=20, miss_rate=0.01, seed=0):
+        """Fit the handle's model (see topk_learned_fit); returns its report."""
+        qmax = self.d if qmax is None else qmax
+        rep = np.zeros(6, np.float64)
+        check(_lib.load().topk_learned_fit(self._h, int(n_train), int(n_val), int(kmin), int(kmax), int(qmin),
+                                           int(qmax), int(epochs), float(miss_rate), int(seed), rep.ctypes.data))
+        keys = ("train_loss", "val_rmse", "margin", "val_miss_rate", "label_s", "train_s")
+        return dict(zip(keys, rep.tolist()))
+
+    def query_learned(self, k, weights, attr):
+        """Exact top-k through the model; returns (ids, scores, threshold, stats, cut)."""
+        w, a = _weights(weights, self.d), _attr(attr)
+        cap = max(1, min(int(k), self.n))
+        ids = np.empty(cap, np.uint64)
+        sc = np.empty(cap, np.float32)
+        st = np.zeros(4, np.uint64)
+        cnt, th, cut = C.c_uint64(), C.c_float(), C.c_float()
+        check(_lib.load().topk_query_learned(self._h, int(k), len(a), w, a, ids, sc, C.byref(cnt), C.byref(th), st,
+                                             C.byref(cut)))
+        c = cnt.value
+        return ids[:c], sc[:c], th.value, tuple(int(x) for x in st), cut.value
+
     def count_ge(self, weights, attr, thr, row_begin=0, row_end=None):
         w, a = _weights(weights, self.d), _attr(attr)
         r1 = self.n if row_end is None else int(row_end)
@@ -145,17 +192,18 @@ class Table:
 
     def set_batch_method(self, method):
         """0 auto, 1 loop of single-query scans, 2 batched FP32, 3 BF16 tensor-core
-        filter with exact rescoring (see include/topk_b200.h)."""
+        filter with exact rescoring, 4 BF16 with the learned start (see
+        include/topk_b200.h)."""
         check(_lib.load().topk_set_batch_method(self._h, int(method)))
 
     def last_batch_stats(self):
         L = _lib.load()
         ms, fb, cand = C.c_double(), C.c_uint64(), C.c_uint64()
         check(L.topk_last_batch_stats(self._h, C.byref(ms), C.byref(fb), C.byref(cand)))
-        method, ratio = C.c_int(), C.c_double()
-        check(L.topk_last_batch_info(self._h, C.byref(method), C.byref(ratio)))
+        method, ratio, miss = C.c_int(), C.c_double(), C.c_uint64()
+        check(L.topk_last_batch_info(self._h, C.byref(method), C.byref(ratio), C.byref(miss)))
         return {"device_ms": ms.value, "fallbacks": fb.value, "candidates": cand.value, "method": method.value,
-                "max_err_ratio": ratio.value}
+                "max_err_ratio": ratio.value, "learned_misses": miss.value}
 
     def set_scan_tuning(self, max_ctas_per_sm=0):
         check(_lib.load().topk_set_scan_tuning(self._h, int(max_ctas_per_sm)))

@@ -17,8 +17,13 @@ flush is needed between queries.
           oracle/_ref) on this host, timed on a 2^25-row sample, scaled to n.
   batched  the multi-query workload: 4096 queries (attribute subsets of size
           U{2..16}, k U{1..1024}) over a 2^26 x 16 table, plain batched FP32
-          against the BF16 tensor-core filter with exact rescoring; identical
-          results checked, speed-up and the filter's tensor roofline reported.
+          against the BF16 tensor-core filter with exact rescoring, without and
+          with the learned start; identical results checked, speed-ups and the
+          filter's tensor roofline reported.
+  pruned   the partitioned workload: 2^27 x 8 anticorrelated in 2^11 partitions of
+          2^16 rows, the learned model fitted on 10^5 exactly labelled queries,
+          2000 fresh queries by full scan, plain pruning and learned pruning:
+          partitions scanned, fallback rate, speed-up, identical results.
 
 Multi-GPU (torchrun): every rank holds its own replica and runs the same query
 steps (weak scaling, no collective on the data path); time = max over ranks.
@@ -231,7 +236,14 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
     t.normalize()
     out = {}
     res = {}
-    for name, method, r in (("fp32", T.BATCH_FP32, 1), ("bf16", T.BATCH_BF16, reps)):
+    # the learned start needs partitions and a fitted model on this table
+    f0 = time.perf_counter()
+    t.build_partitions(1 << 16)
+    fit = t.learned_fit(n_train=16384, n_val=2048, kmin=1, kmax=1024, qmin=2, qmax=16, epochs=40, miss_rate=0.01,
+                        seed=1)
+    fit["total_s"] = time.perf_counter() - f0
+    for name, method, r in (("fp32", T.BATCH_FP32, 1), ("bf16", T.BATCH_BF16, reps),
+                            ("learned_bf16", T.BATCH_LEARNED, reps)):
         t.set_batch_method(method)
         res[name] = t.query_batch(ks, W, A, qqs)  # warm-up (and the BF16 table split)
         ms, walls = [], []
@@ -250,11 +262,14 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
         out[name] = {"device_ms": dev, "queries_per_s": nq * 1000.0 / dev, "e2e_ms": wall,
                      "e2e_queries_per_s": nq * 1000.0 / wall, "fallbacks": st["fallbacks"],
                      "candidates": st["candidates"], "method_ran": st["method"]}
-        if name == "bf16":
+        if name != "fp32":
             out[name]["max_err_ratio"] = st["max_err_ratio"]
+        if name == "learned_bf16":
+            out[name]["learned_misses"] = st["learned_misses"]
+            out[name]["fit"] = fit
     t.close()
     same = all(np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
-               for x, y in zip(res["fp32"], res["bf16"]))
+               for other in ("bf16", "learned_bf16") for x, y in zip(res["fp32"], res[other]))
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -269,12 +284,76 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
                     "weights U(0,1]",
         "identical_results": same,
         "speedup_bf16_vs_fp32": out["fp32"]["device_ms"] / out["bf16"]["device_ms"],
+        "speedup_learned_bf16_vs_fp32": out["fp32"]["device_ms"] / out["learned_bf16"]["device_ms"],
         "roofline_bf16": {"bound": "tensor", "achieved": tf, "peak": tf_peak, "unit": "TFLOP/s",
                           "frac": tf / tf_peak,
                           "note": "dense-contraction flops 2*Q*16*n over the whole batch's device time; "
                                   "the filter issues 3 BF16 MMA passes (hi/lo split) per tile"},
     })
     return out
+
+
+def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000, seed=4):
+    """Partitioned workload: an anticorrelated n x d table in partitions of part_rows
+    rows; the learned model fitted on n_train queries labelled exactly; n_test fresh
+    queries (attribute subsets of size U{2..d}, k log-uniform in [16, 1024]) answered
+    by the plain full scan, the plain pruned method and the learned pruned method,
+    results checked identical; host wall time per query (each call is synchronous)."""
+    t = T.Table(n, d, device=device)
+    t.generate(T.DIST_ANTICORRELATED, 0)
+    t.normalize()
+    b0 = time.perf_counter()
+    t.build_partitions(part_rows)
+    build_s = time.perf_counter() - b0
+    fit = t.learned_fit(n_train=n_train, n_val=max(1000, n_train // 10), kmin=16, kmax=1024, qmin=2, qmax=d,
+                        epochs=30, miss_rate=0.01, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    ks = np.exp(rng.uniform(np.log(16), np.log(1025), n_test)).astype(np.uint64).clip(16, 1024)
+    W = ((rng.integers(0, 1 << 24, size=(n_test, d)) + 1) * 2.0 ** -24).astype(np.float32)
+    attrs = [np.sort(rng.choice(d, size=int(rng.integers(2, d + 1)), replace=False)).astype(np.uint8)
+             for _ in range(n_test)]
+    for j in range(min(3, n_test)):  # warm-up
+        t.query(int(ks[j]), W[j], attrs[j])
+        t.query_pruned(int(ks[j]), W[j], attrs[j])
+        t.query_learned(int(ks[j]), W[j], attrs[j])
+    times = {"full_scan": 0.0, "pruned": 0.0, "learned_pruned": 0.0}
+    scanned_p = scanned_l = accepted = 0
+    identical = True
+    P = 0
+    for j in range(n_test):
+        k, w, a = int(ks[j]), W[j], attrs[j]
+        t0 = time.perf_counter()
+        r0 = t.query(k, w, a)
+        t1 = time.perf_counter()
+        r1 = t.query_pruned(k, w, a)
+        t2 = time.perf_counter()
+        r2 = t.query_learned(k, w, a)
+        t3 = time.perf_counter()
+        times["full_scan"] += t1 - t0
+        times["pruned"] += t2 - t1
+        times["learned_pruned"] += t3 - t2
+        scanned_p += r1[3][0]
+        scanned_l += r2[3][0]
+        accepted += r2[3][2]
+        P = r1[3][1]
+        for x, y, z in zip(r0, r1[:3], r2[:3]):
+            identical &= np.asarray(x).tobytes() == np.asarray(y).tobytes() == np.asarray(z).tobytes()
+    t.close()
+    qps = {key: n_test / v for key, v in times.items()}
+    return {
+        "workload": f"anticorrelated n={n} x {d}, {P} partitions of {part_rows} rows; {n_test} test queries, "
+                    f"|attrs| U{{2..{d}}}, k log-uniform [16, 1024]; model fitted on {n_train} queries",
+        "queries_per_s": qps,
+        "speedup_learned_vs_full_scan": qps["learned_pruned"] / qps["full_scan"],
+        "speedup_learned_vs_pruned": qps["learned_pruned"] / qps["pruned"],
+        "partitions_scanned_fraction": {"pruned": scanned_p / (n_test * P), "learned_pruned": scanned_l / (n_test * P)},
+        "learned_accept_rate": accepted / n_test,
+        "fallback_rate": 1.0 - accepted / n_test,
+        "identical_results": bool(identical),
+        "partition_build_s": build_s,
+        "fit": fit,
+        "timing": "host wall clock per synchronous query call",
+    }
 
 
 def main():
@@ -287,6 +366,9 @@ def main():
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-pruned", action="store_true")
+    ap.add_argument("--pruned-n", type=int, default=1 << 27)
+    ap.add_argument("--pruned-queries", type=int, default=2000)
     ap.add_argument("--batched-n", type=int, default=BATCH_N)
     ap.add_argument("--batched-q", type=int, default=BATCH_Q)
     args = ap.parse_args()
@@ -436,6 +518,8 @@ def main():
     table.close()
     if not args.no_batched:
         result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q)
+    if not args.no_pruned and rank == 0:
+        result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

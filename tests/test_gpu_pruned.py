@@ -119,3 +119,27 @@ def test_pruned_needs_current_partitions():
             t.query_pruned(5, np.ones(4, np.float32), np.array([0, 1], np.uint8))
         with pytest.raises(T.TopKError):
             t.build_partitions(1000)  # not a power of two
+
+
+def test_pruned_ties_in_reordered_rows_go_to_the_lower_original_id():
+    """Few distinct values: many objects tie at the k-th score, and the partitioned
+    copy holds them out of id order; the lower original ids must win every tie,
+    with or without a cut placed exactly at the k-th score."""
+    n, d = (1 << 20) + 3, 3
+    rng = np.random.default_rng(12)
+    raw = (np.floor(O.generate(n, d, 1, 21) * 4) / 4).astype(np.float32)
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.build_partitions(1024)
+        for k in (1, 37, 500, 1024, 4096):
+            for a in (np.array([0, 1], np.uint8), np.array([2, 0, 1], np.uint8), np.array([1], np.uint8)):
+                w = np.array([0.5, 0.25, 0.125], np.float32)
+                want = O.topk_numpy(tn, k, w, a)
+                got = t.query_pruned(k, w, a)
+                H.assert_same_result(got[:3], want)
+                got = t.query_pruned(k, w, a, cut=float(want[2]))
+                H.assert_same_result(got[:3], want)
+                assert got[3][2] == 1

@@ -240,7 +240,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
         ctl->count = kept;
         ctl->reductions++;
         if (kept == p.k) {  // the CTA knows a k-th key
-          ctl->thr_local = ctl->sel.kept_min + 1u;
+          // Rows in id order: a later row has a larger id and loses a tie with the
+          // k-th, so it must beat it strictly.  Rows carrying their own ids (a
+          // reordered copy) may win the tie: the threshold stays inclusive.
+          ctl->thr_local = ctl->sel.kept_min + (p.row_ids ? 0u : 1u);
           atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
         }
       }

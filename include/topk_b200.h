@@ -252,13 +252,19 @@ int topk_set_fault_injection(topk_table_t h, int mode);
 
 /* Methods of topk_query_batch (no reference counterpart; results are identical). */
 #define TOPK_BATCH_AUTO 0  /* TOPK_BATCH_LEARNED with a fitted model, else TOPK_BATCH_BF16
-                            * where it applies, else TOPK_BATCH_FP32 */
+                            * where it applies, else TOPK_BATCH_FP32.  Once a BF16 batch
+                            * overflows the candidate regions of more than a quarter of
+                            * its queries (scores too dense around the thresholds, e.g.
+                            * anticorrelated data), later AUTO batches on the same table
+                            * use the FP32 scorer */
 #define TOPK_BATCH_LOOP 1  /* one fused single-query scan per query */
 #define TOPK_BATCH_FP32 2  /* batched plain FP32: each table tile scored for 64 queries */
 #define TOPK_BATCH_BF16 3  /* BF16 tensor-core filter (tcgen05) with a per-query error
                             * bound; candidates rescored exactly in FP32.  Applies to
                             * d <= 16 with finite table values and weights of magnitude
-                            * <= 2^60; other batches run TOPK_BATCH_FP32 */
+                            * <= 2^60; other batches run TOPK_BATCH_FP32.  A query whose
+                            * candidate region overflows is answered again by a batch
+                            * with the FP32 scorer */
 #define TOPK_BATCH_LEARNED 4 /* TOPK_BATCH_BF16 (or FP32) whose per-query threshold starts
                               * at the learned cut (prediction - margin) * S instead of a
                               * bootstrap over the first rows; a query left with fewer

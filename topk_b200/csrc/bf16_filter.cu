@@ -17,12 +17,13 @@
 // (lane = object, column = query):
 //   D = Xhi.Ahi + Xlo.Ahi + Xhi.Alo        (the lo.lo term lies inside the bound)
 // Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
-//   E = 2^-12 * sum_m |weights[attr[m]]| * max|column attr[m]|  (+ 2^-100 terms for
+//   E = 2^-13 * sum_m |weights[attr[m]]| * max|column attr[m]|  (+ 2^-100 terms for
 //   subnormal flushing).  Split and product errors give 3.1*2^-16, 48 FP32
 //   accumulations 48*2^-22, the reference's own FP32 rounding 17*2^-24: about
-//   2^-14 in all; the factor 4 covers the tensor core's accumulation rounding,
-//   which is not specified.  An object with exact score >= the threshold float t
-//   has D >= t - E, so the cut t - E (rounded down) loses none.
+//   2^-14 in all; the factor 2 covers the tensor core's accumulation rounding,
+//   which is not specified (the largest error measured on rescored candidates is
+//   below 2^-16 of the same sum).  An object with exact score >= the threshold
+//   float t has D >= t - E, so the cut t - E (rounded down) loses none.
 //
 // Roles of the 576 threads of a CTA (one CTA per SM: TMEM is allocated whole):
 //   warps 0-15 epilogue: warp w reads TMEM lanes 32*(w%4).. (one object per

@@ -154,6 +154,9 @@ struct topk_table_s {
   cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
   double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
+  // TOPK_BATCH_AUTO's memory: the table version on which the BF16 filter overflowed
+  // the candidate regions of more than a quarter of a batch (0: none)
+  uint64_t auto_fp32_version = 0;
   int last_batch_method = 0;
 };
 
@@ -635,14 +638,14 @@ int ensure_bf16_table(topk_table_t h, cudaStream_t s) {
 }
 
 // Per-query bound of the BF16 filter, rounded up to a float:
-// 2^-12 * sum_m |w_m| * absmax[attr_m] + 2^-100 * sum_m (|w_m| + absmax[attr_m]).
+// 2^-13 * sum_m |w_m| * absmax[attr_m] + 2^-100 * sum_m (|w_m| + absmax[attr_m]).
 float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
   double rel = 0, tiny = 0;
   for (uint32_t m = 0; m < b.qq; m++) {
     rel += std::fabs((double)b.w[m]) * (double)absmax[b.attr[m]];
     tiny += std::fabs((double)b.w[m]) + (double)absmax[b.attr[m]];
   }
-  const double e = std::ldexp(rel, -12) + std::ldexp(tiny, -100);
+  const double e = std::ldexp(rel, -13) + std::ldexp(tiny, -100);
   float f = (float)e;
   if ((double)f < e) f = std::nextafter(f, INFINITY);
   return f;
@@ -656,7 +659,8 @@ float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
 // cut is answered again by a batch without the learned start.
 int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
               uint64_t wstride, const uint8_t *attrs, uint64_t astride, uint64_t *ids, float *scores,
-              uint64_t kstride, uint64_t *counts, float *thresholds, bool allow_learned = true) {
+              uint64_t kstride, uint64_t *counts, float *thresholds, bool allow_learned = true,
+              bool force_fp32 = false) {
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   std::vector<BatchQuery> q(nq);
@@ -669,7 +673,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     b.qq = qqs[j];
     b.best_off = (uint32_t)best_total;
     best_total += b.k;
-    b.cand_cap = 2 * b.k + 2048;
+    b.cand_cap = 4 * b.k + 4096;
     b.cand_off = (uint32_t)cand_total;
     cand_total += b.cand_cap;
     for (uint32_t m = 0; m < b.qq; m++) {
@@ -685,10 +689,12 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   cudaStream_t s = h->primary->stream;
   // scorer: the BF16 tensor-core filter where the table and every weight allow it
   bool use_bf16 = false;
-  if (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_BF16 ||
-      h->batch_method == TOPK_BATCH_LEARNED) {
+  if (!force_fp32 && (h->batch_method == TOPK_BATCH_AUTO || h->batch_method == TOPK_BATCH_BF16 ||
+                      h->batch_method == TOPK_BATCH_LEARNED)) {
     if ((st = ensure_bf16_table(h, s)) != TOPK_OK) return st;
     use_bf16 = h->xbf_usable && nq <= 0xFFFFFFFFull;
+    // AUTO: scores too dense around the thresholds for the filter on this table
+    if (h->batch_method == TOPK_BATCH_AUTO && h->auto_fp32_version == h->data_version) use_bf16 = false;
     for (uint64_t j = 0; use_bf16 && j < nq; j++)
       for (uint32_t m = 0; m < q[j].qq; m++)
         if (!(std::fabs(q[j].w[m]) <= kBf16MaxAbs)) use_bf16 = false;
@@ -796,62 +802,72 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->b_ev0, h->b_ev1));
-  h->last_batch_ms = ms;
-  uint64_t fallbacks = 0, cands = 0;
-  float err_ratio = 0;
+  uint64_t cands = 0;
+  double err_ratio = 0;
   for (uint64_t j = 0; j < nq; j++) {
     cands += hst[j].cands;
     float r;
     std::memcpy(&r, &hst[j].errmax, 4);
-    err_ratio = std::max(err_ratio, r);
+    err_ratio = std::max(err_ratio, (double)r);
   }
-  h->last_batch_cands = cands;
-  h->last_batch_err_ratio = err_ratio;
-  // learned start too high (fewer than k objects reached the cut): answer those
-  // queries again with a batch that starts from the bootstrap
-  std::vector<uint64_t> miss;
-  if (use_learned)
-    for (uint64_t j = 0; j < nq; j++)
-      if (!(hst[j].flags & 1u) && hcnt[j] < q[j].k) miss.push_back(j);
-  h->last_batch_learned_misses = miss.size();
-  if (!miss.empty()) {
-    const uint64_t nm = miss.size();
-    std::vector<uint64_t> mk(nm), mcnt(nm);
+  // Queries answered again by a smaller batch, whose results replace this batch's:
+  //   a learned start that was too high (fewer than k objects reached the cut):
+  //     again without the learned start;
+  //   a candidate region that overflowed under the BF16 filter (dense scores around
+  //     the threshold): again with the exact FP32 scorer.
+  // What overflows under the FP32 scorer is answered by the single-query scan.
+  double ms_total = ms;
+  uint64_t cands_total = cands, misses_total = 0, scans = 0;
+  double ratio_total = err_ratio;
+  auto rerun = [&](const std::vector<uint64_t> &sub, bool learned, bool fp32) -> int {
+    const uint64_t nm = sub.size();
+    std::vector<uint64_t> mk(nm), mcnt(nm), mids(nm * kmax);
     std::vector<uint32_t> mqq(nm);
-    std::vector<float> mw(nm * wstride), mth(nm);
+    std::vector<float> mw(nm * wstride), mth(nm), msc(nm * kmax);
     std::vector<uint8_t> ma(nm * astride);
     for (uint64_t i = 0; i < nm; i++) {
-      const uint64_t j = miss[i];
+      const uint64_t j = sub[i];
       mk[i] = ks[j];
       mqq[i] = qqs[j];
       std::memcpy(&mw[i * wstride], weights + j * wstride, wstride * 4);
       std::memcpy(&ma[i * astride], attrs + j * astride, astride);
     }
-    std::vector<uint64_t> mids(nm * kmax);
-    std::vector<float> msc(nm * kmax);
-    const double ms0 = ms;
-    const uint64_t cands0 = cands;
-    st = run_batch(h, nm, mk.data(), mqq.data(), mw.data(), wstride, ma.data(), astride, mids.data(), msc.data(),
-                   kmax, mcnt.data(), mth.data(), false);
-    if (st != TOPK_OK) return st;
-    for (uint64_t i = 0; i < nm; i++) {  // these results replace the batch's own below
-      const uint64_t j = miss[i];
+    const int r = run_batch(h, nm, mk.data(), mqq.data(), mw.data(), wstride, ma.data(), astride, mids.data(),
+                            msc.data(), kmax, mcnt.data(), mth.data(), learned, fp32);
+    if (r != TOPK_OK) return r;
+    for (uint64_t i = 0; i < nm; i++) {
+      const uint64_t j = sub[i];
       hcnt[j] = (uint32_t)mcnt[i];
       hth[j] = mth[i];
       std::memcpy(&hid[j * kmax], &mids[i * kmax], mcnt[i] * 8);
       std::memcpy(&hsc[j * kmax], &msc[i * kmax], mcnt[i] * 4);
-      hst[j].flags = 0;  // the rerun already answered overflows of its own
+      hst[j].flags = 0;
     }
-    h->last_batch_ms += ms0;
-    h->last_batch_cands += cands0;
-    h->last_batch_err_ratio = std::max<double>(h->last_batch_err_ratio, err_ratio);
-    h->last_batch_learned_misses = nm;
-    h->last_batch_method = TOPK_BATCH_LEARNED;
+    ms_total += h->last_batch_ms;
+    cands_total += h->last_batch_cands;
+    ratio_total = std::max(ratio_total, h->last_batch_err_ratio);
+    misses_total += h->last_batch_learned_misses;
+    scans += h->last_batch_fallbacks;
+    return TOPK_OK;
+  };
+  std::vector<uint64_t> sub;
+  if (use_learned) {
+    for (uint64_t j = 0; j < nq; j++)
+      if (!(hst[j].flags & 1u) && hcnt[j] < q[j].k) sub.push_back(j);
+    misses_total += sub.size();
+    if (!sub.empty() && (st = rerun(sub, false, force_fp32)) != TOPK_OK) return st;
   }
-  uint64_t fallbacks_rerun = miss.empty() ? 0 : h->last_batch_fallbacks;
+  sub.clear();
+  if (use_bf16) {
+    for (uint64_t j = 0; j < nq; j++)
+      if (hst[j].flags & 1u) sub.push_back(j);
+    // AUTO remembers a table on which the filter overflows too often to pay off
+    if (h->batch_method == TOPK_BATCH_AUTO && 4 * sub.size() > nq) h->auto_fp32_version = h->data_version;
+    if (!sub.empty() && (st = rerun(sub, false, true)) != TOPK_OK) return st;
+  }
   for (uint64_t j = 0; j < nq; j++) {
-    if (hst[j].flags & 1u) {  // a candidate region overflowed: answer exactly with the scan
-      ++fallbacks;
+    if (hst[j].flags & 1u) {  // a candidate region overflowed under FP32: answer exactly with the scan
+      ++scans;
       uint64_t c = 0;
       float th = 0;
       st = run_query_sync(h, 0, h->n, ks[j], qqs[j], weights + j * wstride, attrs + j * astride, ids + j * kstride,
@@ -867,7 +883,12 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if (counts) counts[j] = c;
     if (thresholds) thresholds[j] = hth[j];
   }
-  h->last_batch_fallbacks = fallbacks + fallbacks_rerun;
+  h->last_batch_ms = ms_total;
+  h->last_batch_cands = cands_total;
+  h->last_batch_err_ratio = ratio_total;
+  h->last_batch_learned_misses = misses_total;
+  h->last_batch_fallbacks = scans;
+  h->last_batch_method = use_learned ? TOPK_BATCH_LEARNED : use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
   return TOPK_OK;
 }
 

@@ -226,7 +226,7 @@ def batch_queries(nq, d, seed=3):
     return ks, W, A, qqs
 
 
-def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
+def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "bf16", "learned_bf16")):
     """Batched workload: nq queries over an n x 16 independent table, plain batched
     FP32 against the BF16 tensor-core filter (same results, checked); device time of
     the batch kernels (CUDA events inside topk_query_batch), max over ranks."""
@@ -236,14 +236,17 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
     t.normalize()
     out = {}
     res = {}
-    # the learned start needs partitions and a fitted model on this table
-    f0 = time.perf_counter()
-    t.build_partitions(1 << 16)
-    fit = t.learned_fit(n_train=16384, n_val=2048, kmin=1, kmax=1024, qmin=2, qmax=16, epochs=40, miss_rate=0.01,
-                        seed=1)
-    fit["total_s"] = time.perf_counter() - f0
+    fit = None
+    if "learned_bf16" in methods:  # the learned start needs partitions and a fitted model on this table
+        f0 = time.perf_counter()
+        t.build_partitions(1 << 16)
+        fit = t.learned_fit(n_train=16384, n_val=2048, kmin=1, kmax=1024, qmin=2, qmax=16, epochs=40,
+                            miss_rate=0.01, seed=1)
+        fit["total_s"] = time.perf_counter() - f0
     for name, method, r in (("fp32", T.BATCH_FP32, 1), ("bf16", T.BATCH_BF16, reps),
                             ("learned_bf16", T.BATCH_LEARNED, reps)):
+        if name not in methods:
+            continue
         t.set_batch_method(method)
         res[name] = t.query_batch(ks, W, A, qqs)  # warm-up (and the BF16 table split)
         ms, walls = [], []
@@ -268,8 +271,9 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
             out[name]["learned_misses"] = st["learned_misses"]
             out[name]["fit"] = fit
     t.close()
+    names = list(res)
     same = all(np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
-               for other in ("bf16", "learned_bf16") for x, y in zip(res["fp32"], res[other]))
+               for other in names[1:] for x, y in zip(res[names[0]], res[other]))
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -278,15 +282,16 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3):
         pass
     tf_peak = float(peaks.get("bf16_tflops", 1590.0))
     flops = 2.0 * nq * 16 * n  # the dense Q x 16 by 16 x n contraction
-    tf = flops / (out["bf16"]["device_ms"] * 1e-3) / 1e12
+    speed = {f"speedup_{m}_vs_fp32": out["fp32"]["device_ms"] / out[m]["device_ms"]
+             for m in ("bf16", "learned_bf16") if m in out and "fp32" in out}
+    tf = flops / (out["bf16"]["device_ms"] * 1e-3) / 1e12 if "bf16" in out else None
+    out.update(speed)
     out.update({
         "workload": f"{nq} queries, n={n} x 16 FP32 independent, |attrs| U{{2..16}}, k U{{1..1024}}, "
                     "weights U(0,1]",
         "identical_results": same,
-        "speedup_bf16_vs_fp32": out["fp32"]["device_ms"] / out["bf16"]["device_ms"],
-        "speedup_learned_bf16_vs_fp32": out["fp32"]["device_ms"] / out["learned_bf16"]["device_ms"],
         "roofline_bf16": {"bound": "tensor", "achieved": tf, "peak": tf_peak, "unit": "TFLOP/s",
-                          "frac": tf / tf_peak,
+                          "frac": tf / tf_peak if tf else None,
                           "note": "dense-contraction flops 2*Q*16*n over the whole batch's device time; "
                                   "the filter issues 3 BF16 MMA passes (hi/lo split) per tile"},
     })
@@ -366,6 +371,9 @@ def main():
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--only", choices=["batched", "pruned"], default=None,
+                    help="run one secondary workload alone (no JSON line; for profiling)")
+    ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--no-pruned", action="store_true")
     ap.add_argument("--pruned-n", type=int, default=1 << 27)
     ap.add_argument("--pruned-queries", type=int, default=2000)
@@ -375,6 +383,17 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.only:
+        import torch
+        import topk_b200 as T
+        torch.cuda.set_device(0)
+        if args.only == "batched":
+            out = run_batched(T, torch, None, 0, args.batched_n, args.batched_q,
+                              methods=tuple(args.batched_methods.split(",")))
+        else:
+            out = run_pruned(T, 0, args.pruned_n, n_test=args.pruned_queries)
+        print(json.dumps(out))
+        return 0
 
     import torch
     import topk_b200 as T
@@ -517,7 +536,8 @@ def main():
             result["cpu_baseline"] = {"error": str(e)}
     table.close()
     if not args.no_batched:
-        result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q)
+        result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q,
+                                        methods=tuple(args.batched_methods.split(",")))
     if not args.no_pruned and rank == 0:
         result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
     if dist:

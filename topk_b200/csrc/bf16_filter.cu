@@ -12,8 +12,8 @@
 //   table  each object's 16 attributes split x = hi + lo (bf16 each, |x - hi - lo|
 //          <= 2^-16 |x|); tiles of 128 objects: hi 4 KB, then lo 4 KB  (MMA A, M=128);
 //   query  a 16-wide row a[m] = sum of weights[attr[j]] over the j with attr[j] = m,
-//          split the same way; tiles of 256 queries: hi 8 KB, then lo 8 KB (MMA B, N=256).
-// One (object tile, query tile) pair is three MMAs M=128 N=256 K=16 into FP32 TMEM
+//          split the same way; tiles of 128 queries: hi 4 KB, then lo 4 KB (MMA B, N=128).
+// One (object tile, query tile) pair is three MMAs M=128 N=128 K=16 into FP32 TMEM
 // (lane = object, column = query):
 //   D = Xhi.Ahi + Xlo.Ahi + Xhi.Alo        (the lo.lo term lies inside the bound)
 // Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
@@ -27,16 +27,17 @@
 //
 // Roles of the 576 threads of a CTA (one CTA per SM: TMEM is allocated whole):
 //   warps 0-15 epilogue: warp w reads TMEM lanes 32*(w%4).. (one object per
-//              thread), columns 64*(w/4).. (a quarter of a query tile);
+//              thread), columns 32*(w/4).. (a quarter of a query tile);
 //              one compare per value against the column's cut and a warp vote;
 //              for the rare chunks with survivors a ballot per column gives the
-//              passing objects, appended with one shared atomic per column to the
-//              CTA's survivor log in global memory (no global atomic in the
-//              MMA pipeline);
+//              passing objects, appended to the warp's own segment of the CTA's
+//              survivor log in global memory (a count kept alike in every lane:
+//              no atomic in the MMA pipeline);
 //   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
 //              the CTA's query tiles once and object tiles into a 6-stage ring;
-//   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs for two
-//              accumulators of 256 columns (double buffered against the epilogue).
+//   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into four
+//              accumulators of 128 columns, so an epilogue warp held up by
+//              survivors on one pair delays the MMA only after three more pairs.
 // After the last tile the whole CTA moves its log into the queries' candidate
 // regions (global atomics, many in flight).  A survivor that finds the log full
 // flags its query for the exact single-query fallback.
@@ -59,14 +60,17 @@ namespace {
 
 constexpr uint32_t kOTile = 128;        // objects per tile (MMA M, TMEM lanes)
 constexpr uint32_t kOTileBytes = 8192;  // hi + lo of one object tile
-constexpr uint32_t kQTile = 256;        // queries per tile (MMA N, TMEM columns)
-constexpr uint32_t kQTileBytes = 16384; // hi + lo of one query tile
+constexpr uint32_t kQTile = 128;        // queries per tile (MMA N, TMEM columns)
+constexpr uint32_t kQTileBytes = 8192;  // hi + lo of one query tile
 constexpr uint32_t kStages = 6;
 constexpr uint32_t kEpiWarps = 16;
 constexpr uint32_t kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kMaxQTPerCta = 8;
+constexpr uint32_t kMaxQTPerCta = 16;
+constexpr uint32_t kAcc = kTmemCols / kQTile;  // TMEM accumulators in flight (4)
+constexpr uint32_t kWarpCols = kQTile / 4;      // columns of one epilogue warp per pair
+constexpr uint32_t kWarpChunks = kWarpCols / 32;
 constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
 
 // Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits
@@ -167,16 +171,17 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   const uint64_t te = min(p.tile1, tb + per);
   if (tb >= te) return;  // uniform over the block: no barrier or TMEM touched yet
 
-  // shared layout: query tiles | object ring | cut[QT*256] | barriers and words
+  // shared layout: query tiles | object ring | cut[QT*kQTile] | barriers and words
   unsigned char *sq = smem;
   unsigned char *so = smem + (size_t)QT * kQTileBytes;
   float *scut = reinterpret_cast<float *>(so + (size_t)kStages * kOTileBytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(scut + QT * kQTile);
-  uint64_t *full = bars, *empty = bars + kStages, *accf = bars + 2 * kStages, *acce = accf + 2;
-  uint64_t *qfull = acce + 2, *mdone = qfull + 1;
+  uint64_t *full = bars, *empty = bars + kStages, *accf = bars + 2 * kStages, *acce = accf + kAcc;
+  uint64_t *qfull = acce + kAcc, *mdone = qfull + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 1);
   volatile uint32_t *abort_flag = tmem_slot + 1;
-  uint32_t *log_n = tmem_slot + 2;
+  uint32_t *wlog_n = tmem_slot + 2;  // entries in each epilogue warp's log segment
+  const uint32_t seg_cap = p.log_cap / kEpiWarps;
   uint2 *log = p.log + (size_t)blockIdx.x * p.log_cap;
   uint16_t *log_q = p.log_q + (size_t)blockIdx.x * p.log_cap;
   const uint32_t q0 = qt0 * kQTile;  // first query of this CTA
@@ -188,14 +193,14 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (uint32_t b = 0; b < kAcc; ++b) {
       mbar_init(accf + b, 1);
       mbar_init(acce + b, kEpiWarps);
     }
     mbar_init(qfull, 1);
     mbar_init(mdone, 1);
     *abort_flag = 0u;
-    *log_n = 0u;
+    for (uint32_t w = 0; w < kEpiWarps; ++w) wlog_n[w] = 0u;
     fence_barrier_init();
   }
   // per-query cut: threshold float minus the bound, rounded down; +inf for columns
@@ -252,8 +257,8 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         const uint32_t os = smem_u32(so + (size_t)s * kOTileBytes);
         const uint64_t xhi = smem_desc(os), xlo = smem_desc(os + kOTileBytes / 2);
         for (uint32_t i = 0; i < nqt; ++i, ++seq) {
-          const uint32_t buf = seq & 1u;
-          if (seq >= 2 && !fwait(acce + buf, ((seq >> 1) - 1) & 1u, limit, abort_flag)) {
+          const uint32_t buf = seq % kAcc;
+          if (seq >= kAcc && !fwait(acce + buf, (seq / kAcc - 1) & 1u, limit, abort_flag)) {
             ok = false;
             break;
           }
@@ -275,26 +280,30 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    const uint32_t quarter = warp & 3u, part = warp >> 2;  // TMEM lanes 32*quarter.., columns 64*part..
+    // warp w reads TMEM lanes 32*(w%4).. and columns kWarpCols*(w/4).. of each pair
+    const uint32_t quarter = warp & 3u, part = warp >> 2;
     const uint32_t lane_addr = (quarter * 32u) << 16;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    // this warp's log segment and its fill, the same in every lane (no atomics)
+    const uint32_t seg = warp * seg_cap;
+    uint32_t wcnt = 0;
     uint32_t seq = 0;
     bool ok = true;
     for (uint64_t t = tb; ok && t < te; ++t) {
       const uint64_t obj = t * kOTile + quarter * 32u + lane;  // this thread's object
       const bool valid = obj < p.r1;
       for (uint32_t i = 0; i < nqt; ++i, ++seq) {
-        const uint32_t buf = seq & 1u;
-        ok = __all_sync(0xFFFFFFFFu, fwait(accf + buf, (seq >> 1) & 1u, limit, abort_flag));
+        const uint32_t buf = seq % kAcc;
+        ok = __all_sync(0xFFFFFFFFu, fwait(accf + buf, (seq / kAcc) & 1u, limit, abort_flag));
         if (!ok) break;
         tc_fence_after();
-        const uint32_t col0 = i * kQTile + part * 64u;  // CTA-relative query of chunk 0, column 0
-        const uint32_t tcol = tmem + lane_addr + buf * kQTile + part * 64u;
-        // all 64 columns in one round trip; the accumulator is free as soon as they
-        // are in registers, and everything below works on the registers
-        uint32_t v[64];
-        tmem_ld32(tcol, v);
-        tmem_ld32(tcol + 32, v + 32);
+        const uint32_t col0 = i * kQTile + part * kWarpCols;  // CTA-relative query of column 0
+        const uint32_t tcol = tmem + lane_addr + buf * kQTile + part * kWarpCols;
+        // the warp's columns in one round trip; the accumulator is free as soon as
+        // they are in registers, and everything below works on the registers
+        uint32_t v[kWarpCols];
+#pragma unroll
+        for (uint32_t cc = 0; cc < kWarpChunks; ++cc) tmem_ld32(tcol + cc * 32u, v + cc * 32);
         tmem_wait_ld();
         tc_fence_before();
         __syncwarp();
@@ -304,7 +313,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         {
           const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0);
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc) {
+          for (uint32_t cc = 0; cc < kWarpChunks; ++cc) {
             uint32_t a = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) a = any_ge8(a, v + cc * 32 + k * 8, c4[cc * 8 + 2 * k], c4[cc * 8 + 2 * k + 1]);
@@ -314,13 +323,17 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         const uint32_t hits = __reduce_or_sync(0xFFFFFFFFu, valid ? h : 0u);
         if (hits == 0u) continue;  // common case
         // cold path: per column of a chunk with a hit, a warp ballot gives the passing
-        // objects, appended with one shared atomic
+        // objects, appended to the warp's own log segment
 #pragma unroll 1
-        for (uint32_t cc = 0; cc < 2; ++cc) {
+        for (uint32_t cc = 0; cc < kWarpChunks; ++cc) {
           if (!(hits & (1u << cc))) continue;
           uint32_t u[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) u[j] = cc ? v[32 + j] : v[j];
+          for (int j = 0; j < 32; ++j) {
+            u[j] = v[j];
+#pragma unroll
+            for (uint32_t c2 = 1; c2 < kWarpChunks; ++c2) u[j] = cc == c2 ? v[c2 * 32 + j] : u[j];
+          }
           const float *cut = scut + col0 + cc * 32u;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
@@ -328,15 +341,13 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
             const bool pass = valid && x >= cut[j];
             const uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
             if (b) {
-              uint32_t base = 0;
-              if (lane == 0) base = atomicAdd(log_n, __popc(b));
-              base = __shfl_sync(0xFFFFFFFFu, base, 0);
+              const uint32_t e = wcnt + __popc(b & lt_mask);
+              wcnt += __popc(b);
               if (pass) {
-                const uint32_t e = base + __popc(b & lt_mask);
                 const uint32_t ql = col0 + cc * 32u + j;
-                if (e < p.log_cap) {
-                  log[e] = make_uint2(f2key(x), (uint32_t)obj);
-                  log_q[e] = (uint16_t)ql;
+                if (e < seg_cap) {
+                  log[seg + e] = make_uint2(f2key(x), (uint32_t)obj);
+                  log_q[seg + e] = (uint16_t)ql;
                 } else {
                   atomicOr(&p.st[q0 + ql].flags, 1u);  // lost: the exact scan answers it
                 }
@@ -346,6 +357,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         }
       }
     }
+    if (lane == 0) wlog_n[warp] = min(wcnt, seg_cap);
   }
 
   // ---------------------------------------------------------------- teardown
@@ -361,23 +373,27 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     return;
   }
   // the CTA's survivors into their queries' candidate regions (4 in flight a thread)
-  const uint32_t n = min(*log_n, p.log_cap);
-  for (uint32_t e0 = threadIdx.x; e0 < n; e0 += 4 * kFThreads) {
-    uint32_t pos[4], q[4];
+  for (uint32_t w = 0; w < kEpiWarps; ++w) {
+    const uint32_t n = wlog_n[w];
+    const uint2 *wl = log + (size_t)w * seg_cap;
+    const uint16_t *wq = log_q + (size_t)w * seg_cap;
+    for (uint32_t e0 = threadIdx.x; e0 < n; e0 += 4 * kFThreads) {
+      uint32_t pos[4], q[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const uint32_t e = e0 + u * kFThreads;
-      if (e < n) {
-        q[u] = q0 + log_q[e];
-        pos[u] = atomicAdd(&p.st[q[u]].ccount, 1u);
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t e = e0 + u * kFThreads;
+        if (e < n) {
+          q[u] = q0 + wq[e];
+          pos[u] = atomicAdd(&p.st[q[u]].ccount, 1u);
+        }
       }
-    }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const uint32_t e = e0 + u * kFThreads;
-      if (e < n) {
-        const BatchQuery &bq = p.qs[q[u]];
-        if (pos[u] < bq.cand_cap) p.cand[bq.cand_off + pos[u]] = log[e];
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t e = e0 + u * kFThreads;
+        if (e < n) {
+          const BatchQuery &bq = p.qs[q[u]];
+          if (pos[u] < bq.cand_cap) p.cand[bq.cand_off + pos[u]] = wl[e];
+        }
       }
     }
   }
@@ -431,7 +447,7 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict_
 // ---------------------------------------------------------------- launchers
 // query tiles | object ring | cuts | barriers and words
 size_t filter_smem_bytes(uint32_t qt) {
-  return (size_t)qt * (kQTileBytes + kQTile * 4) + (size_t)kStages * kOTileBytes + 256;
+  return (size_t)qt * (kQTileBytes + kQTile * 4) + (size_t)kStages * kOTileBytes + 512;
 }
 
 uint64_t bf16_table_bytes(uint64_t n) { return (n + kOTile - 1) / kOTile * kOTileBytes; }

@@ -9,13 +9,14 @@
 //
 // Operands, both K-major without swizzle (core matrices of 8 rows x 16 bytes; the
 // K-adjacent core matrix 128 B further on, the next 8 rows 256 B further on):
-//   table  each object's 16 attributes split x = hi + lo (bf16 each, |x - hi - lo|
-//          <= 2^-16 |x|); tiles of 128 objects: hi 4 KB, then lo 4 KB  (MMA A, M=128);
 //   query  a 16-wide row a[m] = sum of weights[attr[j]] over the j with attr[j] = m,
-//          split the same way; tiles of 128 queries: hi 4 KB, then lo 4 KB (MMA B, N=128).
+//          split a = hi + lo (bf16 each, |a - hi - lo| <= 2^-16 |a|); tiles of 128
+//          queries: hi 4 KB, then lo 4 KB                          (MMA A, M=128);
+//   table  each object's 16 attributes split the same way; tiles of 128 objects:
+//          hi 4 KB, then lo 4 KB                                    (MMA B, N=128).
 // One (object tile, query tile) pair is three MMAs M=128 N=128 K=16 into FP32 TMEM
-// (lane = object, column = query):
-//   D = Xhi.Ahi + Xlo.Ahi + Xhi.Alo        (the lo.lo term lies inside the bound)
+// (lane = query, column = object):
+//   D = Ahi.Xhi + Ahi.Xlo + Alo.Xhi        (the lo.lo term lies inside the bound)
 // Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
 //   E = 2^-13 * sum_m |weights[attr[m]]| * max|column attr[m]|  (+ 2^-100 terms for
 //   subnormal flushing).  Split and product errors give 3.1*2^-16, 48 FP32
@@ -26,18 +27,18 @@
 //   float t has D >= t - E, so the cut t - E (rounded down) loses none.
 //
 // Roles of the 576 threads of a CTA (one CTA per SM: TMEM is allocated whole):
-//   warps 0-15 epilogue: warp w reads TMEM lanes 32*(w%4).. (one object per
-//              thread), columns 32*(w/4).. (a quarter of a query tile);
-//              one compare per value against the column's cut and a warp vote;
-//              for the rare chunks with survivors a ballot per column gives the
-//              passing objects, appended to the warp's own segment of the CTA's
-//              survivor log in global memory (a count kept alike in every lane:
-//              no atomic in the MMA pipeline);
+//   warps 0-15 epilogue, four groups of four: group g drains accumulator g (every
+//              fourth pair); warp w reads TMEM lanes 32*(w%4).. (one query per
+//              thread, its cut in a register) over the pair's 128 objects, 32 at a
+//              time: the largest value against the cut and a warp vote; for the
+//              rare round trips with survivors each thread appends its passing
+//              objects to the warp's own segment of the CTA's survivor log in
+//              global memory (offsets from a warp scan: no atomic in the pipeline);
 //   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
 //              the CTA's query tiles once and object tiles into a 6-stage ring;
 //   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into four
-//              accumulators of 128 columns, so an epilogue warp held up by
-//              survivors on one pair delays the MMA only after three more pairs.
+//              accumulators of 128 columns, one per epilogue group, so a group held
+//              up by survivors on one pair delays the MMA only after three more pairs.
 // After the last tile the whole CTA moves its log into the queries' candidate
 // regions (global atomics, many in flight).  A survivor that finds the log full
 // flags its query for the exact single-query fallback.
@@ -68,14 +69,14 @@ constexpr uint32_t kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxQTPerCta = 16;
-constexpr uint32_t kAcc = kTmemCols / kQTile;  // TMEM accumulators in flight (4)
-constexpr uint32_t kWarpCols = kQTile / 4;      // columns of one epilogue warp per pair
-constexpr uint32_t kWarpChunks = kWarpCols / 32;
+constexpr uint32_t kAcc = kTmemCols / kOTile;  // TMEM accumulators in flight (4)
+static_assert(kAcc * 4 == kEpiWarps, "one group of four epilogue warps per accumulator");
+static_assert(kQTile == 128 && kOTile % 32 == 0, "a query per TMEM lane; whole 32-column round trips");
 constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
 
 // Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits
 // 7-9 = 1, 10-12 = 1), both K-major, N>>3 at bits 17-22, M>>4 at bits 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kQTile >> 3) << 17) | ((kOTile >> 4) << 24);
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kOTile >> 3) << 17) | ((kQTile >> 4) << 24);
 
 // Shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B (K-adjacent
 // core matrices), SBO 256 B (next 8 rows), version 1 (bit 46).
@@ -114,22 +115,57 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// 1 if any of the 8 values reaches its cut (v[i] >= c[i]), or acc was already 1: one
-// predicate carried through the compares.
-__device__ __forceinline__ uint32_t any_ge8(uint32_t acc, const uint32_t *v, float4 c0, float4 c1) {
-  uint32_t r;
-  asm("{\n .reg .pred p;\n setp.ne.u32 p, %1, 0;\n"
-      " setp.ge.or.f32 p, %2, %10, p;\n setp.ge.or.f32 p, %3, %11, p;\n"
-      " setp.ge.or.f32 p, %4, %12, p;\n setp.ge.or.f32 p, %5, %13, p;\n"
-      " setp.ge.or.f32 p, %6, %14, p;\n setp.ge.or.f32 p, %7, %15, p;\n"
-      " setp.ge.or.f32 p, %8, %16, p;\n setp.ge.or.f32 p, %9, %17, p;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(r)
-      : "r"(acc), "f"(__uint_as_float(v[0])), "f"(__uint_as_float(v[1])), "f"(__uint_as_float(v[2])),
-        "f"(__uint_as_float(v[3])), "f"(__uint_as_float(v[4])), "f"(__uint_as_float(v[5])),
-        "f"(__uint_as_float(v[6])), "f"(__uint_as_float(v[7])), "f"(c0.x), "f"(c0.y), "f"(c0.z), "f"(c0.w),
-        "f"(c1.x), "f"(c1.y), "f"(c1.z), "f"(c1.w));
+// Largest of 32 FP32 values (three-input max, a tree of depth 4).  A NaN value is
+// ignored, as a NaN also fails the compare it replaces.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
   return r;
+}
+__device__ __forceinline__ float max32(const uint32_t *v) {
+  float m[11];
+#pragma unroll
+  for (int i = 0; i < 10; ++i)
+    m[i] = max3f(__uint_as_float(v[3 * i]), __uint_as_float(v[3 * i + 1]), __uint_as_float(v[3 * i + 2]));
+  m[10] = fmaxf(__uint_as_float(v[30]), __uint_as_float(v[31]));
+  const float a = max3f(m[0], m[1], m[2]), b = max3f(m[3], m[4], m[5]), c = max3f(m[6], m[7], m[8]);
+  return max3f(max3f(a, b, c), m[9], m[10]);
+}
+
+// Survivors of one round trip (32 objects of this thread's query) when some thread of
+// the warp has a hit: each thread's passing objects go to the warp's log segment at
+// wcnt (the same in every lane) plus an exclusive warp scan of the counts.  Entries
+// past the segment flag their query for the exact fallback.  v: this thread's 32
+// values; obj0: the object of v[0]; nvalid: how many of the 32 objects exist.
+__device__ __forceinline__ void log_round(const uint32_t *v, float cut, uint32_t obj0, uint32_t nvalid, uint32_t ql,
+                                          uint32_t lane, uint32_t &wcnt, uint32_t seg_cap, uint2 *wlog,
+                                          uint16_t *wlog_q, BatchState *st0) {
+  uint32_t mask = 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(v[j]) >= cut ? 1u : 0u) << j;
+  if (nvalid < 32u) mask &= (1u << nvalid) - 1u;  // zero-padded rows past the table
+  const uint32_t cnt = __popc(mask);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  uint32_t e = wcnt + incl - cnt;
+  wcnt += __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (mask == 0u) return;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (mask & (1u << j)) {
+      if (e < seg_cap) {
+        wlog[e] = make_uint2(f2key(__uint_as_float(v[j])), obj0 + j);
+        wlog_q[e] = (uint16_t)ql;
+      } else {
+        atomicOr(&st0[ql].flags, 1u);  // lost: the exact scan answers it
+      }
+      ++e;
+    }
+  }
 }
 
 // Bounded wait that also gives up once another role of the CTA has aborted.
@@ -195,7 +231,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
     for (uint32_t b = 0; b < kAcc; ++b) {
       mbar_init(accf + b, 1);
-      mbar_init(acce + b, kEpiWarps);
+      mbar_init(acce + b, kEpiWarps / kAcc);  // the four warps of the accumulator's group
     }
     mbar_init(qfull, 1);
     mbar_init(mdone, 1);
@@ -265,10 +301,10 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
           tc_fence_after();
           const uint32_t qsa = smem_u32(sq + (size_t)i * kQTileBytes);
           const uint64_t ahi = smem_desc(qsa), alo = smem_desc(qsa + kQTileBytes / 2);
-          const uint32_t d = tmem + buf * kQTile;
-          tc_mma(d, xhi, ahi, 0u);
-          tc_mma(d, xlo, ahi, 1u);
-          tc_mma(d, xhi, alo, 1u);
+          const uint32_t d = tmem + buf * kOTile;
+          tc_mma(d, ahi, xhi, 0u);
+          tc_mma(d, ahi, xlo, 1u);
+          tc_mma(d, alo, xhi, 1u);
           tc_commit(accf + buf);
         }
         if (!ok) break;
@@ -280,81 +316,49 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    // warp w reads TMEM lanes 32*(w%4).. and columns kWarpCols*(w/4).. of each pair
-    const uint32_t quarter = warp & 3u, part = warp >> 2;
-    const uint32_t lane_addr = (quarter * 32u) << 16;
-    const uint32_t lt_mask = (1u << lane) - 1u;
+    // warps 4g..4g+3 drain accumulator g, i.e. every kAcc-th pair.  Thread (warp w,
+    // lane l) owns TMEM lane 32*(w%4)+l, one query of the pair's query tile, and reads
+    // its 128 objects in four round trips of 32 columns: one cut in a register, the
+    // largest value against it, a warp vote.  The four warps of an SM sub-partition
+    // belong to different groups, so they work on different pairs.
+    const uint32_t quarter = warp & 3u, grp = warp >> 2;
+    const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile;
     // this warp's log segment and its fill, the same in every lane (no atomics)
-    const uint32_t seg = warp * seg_cap;
+    uint2 *wlog = log + (size_t)warp * seg_cap;
+    uint16_t *wlog_q = log_q + (size_t)warp * seg_cap;
+    BatchState *st0 = p.st + q0;
     uint32_t wcnt = 0;
-    uint32_t seq = 0;
-    bool ok = true;
-    for (uint64_t t = tb; ok && t < te; ++t) {
-      const uint64_t obj = t * kOTile + quarter * 32u + lane;  // this thread's object
-      const bool valid = obj < p.r1;
-      for (uint32_t i = 0; i < nqt; ++i, ++seq) {
-        const uint32_t buf = seq % kAcc;
-        ok = __all_sync(0xFFFFFFFFu, fwait(accf + buf, (seq / kAcc) & 1u, limit, abort_flag));
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t col0 = i * kQTile + part * kWarpCols;  // CTA-relative query of column 0
-        const uint32_t tcol = tmem + lane_addr + buf * kQTile + part * kWarpCols;
-        // the warp's columns in one round trip; the accumulator is free as soon as
-        // they are in registers, and everything below works on the registers
-        uint32_t v[kWarpCols];
-#pragma unroll
-        for (uint32_t cc = 0; cc < kWarpChunks; ++cc) tmem_ld32(tcol + cc * 32u, v + cc * 32);
-        tmem_wait_ld();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(acce + buf);
-        // hot path: one compare per value against the column's cut, carried in a predicate
-        uint32_t h = 0;
-        {
-          const float4 *c4 = reinterpret_cast<const float4 *>(scut + col0);
-#pragma unroll
-          for (uint32_t cc = 0; cc < kWarpChunks; ++cc) {
-            uint32_t a = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a = any_ge8(a, v + cc * 32 + k * 8, c4[cc * 8 + 2 * k], c4[cc * 8 + 2 * k + 1]);
-            h |= a << cc;  // bit cc: chunk cc of 32 columns has a hit
-          }
-        }
-        const uint32_t hits = __reduce_or_sync(0xFFFFFFFFu, valid ? h : 0u);
-        if (hits == 0u) continue;  // common case
-        // cold path: per column of a chunk with a hit, a warp ballot gives the passing
-        // objects, appended to the warp's own log segment
+    const uint64_t npairs = (te - tb) * nqt;
+    uint32_t parity = 0;
+    uint32_t qt = grp % nqt;       // query tile and
+    uint64_t t = tb + grp / nqt;   // object tile of pair seq = t * nqt + qt
+    for (uint64_t seq = grp; seq < npairs; seq += kAcc, parity ^= 1u) {
+      if (!__all_sync(0xFFFFFFFFu, fwait(accf + grp, parity, limit, abort_flag))) break;
+      tc_fence_after();
+      const uint32_t ql = qt * kQTile + quarter * 32u + lane;  // this thread's query, CTA-relative
+      const float cut = scut[ql];
+      const uint64_t obj0 = t * kOTile;
 #pragma unroll 1
-        for (uint32_t cc = 0; cc < kWarpChunks; ++cc) {
-          if (!(hits & (1u << cc))) continue;
-          uint32_t u[32];
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            u[j] = v[j];
-#pragma unroll
-            for (uint32_t c2 = 1; c2 < kWarpChunks; ++c2) u[j] = cc == c2 ? v[c2 * 32 + j] : u[j];
-          }
-          const float *cut = scut + col0 + cc * 32u;
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float x = __uint_as_float(u[j]);
-            const bool pass = valid && x >= cut[j];
-            const uint32_t b = __ballot_sync(0xFFFFFFFFu, pass);
-            if (b) {
-              const uint32_t e = wcnt + __popc(b & lt_mask);
-              wcnt += __popc(b);
-              if (pass) {
-                const uint32_t ql = col0 + cc * 32u + j;
-                if (e < seg_cap) {
-                  log[seg + e] = make_uint2(f2key(x), (uint32_t)obj);
-                  log_q[seg + e] = (uint16_t)ql;
-                } else {
-                  atomicOr(&p.st[q0 + ql].flags, 1u);  // lost: the exact scan answers it
-                }
-              }
-            }
-          }
+      for (uint32_t rt = 0; rt < kOTile / 32u; ++rt) {
+        uint32_t v[32];
+        tmem_ld32(tcol + rt * 32u, v);
+        tmem_wait_ld();
+        if (rt + 1 == kOTile / 32u) {
+          // the accumulator is free once its last columns are in registers
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(acce + grp);
         }
+        // hot path: the largest of the 32 values against the thread's cut
+        if (!__any_sync(0xFFFFFFFFu, max32(v) >= cut)) continue;  // common case
+        const uint64_t ob = obj0 + rt * 32u;
+        const uint32_t nvalid = ob >= p.r1 ? 0u : p.r1 - ob >= 32u ? 32u : (uint32_t)(p.r1 - ob);
+        log_round(v, cut, (uint32_t)ob, nvalid, ql, lane, wcnt, seg_cap, wlog, wlog_q, st0);
+      }
+      qt += kAcc;
+      while (qt >= nqt) {
+        qt -= nqt;
+        ++t;
       }
     }
     if (lane == 0) wlog_n[warp] = min(wcnt, seg_cap);

@@ -31,17 +31,18 @@
 //              fourth pair); warp w reads TMEM lanes 32*(w%4).. (one query per
 //              thread, its cut in a register) over the pair's 128 objects, 32 at a
 //              time: the largest value against the cut and a warp vote; for the
-//              rare round trips with survivors each thread appends its passing
-//              objects to the warp's own segment of the CTA's survivor log in
-//              global memory (offsets from a warp scan: no atomic in the pipeline);
+//              rare round trips with survivors each thread with a hit writes one
+//              record (its passing objects as a bit mask) to the warp's own segment
+//              of the CTA's record log in global memory (a count kept alike in every
+//              lane: no atomic in the pipeline);
 //   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
 //              the CTA's query tiles once and object tiles into a 6-stage ring;
 //   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into four
 //              accumulators of 128 columns, one per epilogue group, so a group held
 //              up by survivors on one pair delays the MMA only after three more pairs.
-// After the last tile the whole CTA moves its log into the queries' candidate
-// regions (global atomics, many in flight).  A survivor that finds the log full
-// flags its query for the exact single-query fallback.
+// After the last tile the whole CTA expands its records into the queries' candidate
+// regions (a global atomic per record, many in flight).  A record that finds its
+// segment full flags its query for the exact single-query fallback.
 // Every mbarrier wait is bounded; a wait that runs out sets the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (bounded),
 // TMEM is freed and the error word is set (the host reports TOPK_ERR_TIMEOUT).
@@ -132,42 +133,6 @@ __device__ __forceinline__ float max32(const uint32_t *v) {
   return max3f(max3f(a, b, c), m[9], m[10]);
 }
 
-// Survivors of one round trip (32 objects of this thread's query) when some thread of
-// the warp has a hit: each thread's passing objects go to the warp's log segment at
-// wcnt (the same in every lane) plus an exclusive warp scan of the counts.  Entries
-// past the segment flag their query for the exact fallback.  v: this thread's 32
-// values; obj0: the object of v[0]; nvalid: how many of the 32 objects exist.
-__device__ __forceinline__ void log_round(const uint32_t *v, float cut, uint32_t obj0, uint32_t nvalid, uint32_t ql,
-                                          uint32_t lane, uint32_t &wcnt, uint32_t seg_cap, uint2 *wlog,
-                                          uint16_t *wlog_q, BatchState *st0) {
-  uint32_t mask = 0;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(v[j]) >= cut ? 1u : 0u) << j;
-  if (nvalid < 32u) mask &= (1u << nvalid) - 1u;  // zero-padded rows past the table
-  const uint32_t cnt = __popc(mask);
-  uint32_t incl = cnt;
-#pragma unroll
-  for (uint32_t o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  uint32_t e = wcnt + incl - cnt;
-  wcnt += __shfl_sync(0xFFFFFFFFu, incl, 31);
-  if (mask == 0u) return;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (mask & (1u << j)) {
-      if (e < seg_cap) {
-        wlog[e] = make_uint2(f2key(__uint_as_float(v[j])), obj0 + j);
-        wlog_q[e] = (uint16_t)ql;
-      } else {
-        atomicOr(&st0[ql].flags, 1u);  // lost: the exact scan answers it
-      }
-      ++e;
-    }
-  }
-}
-
 // Bounded wait that also gives up once another role of the CTA has aborted.
 __device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, uint64_t limit, volatile uint32_t *abort_flag) {
   for (uint64_t it = 0; it < limit; ++it) {
@@ -184,9 +149,9 @@ struct FilterArgs {
   const BatchQuery *qs;
   BatchState *st;
   uint2 *cand;
-  uint2 *log;          // per-CTA survivor logs: (key, id), log_cap entries each
-  uint16_t *log_q;     // query of each log entry, relative to the CTA's first query
-  uint32_t log_cap;
+  uint4 *rec;          // per-CTA survivor records, rec_cap each: (object bit mask,
+                       // first object, CTA-relative query, largest value's bits)
+  uint32_t rec_cap;
   uint32_t nq, nqt;    // queries, query tiles
   uint32_t qt_per_cta, ngroups, cpg;
   uint64_t tile0, tile1;  // object tiles of the chunk
@@ -216,10 +181,9 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   uint64_t *qfull = acce + kAcc, *mdone = qfull + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 1);
   volatile uint32_t *abort_flag = tmem_slot + 1;
-  uint32_t *wlog_n = tmem_slot + 2;  // entries in each epilogue warp's log segment
-  const uint32_t seg_cap = p.log_cap / kEpiWarps;
-  uint2 *log = p.log + (size_t)blockIdx.x * p.log_cap;
-  uint16_t *log_q = p.log_q + (size_t)blockIdx.x * p.log_cap;
+  uint32_t *wrec_n = tmem_slot + 2;  // records in each epilogue warp's segment
+  const uint32_t seg_cap = p.rec_cap / kEpiWarps;
+  uint4 *rec = p.rec + (size_t)blockIdx.x * p.rec_cap;
   const uint32_t q0 = qt0 * kQTile;  // first query of this CTA
 
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,7 +200,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     mbar_init(qfull, 1);
     mbar_init(mdone, 1);
     *abort_flag = 0u;
-    for (uint32_t w = 0; w < kEpiWarps; ++w) wlog_n[w] = 0u;
+    for (uint32_t w = 0; w < kEpiWarps; ++w) wrec_n[w] = 0u;
     fence_barrier_init();
   }
   // per-query cut: threshold float minus the bound, rounded down; +inf for columns
@@ -323,10 +287,10 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     // belong to different groups, so they work on different pairs.
     const uint32_t quarter = warp & 3u, grp = warp >> 2;
     const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile;
-    // this warp's log segment and its fill, the same in every lane (no atomics)
-    uint2 *wlog = log + (size_t)warp * seg_cap;
-    uint16_t *wlog_q = log_q + (size_t)warp * seg_cap;
+    // this warp's record segment and its fill, the same in every lane (no atomics)
+    uint4 *wrec = rec + (size_t)warp * seg_cap;
     BatchState *st0 = p.st + q0;
+    const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t wcnt = 0;
     const uint64_t npairs = (te - tb) * nqt;
     uint32_t parity = 0;
@@ -350,10 +314,23 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
           if (lane == 0) mbar_arrive(acce + grp);
         }
         // hot path: the largest of the 32 values against the thread's cut
-        if (!__any_sync(0xFFFFFFFFu, max32(v) >= cut)) continue;  // common case
-        const uint64_t ob = obj0 + rt * 32u;
-        const uint32_t nvalid = ob >= p.r1 ? 0u : p.r1 - ob >= 32u ? 32u : (uint32_t)(p.r1 - ob);
-        log_round(v, cut, (uint32_t)ob, nvalid, ql, lane, wcnt, seg_cap, wlog, wlog_q, st0);
+        const float m = max32(v);
+        const bool hit = m >= cut;
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
+        if (b == 0u) continue;  // common case
+        // cold path: each thread with a hit writes one record, its passing objects as
+        // a bit mask (expanded after the pipeline, where no accumulator waits on it)
+        const uint32_t e = wcnt + __popc(b & lt_mask);
+        wcnt += __popc(b);
+        if (hit) {
+          uint32_t mask = 0;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(v[j]) >= cut ? 1u : 0u) << j;
+          if (e < seg_cap)
+            wrec[e] = make_uint4(mask, (uint32_t)(obj0 + rt * 32u), ql, __float_as_uint(m));
+          else
+            atomicOr(&st0[ql].flags, 1u);  // lost: the exact scan answers the query
+        }
       }
       qt += kAcc;
       while (qt >= nqt) {
@@ -361,7 +338,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         ++t;
       }
     }
-    if (lane == 0) wlog_n[warp] = min(wcnt, seg_cap);
+    if (lane == 0) wrec_n[warp] = min(wcnt, seg_cap);
   }
 
   // ---------------------------------------------------------------- teardown
@@ -376,28 +353,36 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     if (threadIdx.x == 0) atomicExch(p.err, 1u);
     return;
   }
-  // the CTA's survivors into their queries' candidate regions (4 in flight a thread)
+  // the CTA's records into their queries' candidate regions: one atomic per record
+  // reserves its objects' slots (4 records in flight a thread).  A candidate's key
+  // is its filter score when it was its record's only object (the reduce checks it
+  // against the bound), else key 0, which the reduce does not check.
   for (uint32_t w = 0; w < kEpiWarps; ++w) {
-    const uint32_t n = wlog_n[w];
-    const uint2 *wl = log + (size_t)w * seg_cap;
-    const uint16_t *wq = log_q + (size_t)w * seg_cap;
+    const uint32_t n = wrec_n[w];
+    const uint4 *wr = rec + (size_t)w * seg_cap;
     for (uint32_t e0 = threadIdx.x; e0 < n; e0 += 4 * kFThreads) {
-      uint32_t pos[4], q[4];
+      uint4 r[4];
+      uint32_t pos[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const uint32_t e = e0 + u * kFThreads;
+        r[u] = make_uint4(0u, 0u, 0u, 0u);
         if (e < n) {
-          q[u] = q0 + wq[e];
-          pos[u] = atomicAdd(&p.st[q[u]].ccount, 1u);
+          r[u] = wr[e];
+          r[u].w = __popc(r[u].x) == 1 ? f2key(__uint_as_float(r[u].w)) : 0u;  // the key, as above
+          // objects past the table's last row (zero padding of the last tile) drop out
+          const uint32_t nvalid = r[u].y >= p.r1 ? 0u : p.r1 - r[u].y >= 32u ? 32u : (uint32_t)(p.r1 - r[u].y);
+          if (nvalid < 32u) r[u].x &= (1u << nvalid) - 1u;
+          if (r[u].x) pos[u] = atomicAdd(&p.st[q0 + r[u].z].ccount, (uint32_t)__popc(r[u].x));
         }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const uint32_t e = e0 + u * kFThreads;
-        if (e < n) {
-          const BatchQuery &bq = p.qs[q[u]];
-          if (pos[u] < bq.cand_cap) p.cand[bq.cand_off + pos[u]] = wl[e];
-        }
+        uint32_t mask = r[u].x;
+        if (!mask) continue;
+        const BatchQuery &bq = p.qs[q0 + r[u].z];
+        for (uint32_t at = pos[u]; mask; mask &= mask - 1u, ++at)
+          if (at < bq.cand_cap) p.cand[bq.cand_off + at] = make_uint2(r[u].w, r[u].y + (uint32_t)(__ffs(mask) - 1));
       }
     }
   }
@@ -508,9 +493,8 @@ FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms) 
 }
 
 cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
-                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint2 *log,
-                               uint16_t *log_q, uint32_t log_cap, uint64_t wait_limit, uint32_t *err,
-                               cudaStream_t s) {
+                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *rec,
+                               uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
   if (r0 % kOTile || f.grid == 0 || f.grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
   FilterArgs p{};
   p.xbf = xbf;
@@ -518,9 +502,8 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
   p.qs = qs;
   p.st = st;
   p.cand = cand;
-  p.log = log;
-  p.log_q = log_q;
-  p.log_cap = log_cap;
+  p.rec = rec;
+  p.rec_cap = rec_cap;
   p.nq = nq;
   p.nqt = f.nqt;
   p.qt_per_cta = f.qt_per_cta;

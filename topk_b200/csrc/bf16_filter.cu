@@ -12,9 +12,9 @@
 //   query  a 16-wide row a[m] = sum of weights[attr[j]] over the j with attr[j] = m,
 //          split a = hi + lo (bf16 each, |a - hi - lo| <= 2^-16 |a|); tiles of 128
 //          queries: hi 4 KB, then lo 4 KB                          (MMA A, M=128);
-//   table  each object's 16 attributes split the same way; tiles of 128 objects:
-//          hi 4 KB, then lo 4 KB                                    (MMA B, N=128).
-// One (object tile, query tile) pair is three MMAs M=128 N=128 K=16 into FP32 TMEM
+//   table  each object's 16 attributes split the same way; tiles of 256 objects:
+//          hi 8 KB, then lo 8 KB                                    (MMA B, N=256).
+// One (object tile, query tile) pair is three MMAs M=128 N=256 K=16 into FP32 TMEM
 // (lane = query, column = object):
 //   D = Ahi.Xhi + Ahi.Xlo + Alo.Xhi        (the lo.lo term lies inside the bound)
 // Bound (host-computed per query, BatchQuery::err): |D - s_ref| <= E with
@@ -27,19 +27,20 @@
 //   float t has D >= t - E, so the cut t - E (rounded down) loses none.
 //
 // Roles of the 576 threads of a CTA (one CTA per SM: TMEM is allocated whole):
-//   warps 0-15 epilogue, four groups of four: group g drains accumulator g (every
-//              fourth pair); warp w reads TMEM lanes 32*(w%4).. (one query per
-//              thread, its cut in a register) over the pair's 128 objects, 32 at a
-//              time: the largest value against the cut and a warp vote; for the
+//   warps 0-15 epilogue, two groups of eight: group g drains accumulator g (every
+//              second pair); warp w reads TMEM lanes 32*(w%4).. (one query per
+//              thread, its cut in a register) over half of the pair's 256 objects,
+//              32 at a time: the largest value against the cut and a warp vote; for the
 //              rare round trips with survivors each thread with a hit writes one
 //              record (its passing objects as a bit mask) to the warp's own segment
 //              of the CTA's record log in global memory (a count kept alike in every
 //              lane: no atomic in the pipeline);
 //   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
-//              the CTA's query tiles once and object tiles into a 6-stage ring;
-//   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into four
-//              accumulators of 128 columns, one per epilogue group, so a group held
-//              up by survivors on one pair delays the MMA only after three more pairs.
+//              the CTA's query tiles once and object tiles into a 5-stage ring;
+//   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into two
+//              accumulators of 256 columns, one per epilogue group (at N=256 an MMA
+//              takes longer to run than to issue, so one thread keeps the tensor
+//              core busy).
 // After the last tile the whole CTA expands its records into the queries' candidate
 // regions (a global atomic per record, many in flight).  A record that finds its
 // segment full flags its query for the exact single-query fallback.
@@ -60,19 +61,21 @@ namespace topk {
 
 namespace {
 
-constexpr uint32_t kOTile = 128;        // objects per tile (MMA M, TMEM lanes)
-constexpr uint32_t kOTileBytes = 8192;  // hi + lo of one object tile
-constexpr uint32_t kQTile = 128;        // queries per tile (MMA N, TMEM columns)
-constexpr uint32_t kQTileBytes = 8192;  // hi + lo of one query tile
-constexpr uint32_t kStages = 6;
+constexpr uint32_t kOTile = 256;         // objects per tile (MMA N, TMEM columns)
+constexpr uint32_t kOTileBytes = 16384;  // hi + lo of one object tile
+constexpr uint32_t kQTile = 128;         // queries per tile (MMA M, TMEM lanes)
+constexpr uint32_t kQTileBytes = 8192;   // hi + lo of one query tile
+constexpr uint32_t kStages = 5;
 constexpr uint32_t kEpiWarps = 16;
 constexpr uint32_t kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxQTPerCta = 16;
-constexpr uint32_t kAcc = kTmemCols / kOTile;  // TMEM accumulators in flight (4)
-static_assert(kAcc * 4 == kEpiWarps, "one group of four epilogue warps per accumulator");
-static_assert(kQTile == 128 && kOTile % 32 == 0, "a query per TMEM lane; whole 32-column round trips");
+constexpr uint32_t kAcc = kTmemCols / kOTile;            // TMEM accumulators in flight
+constexpr uint32_t kGroupWarps = kEpiWarps / kAcc;        // epilogue warps draining one accumulator
+constexpr uint32_t kWarpCols = kOTile * 4 / kGroupWarps;  // objects of one warp per pair
+static_assert(kGroupWarps % 4 == 0 && kEpiWarps % kAcc == 0, "whole TMEM lane quarters per group");
+static_assert(kQTile == 128 && kWarpCols % 32 == 0, "a query per TMEM lane; whole 32-column round trips");
 constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
 
 // Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
     for (uint32_t b = 0; b < kAcc; ++b) {
       mbar_init(accf + b, 1);
-      mbar_init(acce + b, kEpiWarps / kAcc);  // the four warps of the accumulator's group
+      mbar_init(acce + b, kGroupWarps);  // the epilogue warps of the accumulator's group
     }
     mbar_init(qfull, 1);
     mbar_init(mdone, 1);
@@ -280,13 +283,13 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    // warps 4g..4g+3 drain accumulator g, i.e. every kAcc-th pair.  Thread (warp w,
-    // lane l) owns TMEM lane 32*(w%4)+l, one query of the pair's query tile, and reads
-    // its 128 objects in four round trips of 32 columns: one cut in a register, the
-    // largest value against it, a warp vote.  The four warps of an SM sub-partition
-    // belong to different groups, so they work on different pairs.
-    const uint32_t quarter = warp & 3u, grp = warp >> 2;
-    const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile;
+    // warps kGroupWarps*g.. drain accumulator g, i.e. every kAcc-th pair.  Thread
+    // (warp w, lane l) owns TMEM lane 32*(w%4)+l, one query of the pair's query tile,
+    // and reads kWarpCols of its objects in round trips of 32 columns: one cut in a
+    // register, the largest value against it, a warp vote.  Each SM sub-partition
+    // holds warps of both groups, which work on different pairs.
+    const uint32_t quarter = warp & 3u, grp = warp / kGroupWarps, part = (warp % kGroupWarps) >> 2;
+    const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile + part * kWarpCols;
     // this warp's record segment and its fill, the same in every lane (no atomics)
     uint4 *wrec = rec + (size_t)warp * seg_cap;
     BatchState *st0 = p.st + q0;
@@ -301,13 +304,13 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
       tc_fence_after();
       const uint32_t ql = qt * kQTile + quarter * 32u + lane;  // this thread's query, CTA-relative
       const float cut = scut[ql];
-      const uint64_t obj0 = t * kOTile;
+      const uint64_t obj0 = t * kOTile + part * kWarpCols;
 #pragma unroll 1
-      for (uint32_t rt = 0; rt < kOTile / 32u; ++rt) {
+      for (uint32_t rt = 0; rt < kWarpCols / 32u; ++rt) {
         uint32_t v[32];
         tmem_ld32(tcol + rt * 32u, v);
         tmem_wait_ld();
-        if (rt + 1 == kOTile / 32u) {
+        if (rt + 1 == kWarpCols / 32u) {
           // the accumulator is free once its last columns are in registers
           tc_fence_before();
           __syncwarp();

@@ -11,7 +11,7 @@ constexpr uint32_t kBatchGroup = 64;   // queries scored per staged table tile (
 constexpr uint32_t kBatchMaxD = 64;    // table width the FP32 scorer stages
 constexpr uint32_t kBatchBootRows = 8192;  // rows of the exact bootstrap
 constexpr uint32_t kBf16MaxD = 16;         // table width of the BF16 tensor-core filter (MMA K)
-constexpr uint32_t kBf16LogCap = 65536;    // survivor records (16 B) per filter CTA
+constexpr uint32_t kBf16LogCap = 32768;    // survivor records (32 values + header, 136 B) per filter CTA
 
 // Per-query descriptor (device, read-only during a batch).
 struct BatchQuery {
@@ -65,8 +65,8 @@ struct FilterPlan {
 FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms);
 // r0 must be a multiple of 128; log/log_q hold grid * log_cap entries.
 cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
-                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *rec,
-                               uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s);
+                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *recv,
+                               uint2 *rech, uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s);
 // Learned k-th-score model (mlp.cu): in -> 64 -> 64 -> 1 ReLU MLP, features of
 // feature_dim(d) values per query from the partition statistics ([P][d] each).
 constexpr uint32_t kHid = 64;

@@ -31,10 +31,10 @@
 //              second pair); warp w reads TMEM lanes 32*(w%4).. (one query per
 //              thread, its cut in a register) over half of the pair's 256 objects,
 //              32 at a time: the largest value against the cut and a warp vote; for the
-//              rare round trips with survivors each thread with a hit writes one
-//              record (its passing objects as a bit mask) to the warp's own segment
-//              of the CTA's record log in global memory (a count kept alike in every
-//              lane: no atomic in the pipeline);
+//              rare round trips with survivors each thread with a hit stores its 32
+//              values as one record in the warp's own segment of the CTA's record
+//              log in global memory (a count kept alike in every lane: no atomic and
+//              no dependent work while the accumulator is held);
 //   warp 16    producer: bulk-copies (cp.async.bulk, no tensor map, no multicast)
 //              the CTA's query tiles once and object tiles into a 5-stage ring;
 //   warp 17    allocates the 512 TMEM columns; lane 0 issues the MMAs into two
@@ -42,8 +42,9 @@
 //              takes longer to run than to issue, so one thread keeps the tensor
 //              core busy).
 // After the last tile the whole CTA expands its records into the queries' candidate
-// regions (a global atomic per record, many in flight).  A record that finds its
-// segment full flags its query for the exact single-query fallback.
+// regions: the values are compared with the cut again and the passing objects take
+// their slots with one global atomic per record.  A record that finds its segment
+// full flags its query for the exact single-query fallback.
 // Every mbarrier wait is bounded; a wait that runs out sets the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (bounded),
 // TMEM is freed and the error word is set (the host reports TOPK_ERR_TIMEOUT).
@@ -152,8 +153,9 @@ struct FilterArgs {
   const BatchQuery *qs;
   BatchState *st;
   uint2 *cand;
-  uint4 *rec;          // per-CTA survivor records, rec_cap each: (object bit mask,
-                       // first object, CTA-relative query, largest value's bits)
+  uint4 *recv;         // per-CTA survivor records, rec_cap each: 32 FP32 values
+                       // (8 x uint4) of one query over 32 consecutive objects
+  uint2 *rech;         // and their headers: (first object, CTA-relative query)
   uint32_t rec_cap;
   uint32_t nq, nqt;    // queries, query tiles
   uint32_t qt_per_cta, ngroups, cpg;
@@ -186,7 +188,8 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   volatile uint32_t *abort_flag = tmem_slot + 1;
   uint32_t *wrec_n = tmem_slot + 2;  // records in each epilogue warp's segment
   const uint32_t seg_cap = p.rec_cap / kEpiWarps;
-  uint4 *rec = p.rec + (size_t)blockIdx.x * p.rec_cap;
+  uint4 *recv = p.recv + (size_t)blockIdx.x * p.rec_cap * 8u;
+  uint2 *rech = p.rech + (size_t)blockIdx.x * p.rec_cap;
   const uint32_t q0 = qt0 * kQTile;  // first query of this CTA
 
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,7 +294,8 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     const uint32_t quarter = warp & 3u, grp = warp / kGroupWarps, part = (warp % kGroupWarps) >> 2;
     const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile + part * kWarpCols;
     // this warp's record segment and its fill, the same in every lane (no atomics)
-    uint4 *wrec = rec + (size_t)warp * seg_cap;
+    uint4 *wrecv = recv + (size_t)warp * seg_cap * 8u;
+    uint2 *wrech = rech + (size_t)warp * seg_cap;
     BatchState *st0 = p.st + q0;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t wcnt = 0;
@@ -321,18 +325,20 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         const bool hit = m >= cut;
         const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
         if (b == 0u) continue;  // common case
-        // cold path: each thread with a hit writes one record, its passing objects as
-        // a bit mask (expanded after the pipeline, where no accumulator waits on it)
+        // cold path: each thread with a hit stores its 32 values as one record (eight
+        // asynchronous 16-byte stores); which objects pass is worked out after the
+        // pipeline, where no accumulator waits on it
         const uint32_t e = wcnt + __popc(b & lt_mask);
         wcnt += __popc(b);
         if (hit) {
-          uint32_t mask = 0;
+          if (e < seg_cap) {
+            uint4 *dst = wrecv + (size_t)e * 8u;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(v[j]) >= cut ? 1u : 0u) << j;
-          if (e < seg_cap)
-            wrec[e] = make_uint4(mask, (uint32_t)(obj0 + rt * 32u), ql, __float_as_uint(m));
-          else
+            for (int c = 0; c < 8; ++c) dst[c] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+            wrech[e] = make_uint2((uint32_t)(obj0 + rt * 32u), ql);
+          } else {
             atomicOr(&st0[ql].flags, 1u);  // lost: the exact scan answers the query
+          }
         }
       }
       qt += kAcc;
@@ -356,37 +362,41 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     if (threadIdx.x == 0) atomicExch(p.err, 1u);
     return;
   }
-  // the CTA's records into their queries' candidate regions: one atomic per record
-  // reserves its objects' slots (4 records in flight a thread).  A candidate's key
-  // is its filter score when it was its record's only object (the reduce checks it
-  // against the bound), else key 0, which the reduce does not check.
+  // the CTA's records into their queries' candidate regions: each thread takes a
+  // record, compares its values with the query's cut again (the same cut, still in
+  // shared memory) and reserves the passing objects' slots with one atomic
   for (uint32_t w = 0; w < kEpiWarps; ++w) {
     const uint32_t n = wrec_n[w];
-    const uint4 *wr = rec + (size_t)w * seg_cap;
-    for (uint32_t e0 = threadIdx.x; e0 < n; e0 += 4 * kFThreads) {
-      uint4 r[4];
-      uint32_t pos[4];
+    const uint4 *wv = recv + (size_t)w * seg_cap * 8u;
+    const uint2 *wh = rech + (size_t)w * seg_cap;
+    for (uint32_t e = threadIdx.x; e < n; e += kFThreads) {
+      const uint2 h = wh[e];
+      uint32_t v[32];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const uint32_t e = e0 + u * kFThreads;
-        r[u] = make_uint4(0u, 0u, 0u, 0u);
-        if (e < n) {
-          r[u] = wr[e];
-          r[u].w = __popc(r[u].x) == 1 ? f2key(__uint_as_float(r[u].w)) : 0u;  // the key, as above
-          // objects past the table's last row (zero padding of the last tile) drop out
-          const uint32_t nvalid = r[u].y >= p.r1 ? 0u : p.r1 - r[u].y >= 32u ? 32u : (uint32_t)(p.r1 - r[u].y);
-          if (nvalid < 32u) r[u].x &= (1u << nvalid) - 1u;
-          if (r[u].x) pos[u] = atomicAdd(&p.st[q0 + r[u].z].ccount, (uint32_t)__popc(r[u].x));
+      for (int c = 0; c < 8; ++c) {
+        const uint4 x = wv[(size_t)e * 8u + c];
+        v[4 * c] = x.x;
+        v[4 * c + 1] = x.y;
+        v[4 * c + 2] = x.z;
+        v[4 * c + 3] = x.w;
+      }
+      const float cut = scut[h.y];
+      uint32_t mask = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) mask |= (__uint_as_float(v[j]) >= cut ? 1u : 0u) << j;
+      // objects past the table's last row (zero padding of the last tile) drop out
+      const uint32_t nvalid = h.x >= p.r1 ? 0u : p.r1 - h.x >= 32u ? 32u : (uint32_t)(p.r1 - h.x);
+      if (nvalid < 32u) mask &= (1u << nvalid) - 1u;
+      if (!mask) continue;
+      const uint32_t q = q0 + h.y;
+      uint32_t at = atomicAdd(&p.st[q].ccount, (uint32_t)__popc(mask));
+      const BatchQuery &bq = p.qs[q];
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (mask & (1u << j)) {
+          if (at < bq.cand_cap) p.cand[bq.cand_off + at] = make_uint2(f2key(__uint_as_float(v[j])), h.x + j);
+          ++at;
         }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        uint32_t mask = r[u].x;
-        if (!mask) continue;
-        const BatchQuery &bq = p.qs[q0 + r[u].z];
-        for (uint32_t at = pos[u]; mask; mask &= mask - 1u, ++at)
-          if (at < bq.cand_cap) p.cand[bq.cand_off + at] = make_uint2(r[u].w, r[u].y + (uint32_t)(__ffs(mask) - 1));
-      }
     }
   }
 }
@@ -496,8 +506,8 @@ FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms) 
 }
 
 cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
-                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *rec,
-                               uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
+                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *recv,
+                               uint2 *rech, uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
   if (r0 % kOTile || f.grid == 0 || f.grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
   FilterArgs p{};
   p.xbf = xbf;
@@ -505,7 +515,8 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
   p.qs = qs;
   p.st = st;
   p.cand = cand;
-  p.rec = rec;
+  p.recv = recv;
+  p.rech = rech;
   p.rec_cap = rec_cap;
   p.nq = nq;
   p.nqt = f.nqt;

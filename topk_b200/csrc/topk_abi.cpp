@@ -131,7 +131,7 @@ struct topk_table_s {
   DevBuf b_q, b_st, b_best, b_cand, b_ids, b_scores, b_count, b_thr;
   // BF16 filter: split copy of the table (rebuilt when the table changed), the
   // per-column max |x| it was built from, the batch's query tiles and error word
-  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_feat, b_pred;
+  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logh, b_feat, b_pred;
   uint64_t data_version = 1, xbf_version = 0;
   std::vector<float> absmax;
   bool xbf_usable = false;
@@ -587,7 +587,7 @@ int ensure(topk_table_s::DevBuf &b, size_t bytes) {
 void free_batch_buffers(topk_table_t h) {
   for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
                                   &h->b_thr, &h->xbf, &h->xbf_absmax, &h->b_abf, &h->b_err, &h->b_log,
-                                  &h->b_feat, &h->b_pred}) {
+                                  &h->b_logh, &h->b_feat, &h->b_pred}) {
     cudaFree(b->p);
     b->p = nullptr;
     b->bytes = 0;
@@ -724,7 +724,8 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     // survivor logs: one per filter CTA (at most max(num_sms, query groups) CTAs)
     const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms);
     log_ctas = std::max<uint64_t>((uint64_t)h->num_sms, fp.ngroups);
-    if ((st = ensure(h->b_log, log_ctas * kBf16LogCap * sizeof(uint4))) != TOPK_OK) return st;
+    if ((st = ensure(h->b_log, log_ctas * kBf16LogCap * 8 * sizeof(uint4))) != TOPK_OK) return st;
+    if ((st = ensure(h->b_logh, log_ctas * kBf16LogCap * sizeof(uint2))) != TOPK_OK) return st;
     CK(cudaMemcpyAsync(h->b_abf.p, habf.data(), habf.size(), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(h->b_err.p, 0, sizeof(uint32_t), s));
     CK(cudaStreamSynchronize(s));  // habf is pageable and goes out of scope
@@ -773,7 +774,8 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       const FilterPlan fp = plan_bf16_filter(nqq, r, e, h->num_sms);
       if (fp.grid > log_ctas) return fail(TOPK_ERR_STATE, "filter grid %llu above its logs", (unsigned long long)fp.grid);
       CK(launch_bf16_filter(fp, static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf.p), r, e,
-                            dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p), kBf16LogCap, h->wait_limit,
+                            dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
+                            static_cast<uint2 *>(h->b_logh.p), kBf16LogCap, h->wait_limit,
                             static_cast<uint32_t *>(h->b_err.p), s));
     } else {
       CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, s));

@@ -721,7 +721,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     }
     if ((st = ensure(h->b_abf, habf.size())) != TOPK_OK) return st;
     if ((st = ensure(h->b_err, sizeof(uint32_t))) != TOPK_OK) return st;
-    // survivor logs: one per filter CTA (at most max(num_sms, query groups) CTAs)
+    // survivor records: one log per filter CTA (at most max(num_sms, query groups) CTAs)
     const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms);
     log_ctas = std::max<uint64_t>((uint64_t)h->num_sms, fp.ngroups);
     if ((st = ensure(h->b_log, log_ctas * kBf16LogCap * 8 * sizeof(uint4))) != TOPK_OK) return st;

@@ -24,6 +24,10 @@ flush is needed between queries.
           2^16 rows, the learned model fitted on 10^5 exactly labelled queries,
           2000 fresh queries by full scan, plain pruning and learned pruning:
           partitions scanned, fallback rate, speed-up, identical results.
+  c5       (with --c5, or alone with --only c5) the full chosen form: 16384 queries
+          (k log-uniform in [1, 1024]) over a 2^28 x 16 table mixed 1/3 each
+          independent/correlated/anticorrelated, plain batched FP32 against the
+          learned start with the BF16 filter, identical results checked.
 
 Multi-GPU (torchrun): every rank holds its own replica and runs the same query
 steps (weak scaling, no collective on the data path); time = max over ranks.
@@ -52,6 +56,8 @@ QS = (2, 4, 8, 16)
 KS = (16, 64, 256, 1024)
 BATCH_N = 1 << 26  # batched workload: 4096 queries over a 2^26 x 16 table
 BATCH_Q = 4096
+C5_N = 1 << 28  # full-form workload: 16384 queries over a mixed 2^28 x 16 table
+C5_Q = 16384
 
 
 def weights_u01(d, seed):
@@ -211,9 +217,10 @@ def run_reference(args):
     return 0
 
 
-def batch_queries(nq, d, seed=3):
+def batch_queries(nq, d, seed=3, k_log=False):
     """The batched workload's queries: random attribute subsets of size U{2..16}
-    (ascending), weights U(0,1] on the 2^-24 grid, k U{1..1024}; seeded."""
+    (ascending), weights U(0,1] on the 2^-24 grid, k U{1..1024} (log-uniform in
+    [1, 1024] with k_log); seeded."""
     rng = np.random.default_rng(seed)
     W = ((rng.integers(0, 1 << 24, size=(nq, d)) + 1) * 2.0 ** -24).astype(np.float32)
     A = np.zeros((nq, 16), np.uint8)
@@ -222,17 +229,22 @@ def batch_queries(nq, d, seed=3):
         q = int(rng.integers(2, 17))
         A[j, :q] = np.sort(rng.choice(d, size=q, replace=False))
         qqs[j] = q
-    ks = rng.integers(1, 1025, size=nq).astype(np.uint64)
+    if k_log:
+        ks = np.exp(rng.uniform(0.0, np.log(1025.0), nq)).astype(np.uint64).clip(1, 1024)
+    else:
+        ks = rng.integers(1, 1025, size=nq).astype(np.uint64)
     return ks, W, A, qqs
 
 
-def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "bf16", "learned_bf16")):
-    """Batched workload: nq queries over an n x 16 independent table, plain batched
-    FP32 against the BF16 tensor-core filter (same results, checked); device time of
-    the batch kernels (CUDA events inside topk_query_batch), max over ranks."""
-    ks, W, A, qqs = batch_queries(nq, d)
+def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "bf16", "learned_bf16"),
+                table_dist=None, k_log=False, fp32_reps=1, label="independent"):
+    """Batched workload: nq queries over an n x 16 table (independent unless
+    table_dist says otherwise), plain batched FP32 against the BF16 tensor-core filter
+    without and with the learned start (same results, checked); device time of the
+    batch kernels (CUDA events inside topk_query_batch), max over ranks."""
+    ks, W, A, qqs = batch_queries(nq, d, k_log=k_log)
     t = T.Table(n, d, device=device)
-    t.generate(T.DIST_INDEPENDENT, 0)
+    t.generate(T.DIST_INDEPENDENT if table_dist is None else table_dist, 0)
     t.normalize()
     out = {}
     res = {}
@@ -243,8 +255,8 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
         fit = t.learned_fit(n_train=16384, n_val=2048, kmin=1, kmax=1024, qmin=2, qmax=16, epochs=40,
                             miss_rate=0.01, seed=1)
         fit["total_s"] = time.perf_counter() - f0
-    for name, method, r in (("fp32", T.BATCH_FP32, 1), ("bf16", T.BATCH_BF16, reps),
-                            ("learned_bf16", T.BATCH_LEARNED, reps)):
+    for name, method, r in (("fp32", T.BATCH_FP32, fp32_reps), ("bf16", T.BATCH_BF16, reps),
+                            ("learned_bf16", T.BATCH_LEARNED, reps), ("auto", T.BATCH_AUTO, reps)):
         if name not in methods:
             continue
         t.set_batch_method(method)
@@ -283,19 +295,31 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
     tf_peak = float(peaks.get("bf16_tflops", 1590.0))
     flops = 2.0 * nq * 16 * n  # the dense Q x 16 by 16 x n contraction
     speed = {f"speedup_{m}_vs_fp32": out["fp32"]["device_ms"] / out[m]["device_ms"]
-             for m in ("bf16", "learned_bf16") if m in out and "fp32" in out}
-    tf = flops / (out["bf16"]["device_ms"] * 1e-3) / 1e12 if "bf16" in out else None
+             for m in ("bf16", "learned_bf16", "auto") if m in out and "fp32" in out}
+    fm = next((m for m in ("bf16", "learned_bf16") if m in out), None)
+    tf = flops / (out[fm]["device_ms"] * 1e-3) / 1e12 if fm else None
     out.update(speed)
     out.update({
-        "workload": f"{nq} queries, n={n} x 16 FP32 independent, |attrs| U{{2..16}}, k U{{1..1024}}, "
-                    "weights U(0,1]",
+        "workload": f"{nq} queries, n={n} x 16 FP32 {label}, |attrs| U{{2..16}}, "
+                    f"k {'log-uniform in [1, 1024]' if k_log else 'U{1..1024}'}, weights U(0,1]",
         "identical_results": same,
         "roofline_bf16": {"bound": "tensor", "achieved": tf, "peak": tf_peak, "unit": "TFLOP/s",
-                          "frac": tf / tf_peak if tf else None,
+                          "frac": tf / tf_peak if tf else None, "method": fm,
                           "note": "dense-contraction flops 2*Q*16*n over the whole batch's device time; "
                                   "the filter issues 3 BF16 MMA passes (hi/lo split) per tile"},
     })
     return out
+
+
+def run_c5(T, torch, dist, device, n, nq, methods=("fp32", "learned_bf16")):
+    """Full chosen form against plain: an n x 16 table whose objects are 1/3 each
+    independent, correlated and anticorrelated (object i takes distribution i mod 3),
+    a stream of nq queries (attribute subsets of size U{2..16}, weights U(0,1], k
+    log-uniform in [1, 1024]) answered as one batch by plain batched FP32 and by the
+    BF16 filter with the learned start (partitions of 2^16 rows, model fitted on
+    16384 + 2048 exactly labelled queries); identical results checked."""
+    return run_batched(T, torch, dist, device, n, nq, reps=2, methods=methods, table_dist=T.DIST_MIXED,
+                       k_log=True, fp32_reps=1, label="mixed 1/3 independent/correlated/anticorrelated")
 
 
 def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000, seed=4):
@@ -371,8 +395,13 @@ def main():
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--only", choices=["batched", "pruned"], default=None,
+    ap.add_argument("--only", choices=["batched", "pruned", "c5"], default=None,
                     help="run one secondary workload alone (no JSON line; for profiling)")
+    ap.add_argument("--c5", action="store_true",
+                    help="add the full-form workload: 16384 queries over a mixed 2^28 x 16 table")
+    ap.add_argument("--c5-n", type=int, default=C5_N)
+    ap.add_argument("--c5-q", type=int, default=C5_Q)
+    ap.add_argument("--c5-methods", default="fp32,learned_bf16")
     ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--no-pruned", action="store_true")
     ap.add_argument("--pruned-n", type=int, default=1 << 27)
@@ -390,6 +419,8 @@ def main():
         if args.only == "batched":
             out = run_batched(T, torch, None, 0, args.batched_n, args.batched_q,
                               methods=tuple(args.batched_methods.split(",")))
+        elif args.only == "c5":
+            out = run_c5(T, torch, None, 0, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
         else:
             out = run_pruned(T, 0, args.pruned_n, n_test=args.pruned_queries)
         print(json.dumps(out))
@@ -540,6 +571,8 @@ def main():
                                         methods=tuple(args.batched_methods.split(",")))
     if not args.no_pruned and rank == 0:
         result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
+    if args.c5:
+        result["c5"] = run_c5(T, torch, dist, local, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -276,7 +276,8 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
             dev, wall = float(tt[0].item()), float(tt[1].item())
         out[name] = {"device_ms": dev, "queries_per_s": nq * 1000.0 / dev, "e2e_ms": wall,
                      "e2e_queries_per_s": nq * 1000.0 / wall, "fallbacks": st["fallbacks"],
-                     "candidates": st["candidates"], "method_ran": st["method"]}
+                     "candidates": st["candidates"], "method_ran": st["method"],
+                     "switched_fp32": st["switched_fp32"]}
         if name != "fp32":
             out[name]["max_err_ratio"] = st["max_err_ratio"]
         if name == "learned_bf16":

@@ -253,18 +253,20 @@ int topk_set_fault_injection(topk_table_t h, int mode);
 /* Methods of topk_query_batch (no reference counterpart; results are identical). */
 #define TOPK_BATCH_AUTO 0  /* TOPK_BATCH_LEARNED with a fitted model, else TOPK_BATCH_BF16
                             * where it applies, else TOPK_BATCH_FP32.  Once a BF16 batch
-                            * overflows the candidate regions of more than a quarter of
-                            * its queries (scores too dense around the thresholds, e.g.
+                            * hands more than three quarters of its queries to the FP32
+                            * scorer (scores too dense around the thresholds, e.g.
                             * anticorrelated data), later AUTO batches on the same table
-                            * use the FP32 scorer */
+                            * use the FP32 scorer from the start */
 #define TOPK_BATCH_LOOP 1  /* one fused single-query scan per query */
 #define TOPK_BATCH_FP32 2  /* batched plain FP32: each table tile scored for 64 queries */
 #define TOPK_BATCH_BF16 3  /* BF16 tensor-core filter (tcgen05) with a per-query error
                             * bound; candidates rescored exactly in FP32.  Applies to
                             * d <= 16 with finite table values and weights of magnitude
-                            * <= 2^60; other batches run TOPK_BATCH_FP32.  A query whose
-                            * candidate region overflows is answered again by a batch
-                            * with the FP32 scorer */
+                            * <= 2^60; other batches run TOPK_BATCH_FP32.  Hybrid: a
+                            * query for which the filter passes too much (tied or dense
+                            * scores at its threshold: more than 2k + 2048 candidates in
+                            * a chunk, or lost ones) moves to the exact FP32 scorer for
+                            * the rest of the batch, inside the same call */
 #define TOPK_BATCH_LEARNED 4 /* TOPK_BATCH_BF16 (or FP32) whose per-query threshold starts
                               * at the learned cut (prediction - margin) * S instead of a
                               * bootstrap over the first rows; a query left with fewer
@@ -287,6 +289,10 @@ int topk_last_batch_stats(topk_table_t h, double *device_ms, uint64_t *fallbacks
  * rescored candidates (must stay below 1; 0 for the other methods), and the
  * queries whose learned start was too high (answered again without it). */
 int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uint64_t *learned_misses);
+
+/* How many queries of the last topk_query_batch the hybrid BF16 batch moved to the
+ * exact FP32 scorer (0 for the other methods). */
+int topk_last_batch_switched(topk_table_t h, uint64_t *switched);
 
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */

@@ -259,4 +259,34 @@ def test_batch_bf16_overflow_falls_back_exactly():
         qqs = np.array([3, 3, 3], np.uint32)
         check_batch(t, tn, ks, W, A, qqs)
         st = t.last_batch_stats()
-        assert st["method"] == BF16 and st["fallbacks"] >= 1
+        # dense scores: the filter hands the queries to the exact FP32 scorer
+        assert st["method"] == BF16 and st["switched_fp32"] >= 1
+
+
+def test_batch_bf16_hybrid_redoes_discarded_chunks():
+    """Objects just below the top score (inside the filter's error band, below the
+    exact threshold) fill the candidate regions under the filter in a middle chunk
+    (rows [32768, 65536)) and in the last one; the filter loses candidates there, the
+    query moves to the exact FP32 scorer, which answers the discarded chunk again
+    (with the next chunk, and after the loop for the last one): exact results."""
+    n, d = 100003, 3
+    rng = np.random.default_rng(11)
+    raw = (rng.integers(0, 1 << 23, size=(d, n)) * 2.0 ** -24).astype(np.float32)  # [0, 0.5)
+    raw[:, 0] = 0.0
+    raw[:, 100:110] = 1.0  # the top, in the bootstrap rows
+    near = np.float32(1.0 - 2.0 ** -20)
+    raw[:, 40000:45000] = near
+    raw[:, 70000:75000] = near
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.set_batch_method(BF16)
+        ks = np.array([5, 10, 64, 3000], np.uint64)
+        W = np.ones((4, d), np.float32)
+        A = np.tile(np.arange(d, dtype=np.uint8), (4, 1))
+        qqs = np.full(4, d, np.uint32)
+        check_batch(t, tn, ks, W, A, qqs)
+        st = t.last_batch_stats()
+        assert st["method"] == BF16 and st["switched_fp32"] >= 1

@@ -86,6 +86,7 @@ SIGNATURES = [
     ("topk_set_batch_method", C.c_int, [_H, C.c_int]),
     ("topk_last_batch_stats", C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    ("topk_last_batch_switched", C.c_int, [_H, C.POINTER(C.c_uint64)]),
     ("topk_query_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, _f32p,
                                      _u8p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("topk_last_stats", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -87,13 +87,16 @@ __global__ void __launch_bounds__(kBT) batch_bootstrap_kernel(const float *__res
 
 // ---------------------------------------------------------------- FP32 scorer
 // Block (query group g, tile): rows [row0, row0 + OPT*256) of the chunk, all d
-// columns staged in shared memory once, scored for the group's queries.
+// columns staged in shared memory once, scored for the group's queries.  With a
+// query list the groups are formed from qlist[0..nq) (the queries a hybrid batch has
+// moved to this scorer), else from queries 0..nq-1.
 template <int OPT>
 __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__restrict__ table, uint64_t ld,
                                                                uint32_t d, uint64_t r0, uint64_t r1,
                                                                const BatchQuery *__restrict__ qs, uint32_t nq,
                                                                BatchState *__restrict__ st,
-                                                               uint2 *__restrict__ cand) {
+                                                               uint2 *__restrict__ cand,
+                                                               const uint32_t *__restrict__ qlist) {
   constexpr uint32_t TO = kBT * OPT;
   extern __shared__ __align__(16) unsigned char smem[];
   float *xs = reinterpret_cast<float *>(smem);                       // d x TO
@@ -101,6 +104,7 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
   float *gw = reinterpret_cast<float *>(gattr + kBatchGroup * kBatchMaxQ);  // kBatchGroup x kBatchMaxQ
   uint32_t *gthr = reinterpret_cast<uint32_t *>(gw + kBatchGroup * kBatchMaxQ);
   uint32_t *gqq = gthr + kBatchGroup;
+  uint32_t *gq = gqq + kBatchGroup;  // query of each group slot
 
   const int t = threadIdx.x;
   // block -> (query group, tile), groups fastest: the blocks of one tile run together
@@ -116,14 +120,16 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
     const float *col = table + (uint64_t)m * ld + base;
     for (uint32_t i = t; i < TO; i += kBT) xs[m * TO + i] = i < valid ? __ldcs(col + i) : 0.0f;
   }
+  for (uint32_t j = t; j < nqg; j += kBT) gq[j] = qlist ? qlist[q0 + j] : q0 + j;
+  __syncthreads();
   for (uint32_t j = t; j < nqg * kBatchMaxQ; j += kBT) {
     const uint32_t qj = j / kBatchMaxQ, m = j % kBatchMaxQ;
-    gattr[j] = qs[q0 + qj].attr[m];
-    gw[j] = qs[q0 + qj].w[m];
+    gattr[j] = qs[gq[qj]].attr[m];
+    gw[j] = qs[gq[qj]].w[m];
   }
   for (uint32_t j = t; j < nqg; j += kBT) {
-    gthr[j] = st[q0 + j].thr;
-    gqq[j] = qs[q0 + j].qq;
+    gthr[j] = st[gq[j]].thr;
+    gqq[j] = qs[gq[j]].qq;
   }
   __syncthreads();
 
@@ -165,9 +171,9 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
         if (lane >= o) incl += y;
       }
       const uint32_t wtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-      const BatchQuery &q = qs[q0 + j];
+      const BatchQuery &q = qs[gq[j]];
       uint32_t pos = 0;
-      if (lane == 31) pos = atomicAdd(&st[q0 + j].ccount, wtot);
+      if (lane == 31) pos = atomicAdd(&st[gq[j]].ccount, wtot);
       pos = __shfl_sync(0xFFFFFFFFu, pos, 31) + incl - np;
 #pragma unroll
       for (int v = 0; v < OPT; ++v)
@@ -184,10 +190,18 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
 // top-k.  Candidates of the BF16 filter carry approximate keys: with `rescore`
 // each is first scored exactly in the reference order (and the filter's error,
 // relative to its bound, recorded).
+// Hybrid batches (`sw` non-null: sw[0], sw[1] counts, then two lists of nq
+// queries) move a query from the filter to the exact FP32 scorer for the rest of
+// the batch when the filter passes too much for it (scores tied or dense at its
+// threshold): with more than 2k + 2048 candidates in a chunk the chunk is merged and
+// the query is listed in the first list; when candidates were lost (its region or a
+// filter log overflowed) the chunk is discarded and the query is listed in both, the
+// second list naming the queries whose chunk the FP32 scorer answers again.
 __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restrict__ table, uint64_t ld,
                                                            const BatchQuery *__restrict__ qs,
                                                            BatchState *__restrict__ st, uint2 *__restrict__ best,
-                                                           const uint2 *__restrict__ cand, int rescore) {
+                                                           const uint2 *__restrict__ cand, int rescore,
+                                                           uint32_t *__restrict__ sw, uint32_t nq) {
   extern __shared__ __align__(16) unsigned char smem[];
   BatchShared *sh = reinterpret_cast<BatchShared *>(smem);
   uint32_t *hist = reinterpret_cast<uint32_t *>(smem + 128);
@@ -211,6 +225,21 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
   const uint32_t cnt = min(s.cnt, k);
   const uint32_t thr = s.thr;
   const uint32_t nc_raw = s.ccount;
+  const bool filtered = rescore && !(s.flags & kFlagFp32);  // this chunk's candidates came from the filter
+  if (sw && filtered && (nc_raw > q.cand_cap || (s.flags & kFlagOverflow))) {
+    // block-uniform (every thread read the same state): discard the chunk
+    __syncthreads();
+    if (t == 0) {
+      BatchState ns = s;
+      ns.flags = (ns.flags | kFlagFp32) & ~kFlagOverflow;
+      ns.cands = (ns.cands + nc_raw < ns.cands) ? 0xFFFFFFFFu : ns.cands + nc_raw;
+      ns.ccount = 0;
+      s = ns;
+      sw[2 + atomicAdd(&sw[0], 1u)] = blockIdx.x;
+      sw[2 + nq + atomicAdd(&sw[1], 1u)] = blockIdx.x;
+    }
+    return;
+  }
   const uint32_t nc = min(nc_raw, q.cand_cap);
   const uint32_t total = cnt + nc;
   uint2 *out = ent + cnt + q.cand_cap;
@@ -220,7 +249,7 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
   for (uint32_t j = t; j < cnt; j += kBT) ent[j] = b[j];
   for (uint32_t j = t; j < nc; j += kBT) {
     uint2 e = c[j];
-    if (rescore) {
+    if (filtered) {
       const float exact = score_row(table, ld, e.y, attr, w, qq);
       const float ratio = fabsf(key2f(e.x) - exact) / err;
       if (ratio == ratio) atomicMax(&sh->pad[0], __float_as_uint(ratio));
@@ -247,7 +276,11 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
     BatchState ns = s;
     ns.cnt = kept;
     if (kept == k) ns.thr = max(thr, sh->sel.kept_min + 1u);
-    if (nc_raw > q.cand_cap) ns.flags |= 1u;
+    if (nc_raw > q.cand_cap) ns.flags |= kFlagOverflow;
+    if (sw && filtered && nc_raw > 2 * k + 2048) {  // tie-dense under the filter: exact scorer from now on
+      ns.flags |= kFlagFp32;
+      sw[2 + atomicAdd(&sw[0], 1u)] = blockIdx.x;
+    }
     ns.cands = (ns.cands + nc_raw < ns.cands) ? 0xFFFFFFFFu : ns.cands + nc_raw;
     ns.errmax = max(ns.errmax, sh->pad[0]);
     ns.ccount = 0;
@@ -301,11 +334,13 @@ cudaError_t launch_batch_bootstrap(const float *table, uint64_t ld, uint32_t row
 
 size_t batch_score_smem(uint32_t d) {
   const uint32_t to = (d <= 16 ? 4u : 1u) * kBT;
-  return (size_t)d * to * 4 + kBatchGroup * kBatchMaxQ * 5 + kBatchGroup * 8;
+  return (size_t)d * to * 4 + kBatchGroup * kBatchMaxQ * 5 + kBatchGroup * 12;
 }
 
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
-                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, cudaStream_t s) {
+                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand,
+                                    const uint32_t *qlist, cudaStream_t s) {
+  if (nq == 0 || r1 <= r0) return cudaSuccess;
   const size_t smem = batch_score_smem(d);
   const uint32_t opt = d <= 16 ? 4u : 1u;
   const uint64_t to = (uint64_t)opt * kBT;
@@ -317,12 +352,12 @@ cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d,
     if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
         cudaSuccess)
       return e;
-    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand);
+    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist);
   } else {
     if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
         cudaSuccess)
       return e;
-    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand);
+    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist);
   }
   return cudaGetLastError();
 }
@@ -331,11 +366,11 @@ size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax) { return kQueryShared +
 
 cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
                                 uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,
-                                cudaStream_t s) {
+                                uint32_t *sw, cudaStream_t s) {
   const size_t smem = batch_reduce_smem(kmax, capmax);
   cudaError_t e = cudaFuncSetAttribute(batch_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  batch_reduce_kernel<<<nq, kBT, smem, s>>>(table, ld, qs, st, best, cand, rescore ? 1 : 0);
+  batch_reduce_kernel<<<nq, kBT, smem, s>>>(table, ld, qs, st, best, cand, rescore ? 1 : 0, sw, nq);
   return cudaGetLastError();
 }
 

@@ -27,11 +27,15 @@ struct BatchQuery {
 };
 
 // Per-query running state (device).
+// BatchState::flags
+constexpr uint32_t kFlagOverflow = 1u;  // candidates were lost (a region or a filter log overflowed)
+constexpr uint32_t kFlagFp32 = 2u;      // hybrid batch: the query has moved to the exact FP32 scorer
+
 struct BatchState {
   uint32_t thr;     // min key a later object needs (k-th key + 1 once best[] is full)
   uint32_t cnt;     // entries in best[]
   uint32_t ccount;  // candidates appended since the last reduce (may exceed the cap)
-  uint32_t flags;   // bit 0: a candidate region overflowed (exact fallback needed)
+  uint32_t flags;   // kFlagOverflow | kFlagFp32
   uint32_t cands;   // candidates appended over the whole batch (saturating)
   uint32_t errmax;  // BF16 filter: max |filter score - exact score| / err, FP32 bits
   uint32_t seed;    // learned start: every kept entry needs key >= seed (0: none)
@@ -43,11 +47,12 @@ cudaError_t launch_batch_bootstrap(const float *table, uint64_t ld, uint32_t row
                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *best, cudaStream_t s);
 size_t batch_score_smem(uint32_t d);
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
-                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, cudaStream_t s);
+                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand,
+                                    const uint32_t *qlist, cudaStream_t s);
 size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax);
 cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
                                 uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,
-                                cudaStream_t s);
+                                uint32_t *sw, cudaStream_t s);
 // BF16 tensor-core filter (bf16_filter.cu).
 uint64_t bf16_table_bytes(uint64_t n);
 cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,

@@ -215,8 +215,10 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     const uint32_t q = q0 + j;
     float cut = __int_as_float(0x7F800000);
     if (j < nqt * kQTile && q < p.nq) {
-      const uint32_t thr = p.st[q].thr;
-      cut = thr == 0u ? __int_as_float(0xFF800000) : __fsub_rd(thr_float(thr), p.qs[q].err);
+      const BatchState sq_st = p.st[q];
+      // a query moved to the exact FP32 scorer keeps +inf: nothing passes for it
+      if (!(sq_st.flags & kFlagFp32))
+        cut = sq_st.thr == 0u ? __int_as_float(0xFF800000) : __fsub_rd(thr_float(sq_st.thr), p.qs[q].err);
     }
     scut[j] = cut;
   }
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
             for (int c = 0; c < 8; ++c) dst[c] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
             wrech[e] = make_uint2((uint32_t)(obj0 + rt * 32u), ql);
           } else {
-            atomicOr(&st0[ql].flags, 1u);  // lost: the exact scan answers the query
+            atomicOr(&st0[ql].flags, kFlagOverflow);  // lost: the query moves to the exact scorer
           }
         }
       }

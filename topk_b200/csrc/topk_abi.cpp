@@ -131,7 +131,7 @@ struct topk_table_s {
   DevBuf b_q, b_st, b_best, b_cand, b_ids, b_scores, b_count, b_thr;
   // BF16 filter: split copy of the table (rebuilt when the table changed), the
   // per-column max |x| it was built from, the batch's query tiles and error word
-  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logh, b_feat, b_pred;
+  DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logh, b_sw, b_feat, b_pred;
   uint64_t data_version = 1, xbf_version = 0;
   std::vector<float> absmax;
   bool xbf_usable = false;
@@ -154,8 +154,9 @@ struct topk_table_s {
   cudaEvent_t b_ev0 = nullptr, b_ev1 = nullptr;
   double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
-  // TOPK_BATCH_AUTO's memory: the table version on which the BF16 filter overflowed
-  // the candidate regions of more than a quarter of a batch (0: none)
+  uint64_t last_batch_switched = 0;  // queries a hybrid batch moved from the filter to the FP32 scorer
+  // TOPK_BATCH_AUTO's memory: the table version on which the BF16 filter handed more
+  // than three quarters of a batch's queries to the FP32 scorer (0: none)
   uint64_t auto_fp32_version = 0;
   int last_batch_method = 0;
 };
@@ -587,7 +588,7 @@ int ensure(topk_table_s::DevBuf &b, size_t bytes) {
 void free_batch_buffers(topk_table_t h) {
   for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
                                   &h->b_thr, &h->xbf, &h->xbf_absmax, &h->b_abf, &h->b_err, &h->b_log,
-                                  &h->b_logh, &h->b_feat, &h->b_pred}) {
+                                  &h->b_logh, &h->b_sw, &h->b_feat, &h->b_pred}) {
     cudaFree(b->p);
     b->p = nullptr;
     b->bytes = 0;
@@ -767,6 +768,18 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   } else {
     CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
   }
+  // Hybrid batch under the filter: a query for which the filter passes too much
+  // (scores tied or dense at its threshold) moves to the exact FP32 scorer for the
+  // rest of the batch; the reduce lists it (sw[0] counts the moved queries, sw[1] those
+  // whose last chunk was discarded and is answered again with the next one).
+  uint32_t *dsw = nullptr;
+  if (use_bf16) {
+    if ((st = ensure(h->b_sw, (2 + 2 * nq) * sizeof(uint32_t))) != TOPK_OK) return st;
+    dsw = static_cast<uint32_t *>(h->b_sw.p);
+    CK(cudaMemsetAsync(dsw, 0, 2 * sizeof(uint32_t), s));
+  }
+  uint32_t hsw[2] = {0, 0}, redo_done = 0;
+  uint64_t prev_r = r_start;
   // chunk boundaries stay multiples of 256 rows (the filter's object tiles)
   for (uint64_t r = r_start, size = kBatchBootRows; r < h->n; size *= 2) {
     const uint64_t e = std::min<uint64_t>(h->n, r + size);
@@ -777,12 +790,27 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
                             dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
                             static_cast<uint2 *>(h->b_logh.p), kBf16LogCap, h->wait_limit,
                             static_cast<uint32_t *>(h->b_err.p), s));
+      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, hsw[0], dst, dcand, dsw + 2, s));
+      CK(launch_batch_score_fp32(h->table, h->ld, h->d, prev_r, r, dq, hsw[1] - redo_done, dst, dcand,
+                                 dsw + 2 + nq + redo_done, s));
+      redo_done = hsw[1];
     } else {
-      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, s));
+      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, nullptr, s));
     }
-    CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, s));
+    CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
+    if (use_bf16) {
+      CK(cudaMemcpyAsync(hsw, dsw, sizeof(hsw), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    prev_r = r;
     r = e;
   }
+  if (use_bf16 && hsw[1] > redo_done) {  // the last chunk again for the queries that discarded it
+    CK(launch_batch_score_fp32(h->table, h->ld, h->d, prev_r, h->n, dq, hsw[1] - redo_done, dst, dcand,
+                               dsw + 2 + nq + redo_done, s));
+    CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
+  }
+  uint64_t switched_total = hsw[0];
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
                          static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
                          static_cast<float *>(h->b_thr.p), s));
@@ -811,11 +839,9 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     err_ratio = std::max(err_ratio, (double)r);
   }
   // Queries answered again by a smaller batch, whose results replace this batch's:
-  //   a learned start that was too high (fewer than k objects reached the cut):
-  //     again without the learned start;
-  //   a candidate region that overflowed under the BF16 filter (dense scores around
-  //     the threshold): again with the exact FP32 scorer.
-  // What overflows under the FP32 scorer is answered by the single-query scan.
+  // a learned start that was too high (fewer than k objects reached the cut) runs
+  // again without the learned start.  What overflows under the FP32 scorer is
+  // answered by the single-query scan.
   double ms_total = ms;
   uint64_t cands_total = cands, misses_total = 0, scans = 0;
   double ratio_total = err_ratio;
@@ -848,23 +874,21 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     ratio_total = std::max(ratio_total, h->last_batch_err_ratio);
     misses_total += h->last_batch_learned_misses;
     scans += h->last_batch_fallbacks;
+    switched_total += h->last_batch_switched;
     return TOPK_OK;
   };
   std::vector<uint64_t> sub;
   if (use_learned) {
+    // too high a start (fewer than k objects reached it), or so low a one that even
+    // the exact scorer's candidate region overflowed: again without it
     for (uint64_t j = 0; j < nq; j++)
-      if (!(hst[j].flags & 1u) && hcnt[j] < q[j].k) sub.push_back(j);
+      if ((hst[j].flags & kFlagOverflow) || hcnt[j] < q[j].k) sub.push_back(j);
     misses_total += sub.size();
     if (!sub.empty() && (st = rerun(sub, false, force_fp32)) != TOPK_OK) return st;
   }
-  sub.clear();
-  if (use_bf16) {
-    for (uint64_t j = 0; j < nq; j++)
-      if (hst[j].flags & 1u) sub.push_back(j);
-    // AUTO remembers a table on which the filter overflows too often to pay off
-    if (h->batch_method == TOPK_BATCH_AUTO && 4 * sub.size() > nq) h->auto_fp32_version = h->data_version;
-    if (!sub.empty() && (st = rerun(sub, false, true)) != TOPK_OK) return st;
-  }
+  // AUTO remembers a table on which the filter handed most queries to the FP32 scorer
+  if (use_bf16 && h->batch_method == TOPK_BATCH_AUTO && 4 * (uint64_t)hsw[0] > 3 * nq)
+    h->auto_fp32_version = h->data_version;
   for (uint64_t j = 0; j < nq; j++) {
     if (hst[j].flags & 1u) {  // a candidate region overflowed under FP32: answer exactly with the scan
       ++scans;
@@ -888,6 +912,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   h->last_batch_err_ratio = ratio_total;
   h->last_batch_learned_misses = misses_total;
   h->last_batch_fallbacks = scans;
+  h->last_batch_switched = switched_total;
   h->last_batch_method = use_learned ? TOPK_BATCH_LEARNED : use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
   return TOPK_OK;
 }
@@ -1107,6 +1132,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
     return run_batch(h, nq, ks, qqs, weights, wstride, attrs, astride, ids, scores, kstride, counts, thresholds);
   h->last_batch_ms = 0;
   h->last_batch_fallbacks = 0;
+  h->last_batch_switched = 0;
   h->last_batch_cands = 0;
   h->last_batch_err_ratio = 0;
   h->last_batch_learned_misses = 0;
@@ -1147,6 +1173,13 @@ int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uin
   if (method) *method = h->last_batch_method;
   if (max_err_ratio) *max_err_ratio = h->last_batch_err_ratio;
   if (learned_misses) *learned_misses = h->last_batch_learned_misses;
+  return TOPK_OK;
+}
+
+int topk_last_batch_switched(topk_table_t h, uint64_t *switched) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  if (switched) *switched = h->last_batch_switched;
   return TOPK_OK;
 }
 
@@ -1573,8 +1606,31 @@ extern "C" int topk_learned_fit(topk_table_t h, uint64_t n_train, uint64_t n_val
     std::vector<float> b1s(N);
     CK(cudaMemcpy2D(b1s.data(), 4, dX + feature_bound_col(d), (size_t)F * 4, 4, N, cudaMemcpyDeviceToHost));
     for (uint64_t j = 0; j < N; j++) y[j] = learned_target(kth[j], b1s[j], query_scale(q[j]), q[j].qq);
+    // Queries whose k-th score ties the largest partition bound (objects at the top
+    // of every queried column, e.g. values clipped at 1) have no gap to predict: a
+    // batch answers them from its bootstrap instead (their learned start overflows
+    // and runs again without it).  Leave them out of training and calibration, so
+    // that they do not widen the margin of every other query.
+    std::vector<uint64_t> keep_tr, keep_val;
+    for (uint64_t j = 0; j < N; j++) {
+      const bool tie = !((double)b1s[j] - (double)kth[j] / (double)query_scale(q[j]) > 0x1p-20);
+      if (!tie) (j < n_train ? keep_tr : keep_val).push_back(j);
+    }
+    if (keep_tr.size() >= 128 && !keep_val.empty() && keep_tr.size() + keep_val.size() < N) {
+      std::vector<float> X(N * F), X2, y2;
+      CK(cudaMemcpy(X.data(), dX, N * F * 4, cudaMemcpyDeviceToHost));
+      for (const auto *v : {&keep_tr, &keep_val})
+        for (uint64_t j : *v) {
+          X2.insert(X2.end(), X.begin() + j * F, X.begin() + (j + 1) * F);
+          y2.push_back(y[j]);
+        }
+      n_train = keep_tr.size();
+      n_val = keep_val.size();
+      CK(cudaMemcpy(dX, X2.data(), X2.size() * 4, cudaMemcpyHostToDevice));
+      y.assign(y2.begin(), y2.end());
+    }
   }
-  CK(cudaMemcpy(dy, y.data(), N * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y.data(), y.size() * 4, cudaMemcpyHostToDevice));
   // initial parameters: uniform +-sqrt(6 / fan_in) weights, zero biases, b3 = mean target
   std::vector<float> params(P, 0.0f);
   {

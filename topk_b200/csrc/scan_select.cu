@@ -12,7 +12,9 @@
 //     an SM with several CTAs keeps far more than the ~45 KB that HBM3e latency
 //     needs.  Only the queried columns are read.  (A TMA bulk-copy ring with a
 //     producer warp was measured on this GPU at 2.6-4.9 TB/s against 3.1-5.9 TB/s
-//     for plain loads, so the scan uses plain loads.)
+//     for plain loads, so the scan uses plain loads.)  For q <= 4 a thread also keeps
+//     the next tile's loads in flight while it scores, appends and synchronises on
+//     the current one (q = 2: 3.3 -> 3.6 TB/s, q = 4: 4.6 -> 4.8 TB/s).
 //   * An object passes if its score is >= the running threshold; passing objects
 //     go to a shared candidate buffer (warp-aggregated append).  When the buffer
 //     nears capacity (a barrier vote, so every thread decides alike) the CTA keeps
@@ -131,6 +133,34 @@ __device__ __forceinline__ float4 score4(const ScanParams &p, const float *wsm, 
   return make_float4(a0, a1, a2, a3);
 }
 
+// Loads of this thread's 4 objects at rows [row0, row0+4) in the QQ queried columns
+// (zeros past tile_end when `guard`), and their scores in reference order.
+template <int QQ>
+__device__ __forceinline__ void load_cols(const ScanParams &p, uint64_t row0, bool guard, float4 *x) {
+  const bool inb = !guard || row0 < p.tile_end;
+#pragma unroll
+  for (int m = 0; m < QQ; ++m)
+    x[m] = inb ? ld_stream(p.table + (uint64_t)p.attr[m] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+template <int QQ>
+__device__ __forceinline__ float4 score_cols(const ScanParams &p, const float4 *x) {
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+  for (int m = 0; m < QQ; ++m) {
+    const float w = p.w[m];
+    a0 = __fadd_rn(a0, __fmul_rn(x[m].x, w));
+    a1 = __fadd_rn(a1, __fmul_rn(x[m].y, w));
+    a2 = __fadd_rn(a2, __fmul_rn(x[m].z, w));
+    a3 = __fadd_rn(a3, __fmul_rn(x[m].w, w));
+  }
+  return make_float4(a0, a1, a2, a3);
+}
+
+// Up to this many queried columns the scan keeps the next tile's loads in flight
+// while it scores, appends and synchronises on the current one (few columns give a
+// thread too few bytes in flight otherwise).
+constexpr int kPrefetchQ = 4;
+
 // QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).
 template <int QQ>
 __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_constant__ ScanParams p) {
@@ -173,6 +203,23 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   }
 
   uint32_t g_pending = 0;  // thread 0's in-flight copy of the global threshold
+  // next-tile prefetch (rows in id order only; a partition list resolves a tile's rows
+  // one tile ahead, too late to issue its loads early)
+  constexpr int kPQ = (QQ >= 1 && QQ <= kPrefetchQ) ? QQ : 1;
+  // tiles loaded ahead of the one being scored (two ahead for q <= 2 measured slower:
+  // the extra registers cost a CTA per SM)
+  constexpr int kDepth = 1;
+  const bool prefetch = QQ >= 1 && QQ <= kPrefetchQ && p.part_list == nullptr;
+  auto load_tile = [&](uint32_t j, float4 *dst) {  // tile j of this CTA
+    const uint64_t tl = p.tile_begin + ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) * kTile;
+    load_cols<kPQ>(p, tl + (uint64_t)t * kVec, !(tl >= p.row_begin && tl + kTile <= p.row_end), dst);
+  };
+  float4 xn[kDepth][kPQ];
+  if (prefetch) {
+#pragma unroll
+    for (int dd = 0; dd < kDepth; ++dd)
+      if ((uint32_t)dd < my_tiles) load_tile(dd, xn[dd]);
+  }
   // partition mode: the partition of the next tile is loaded one tile ahead
   const uint32_t pmask = (1u << p.part_shift) - 1u;
   uint32_t part_next = (p.part_list && my_tiles) ? __ldg(p.part_list + (blockIdx.x >> p.part_shift)) : 0u;
@@ -188,7 +235,20 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
     const uint32_t thr = max(ctl->thr_local, ctl->thr_g);
-    const float4 s = score4<QQ>(p, wsm, qq, row0, !interior);
+    float4 s;
+    if (prefetch) {
+      float4 x[kPQ];
+#pragma unroll
+      for (int m = 0; m < kPQ; ++m) x[m] = xn[0][m];
+#pragma unroll
+      for (int dd = 0; dd + 1 < kDepth; ++dd)
+#pragma unroll
+        for (int m = 0; m < kPQ; ++m) xn[dd][m] = xn[dd + 1][m];
+      if (i + kDepth < my_tiles) load_tile(i + kDepth, xn[kDepth - 1]);
+      s = score_cols<kPQ>(p, x);
+    } else {
+      s = score4<QQ>(p, wsm, qq, row0, !interior);
+    }
 
     // key(score) >= thr  <=>  thr == 0 (everything, NaN included) or score >= thr_float(thr)
     const bool take_all = thr == 0u;

@@ -14,7 +14,9 @@
 //     producer warp was measured on this GPU at 2.6-4.9 TB/s against 3.1-5.9 TB/s
 //     for plain loads, so the scan uses plain loads.)  For q <= 4 a thread also keeps
 //     the next tile's loads in flight while it scores, appends and synchronises on
-//     the current one (q = 2: 3.3 -> 3.6 TB/s, q = 4: 4.6 -> 4.8 TB/s).
+//     the current one, and loads a partial tile's rows past its end from row 0 (in
+//     bounds, masked out) instead of selecting zeros value by value (q = 2: 3.3 ->
+//     3.6 TB/s; q = 4: 4.5 -> 5.5 TB/s, same-box A/B).
 //   * An object passes if its score is >= the running threshold; passing objects
 //     go to a shared candidate buffer (warp-aggregated append).  When the buffer
 //     nears capacity (a barrier vote, so every thread decides alike) the CTA keeps
@@ -133,14 +135,17 @@ __device__ __forceinline__ float4 score4(const ScanParams &p, const float *wsm, 
   return make_float4(a0, a1, a2, a3);
 }
 
-// Loads of this thread's 4 objects at rows [row0, row0+4) in the QQ queried columns
-// (zeros past tile_end when `guard`), and their scores in reference order.
+// Loads of this thread's 4 objects at rows [row0, row0+4) in the QQ queried columns,
+// and their scores in reference order.  `guard`: partial tile; a thread whose rows
+// lie at or past tile_end loads row 0 instead (always in bounds) and its scores are
+// meaningless — the caller's row-range mask drops them.  One select per tile, none
+// per value, and the column pointers computed once by the caller.
 template <int QQ>
-__device__ __forceinline__ void load_cols(const ScanParams &p, uint64_t row0, bool guard, float4 *x) {
-  const bool inb = !guard || row0 < p.tile_end;
+__device__ __forceinline__ void load_cols(const ScanParams &p, const float *const *col, uint64_t row0, bool guard,
+                                          float4 *x) {
+  row0 = (!guard || row0 < p.tile_end) ? row0 : 0;
 #pragma unroll
-  for (int m = 0; m < QQ; ++m)
-    x[m] = inb ? ld_stream(p.table + (uint64_t)p.attr[m] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int m = 0; m < QQ; ++m) x[m] = ld_stream(col[m] + row0);
 }
 template <int QQ>
 __device__ __forceinline__ float4 score_cols(const ScanParams &p, const float4 *x) {
@@ -210,9 +215,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   // the extra registers cost a CTA per SM)
   constexpr int kDepth = 1;
   const bool prefetch = QQ >= 1 && QQ <= kPrefetchQ && p.part_list == nullptr;
+  // queried columns: computed once for q >= 3; for q <= 2 per tile (two more 64-bit
+  // registers would cost a CTA per SM there, measured slower)
+  constexpr bool kHoist = kPQ >= 3;
+  const float *col[kPQ];
+#pragma unroll
+  for (int m = 0; m < kPQ; ++m) col[m] = kHoist ? p.table + (uint64_t)p.attr[m] * p.ld : nullptr;
   auto load_tile = [&](uint32_t j, float4 *dst) {  // tile j of this CTA
     const uint64_t tl = p.tile_begin + ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) * kTile;
-    load_cols<kPQ>(p, tl + (uint64_t)t * kVec, !(tl >= p.row_begin && tl + kTile <= p.row_end), dst);
+    const float *c[kPQ];
+#pragma unroll
+    for (int m = 0; m < kPQ; ++m) c[m] = kHoist ? col[m] : p.table + (uint64_t)p.attr[m] * p.ld;
+    load_cols<kPQ>(p, c, tl + (uint64_t)t * kVec, !(tl >= p.row_begin && tl + kTile <= p.row_end), dst);
   };
   float4 xn[kDepth][kPQ];
   if (prefetch) {

@@ -155,6 +155,10 @@ struct topk_table_s {
   double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
   uint64_t last_batch_switched = 0;  // queries a hybrid batch moved from the filter to the FP32 scorer
+  // pinned host copies of a batch's results (grow-only): copied at full link speed,
+  // no page faults on the critical path
+  void *hb_res = nullptr;
+  size_t hb_bytes = 0;
   // TOPK_BATCH_AUTO's memory: the table version on which the BF16 filter handed more
   // than three quarters of a batch's queries to the FP32 scorer (0: none)
   uint64_t auto_fp32_version = 0;
@@ -596,6 +600,9 @@ void free_batch_buffers(topk_table_t h) {
   if (h->b_ev0) cudaEventDestroy(h->b_ev0);
   if (h->b_ev1) cudaEventDestroy(h->b_ev1);
   h->b_ev0 = h->b_ev1 = nullptr;
+  if (h->hb_res) cudaFreeHost(h->hb_res);
+  h->hb_res = nullptr;
+  h->hb_bytes = 0;
 }
 
 // The device table is about to change: derived copies (the BF16 split) are stale.
@@ -815,12 +822,24 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
                          static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
                          static_cast<float *>(h->b_thr.p), s));
   CK(cudaEventRecord(h->b_ev1, s));
-  std::vector<uint64_t> hid(nq * kmax);
-  std::vector<float> hsc(nq * kmax), hth(nq);
+  // results through the handle's pinned buffers (grown once), then into the caller's
+  // arrays before anything below runs a nested batch that reuses them
+  const size_t res_bytes = (size_t)nq * kmax * 12;
+  if (h->hb_bytes < res_bytes) {
+    if (h->hb_res) cudaFreeHost(h->hb_res);
+    h->hb_res = nullptr;
+    h->hb_bytes = 0;
+    if (cudaHostAlloc(&h->hb_res, res_bytes, cudaHostAllocDefault) != cudaSuccess)
+      return fail(TOPK_ERR_OOM, "pinned result buffer of %zu bytes", res_bytes);
+    h->hb_bytes = res_bytes;
+  }
+  uint64_t *hid = static_cast<uint64_t *>(h->hb_res);
+  float *hsc = reinterpret_cast<float *>(hid + nq * kmax);
+  std::vector<float> hth(nq);
   std::vector<uint32_t> hcnt(nq);
   std::vector<BatchState> hst(nq);
-  CK(cudaMemcpyAsync(hid.data(), h->b_ids.p, hid.size() * 8, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(hsc.data(), h->b_scores.p, hsc.size() * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hid, h->b_ids.p, nq * kmax * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hsc, h->b_scores.p, nq * kmax * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hcnt.data(), h->b_count.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hth.data(), h->b_thr.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
@@ -828,6 +847,11 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (use_bf16) CK(cudaMemcpyAsync(&herr, h->b_err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
+  for (uint64_t j = 0; j < nq; j++) {  // queries answered again below overwrite theirs
+    const uint32_t c = std::min<uint32_t>(hcnt[j], (uint32_t)std::min<uint64_t>(kmax, kstride));
+    std::memcpy(ids + j * kstride, hid + j * kmax, (size_t)c * 8);
+    std::memcpy(scores + j * kstride, hsc + j * kmax, (size_t)c * 4);
+  }
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->b_ev0, h->b_ev1));
   uint64_t cands = 0;
@@ -865,8 +889,8 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       const uint64_t j = sub[i];
       hcnt[j] = (uint32_t)mcnt[i];
       hth[j] = mth[i];
-      std::memcpy(&hid[j * kmax], &mids[i * kmax], mcnt[i] * 8);
-      std::memcpy(&hsc[j * kmax], &msc[i * kmax], mcnt[i] * 4);
+      std::memcpy(ids + j * kstride, &mids[i * kmax], mcnt[i] * 8);
+      std::memcpy(scores + j * kstride, &msc[i * kmax], mcnt[i] * 4);
       hst[j].flags = 0;
     }
     ms_total += h->last_batch_ms;
@@ -901,10 +925,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       if (thresholds) thresholds[j] = th;
       continue;
     }
-    const uint32_t c = hcnt[j];
-    std::memcpy(ids + j * kstride, &hid[j * kmax], (size_t)c * 8);
-    std::memcpy(scores + j * kstride, &hsc[j * kmax], (size_t)c * 4);
-    if (counts) counts[j] = c;
+    if (counts) counts[j] = hcnt[j];
     if (thresholds) thresholds[j] = hth[j];
   }
   h->last_batch_ms = ms_total;

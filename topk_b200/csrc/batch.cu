@@ -89,14 +89,23 @@ __global__ void __launch_bounds__(kBT) batch_bootstrap_kernel(const float *__res
 // Block (query group g, tile): rows [row0, row0 + OPT*256) of the chunk, all d
 // columns staged in shared memory once, scored for the group's queries.  With a
 // query list the groups are formed from qlist[0..nq) (the queries a hybrid batch has
-// moved to this scorer), else from queries 0..nq-1.
+// moved to this scorer), else from queries 0..nq-1.  With `list_end` the list is
+// qlist[*list_begin .. *list_end) as the device holds it when the kernel starts (a
+// hybrid batch's lists grow in its reduce, which the host does not wait for): the grid
+// is then a fixed set of blocks taking (group, tile) items in order from the counter
+// `work` (zero at launch; in order, so the groups reading one tile run together and
+// find it in L2), and an empty list costs one read.
 template <int OPT>
 __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__restrict__ table, uint64_t ld,
                                                                uint32_t d, uint64_t r0, uint64_t r1,
                                                                const BatchQuery *__restrict__ qs, uint32_t nq,
                                                                BatchState *__restrict__ st,
                                                                uint2 *__restrict__ cand,
-                                                               const uint32_t *__restrict__ qlist) {
+                                                               const uint32_t *__restrict__ qlist,
+                                                               const uint32_t *__restrict__ list_end,
+                                                               const uint32_t *__restrict__ list_begin,
+                                                               uint32_t *__restrict__ work) {
+  __shared__ uint32_t next_item;
   constexpr uint32_t TO = kBT * OPT;
   extern __shared__ __align__(16) unsigned char smem[];
   float *xs = reinterpret_cast<float *>(smem);                       // d x TO
@@ -107,11 +116,24 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
   uint32_t *gq = gqq + kBatchGroup;  // query of each group slot
 
   const int t = threadIdx.x;
-  // block -> (query group, tile), groups fastest: the blocks of one tile run together
+  if (list_end) {
+    const uint32_t b = list_begin ? *list_begin : 0u;
+    nq = *list_end - b;
+    qlist += b;
+  }
+  // item -> (query group, tile), groups fastest: the items of one tile run together
   // and its second and later reads come from L2
   const uint32_t ngroups = (nq + kBatchGroup - 1) / kBatchGroup;
-  const uint32_t q0 = (blockIdx.x % ngroups) * kBatchGroup;
-  const uint64_t tile = blockIdx.x / ngroups;
+  const uint64_t items = (uint64_t)ngroups * ((r1 - r0 + TO - 1) / TO);
+  uint64_t item = blockIdx.x;  // without a list: one item per block
+  if (list_end) {
+    if (t == 0) next_item = atomicAdd(work, 1u);
+    __syncthreads();
+    item = next_item;
+  }
+  while (item < items) {
+  const uint32_t q0 = (uint32_t)(item % ngroups) * kBatchGroup;
+  const uint64_t tile = item / ngroups;
   const uint32_t nqg = min(kBatchGroup, nq - q0);
   const uint64_t base = r0 + tile * TO;
   const uint32_t valid = (uint32_t)min((uint64_t)TO, r1 - base);
@@ -183,7 +205,15 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
         }
     }
   }
+  __syncthreads();  // the next item restages the shared tile
+  if (!list_end) break;
+  if (t == 0) next_item = atomicAdd(work, 1u);
+  __syncthreads();
+  item = next_item;
+  }
 }
+
+__global__ void copy_word_kernel(uint32_t *dst, const uint32_t *src) { *dst = *src; }
 
 // ---------------------------------------------------------------- reduce
 // One block per query: merge best[] with the chunk's candidates into the new
@@ -225,6 +255,7 @@ __global__ void __launch_bounds__(kBT) batch_reduce_kernel(const float *__restri
   const uint32_t cnt = min(s.cnt, k);
   const uint32_t thr = s.thr;
   const uint32_t nc_raw = s.ccount;
+  if (nc_raw == 0u && !(s.flags & kFlagOverflow)) return;  // nothing new: best[] and the state stand
   const bool filtered = rescore && !(s.flags & kFlagFp32);  // this chunk's candidates came from the filter
   if (sw && filtered && (nc_raw > q.cand_cap || (s.flags & kFlagOverflow))) {
     // block-uniform (every thread read the same state): discard the chunk
@@ -352,13 +383,44 @@ cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d,
     if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
         cudaSuccess)
       return e;
-    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist);
+    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist, nullptr, nullptr,
+                                                        nullptr);
   } else {
     if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
         cudaSuccess)
       return e;
-    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist);
+    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist, nullptr, nullptr,
+                                                        nullptr);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_score_fp32_list(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
+                                         const BatchQuery *qs, BatchState *st, uint2 *cand, const uint32_t *qlist,
+                                         const uint32_t *list_end, const uint32_t *list_begin, uint32_t *work,
+                                         int num_sms, cudaStream_t s) {
+  if (r1 <= r0) return cudaSuccess;
+  const size_t smem = batch_score_smem(d);
+  const bool four = d <= 16;
+  const void *fn = four ? reinterpret_cast<const void *>(batch_score_fp32_kernel<4>)
+                        : reinterpret_cast<const void *>(batch_score_fp32_kernel<1>);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBT, smem)) != cudaSuccess) return e;
+  const dim3 grid((unsigned)(std::max(1, per_sm) * std::max(1, num_sms)));
+  if ((e = cudaMemsetAsync(work, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if (four)
+    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, 0, st, cand, qlist, list_end, list_begin,
+                                                        work);
+  else
+    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, 0, st, cand, qlist, list_end, list_begin,
+                                                        work);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_word(uint32_t *dst, const uint32_t *src, cudaStream_t s) {
+  copy_word_kernel<<<1, 1, 0, s>>>(dst, src);
   return cudaGetLastError();
 }
 

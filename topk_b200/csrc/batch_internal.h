@@ -49,6 +49,14 @@ size_t batch_score_smem(uint32_t d);
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                     const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand,
                                     const uint32_t *qlist, cudaStream_t s);
+// The same scorer over the queries qlist[*list_begin .. *list_end) (list_begin may be
+// null: from 0), read from device memory when the kernel starts; a fixed grid of
+// blocks takes the work items from the counter `work` (zeroed here, in stream order).
+cudaError_t launch_batch_score_fp32_list(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
+                                         const BatchQuery *qs, BatchState *st, uint2 *cand, const uint32_t *qlist,
+                                         const uint32_t *list_end, const uint32_t *list_begin, uint32_t *work,
+                                         int num_sms, cudaStream_t s);
+cudaError_t launch_copy_word(uint32_t *dst, const uint32_t *src, cudaStream_t s);  // *dst = *src, in stream order
 size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax);
 cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
                                 uint2 *best, const uint2 *cand, uint32_t kmax, uint32_t capmax, bool rescore,

@@ -777,15 +777,21 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   }
   // Hybrid batch under the filter: a query for which the filter passes too much
   // (scores tied or dense at its threshold) moves to the exact FP32 scorer for the
-  // rest of the batch; the reduce lists it (sw[0] counts the moved queries, sw[1] those
-  // whose last chunk was discarded and is answered again with the next one).
-  uint32_t *dsw = nullptr;
+  // rest of the batch.  The reduce lists it: sw[0] counts the moved queries (list A at
+  // sw + 2), sw[1] those whose last chunk was discarded (list B at sw + 2 + nq), and
+  // sw[2 + 2nq] is how far list B has been answered again, sw[3 + 2nq] the scorer's
+  // work counter.  The scorer reads the counts on the device, so the host never waits
+  // inside the loop.
+  uint32_t *dsw = nullptr, *dredo = nullptr, *dwork = nullptr;
   if (use_bf16) {
-    if ((st = ensure(h->b_sw, (2 + 2 * nq) * sizeof(uint32_t))) != TOPK_OK) return st;
+    if ((st = ensure(h->b_sw, (4 + 2 * nq) * sizeof(uint32_t))) != TOPK_OK) return st;
     dsw = static_cast<uint32_t *>(h->b_sw.p);
+    dredo = dsw + 2 + 2 * nq;
+    dwork = dredo + 1;
     CK(cudaMemsetAsync(dsw, 0, 2 * sizeof(uint32_t), s));
+    CK(cudaMemsetAsync(dredo, 0, sizeof(uint32_t), s));
   }
-  uint32_t hsw[2] = {0, 0}, redo_done = 0;
+  uint32_t hsw[2] = {0, 0};
   uint64_t prev_r = r_start;
   // chunk boundaries stay multiples of 256 rows (the filter's object tiles)
   for (uint64_t r = r_start, size = kBatchBootRows; r < h->n; size *= 2) {
@@ -797,27 +803,24 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
                             dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
                             static_cast<uint2 *>(h->b_logh.p), kBf16LogCap, h->wait_limit,
                             static_cast<uint32_t *>(h->b_err.p), s));
-      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, hsw[0], dst, dcand, dsw + 2, s));
-      CK(launch_batch_score_fp32(h->table, h->ld, h->d, prev_r, r, dq, hsw[1] - redo_done, dst, dcand,
-                                 dsw + 2 + nq + redo_done, s));
-      redo_done = hsw[1];
+      // this chunk for every moved query; the previous one again for those that discarded it
+      CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, r, e, dq, dst, dcand, dsw + 2, dsw, nullptr, dwork,
+                                      h->num_sms, s));
+      CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, prev_r, r, dq, dst, dcand, dsw + 2 + nq, dsw + 1,
+                                      dredo, dwork, h->num_sms, s));
+      CK(launch_copy_word(dredo, dsw + 1, s));
     } else {
       CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, nullptr, s));
     }
     CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
-    if (use_bf16) {
-      CK(cudaMemcpyAsync(hsw, dsw, sizeof(hsw), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-    }
     prev_r = r;
     r = e;
   }
-  if (use_bf16 && hsw[1] > redo_done) {  // the last chunk again for the queries that discarded it
-    CK(launch_batch_score_fp32(h->table, h->ld, h->d, prev_r, h->n, dq, hsw[1] - redo_done, dst, dcand,
-                               dsw + 2 + nq + redo_done, s));
+  if (use_bf16) {  // the last chunk again for the queries that discarded it (none: two empty launches)
+    CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, prev_r, h->n, dq, dst, dcand, dsw + 2 + nq, dsw + 1,
+                                    dredo, dwork, h->num_sms, s));
     CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
   }
-  uint64_t switched_total = hsw[0];
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
                          static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
                          static_cast<float *>(h->b_thr.p), s));
@@ -845,8 +848,10 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
   uint32_t herr = 0;
   if (use_bf16) CK(cudaMemcpyAsync(&herr, h->b_err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (use_bf16) CK(cudaMemcpyAsync(hsw, dsw, sizeof(hsw), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
+  uint64_t switched_total = hsw[0];
   for (uint64_t j = 0; j < nq; j++) {  // queries answered again below overwrite theirs
     const uint32_t c = std::min<uint32_t>(hcnt[j], (uint32_t)std::min<uint64_t>(kmax, kstride));
     std::memcpy(ids + j * kstride, hid + j * kmax, (size_t)c * 8);

@@ -159,6 +159,15 @@ struct topk_table_s {
   // no page faults on the critical path
   void *hb_res = nullptr;
   size_t hb_bytes = 0;
+  // the device work of a batch, captured once per shape and replayed (a few shapes:
+  // a learned batch's rerun of its misses is a second one)
+  struct BatchGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+  };
+  BatchGraph b_graphs[4];
+  uint64_t b_graph_tick = 0;
   // TOPK_BATCH_AUTO's memory: the table version on which the BF16 filter handed more
   // than three quarters of a batch's queries to the FP32 scorer (0: none)
   uint64_t auto_fp32_version = 0;
@@ -603,6 +612,10 @@ void free_batch_buffers(topk_table_t h) {
   if (h->hb_res) cudaFreeHost(h->hb_res);
   h->hb_res = nullptr;
   h->hb_bytes = 0;
+  for (auto &g : h->b_graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = topk_table_s::BatchGraph{};
+  }
 }
 
 // The device table is about to change: derived copies (the BF16 split) are stale.
@@ -759,29 +772,15 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if ((st = ensure(h->b_feat, nq * feature_dim(h->d) * sizeof(float))) != TOPK_OK) return st;
     if ((st = ensure(h->b_pred, nq * sizeof(float))) != TOPK_OK) return st;
   }
-  CK(cudaEventRecord(h->b_ev0, s));
   const uint64_t boot = std::min<uint64_t>(h->n, kBatchBootRows);
-  uint64_t r_start = boot;
-  if (use_learned) {
-    // features and the model in one kernel, then each query's threshold starts at
-    // its cut (prediction - margin) * S; no bootstrap
-    std::lock_guard<std::mutex> lk(h->learned_mu);
-    const size_t P = h->num_parts, d = h->d;
-    CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, dq, nqq,
-                       static_cast<float *>(h->b_feat.p), h->mlp, static_cast<float *>(h->b_pred.p), s));
-    CK(launch_learned_seed(static_cast<const float *>(h->b_pred.p), static_cast<const float *>(h->b_feat.p), h->d, dq,
-                           h->mlp_margin, dst, nqq, s));
-    r_start = 0;
-  } else {
-    CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
-  }
+  const uint64_t r_start = use_learned ? 0 : boot;
   // Hybrid batch under the filter: a query for which the filter passes too much
   // (scores tied or dense at its threshold) moves to the exact FP32 scorer for the
   // rest of the batch.  The reduce lists it: sw[0] counts the moved queries (list A at
   // sw + 2), sw[1] those whose last chunk was discarded (list B at sw + 2 + nq), and
   // sw[2 + 2nq] is how far list B has been answered again, sw[3 + 2nq] the scorer's
   // work counter.  The scorer reads the counts on the device, so the host never waits
-  // inside the loop.
+  // inside the batch.
   uint32_t *dsw = nullptr, *dredo = nullptr, *dwork = nullptr;
   if (use_bf16) {
     if ((st = ensure(h->b_sw, (4 + 2 * nq) * sizeof(uint32_t))) != TOPK_OK) return st;
@@ -792,6 +791,20 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     CK(cudaMemsetAsync(dredo, 0, sizeof(uint32_t), s));
   }
   uint32_t hsw[2] = {0, 0};
+  // the device work of the batch, from the first threshold to the results
+  auto issue = [&]() -> int {
+  if (use_learned) {
+    // features and the model in one kernel, then each query's threshold starts at
+    // its cut (prediction - margin) * S; no bootstrap
+    std::lock_guard<std::mutex> lk(h->learned_mu);
+    const size_t P = h->num_parts, d = h->d;
+    CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, dq, nqq,
+                       static_cast<float *>(h->b_feat.p), h->mlp, static_cast<float *>(h->b_pred.p), s));
+    CK(launch_learned_seed(static_cast<const float *>(h->b_pred.p), static_cast<const float *>(h->b_feat.p), h->d, dq,
+                           h->mlp_margin, dst, nqq, s));
+  } else {
+    CK(launch_batch_bootstrap(h->table, h->ld, (uint32_t)boot, kmax, dq, nqq, dst, dbest, s));
+  }
   uint64_t prev_r = r_start;
   // chunk boundaries stay multiples of 256 rows (the filter's object tiles)
   for (uint64_t r = r_start, size = kBatchBootRows; r < h->n; size *= 2) {
@@ -824,6 +837,52 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
                          static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
                          static_cast<float *>(h->b_thr.p), s));
+  return TOPK_OK;
+  };
+  // Captured into a CUDA graph once per shape and replayed: the key holds every
+  // pointer and scalar the captured launches take (a buffer that grew or a new model
+  // margin makes a new shape).  The graph reads the query descriptors and states that
+  // the stream uploaded and cleared before it.
+  std::vector<uint64_t> key = {nq, kmax, capmax, use_bf16, use_learned, h->n, h->d, h->ld, boot,
+                               (uint64_t)h->num_sms, log_ctas, h->wait_limit, h->num_parts};
+  const void *key_ptrs[] = {h->table, dq, dst, dbest, dcand, h->b_ids.p, h->b_scores.p, h->b_count.p,
+                            h->b_thr.p, h->xbf.p, h->b_abf.p, h->b_log.p, h->b_logh.p, h->b_err.p, h->b_sw.p,
+                            h->b_feat.p, h->b_pred.p, h->pstats, h->mlp};
+  for (const void *ptr : key_ptrs) key.push_back((uint64_t)(uintptr_t)ptr);
+  {
+    uint32_t mb;
+    std::memcpy(&mb, &h->mlp_margin, 4);
+    key.push_back(use_learned ? mb : 0u);
+  }
+  topk_table_s::BatchGraph *gr = nullptr;
+  for (auto &g : h->b_graphs)
+    if (g.exec && g.key == key) gr = &g;
+  if (!gr) {  // capture into the least recently used slot
+    gr = &h->b_graphs[0];
+    for (auto &g : h->b_graphs)
+      if (g.used < gr->used) gr = &g;
+    if (gr->exec) cudaGraphExecDestroy(gr->exec);
+    *gr = topk_table_s::BatchGraph{};
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    const int ist = issue();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ist != TOPK_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return ist;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&gr->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      gr->exec = nullptr;
+      return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    gr->key = key;
+  }
+  gr->used = ++h->b_graph_tick;
+  CK(cudaEventRecord(h->b_ev0, s));
+  CK(cudaGraphLaunch(gr->exec, s));
   CK(cudaEventRecord(h->b_ev1, s));
   // results through the handle's pinned buffers (grown once), then into the caller's
   // arrays before anything below runs a nested batch that reuses them

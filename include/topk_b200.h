@@ -278,6 +278,21 @@ int topk_set_fault_injection(topk_table_t h, int mode);
 /* Choose the method of topk_query_batch on this handle. */
 int topk_set_batch_method(topk_table_t h, int method);
 
+/* Tiles of the batched path (no reference counterpart; results never depend on
+ * them): query tiles of 128 per BF16-filter CTA (1..16, 0 = up to 16) and rows of the
+ * exact bootstrap, which is also the first chunk (a multiple of 256 in [256, 16384];
+ * default 8192). */
+int topk_set_batch_tiles(topk_table_t h, uint32_t qt_per_cta, uint32_t boot_rows);
+int topk_get_batch_tiles(topk_table_t h, uint32_t *qt_per_cta, uint32_t *boot_rows);
+
+/* Autotuner of the batched path: runs the caller's queries (arguments as in
+ * topk_query_batch, with the handle's current method) under query tiles per CTA of
+ * 4, 8 and 16 and bootstraps of 8192 and 16384 rows, each twice, keeps the fastest
+ * device time in the handle and reports {query tiles, bootstrap rows, best ms, ms of
+ * the default 16 / 8192}.  Twelve batches: call it once per workload shape. */
+int topk_tune_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+                    uint64_t wstride, const uint8_t *attrs, uint64_t astride, double *report);
+
 /* Statistics of the handle's last topk_query_batch: device time of the batched
  * kernels (CUDA events; 0 for the loop method), queries answered again by the
  * single-query scan after a candidate overflow, candidates appended by the

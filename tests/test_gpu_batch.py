@@ -290,3 +290,27 @@ def test_batch_bf16_hybrid_redoes_discarded_chunks():
         check_batch(t, tn, ks, W, A, qqs)
         st = t.last_batch_stats()
         assert st["method"] == BF16 and st["switched_fp32"] >= 1
+
+
+def test_batch_tune_keeps_results():
+    """The autotuner tries its tiles on the caller's queries, keeps the fastest in the
+    handle and reports it; batches afterwards return the same exact results."""
+    rng = np.random.default_rng(21)
+    n, d = 300007, 16
+    with T.Table(n, d) as t:
+        t.generate(1, 5)
+        t.normalize()
+        tn = t.download()
+        t.set_batch_method(BF16)
+        ks, W, A, qqs = make_batch(rng, 300, d, 1024, qmax=16)
+        rep = t.tune_batch(ks, W, A, qqs)
+        assert rep["query_tiles_per_cta"] in (4, 8, 16) and rep["boot_rows"] in (8192, 16384)
+        assert 0 < rep["best_ms"] <= rep["default_ms"]
+        qt, boot = t.batch_tiles()
+        assert (qt or 16) == rep["query_tiles_per_cta"] and boot == rep["boot_rows"]
+        check_batch(t, tn, ks, W, A, qqs)
+        bf16_ran(t)
+        t.set_batch_tiles(8, 16384)
+        check_batch(t, tn, ks, W, A, qqs)
+        with pytest.raises(T.TopKError):
+            t.set_batch_tiles(4, 1000)

@@ -42,6 +42,7 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _H = C.c_void_p
 
 # (name, restype, argtypes) for every entry of include/topk_b200.h
@@ -87,6 +88,9 @@ SIGNATURES = [
     ("topk_last_batch_stats", C.c_int, [_H, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("topk_last_batch_switched", C.c_int, [_H, C.POINTER(C.c_uint64)]),
+    ("topk_set_batch_tiles", C.c_int, [_H, C.c_uint32, C.c_uint32]),
+    ("topk_get_batch_tiles", C.c_int, [_H, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("topk_tune_batch", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _f64p]),
     ("topk_query_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, _f32p,
                                      _u8p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("topk_last_stats", C.c_int, [_H, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -9,7 +9,8 @@ namespace topk {
 constexpr uint32_t kBatchMaxQ = 32;    // attributes per query on the batched path
 constexpr uint32_t kBatchGroup = 64;   // queries scored per staged table tile (FP32 scorer)
 constexpr uint32_t kBatchMaxD = 64;    // table width the FP32 scorer stages
-constexpr uint32_t kBatchBootRows = 8192;  // rows of the exact bootstrap
+constexpr uint32_t kBatchBootRows = 8192;  // rows of the exact bootstrap (default)
+constexpr uint32_t kBatchBootMax = 16384;  // its shared-memory limit
 constexpr uint32_t kBf16MaxD = 16;         // table width of the BF16 tensor-core filter (MMA K)
 constexpr uint32_t kBf16LogCap = 32768;    // survivor records (32 values + header, 136 B) per filter CTA
 
@@ -75,7 +76,8 @@ struct FilterPlan {
   uint32_t nqt, qt_per_cta, ngroups, cpg;
   uint64_t grid;
 };
-FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms);
+// qt_cap: query tiles of 128 per CTA at most (0: the kernel's maximum)
+FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms, uint32_t qt_cap = 0);
 // r0 must be a multiple of 128; log/log_q hold grid * log_cap entries.
 cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
                                const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *recv,

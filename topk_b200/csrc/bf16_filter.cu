@@ -494,12 +494,12 @@ void bf16_pack_query(const float *a, uint32_t j, uint8_t *abf) {
   }
 }
 
-FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms) {
+FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms, uint32_t qt_cap) {
   FilterPlan f{};
   f.tile0 = r0 / kOTile;
   f.tile1 = (r1 + kOTile - 1) / kOTile;
   f.nqt = (nq + kQTile - 1) / kQTile;
-  f.qt_per_cta = std::min<uint32_t>(f.nqt, kMaxQTPerCta);
+  f.qt_per_cta = std::min<uint32_t>(f.nqt, (qt_cap >= 1 && qt_cap < kMaxQTPerCta) ? qt_cap : kMaxQTPerCta);
   f.ngroups = (f.nqt + f.qt_per_cta - 1) / f.qt_per_cta;
   const uint64_t ntiles = f.tile1 - f.tile0;
   f.cpg = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)std::max(1, num_sms / (int)f.ngroups)));

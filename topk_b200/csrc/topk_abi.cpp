@@ -124,6 +124,9 @@ struct topk_table_s {
   // batched path: one batch at a time per handle, device buffers grow and are kept
   std::mutex batch_mu;
   int batch_method = TOPK_BATCH_AUTO;
+  // batch tiles (topk_set_batch_tiles / topk_tune_batch): query tiles per filter CTA
+  // (0: up to the kernel's 16) and rows of the exact bootstrap (= the first chunk)
+  uint32_t batch_qt = 0, batch_boot = kBatchBootRows;
   struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -743,7 +746,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if ((st = ensure(h->b_abf, habf.size())) != TOPK_OK) return st;
     if ((st = ensure(h->b_err, sizeof(uint32_t))) != TOPK_OK) return st;
     // survivor records: one log per filter CTA (at most max(num_sms, query groups) CTAs)
-    const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms);
+    const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms, h->batch_qt);
     log_ctas = std::max<uint64_t>((uint64_t)h->num_sms, fp.ngroups);
     if ((st = ensure(h->b_log, log_ctas * kBf16LogCap * 8 * sizeof(uint4))) != TOPK_OK) return st;
     if ((st = ensure(h->b_logh, log_ctas * kBf16LogCap * sizeof(uint2))) != TOPK_OK) return st;
@@ -772,7 +775,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if ((st = ensure(h->b_feat, nq * feature_dim(h->d) * sizeof(float))) != TOPK_OK) return st;
     if ((st = ensure(h->b_pred, nq * sizeof(float))) != TOPK_OK) return st;
   }
-  const uint64_t boot = std::min<uint64_t>(h->n, kBatchBootRows);
+  const uint64_t boot = std::min<uint64_t>(h->n, h->batch_boot);
   const uint64_t r_start = use_learned ? 0 : boot;
   // Hybrid batch under the filter: a query for which the filter passes too much
   // (scores tied or dense at its threshold) moves to the exact FP32 scorer for the
@@ -807,10 +810,10 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   }
   uint64_t prev_r = r_start;
   // chunk boundaries stay multiples of 256 rows (the filter's object tiles)
-  for (uint64_t r = r_start, size = kBatchBootRows; r < h->n; size *= 2) {
+  for (uint64_t r = r_start, size = h->batch_boot; r < h->n; size *= 2) {
     const uint64_t e = std::min<uint64_t>(h->n, r + size);
     if (use_bf16) {
-      const FilterPlan fp = plan_bf16_filter(nqq, r, e, h->num_sms);
+      const FilterPlan fp = plan_bf16_filter(nqq, r, e, h->num_sms, h->batch_qt);
       if (fp.grid > log_ctas) return fail(TOPK_ERR_STATE, "filter grid %llu above its logs", (unsigned long long)fp.grid);
       CK(launch_bf16_filter(fp, static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf.p), r, e,
                             dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
@@ -844,7 +847,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   // margin makes a new shape).  The graph reads the query descriptors and states that
   // the stream uploaded and cleared before it.
   std::vector<uint64_t> key = {nq, kmax, capmax, use_bf16, use_learned, h->n, h->d, h->ld, boot,
-                               (uint64_t)h->num_sms, log_ctas, h->wait_limit, h->num_parts};
+                               (uint64_t)h->num_sms, log_ctas, h->wait_limit, h->num_parts, h->batch_qt};
   const void *key_ptrs[] = {h->table, dq, dst, dbest, dcand, h->b_ids.p, h->b_scores.p, h->b_count.p,
                             h->b_thr.p, h->xbf.p, h->b_abf.p, h->b_log.p, h->b_logh.p, h->b_err.p, h->b_sw.p,
                             h->b_feat.p, h->b_pred.p, h->pstats, h->mlp};
@@ -1230,6 +1233,77 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
     if (st != TOPK_OK) return st;
     if (counts) counts[j] = c;
     if (thresholds) thresholds[j] = th;
+  }
+  return TOPK_OK;
+}
+
+int topk_set_batch_tiles(topk_table_t h, uint32_t qt_per_cta, uint32_t boot_rows) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (qt_per_cta > 16) return fail(TOPK_ERR_ARG, "qt_per_cta %u above 16", qt_per_cta);
+  if (boot_rows < 256 || boot_rows > kBatchBootMax || boot_rows % 256)
+    return fail(TOPK_ERR_ARG, "boot_rows %u: a multiple of 256 in [256, %u]", boot_rows, kBatchBootMax);
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  h->batch_qt = qt_per_cta;
+  h->batch_boot = boot_rows;
+  return TOPK_OK;
+}
+
+int topk_get_batch_tiles(topk_table_t h, uint32_t *qt_per_cta, uint32_t *boot_rows) {
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->batch_mu);
+  if (qt_per_cta) *qt_per_cta = h->batch_qt;
+  if (boot_rows) *boot_rows = h->batch_boot;
+  return TOPK_OK;
+}
+
+int topk_tune_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,
+                    uint64_t wstride, const uint8_t *attrs, uint64_t astride, double *report) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (nq == 0 || !ks) return fail(TOPK_ERR_ARG, "empty query set");
+  uint64_t kmax = 1;
+  for (uint64_t j = 0; j < nq; j++) kmax = std::max<uint64_t>(kmax, std::min<uint64_t>(ks[j], h->n));
+  std::vector<uint64_t> ids(nq * kmax), cnt(nq);
+  std::vector<float> sc(nq * kmax), th(nq);
+  const uint32_t qts[3] = {4, 8, 0}, boots[2] = {kBatchBootRows, kBatchBootMax};
+  double best_ms = -1.0, default_ms = -1.0;
+  uint32_t best_qt = 0, best_boot = kBatchBootRows, keep_qt, keep_boot;
+  {
+    std::lock_guard<std::mutex> lk(h->batch_mu);
+    keep_qt = h->batch_qt;
+    keep_boot = h->batch_boot;
+  }
+  auto set = [&](uint32_t qt, uint32_t b) {
+    std::lock_guard<std::mutex> lk(h->batch_mu);
+    h->batch_qt = qt;
+    h->batch_boot = b;
+  };
+  for (uint32_t b : boots)
+    for (uint32_t qt : qts) {
+      set(qt, b);
+      double ms = 0;
+      for (int rep = 0; rep < 2; rep++) {  // the first run captures the batch's graph
+        const int st = topk_query_batch(h, nq, ks, qqs, weights, wstride, attrs, astride, ids.data(), sc.data(), kmax,
+                                        cnt.data(), th.data());
+        if (st != TOPK_OK) {
+          set(keep_qt, keep_boot);
+          return st;
+        }
+        if ((topk_last_batch_stats(h, &ms, nullptr, nullptr)) != TOPK_OK) return TOPK_ERR_STATE;
+      }
+      if (qt == 0 && b == kBatchBootRows) default_ms = ms;
+      if (best_ms < 0 || ms < best_ms) {
+        best_ms = ms;
+        best_qt = qt;
+        best_boot = b;
+      }
+    }
+  set(best_qt, best_boot);
+  if (report) {
+    report[0] = best_qt ? best_qt : 16;
+    report[1] = best_boot;
+    report[2] = best_ms;
+    report[3] = default_ms;
   }
   return TOPK_OK;
 }

@@ -104,6 +104,28 @@ class Table:
                                  ids.reshape(-1), sc.reshape(-1), kstride, counts.ctypes.data, ths.ctypes.data))
         return ids, sc, counts, ths
 
+    def set_batch_tiles(self, qt_per_cta=0, boot_rows=8192):
+        check(_lib.load().topk_set_batch_tiles(self._h, int(qt_per_cta), int(boot_rows)))
+
+    def batch_tiles(self):
+        qt, boot = C.c_uint32(), C.c_uint32()
+        check(_lib.load().topk_get_batch_tiles(self._h, C.byref(qt), C.byref(boot)))
+        return qt.value, boot.value
+
+    def tune_batch(self, ks, weights, attrs, qqs=None):
+        """Autotune the batched path's tiles on these queries (see topk_tune_batch);
+        returns {query_tiles_per_cta, boot_rows, best_ms, default_ms}."""
+        ks = np.ascontiguousarray(ks, np.uint64)
+        nq = len(ks)
+        W = np.ascontiguousarray(weights, np.float32).reshape(nq, -1)
+        A = np.ascontiguousarray(attrs, np.uint8).reshape(nq, -1)
+        qqs = np.full(nq, A.shape[1], np.uint32) if qqs is None else np.ascontiguousarray(qqs, np.uint32)
+        rep = np.zeros(4, np.float64)
+        check(_lib.load().topk_tune_batch(self._h, nq, ks, qqs, W.reshape(-1), W.shape[1], A.reshape(-1), A.shape[1],
+                                          rep))
+        return {"query_tiles_per_cta": int(rep[0]), "boot_rows": int(rep[1]), "best_ms": float(rep[2]),
+                "default_ms": float(rep[3])}
+
     # -- partitions and pruned queries -------------------------------------
     def build_partitions(self, part_rows=1 << 16):
         check(_lib.load().topk_build_partitions(self._h, int(part_rows)))

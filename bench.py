@@ -23,7 +23,9 @@ flush is needed between queries.
   pruned   the partitioned workload: 2^27 x 8 anticorrelated in 2^11 partitions of
           2^16 rows, the learned model fitted on 10^5 exactly labelled queries,
           2000 fresh queries by full scan, plain pruning and learned pruning:
-          partitions scanned, fallback rate, speed-up, identical results.
+          partitions scanned, fallback rate, speed-up, identical results; then
+          500 of them pruned over partitions rebuilt in VTA's and in PTA's order
+          (device index builds timed).
   c5       (with --c5, or alone with --only c5) the full chosen form: 16384 queries
           (k log-uniform in [1, 1024]) over a 2^28 x 16 table mixed 1/3 each
           independent/correlated/anticorrelated, plain batched FP32 against the
@@ -326,12 +328,36 @@ def run_c5(T, torch, dist, device, n, nq, methods=("fp32", "learned_bf16")):
                        k_log=True, fp32_reps=1, label="mixed 1/3 independent/correlated/anticorrelated", tune=False)
 
 
+def reference_index_build(d, sample_rows=1 << 22):
+    """The reference's own VTA (threaded build, IMP 2) and PTA index builds (oracle/_ref,
+    compiled from cpu/VTA.h and cpu/PTA.h) on an anticorrelated sample of the same
+    shape; their own init timers (tt_init, normalisation excluded)."""
+    from oracle import oracle as O
+    from oracle.vta_oracle import ref_index_rows
+    raw = O.generate(sample_rows, d, 2, 0)
+    out = {"sample_rows": sample_rows, "cores": os.cpu_count(), "kind": "reference"}
+    for kind in ("vta", "pta"):
+        try:
+            got = ref_index_rows(kind, raw, 2)
+        except Exception as e:  # report, do not fail the bench
+            got, out[f"{kind}_error"] = None, str(e)[:200]
+        if got is None:
+            out.setdefault("unavailable", "reference index library not built")
+            continue
+        out[f"{kind}_init_s"] = got[1] / 1000.0
+    return out
+
+
 def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000, seed=4):
     """Partitioned workload: an anticorrelated n x d table in partitions of part_rows
     rows; the learned model fitted on n_train queries labelled exactly; n_test fresh
     queries (attribute subsets of size U{2..d}, k log-uniform in [16, 1024]) answered
     by the plain full scan, the plain pruned method and the learned pruned method,
-    results checked identical; host wall time per query (each call is synchronous)."""
+    results checked identical; host wall time per query (each call is synchronous).
+    Then the partitions are rebuilt in VTA's order (one range and the threaded build's
+    16), then in PTA's, each time the first 500 queries answered pruned again (checked
+    identical); the reference's own VTA and PTA index builds are timed on a 2^22-row
+    sample on the host."""
     t = T.Table(n, d, device=device)
     t.generate(T.DIST_ANTICORRELATED, 0)
     t.normalize()
@@ -353,10 +379,14 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000
     scanned_p = scanned_l = accepted = 0
     identical = True
     P = 0
+    n_vta = min(n_test, 500)
+    kept = []
     for j in range(n_test):
         k, w, a = int(ks[j]), W[j], attrs[j]
         t0 = time.perf_counter()
         r0 = t.query(k, w, a)
+        if j < n_vta:
+            kept.append(r0)
         t1 = time.perf_counter()
         r1 = t.query_pruned(k, w, a)
         t2 = time.perf_counter()
@@ -371,6 +401,31 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000
         P = r1[3][1]
         for x, y, z in zip(r0, r1[:3], r2[:3]):
             identical &= np.asarray(x).tobytes() == np.asarray(y).tobytes() == np.asarray(z).tobytes()
+    # the first n_vta queries again over partitions in VTA's and in PTA's order
+    # (cpu/VTA.h:121-135, cpu/PTA.h:88-236)
+    index_orders = {}
+    for name, order in (("vta_order", T.ORDER_VTA), ("vta_threads_order", T.ORDER_VTA_THREADS),
+                        ("pta_order", T.ORDER_PTA)):
+        b0 = time.perf_counter()
+        t.build_partitions(part_rows, order=order)  # first build: module loading, allocations
+        first_s = time.perf_counter() - b0
+        b0 = time.perf_counter()
+        t.build_partitions(part_rows, order=order)
+        ob_s = time.perf_counter() - b0
+        for j in range(min(3, n_vta)):
+            t.query_pruned(int(ks[j]), W[j], attrs[j])
+        o_s, scanned_o = 0.0, 0
+        for j in range(n_vta):
+            t0 = time.perf_counter()
+            r = t.query_pruned(int(ks[j]), W[j], attrs[j])
+            o_s += time.perf_counter() - t0
+            scanned_o += r[3][0]
+            for x, y in zip(kept[j], r[:3]):
+                identical &= np.asarray(x).tobytes() == np.asarray(y).tobytes()
+        index_orders[name] = {"queries": n_vta, "pruned_queries_per_s": n_vta / o_s,
+                              "partitions_scanned_fraction": scanned_o / (n_vta * P), "partition_build_s": ob_s,
+                              "first_build_s": first_s}
+    index_orders["index_build_cpu_reference"] = reference_index_build(d)
     t.close()
     qps = {key: n_test / v for key, v in times.items()}
     return {
@@ -384,6 +439,7 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000
         "fallback_rate": 1.0 - accepted / n_test,
         "identical_results": bool(identical),
         "partition_build_s": build_s,
+        **index_orders,
         "fit": fit,
         "timing": "host wall clock per synchronous query call",
     }

@@ -151,6 +151,36 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
  * 4*(d+1)*n more bytes of device memory; rebuild after the table changes. */
 int topk_build_partitions(topk_table_t h, uint32_t part_rows);
 
+/* Orders of the partitioned copy. */
+#define TOPK_ORDER_MORTON 0 /* Morton code of the attribute values (topk_build_partitions) */
+#define TOPK_ORDER_VTA 1    /* VTA's order (cpu/VTA.h:121-135): each attribute's list sorted
+                             * by value descending, each row's minimum position over the
+                             * lists, rows by that position.  With part_rows = 1024 the
+                             * partitions are VTA's blocks; their per-attribute max bounds
+                             * every row of the block, at most the reference's tarray of
+                             * the block before. */
+#define TOPK_ORDER_PTA 2    /* PTA's order (cpu/PTA.h:88-167, 203-236): rows split into
+                             * 2^(d-1) groups by the medians of their d-1 hyperspherical
+                             * angles, each group in VTA's order, groups by number.
+                             * Partitions are part_rows consecutive rows of that order, so
+                             * one may span two groups (the reference starts a block at
+                             * each group).  Needs n >= 2 and d <= 32. */
+#define TOPK_ORDER_VTA_THREADS 3 /* VTA's order as its threaded build makes it (IMP 2, the
+                                  * reference's default): 16 ranges of ceil(n/16) rows,
+                                  * each in VTA's order on its own (cpu/VTA.h:13,78-85). */
+/* In the VTA and PTA orders ties go to the lower row id (the reference's sorts are not
+ * stable and leave them unspecified: rows sharing a minimum position, equal values);
+ * PTA's angles order as their tangents, which are compared. */
+
+/* topk_build_partitions with a choice of order.  The VTA and PTA orders sort on the
+ * device (radix sorts, n < 2^31) and need about 20*n (VTA) or 32*n (VTA_THREADS, PTA)
+ * bytes of scratch while they run. */
+int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order);
+
+/* The partitioned copy's row ids (n entries): row i of the copy is row ids[i] of the
+ * table. */
+int topk_partition_ids(topk_table_t h, uint32_t *ids);
+
 /* The partitions: count, rows each, and (arrays of num_parts*d, row p*d + m for
  * partition p, attribute m; any may be NULL) per-attribute min, max and mean. */
 int topk_partition_info(topk_table_t h, uint32_t *num_parts, uint32_t *part_rows, float *mins, float *maxs,

@@ -1,11 +1,13 @@
 """Build recipe for the CPU checker (TEST INFRASTRUCTURE ONLY).
 
-Two products:
+Products:
   * oracle/_build/liboracle.so  - the C restatement (topk_oracle.c), strict FP flags.
   * oracle/_ref/libref_tpac.so  - the reference's own TPAc (cpu/TPAc.h, cpu/AA.h,
     common/common.h, time/Time.h) compiled from where its sources lie, through the
     forwarding shim ref_tpac_shim.cpp.  Built only when the reference tree is present
     (TOPK_REFERENCE, default /root/reference); the .so then travels with the repo.
+  * oracle/_ref/libref_index_d{D}_imp{I}.so - the reference's VTA and PTA index
+    builds (cpu/VTA.h, cpu/PTA.h) through ref_index_shim.cpp, likewise.
 
 Strict flags for both: -O3 -ffp-contract=off, never -ffast-math.  The reference's
 own Makefile:60 adds -ffast-math, which changes the normalised table and the
@@ -64,7 +66,37 @@ def build_ref(verbose=False, force=False):
     return REF_SO
 
 
+# (NUM_DIMS, IMP) of the reference index builds compiled for the tests and the
+# benchmark: the reference fixes both at compile time (Makefile:22-23,60).
+INDEX_CONFIGS = ((4, 2), (4, 1), (8, 2), (8, 1))
+
+
+def ref_index_so(num_dims, imp):
+    return os.path.join(REF_OUT, f"libref_index_d{num_dims}_imp{imp}.so")
+
+
+def build_ref_index(verbose=False, force=False):
+    """Compile the reference VTA / PTA index builds through ref_index_shim.cpp, one
+    library per (NUM_DIMS, IMP).  Returns the list of built paths (those present when
+    the reference tree is absent)."""
+    root = reference_root()
+    hdrs = [os.path.join(root, p) for p in ("cpu/VTA.h", "cpu/PTA.h", "cpu/AA.h", "common/common.h",
+                                            "time/Time.h")]
+    outs = [ref_index_so(dd, imp) for dd, imp in INDEX_CONFIGS]
+    if not all(os.path.exists(h) for h in hdrs):
+        return [o for o in outs if os.path.exists(o)]
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_index_shim.cpp")
+    for (dd, imp), out in zip(INDEX_CONFIGS, outs):
+        if force or _stale(out, [shim] + hdrs):
+            _run(["g++", "-std=c++14", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math",
+                  "-fopenmp", "-fPIC", "-shared", "-w", f"-DNUM_DIMS={dd}", f"-DIMP={imp}",
+                  "-I", root, "-I", os.path.join(HERE, "stub"), shim, "-o", out], verbose)
+    return outs
+
+
 if __name__ == "__main__":
     v = "-v" in sys.argv
     print(build_oracle(v, force="-f" in sys.argv))
     print(build_ref(v, force="-f" in sys.argv))
+    print(build_ref_index(v, force="-f" in sys.argv))

@@ -143,3 +143,67 @@ def test_pruned_ties_in_reordered_rows_go_to_the_lower_original_id():
                 got = t.query_pruned(k, w, a, cut=float(want[2]))
                 H.assert_same_result(got[:3], want)
                 assert got[3][2] == 1
+
+
+@pytest.mark.parametrize("order", ["vta", "vta16", "pta"])
+@pytest.mark.parametrize("n,d,dist,ties", [(200003, 6, 0, False), (200003, 6, 1, False), (200003, 6, 2, False),
+                                          (200003, 6, 3, False), (200003, 6, 0, True), (65536, 1, 0, False),
+                                          (70001, 2, 2, False), (50001, 20, 0, False)])
+def test_index_order_matches_oracle(order, n, d, dist, ties):
+    """The device VTA / PTA orders (stable radix sorts) equal the restatements of
+    VTA::init (one row range, or 16 as its threaded build) and PTA::polar +
+    create_partitions, ties by the lower id; the partitioned copy holds the rows in
+    that order and its block bounds are those rows' maxima."""
+    from oracle.vta_oracle import pta_order, vta_order
+    codes = {"vta": T.ORDER_VTA, "vta16": T.ORDER_VTA_THREADS, "pta": T.ORDER_PTA}
+    want = {"vta": lambda x: vta_order(x), "vta16": lambda x: vta_order(x, 16), "pta": pta_order}
+    with T.Table(n, d) as t:
+        t.generate(dist, 11 + dist)
+        t.normalize()
+        if ties:  # few distinct values per attribute: long runs of equal keys
+            t.upload(np.round(t.download() * 8) / 8)
+        tn = t.download()
+        t.build_partitions(1024, order=codes[order])
+        perm = t.partition_ids()
+        assert np.array_equal(perm, want[order](tn))
+        R, mins, maxs, means = t.partition_info()
+        pad = (-n) % R
+        blocks = np.pad(tn[:, perm], ((0, 0), (0, pad)), constant_values=-np.inf).reshape(d, -1, R)
+        assert np.array_equal(maxs, blocks.max(axis=2).T)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("dist", [2, 0])
+def test_pruned_on_vta_pta_partitions_matches_oracle(dist, order):
+    n, d = (1 << 19) + 77, 8
+    rng = np.random.default_rng(40 + dist)
+    with T.Table(n, d) as t:
+        t.generate(dist, 5)
+        t.normalize()
+        tn = t.download()
+        t.build_partitions(4096, order=order)
+        scanned = []
+        for j in range(16):
+            w, a = H.random_query(rng, d)
+            k = int(rng.choice([1, 10, 256, 1024]))
+            ids, sc, th, st = t.query_pruned(k, w, a)
+            H.assert_same_result((ids, sc, th), O.topk_numpy(tn, k, w, a))
+            scanned.append(st[0] / st[1])
+        print(f"order {order} dist {dist}: mean fraction of partitions scanned {np.mean(scanned):.3f}")
+        # the Morton copy is replaced: a rebuild in Morton order still answers exactly
+        t.build_partitions(4096)
+        w, a = H.random_query(rng, d)
+        H.assert_same_result(t.query_pruned(64, w, a)[:3], O.topk_numpy(tn, 64, w, a))
+
+
+def test_partition_order_errors():
+    with T.Table(5000, 4) as t:
+        t.generate(0, 1)
+        with pytest.raises(T.TopKError):
+            t.partition_ids()  # nothing built yet
+        with pytest.raises(T.TopKError):
+            t.build_partitions(1024, order=7)
+    with T.Table(5000, 33) as t:
+        t.generate(0, 1)
+        with pytest.raises(T.TopKError):
+            t.build_partitions(1024, order=T.ORDER_PTA)  # 2^32 groups

@@ -5,10 +5,12 @@ Drop-in for the TPAc path of avionicscode/TopK: the C ABI is include/topk_b200.h
 Python face, mirroring the reference's AA / TPAc algorithm-class API.
 """
 from ._lib import (BATCH_AUTO, BATCH_BF16, BATCH_FP32, BATCH_LEARNED, BATCH_LOOP, DIST_ANTICORRELATED, DIST_CORRELATED,
-                   DIST_INDEPENDENT, DIST_MIXED, MAX_D, MAX_K, MAX_Q, TopKError, load)
+                   DIST_INDEPENDENT, DIST_MIXED, MAX_D, MAX_K, MAX_Q, ORDER_MORTON, ORDER_PTA, ORDER_VTA,
+                   ORDER_VTA_THREADS, TopKError, load)
 from .table import Table
 from .tpac import AA, TPAc
 
 __all__ = ["Table", "AA", "TPAc", "TopKError", "load", "MAX_K", "MAX_Q", "MAX_D", "DIST_CORRELATED",
            "DIST_INDEPENDENT", "DIST_ANTICORRELATED", "DIST_MIXED", "BATCH_AUTO", "BATCH_LOOP", "BATCH_FP32",
-           "BATCH_BF16", "BATCH_LEARNED"]
+           "BATCH_BF16", "BATCH_LEARNED", "ORDER_MORTON", "ORDER_VTA", "ORDER_PTA",
+           "ORDER_VTA_THREADS"]

@@ -28,6 +28,7 @@ DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
 
 # topk_query_batch methods (TOPK_BATCH_* in include/topk_b200.h)
 BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16, BATCH_LEARNED = 0, 1, 2, 3, 4
+ORDER_MORTON, ORDER_VTA, ORDER_PTA, ORDER_VTA_THREADS = 0, 1, 2, 3
 
 
 class TopKError(RuntimeError):
@@ -89,6 +90,8 @@ SIGNATURES = [
     ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("topk_last_batch_switched", C.c_int, [_H, C.POINTER(C.c_uint64)]),
     ("topk_set_batch_tiles", C.c_int, [_H, C.c_uint32, C.c_uint32]),
+    ("topk_build_partitions_ordered", C.c_int, [_H, C.c_uint32, C.c_int]),
+    ("topk_partition_ids", C.c_int, [_H, _u32p]),
     ("topk_get_batch_tiles", C.c_int, [_H, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("topk_tune_batch", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _f64p]),
     ("topk_query_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, _f32p,

@@ -18,7 +18,10 @@
 //
 // Device layout: ptable column-major with the table's stride (partition p = rows
 // [p*R, (p+1)*R)), row_ids[row] = original id, stats [P][d] each.
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include <cstdint>
 
@@ -136,6 +139,83 @@ __global__ void __launch_bounds__(256) part_stats_kernel(const float *__restrict
   }
 }
 
+// ------------------------------------------------------- VTA and PTA orders
+// VTA's index (cpu/VTA.h:121-135): each attribute's list sorted by value, descending;
+// each tuple's minimum position over the lists; tuples sorted by that position.
+// PTA's (cpu/PTA.h:88-167, 203-236): the tuples first split into partitions by the
+// medians of their d-1 hyperspherical angles, then VTA's order inside each partition.
+// VTA's threaded build (IMP 2) orders THREADS = 16 equal row ranges on their own.
+// Here with stable device radix sorts, so ties go to the lower id (the reference's
+// parallel sorts leave them unspecified).  The partition comes in as the high word of
+// each list's 64-bit key (partition, then value descending); a partition's rows then
+// hold one range of positions in every list, so the global minimum position orders
+// the tuples by partition and, inside one, by the partition-local minimum position.
+__global__ void col_keys_kernel(const float *__restrict__ col, uint64_t n, uint32_t *__restrict__ keys,
+                                uint32_t *__restrict__ ids) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    keys[i] = f2key(__ldg(col + i));  // NaN -> 0: last in a descending list
+    ids[i] = (uint32_t)i;
+  }
+}
+
+// partition in the high word, value descending below it; part clamped to pmax
+// (cpu/PTA.h:166)
+__global__ void col_keys64_kernel(const float *__restrict__ col, uint64_t n, const uint32_t *__restrict__ part,
+                                  uint32_t pmax, uint64_t *__restrict__ keys, uint32_t *__restrict__ ids) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    keys[i] = ((uint64_t)min(part[i], pmax) << 32) | (uint64_t)(~f2key(__ldg(col + i)));
+    ids[i] = (uint32_t)i;
+  }
+}
+
+// PTA's angle coordinate c of every row as a sort key (cpu/PTA.h:108-134):
+// f_c = sqrt(sum_{j>c} (x_j - 1.1f)^2) / (x_c - 1.1f), every operation rounded on its
+// own as in the reference's AVX path.  The reference keeps |atan(f_c)| * 180/pi, a
+// monotone image of |f_c|, so |f_c| orders the rows the same way up to the ties its
+// sort leaves unspecified.
+__global__ void pta_angle_keys_kernel(const float *__restrict__ table, uint64_t ld, uint32_t d, uint64_t n,
+                                      uint32_t c, uint32_t *__restrict__ keys, uint32_t *__restrict__ ids) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    float curr = __fsub_rn(__ldg(table + (uint64_t)(d - 1) * ld + i), 1.1f), s = 0.0f, nxt = 0.0f;
+    for (uint32_t m = d - 1; m > c; --m) {
+      nxt = __fsub_rn(__ldg(table + (uint64_t)(m - 1) * ld + i), 1.1f);
+      s = __fadd_rn(s, __fmul_rn(curr, curr));
+      curr = nxt;
+    }
+    keys[i] = f2key(fabsf(__fdiv_rn(__fsqrt_rn(s), nxt)));
+    ids[i] = (uint32_t)i;
+  }
+}
+
+// part[id] += mul * (rank / mod) over one angle's ascending list (cpu/PTA.h:152-163);
+// rank < n <= 2 * mod + 1, so the quotient is 0, 1 or 2
+__global__ void pta_part_add_kernel(const uint32_t *__restrict__ sorted_ids, uint64_t n, uint64_t mod, uint32_t mul,
+                                    uint32_t *__restrict__ part) {
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t q = p >= 2 * mod ? 2u : (p >= mod ? 1u : 0u);
+    if (q) part[sorted_ids[p]] += mul * q;  // each id once per list: no race
+  }
+}
+
+// VTA's threaded build (IMP 2): rows in `slices` ranges of ceil(n / slices) rows, each
+// ordered on its own (cpu/VTA.h:13,78-85)
+__global__ void range_part_kernel(uint64_t n, uint64_t range_rows, uint32_t *__restrict__ part) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    part[i] = (uint32_t)(i / range_rows);
+}
+
+__global__ void iota_kernel(uint32_t *__restrict__ v, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+
+__global__ void min_rank_kernel(const uint32_t *__restrict__ sorted_ids, uint64_t n, uint32_t *__restrict__ rank) {
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = sorted_ids[p];  // each id once per list: no race
+    rank[id] = min(rank[id], (uint32_t)p);
+  }
+}
+
 int grid_for(uint64_t n, int num_sms) {
   const uint64_t b = (n + 255) / 256;
   return (int)(b < (uint64_t)num_sms * 16 ? (b ? b : 1) : (uint64_t)num_sms * 16);
@@ -154,6 +234,67 @@ cudaError_t launch_partition_build(const float *table, uint64_t ld, uint32_t d, 
   bin_scan_kernel<<<1, 1024, 0, s>>>(hist);
   scatter_kernel<<<g, 256, 0, s>>>(keys, n, hist, perm);
   gather_rows_kernel<<<g, 256, 0, s>>>(table, ld, d, n, perm, ptable);
+  return cudaGetLastError();
+}
+
+uint64_t index_order_work_words(uint64_t n, IndexOrder kind) { return (kind == IndexOrder::kVta ? 5 : 8) * n; }
+
+cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, IndexOrder kind,
+                               uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
+                               cudaStream_t s) {
+  const bool pta = kind == IndexOrder::kPta, grouped = kind != IndexOrder::kVta;
+  if (n > 0x7FFFFFFFull || (pta && (n < 2 || d > 32))) return cudaErrorInvalidValue;
+  // work, VTA: keys in/out, ids in/out, min ranks (n words each); grouped orders:
+  // 64-bit keys in/out (2n words each, the angle sorts use their first halves), ids
+  // in/out, min ranks, groups
+  uint32_t *kin = work, *kout = work + (grouped ? 2 * n : n);
+  uint32_t *iin = work + (grouped ? 4 * n : 2 * n), *iout = iin + n, *rank = iout + n, *part = rank + n;
+  uint64_t *kin64 = reinterpret_cast<uint64_t *>(kin), *kout64 = reinterpret_cast<uint64_t *>(kout);
+  const uint32_t gbits = pta ? d - 1 : (grouped ? 4 : 0);  // groups < 2^gbits
+  const int nn = (int)n;
+  if (!temp) {  // size query
+    size_t a = 0, b = 0, c = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(nullptr, a, kin, kout, iin, iout, nn, 0, 32, s);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, b, kin, kout, iin, iout, nn, 0, 32, s);
+    if (e == cudaSuccess && grouped)
+      e = cub::DeviceRadixSort::SortPairs(nullptr, c, kin64, kout64, iin, iout, nn, 0, 32 + (int)gbits, s);
+    *temp_bytes = std::max(a, std::max(b, c));
+    return e;
+  }
+  const int g = grid_for(n, num_sms);
+  size_t tb = *temp_bytes;
+  cudaError_t e = cudaMemsetAsync(rank, 0xFF, n * sizeof(uint32_t), s);
+  if (pta) {
+    if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, n * sizeof(uint32_t), s);
+    for (uint32_t c = 0; e == cudaSuccess && c + 1 < d; ++c) {  // median split per angle
+      pta_angle_keys_kernel<<<g, 256, 0, s>>>(table, ld, d, n, c, kin, iin);
+      e = cub::DeviceRadixSort::SortPairs(temp, tb, kin, kout, iin, iout, nn, 0, 32, s);
+      if (e == cudaSuccess) pta_part_add_kernel<<<g, 256, 0, s>>>(iout, n, n / 2, 1u << c, part);
+    }
+  } else if (grouped) {
+    range_part_kernel<<<g, 256, 0, s>>>(n, (n - 1) / kVtaThreadRanges + 1, part);
+  }
+  for (uint32_t m = 0; e == cudaSuccess && m < d; ++m) {
+    if (grouped) {
+      col_keys64_kernel<<<g, 256, 0, s>>>(table + (uint64_t)m * ld, n, part, (1u << gbits) - 1u, kin64, iin);
+      e = cub::DeviceRadixSort::SortPairs(temp, tb, kin64, kout64, iin, iout, nn, 0, 32 + (int)gbits, s);
+    } else {
+      col_keys_kernel<<<g, 256, 0, s>>>(table + (uint64_t)m * ld, n, kin, iin);
+      e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, kin, kout, iin, iout, nn, 0, 32, s);
+    }
+    if (e == cudaSuccess) min_rank_kernel<<<g, 256, 0, s>>>(iout, n, rank);
+  }
+  if (e != cudaSuccess) return e;
+  // tuples by minimum position, ties by the lower id
+  iota_kernel<<<g, 256, 0, s>>>(iin, n);
+  e = cub::DeviceRadixSort::SortPairs(temp, tb, rank, kout, iin, perm, nn, 0, 32, s);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
+                               float *ptable, int num_sms, cudaStream_t s) {
+  gather_rows_kernel<<<grid_for(n, num_sms), 256, 0, s>>>(table, ld, d, n, perm, ptable);
   return cudaGetLastError();
 }
 

@@ -1343,9 +1343,30 @@ int topk_last_batch_switched(topk_table_t h, uint64_t *switched) {
 }
 
 int topk_build_partitions(topk_table_t h, uint32_t part_rows) {
+  return topk_build_partitions_ordered(h, part_rows, TOPK_ORDER_MORTON);
+}
+
+int topk_partition_ids(topk_table_t h, uint32_t *ids) {
   g_last_error.clear();
+  if (!h || !ids) return fail(TOPK_ERR_ARG, "null argument");
+  if (!h->pids || h->part_version != h->data_version) return fail(TOPK_ERR_STATE, "no partitions of the current table");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  CK(cudaMemcpy(ids, h->pids, h->n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return TOPK_OK;
+}
+
+int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order) {
+  g_last_error.clear();
+  if (order != TOPK_ORDER_MORTON && order != TOPK_ORDER_VTA && order != TOPK_ORDER_PTA &&
+      order != TOPK_ORDER_VTA_THREADS)
+    return fail(TOPK_ERR_ARG, "unknown order %d", order);
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  if (order != TOPK_ORDER_MORTON && h->n > 0x7FFFFFFFull)
+    return fail(TOPK_ERR_UNSUPPORTED, "VTA and PTA orders need n < 2^31 rows");
+  if (order == TOPK_ORDER_PTA && (h->n < 2 || h->d > 32))
+    return fail(TOPK_ERR_UNSUPPORTED, "PTA order needs n >= 2 and d <= 32");
   if (part_rows < 1024 || part_rows > (1u << 24) || (part_rows & (part_rows - 1)))
     return fail(TOPK_ERR_ARG, "part_rows must be a power of two in [1024, 2^24]");
   uint32_t lg = 0;
@@ -1399,9 +1420,26 @@ int topk_build_partitions(topk_table_t h, uint32_t part_rows) {
   if (e == cudaSuccess) e = cudaMalloc(&h->pstats, 3 * P * h->d * sizeof(float));
   if (e == cudaSuccess) e = cudaMemsetAsync(h->ptable, 0, h->ld * h->d * sizeof(float), s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dls, lo_scale.data(), lo_scale.size() * 4, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && order == TOPK_ORDER_MORTON)
     e = launch_partition_build(h->table, h->ld, h->d, h->n, dls, dls + h->d, bits, keys, hist, h->pids, h->ptable,
                                h->num_sms, s);
+  if (e == cudaSuccess && order != TOPK_ORDER_MORTON) {
+    const IndexOrder kind = order == TOPK_ORDER_PTA           ? IndexOrder::kPta
+                            : order == TOPK_ORDER_VTA_THREADS ? IndexOrder::kVtaThreads
+                                                              : IndexOrder::kVta;
+    uint32_t *work = nullptr;
+    void *temp = nullptr;
+    size_t temp_bytes = 0;
+    e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, nullptr, nullptr, &temp_bytes, h->num_sms, s);
+    if (e == cudaSuccess) e = cudaMalloc(&work, index_order_work_words(h->n, kind) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&temp, std::max<size_t>(temp_bytes, 16));
+    if (e == cudaSuccess)
+      e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, work, temp, &temp_bytes, h->num_sms, s);
+    if (e == cudaSuccess) e = launch_gather_rows(h->table, h->ld, h->d, h->n, h->pids, h->ptable, h->num_sms, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // before the scratch goes
+    cudaFree(work);
+    cudaFree(temp);
+  }
   float *pmin = h->pstats, *pmax = h->pstats + P * h->d, *pmean = h->pstats + 2 * P * h->d;
   if (e == cudaSuccess) e = launch_partition_stats(h->ptable, h->ld, h->d, h->n, lg, (uint32_t)P, pmin, pmax, pmean, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

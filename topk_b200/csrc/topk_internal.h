@@ -129,6 +129,20 @@ cudaError_t launch_gather(const float *table, uint64_t ld, uint32_t d, const uin
 cudaError_t launch_partition_build(const float *table, uint64_t ld, uint32_t d, uint64_t n, const float *lo,
                                    const float *scale, uint32_t bits, uint16_t *keys, uint32_t *hist,
                                    uint32_t *perm, float *ptable, int num_sms, cudaStream_t s);
+// Index orders of the reference as a row permutation: VTA's (cpu/VTA.h:121-135), the
+// same over kVtaThreadRanges equal row ranges as VTA's threaded build makes it (IMP 2,
+// VPARTITIONS = THREADS, cpu/VTA.h:13,78-85), PTA's (cpu/PTA.h:88-167, 203-236).
+// work holds index_order_work_words(n, kind) words; temp is the radix sorts' scratch
+// (first call with temp == nullptr to size it).  n < 2^31; PTA also needs n >= 2 and
+// d <= 32.
+enum class IndexOrder { kVta, kVtaThreads, kPta };
+constexpr uint32_t kVtaThreadRanges = 16;
+uint64_t index_order_work_words(uint64_t n, IndexOrder kind);
+cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, IndexOrder kind,
+                               uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
+                               cudaStream_t s);
+cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
+                               float *ptable, int num_sms, cudaStream_t s);
 // Per-partition min / max / mean of each attribute, [num_parts][d] each.
 cudaError_t launch_partition_stats(const float *ptable, uint64_t ld, uint32_t d, uint64_t n, uint32_t rows_log2,
                                    uint32_t num_parts, float *mins, float *maxs, float *means, cudaStream_t s);

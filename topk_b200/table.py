@@ -127,8 +127,16 @@ class Table:
                 "default_ms": float(rep[3])}
 
     # -- partitions and pruned queries -------------------------------------
-    def build_partitions(self, part_rows=1 << 16):
-        check(_lib.load().topk_build_partitions(self._h, int(part_rows)))
+    def build_partitions(self, part_rows=1 << 16, order=0):
+        """order: ORDER_MORTON (0), ORDER_VTA (1), ORDER_PTA (2) or ORDER_VTA_THREADS (3),
+        see topk_build_partitions_ordered."""
+        check(_lib.load().topk_build_partitions_ordered(self._h, int(part_rows), int(order)))
+
+    def partition_ids(self):
+        """Row ids of the partitioned copy (row i of the copy is table row ids[i])."""
+        out = np.empty(self.n, np.uint32)
+        check(_lib.load().topk_partition_ids(self._h, out))
+        return out
 
     def partition_info(self):
         """(part_rows, mins, maxs, means) with arrays of shape (num_parts, d)."""

@@ -26,6 +26,9 @@ flush is needed between queries.
           partitions scanned, fallback rate, speed-up, identical results; then
           500 of them pruned over partitions rebuilt in VTA's and in PTA's order
           (device index builds timed).
+  loader   table files: a 2^22 x 16 table as the reference's '%f' CSV read by the
+          device loader (GB/s, rows/s) against the reference's fscanf loader on a
+          2^18-row sample (bit-identical check), and the binary format.
   c5       (with --c5, or alone with --only c5) the full chosen form: 16384 queries
           (k log-uniform in [1, 1024]) over a 2^28 x 16 table mixed 1/3 each
           independent/correlated/anticorrelated, plain batched FP32 against the
@@ -445,6 +448,72 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000
     }
 
 
+def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
+    """Table files: an n x d table written as the reference's text format ("%f", ','
+    separated, one object per line) and read back by the device CSV loader (host wall
+    time of topk_load_csv, file in the page cache, best of 3); the reference's own
+    fscanf loader (File<float>::load, oracle/_ref) timed on the file's first
+    sample_rows lines and checked bit for bit against the device loader on them; the
+    binary column-major file written and read."""
+    import shutil
+    import tempfile
+    from oracle import csv_oracle as CO
+    tmp = tempfile.mkdtemp(prefix="topk_loader_")
+    try:
+        p, ps, pb = (os.path.join(tmp, x) for x in ("t.csv", "s.csv", "t.bin"))
+        with T.Table(n, d, device=device) as t:
+            t.generate(T.DIST_INDEPENDENT, 21)
+            t.normalize()
+            b0 = time.perf_counter()
+            t.save_csv(p)
+            save_s = time.perf_counter() - b0
+            t.save_binary(pb)
+        size = os.path.getsize(p)
+        with open(p, "rb") as f, open(ps, "wb") as g:  # the first sample_rows lines
+            for _ in range(sample_rows):
+                g.write(f.readline())
+        times = []
+        with T.Table(n, d, device=device) as t:
+            st = t.load_csv(p)
+            for _ in range(3):
+                b0 = time.perf_counter()
+                st = t.load_csv(p)
+                times.append(time.perf_counter() - b0)
+            head = t.download()[:, :sample_rows]
+            btimes = []
+            for _ in range(3):
+                b0 = time.perf_counter()
+                t.load_binary(pb)
+                btimes.append(time.perf_counter() - b0)
+        b0 = time.perf_counter()
+        ref = CO.ref_load(ps, sample_rows, d)
+        ref_s = time.perf_counter() - b0
+        best = min(times)
+        out = {
+            "workload": f"n={n} x d={d} FP32 table as '%f' CSV ({size / 1e9:.2f} GB), page-cached file",
+            "csv_bytes": size,
+            "load_csv_s": best,
+            "load_csv_GBps": size / best / 1e9,
+            "load_csv_rows_per_s": n / best,
+            "host_converted": st["host_converted"],
+            "chunks": st["chunks"],
+            "save_csv_s": save_s,
+            "binary": {"bytes": os.path.getsize(pb), "load_s": min(btimes),
+                       "load_GBps": os.path.getsize(pb) / min(btimes) / 1e9},
+            "timing": "host wall clock of the whole call (file read, copies, parse, sync)",
+        }
+        if ref is not None:
+            out["cpu_reference"] = {"kind": "reference", "cores": 1, "sample_rows": sample_rows,
+                                    "sample": "File<float>::load (fscanf, transpose) on the first sample_rows lines",
+                                    "rows_per_s": sample_rows / ref_s}
+            out["speedup_vs_reference"] = (n / best) / (sample_rows / ref_s)
+            out["identical_to_reference_on_sample"] = bool(
+                np.array_equal(head.view(np.uint32), ref.view(np.uint32)))
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -455,7 +524,7 @@ def main():
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--only", choices=["batched", "pruned", "c5"], default=None,
+    ap.add_argument("--only", choices=["batched", "pruned", "c5", "loader"], default=None,
                     help="run one secondary workload alone (no JSON line; for profiling)")
     ap.add_argument("--c5", action="store_true",
                     help="add the full-form workload: 16384 queries over a mixed 2^28 x 16 table")
@@ -464,6 +533,7 @@ def main():
     ap.add_argument("--c5-methods", default="fp32,learned_bf16")
     ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--no-pruned", action="store_true")
+    ap.add_argument("--no-loader", action="store_true")
     ap.add_argument("--pruned-n", type=int, default=1 << 27)
     ap.add_argument("--pruned-queries", type=int, default=2000)
     ap.add_argument("--batched-n", type=int, default=BATCH_N)
@@ -481,6 +551,8 @@ def main():
                               methods=tuple(args.batched_methods.split(",")))
         elif args.only == "c5":
             out = run_c5(T, torch, None, 0, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
+        elif args.only == "loader":
+            out = run_loader(T, 0)
         else:
             out = run_pruned(T, 0, args.pruned_n, n_test=args.pruned_queries)
         print(json.dumps(out))
@@ -631,6 +703,8 @@ def main():
                                         methods=tuple(args.batched_methods.split(",")))
     if not args.no_pruned and rank == 0:
         result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
+    if not args.no_loader and rank == 0:
+        result["loader"] = run_loader(T, local)
     if args.c5:
         result["c5"] = run_c5(T, torch, dist, local, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
     if dist:

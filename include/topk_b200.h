@@ -12,6 +12,9 @@
  *   TPAc::init() -> normalize_transpose       cpu/TPAc.h:28-32,
  *                                             common/common.h:30-61 -> topk_normalize
  *   File<T>::gen(data, type)                  input/File.h:335-354  -> topk_generate
+ *   File<T>::count, load (transpose), store   input/File.h:108-132,
+ *                                             233-330, 405-431      -> topk_csv_shape, topk_load_csv,
+ *                                                                      topk_save_csv
  *   TPAc::findTopKscalar/simd/threads         cpu/TPAc.h:35,118,257 -> topk_query
  *   TPAc::findTopKsimdMQ + MQ loop            cpu/TPAc.h:210-254,
  *                                             validation/bench_cpu.h:198-232 -> topk_query_batch
@@ -90,6 +93,41 @@ int topk_normalize(topk_table_t h, float *mins, float *maxs);
 
 /* Copy the device table back (column-major, host stride ld_host >= n). */
 int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host);
+
+/* Table files.  Replace File<T> (input/File.h).
+ *
+ * topk_csv_shape: the shape File<T>::count reads from a comma-separated file
+ * (input/File.h:108-132): d = 1 + the commas of the first line, n = the number of
+ * '\n' (a last line without one is not counted, as there).
+ *
+ * topk_load_csv: the first n rows of a comma-separated file into the table,
+ * column-major, as File<T>::load with transpose (input/File.h:233-265, 306-330), each
+ * value rounded to FP32 as fscanf's "%f" does (correctly rounded).  The text is parsed
+ * on the device: the file streams through pinned buffers (chunk_bytes each, 0 = 16 MiB;
+ * a line must fit in one) and each chunk is split into rows and parsed there; values
+ * outside the device parser's exact range (more than 19 significant digits, exponents
+ * beyond +-22 after scaling, inf, nan, hex; at most 2^20 per load) are converted on the
+ * host with strtof.  Fields are separated by ',' with optional blanks, one object per
+ * line, blank lines skipped.  Rows with fewer or more than d fields, fields that are not
+ * numbers, or fewer than n rows return TOPK_ERR_ARG naming the row, and leave the table
+ * without data.  stats (4 entries, may be NULL): bytes parsed, rows found, values
+ * converted on the host, chunks.  The handle keeps the pipeline's buffers (two pinned
+ * and two device chunk buffers with their row arrays) for later loads; loads on one
+ * handle must not overlap.
+ *
+ * topk_save_csv: the table as File<T>::store writes it (input/File.h:405-431): one
+ * line per object, "%f" fields separated by ','.
+ *
+ * Binary column-major files (topk_save_binary / topk_load_binary / topk_binary_shape):
+ * a 64-byte header ("TOPKCOL1", uint32 version 1, uint32 element size 4, uint64 n,
+ * uint64 d, 32 reserved bytes), then the d columns of n FP32 values; loads stream
+ * through pinned buffers.  The file's n and d must equal the table's. */
+int topk_csv_shape(const char *path, uint64_t *n, uint64_t *d);
+int topk_load_csv(topk_table_t h, const char *path, uint64_t chunk_bytes, uint64_t *stats);
+int topk_save_csv(topk_table_t h, const char *path);
+int topk_binary_shape(const char *path, uint64_t *n, uint64_t *d);
+int topk_load_binary(topk_table_t h, const char *path);
+int topk_save_binary(topk_table_t h, const char *path);
 
 /* Exact top-k over all n objects with host inputs and host outputs (synchronous).
  * ids/scores must hold min(k, n) entries; count/threshold may be NULL.

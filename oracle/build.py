@@ -8,6 +8,8 @@ Products:
     (TOPK_REFERENCE, default /root/reference); the .so then travels with the repo.
   * oracle/_ref/libref_index_d{D}_imp{I}.so - the reference's VTA and PTA index
     builds (cpu/VTA.h, cpu/PTA.h) through ref_index_shim.cpp, likewise.
+  * oracle/_ref/libref_file.so - the reference's table loader (input/File.h) through
+    ref_file_shim.cpp, likewise.
 
 Strict flags for both: -O3 -ffp-contract=off, never -ffast-math.  The reference's
 own Makefile:60 adds -ffast-math, which changes the normalised table and the
@@ -95,8 +97,28 @@ def build_ref_index(verbose=False, force=False):
     return outs
 
 
+REF_FILE_SO = os.path.join(REF_OUT, "libref_file.so")
+
+
+def build_ref_file(verbose=False, force=False):
+    """Compile the reference table loader (input/File.h) through ref_file_shim.cpp.
+    Returns the .so path or None."""
+    root = reference_root()
+    hdrs = [os.path.join(root, p) for p in ("input/File.h", "time/Time.h",
+                                            "input/randdataset-1.1.0/src/randdataset.h")]
+    if not all(os.path.exists(h) for h in hdrs):
+        return REF_FILE_SO if os.path.exists(REF_FILE_SO) else None
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_file_shim.cpp")
+    if force or _stale(REF_FILE_SO, [shim] + hdrs):
+        _run(["g++", "-std=c++14", "-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-w",
+              "-I", root, shim, "-o", REF_FILE_SO], verbose)
+    return REF_FILE_SO
+
+
 if __name__ == "__main__":
     v = "-v" in sys.argv
     print(build_oracle(v, force="-f" in sys.argv))
     print(build_ref(v, force="-f" in sys.argv))
     print(build_ref_index(v, force="-f" in sys.argv))
+    print(build_ref_file(v, force="-f" in sys.argv))

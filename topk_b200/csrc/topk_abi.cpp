@@ -141,6 +141,7 @@ struct topk_table_s {
   // partitioned copy for pruned queries (topk_build_partitions): rows reordered,
   // original ids, per-partition [P][d] min / max / mean (device and host copies)
   float *ptable = nullptr;
+  LoaderState *loader = nullptr;  // table-file pipeline buffers, made on the first load
   uint32_t *pids = nullptr;
   float *pstats = nullptr;
   uint32_t part_log2 = 0, num_parts = 0;
@@ -1085,6 +1086,7 @@ int topk_destroy(topk_table_t h) {
   cudaFree(h->pids);
   cudaFree(h->pstats);
   cudaFree(h->table);
+  loader_state_free(h->loader);
   cudaFree(h->d_minmax);
   cudaFree(h->d_norm);
   delete h;
@@ -1114,6 +1116,70 @@ int topk_upload_colmajor(topk_table_t h, const float *host, uint64_t ld_host) {
                   cudaMemcpyHostToDevice));
   h->has_data = true;
   return TOPK_OK;
+}
+
+int topk_csv_shape(const char *path, uint64_t *n, uint64_t *d) {
+  g_last_error.clear();
+  if (!path || !n || !d) return fail(TOPK_ERR_ARG, "null argument");
+  std::string msg;
+  const int rc = csv_shape(path, n, d, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_load_csv(topk_table_t h, const char *path, uint64_t chunk_bytes, uint64_t *stats) {
+  g_last_error.clear();
+  if (!h || !path) return fail(TOPK_ERR_ARG, "null argument");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  table_changed(h);
+  std::string msg;
+  if (!h->loader) h->loader = loader_state_new();
+  const int rc = load_csv_device(h->loader, path, h->table, h->ld, h->d, h->n, h->num_sms, chunk_bytes, stats, &msg);
+  h->has_data = rc == TOPK_OK;  // a failed load leaves the table undefined
+  return rc == TOPK_OK ? rc : fail(rc, "%s: %s", path, msg.c_str());
+}
+
+int topk_save_csv(topk_table_t h, const char *path) {
+  g_last_error.clear();
+  if (!h || !path) return fail(TOPK_ERR_ARG, "null argument");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::string msg;
+  const int rc = save_csv(path, h->table, h->ld, h->d, h->n, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_binary_shape(const char *path, uint64_t *n, uint64_t *d) {
+  g_last_error.clear();
+  if (!path || !n || !d) return fail(TOPK_ERR_ARG, "null argument");
+  std::string msg;
+  const int rc = binary_shape(path, n, d, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_load_binary(topk_table_t h, const char *path) {
+  g_last_error.clear();
+  if (!h || !path) return fail(TOPK_ERR_ARG, "null argument");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  table_changed(h);
+  std::string msg;
+  if (!h->loader) h->loader = loader_state_new();
+  const int rc = load_binary_device(h->loader, path, h->table, h->ld, h->d, h->n, &msg);
+  h->has_data = rc == TOPK_OK;
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_save_binary(topk_table_t h, const char *path) {
+  g_last_error.clear();
+  if (!h || !path) return fail(TOPK_ERR_ARG, "null argument");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::string msg;
+  const int rc = save_binary(path, h->table, h->ld, h->d, h->n, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
 }
 
 int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host) {

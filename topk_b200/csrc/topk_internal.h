@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <string>
+
 namespace topk {
 
 constexpr int kScanThreads = 256;     // threads per scan CTA
@@ -146,5 +148,24 @@ cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint
 // Per-partition min / max / mean of each attribute, [num_parts][d] each.
 cudaError_t launch_partition_stats(const float *ptable, uint64_t ld, uint32_t d, uint64_t n, uint32_t rows_log2,
                                    uint32_t num_parts, float *mins, float *maxs, float *means, cudaStream_t s);
+
+// Table files (loader.cu).  csv_shape: File<T>::count's n (newlines) and d (1 + commas
+// of the first line).  load_csv_device: parses the first n rows of a comma-separated
+// file into the column-major table on the device (FP32 correctly rounded, as fscanf's
+// "%f"); stats (may be null): bytes consumed, rows found, host-converted values,
+// chunks.  Both return a TOPK_* code and a message on failure.
+int csv_shape(const char *path, uint64_t *n, uint64_t *d, std::string *msg);
+struct LoaderState;  // the loader's pipeline buffers, kept between loads
+LoaderState *loader_state_new();
+void loader_state_free(LoaderState *L);
+int load_csv_device(LoaderState *L, const char *path, float *table, uint64_t ld, uint32_t d, uint64_t n,
+                    int num_sms, uint64_t chunk_bytes, uint64_t stats[4], std::string *msg);
+int save_csv(const char *path, const float *table, uint64_t ld, uint32_t d, uint64_t n, std::string *msg);
+// Binary column-major files: 64-byte header ("TOPKCOL1", version 1, element size 4, n,
+// d), then d columns of n FP32 values.
+int binary_shape(const char *path, uint64_t *n, uint64_t *d, std::string *msg);
+int save_binary(const char *path, const float *table, uint64_t ld, uint32_t d, uint64_t n, std::string *msg);
+int load_binary_device(LoaderState *L, const char *path, float *table, uint64_t ld, uint32_t d, uint64_t n,
+                       std::string *msg);
 
 }  // namespace topk

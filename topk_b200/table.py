@@ -1,5 +1,6 @@
 """Python handle over the C ABI: one n x d FP32 table resident on one GPU."""
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -41,6 +42,37 @@ class Table:
         if t.ndim != 2 or t.shape[0] != self.d or t.shape[1] < self.n:
             raise ValueError(f"expected a ({self.d}, >= {self.n}) array, got {t.shape}")
         check(_lib.load().topk_upload_colmajor(self._h, t.reshape(-1), t.shape[1]))
+
+    def load_csv(self, path, chunk_bytes=0):
+        """The first n rows of a comma-separated file, parsed on the device (File<float>::load
+        with transpose, input/File.h:233-265).  Returns the loader's counters."""
+        st = np.zeros(4, np.uint64)
+        check(_lib.load().topk_load_csv(self._h, os.fsencode(path), int(chunk_bytes), st))
+        return {"bytes": int(st[0]), "rows": int(st[1]), "host_converted": int(st[2]), "chunks": int(st[3])}
+
+    def save_csv(self, path):
+        """One line per object, "%f" fields separated by ',' (File<float>::store)."""
+        check(_lib.load().topk_save_csv(self._h, os.fsencode(path)))
+
+    def load_binary(self, path):
+        check(_lib.load().topk_load_binary(self._h, os.fsencode(path)))
+
+    def save_binary(self, path):
+        check(_lib.load().topk_save_binary(self._h, os.fsencode(path)))
+
+    @classmethod
+    def from_csv(cls, path, device=0, chunk_bytes=0):
+        n, d = csv_shape(path)
+        t = cls(n, d, device)
+        t.load_csv(path, chunk_bytes)
+        return t
+
+    @classmethod
+    def from_binary(cls, path, device=0):
+        n, d = binary_shape(path)
+        t = cls(n, d, device)
+        t.load_binary(path)
+        return t
 
     def generate(self, dist, seed):
         check(_lib.load().topk_generate(self._h, int(dist), int(seed)))
@@ -268,3 +300,17 @@ class Table:
             self.close()
         except Exception:
             pass
+
+
+def csv_shape(path):
+    """(n, d) of a comma-separated table file as File<T>::count reads it."""
+    n, d = C.c_uint64(), C.c_uint64()
+    check(_lib.load().topk_csv_shape(os.fsencode(path), C.byref(n), C.byref(d)))
+    return n.value, d.value
+
+
+def binary_shape(path):
+    """(n, d) of a TOPKCOL1 binary table file."""
+    n, d = C.c_uint64(), C.c_uint64()
+    check(_lib.load().topk_binary_shape(os.fsencode(path), C.byref(n), C.byref(d)))
+    return n.value, d.value

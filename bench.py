@@ -454,7 +454,8 @@ def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
     time of topk_load_csv, file in the page cache, best of 3); the reference's own
     fscanf loader (File<float>::load, oracle/_ref) timed on the file's first
     sample_rows lines and checked bit for bit against the device loader on them; the
-    binary column-major file written and read."""
+    binary column-major file written and read; the table's rows (TPAr's row-major
+    layout) uploaded through the device transpose."""
     import shutil
     import tempfile
     from oracle import csv_oracle as CO
@@ -485,6 +486,13 @@ def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
                 b0 = time.perf_counter()
                 t.load_binary(pb)
                 btimes.append(time.perf_counter() - b0)
+            rows = t.download_rowmajor()  # TPAr's layout: upload with the device transpose
+            rtimes = []
+            for _ in range(3):
+                b0 = time.perf_counter()
+                t.upload_rowmajor(rows)
+                rtimes.append(time.perf_counter() - b0)
+            rows_ok = bool(np.array_equal(t.download_rowmajor().view(np.uint32), rows.view(np.uint32)))
         b0 = time.perf_counter()
         ref = CO.ref_load(ps, sample_rows, d)
         ref_s = time.perf_counter() - b0
@@ -500,6 +508,9 @@ def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
             "save_csv_s": save_s,
             "binary": {"bytes": os.path.getsize(pb), "load_s": min(btimes),
                        "load_GBps": os.path.getsize(pb) / min(btimes) / 1e9},
+            "rowmajor_upload": {"bytes": rows.nbytes, "s": min(rtimes), "GBps": rows.nbytes / min(rtimes) / 1e9,
+                                "round_trip_identical": rows_ok,
+                                "note": "pageable host rows, strided copies + device transpose"},
             "timing": "host wall clock of the whole call (file read, copies, parse, sync)",
         }
         if ref is not None:

@@ -12,6 +12,9 @@
  *   TPAc::init() -> normalize_transpose       cpu/TPAc.h:28-32,
  *                                             common/common.h:30-61 -> topk_normalize
  *   File<T>::gen(data, type)                  input/File.h:335-354  -> topk_generate
+ *   TPAr<T,Z> (row-major cdata), normalize    cpu/TPAr.h:6-33,
+ *                                             common/common.h:63-92 -> topk_upload_rowmajor,
+ *                                                                      topk_download_rowmajor
  *   File<T>::count, load (transpose), store   input/File.h:108-132,
  *                                             233-330, 405-431      -> topk_csv_shape, topk_load_csv,
  *                                                                      topk_save_csv
@@ -93,6 +96,15 @@ int topk_normalize(topk_table_t h, float *mins, float *maxs);
 
 /* Copy the device table back (column-major, host stride ld_host >= n). */
 int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host);
+
+/* Row-major host tables (row i at host + i*row_stride floats, row_stride >= d), the
+ * layout of the reference's TPAr (cpu/TPAr.h: cdata[i*d + m]).  The rows are copied in
+ * blocks and transposed on the device into the column-major table, so every query
+ * entry serves them; TPAr's normalize (common/common.h:63-92) is the same arithmetic
+ * per attribute as topk_normalize.  Replace filling TPAr's get_cdata() and reading it
+ * back. */
+int topk_upload_rowmajor(topk_table_t h, const float *host, uint64_t row_stride);
+int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride);
 
 /* Table files.  Replace File<T> (input/File.h).
  *

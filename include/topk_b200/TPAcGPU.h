@@ -85,6 +85,7 @@ class TPAcGPU : public AA<T, Z> {
  private:
   topk_table_t h_ = nullptr;
 
+ protected:
   [[noreturn]] static void die(int st, const char *msg) {
     std::cout << "topk_b200: " << topk_status_name(st) << ": " << msg << std::endl;
     exit(1);
@@ -93,6 +94,7 @@ class TPAcGPU : public AA<T, Z> {
     if (st != TOPK_OK) die(st, topk_last_error());
   }
 
+ private:
   void query(uint64_t k, uint8_t qq, T *weights, uint8_t *attr, const char *how) {
     std::cout << this->algo << " find top-" << k << " " << how << " (" << (int)qq << "D) ...";
     if (this->res.size() > 0) this->res.clear();

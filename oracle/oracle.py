@@ -6,6 +6,7 @@ reference legs.  The product package never imports this module.
   Oracle  - the C restatement in topk_oracle.c (cites the reference per function).
   RefTPAc - the reference's own TPAc<float,uint64_t> (cpu/TPAc.h) compiled strict
             into oracle/_ref/libref_tpac.so by oracle/build.py.
+  RefTPAr - the reference's row-major TPAr<float,uint64_t> (cpu/TPAr.h), same library.
 """
 import ctypes as C
 import os
@@ -215,6 +216,73 @@ class RefTPAc:
     def close(self):
         if self.h:
             self.lib().ref_tpac_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefTPAr:
+    """The reference TPAr<float,uint64_t> (cpu/TPAr.h, the row-major variant) through
+    oracle/_ref/libref_tpac.so.  Its query loops step 8 or 16 objects with no tail, so
+    n must be a multiple of 16 * THREADS (256)."""
+
+    _L = None
+
+    @classmethod
+    def lib(cls):
+        if cls._L is None:
+            L = RefTPAc.lib()
+            L.ref_tpar_create.argtypes = [C.c_uint64, C.c_uint64]
+            L.ref_tpar_create.restype = C.c_void_p
+            L.ref_tpar_destroy.argtypes = [C.c_void_p]
+            L.ref_tpar_load.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_uint64]
+            L.ref_tpar_init.argtypes = [C.c_void_p]
+            L.ref_tpar_get_data.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_uint64]
+            L.ref_tpar_query.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint8, _f32p, _u8p, _u64p, _f32p,
+                                         C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_double)]
+            L.ref_tpar_query.restype = C.c_uint64
+            cls._L = L
+        return cls._L
+
+    def __init__(self, rows):
+        """rows: (n, d) float32 row-major; copied into reference-owned memory."""
+        self.n, self.d = rows.shape
+        if self.n % 256:
+            raise ValueError("the reference TPAr needs n to be a multiple of 256")
+        L = self.lib()
+        self.h = L.ref_tpar_create(self.n, self.d)
+        if L.ref_tpar_load(self.h, np.ascontiguousarray(rows, np.float32).reshape(-1), self.n, self.d):
+            raise MemoryError("reference table allocation failed")
+
+    def init(self):
+        self.lib().ref_tpar_init(self.h)
+
+    def data(self):
+        out = np.empty((self.n, self.d), np.float32)
+        self.lib().ref_tpar_get_data(self.h, out.reshape(-1), self.n, self.d)
+        return out
+
+    def query(self, impl, k, weights, attr):
+        """impl 0 scalar, 1 simd, 2 threads. Returns (ids, scores, threshold, ms)."""
+        w = np.zeros(max(self.d, len(weights)), np.float32)
+        w[: len(weights)] = weights
+        a = np.ascontiguousarray(attr, np.uint8)
+        cap = max(1, min(k, self.n))
+        ids = np.zeros(cap, np.uint64)
+        sc = np.zeros(cap, np.float32)
+        th = C.c_float(0)
+        ms = C.c_double(0)
+        c = self.lib().ref_tpar_query(self.h, impl, k, len(a), w, a, ids, sc, cap, C.byref(th), C.byref(ms))
+        c = min(c, cap)
+        return ids[:c], sc[:c], th.value, ms.value
+
+    def close(self):
+        if self.h:
+            self.lib().ref_tpar_destroy(self.h)
             self.h = None
 
     def __del__(self):

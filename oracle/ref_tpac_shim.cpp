@@ -44,6 +44,7 @@
 
 #include "time/Time.h"
 #include "cpu/TPAc.h"
+#include "cpu/TPAr.h"
 
 namespace {
 
@@ -56,6 +57,37 @@ struct Quiet {
 };
 
 using RefTPAc = TPAc<float, uint64_t>;
+using RefTPAr = TPAr<float, uint64_t>;
+
+template <class A>
+uint64_t run_query(A *t, int impl, uint64_t k, uint8_t qq, float *weights, uint8_t *attr, uint64_t *ids,
+                   float *scores, uint64_t cap, float *thres, double *ms) {
+  Quiet q;
+  t->reset_clocks();
+  double t0 = omp_get_wtime();
+  if (impl == 0) t->findTopKscalar(k, qq, weights, attr);
+  else if (impl == 1) t->findTopKsimd(k, qq, weights, attr);
+  else t->findTopKthreads(k, qq, weights, attr);
+  double t1 = omp_get_wtime();
+  std::vector<tuple_<float, uint64_t>> res = t->get_res();
+  uint64_t c = res.size() < cap ? res.size() : cap;
+  for (uint64_t j = 0; j < c; j++) { ids[j] = res[j].tid; scores[j] = res[j].score; }
+  if (thres) *thres = t->get_thres();
+  if (ms) *ms = (t1 - t0) * 1e3;
+  return res.size();
+}
+
+template <class A>
+int load_table(A *t, const float *src, uint64_t n, uint64_t d) {
+  size_t bytes = sizeof(float) * n * d;
+  float *buf = static_cast<float *>(aligned_alloc(64, (bytes + 63) / 64 * 64));
+  if (!buf) return 1;
+  std::memcpy(buf, src, bytes);
+  float *&cd = t->get_cdata();
+  if (cd) std::free(cd);
+  cd = buf;
+  return 0;
+}
 
 }  // namespace
 
@@ -136,5 +168,27 @@ void ref_normalize_transpose(float *data, uint64_t n, uint64_t d) {
 }
 
 int ref_threads_constant(void) { return THREADS; }
+
+/* TPAr<float,uint64_t> (cpu/TPAr.h): the row-major variant.  load copies an n x d
+ * row-major table (object i at src + i*d); init normalises it (common/common.h:63-92);
+ * impl as ref_tpac_query.  Its query loops take 8 (scalar, simd) or 16 (threads,
+ * per thread share) objects per step with no tail: n must be a multiple of 16*THREADS
+ * for all three to stay inside the table. */
+void *ref_tpar_create(uint64_t n, uint64_t d) { return new RefTPAr(n, d); }
+void ref_tpar_destroy(void *h) { delete static_cast<RefTPAr *>(h); }
+int ref_tpar_load(void *h, const float *rows, uint64_t n, uint64_t d) {
+  return load_table(static_cast<RefTPAr *>(h), rows, n, d);
+}
+void ref_tpar_init(void *h) {
+  Quiet q;
+  static_cast<RefTPAr *>(h)->init();
+}
+void ref_tpar_get_data(void *h, float *out, uint64_t n, uint64_t d) {
+  std::memcpy(out, static_cast<RefTPAr *>(h)->get_cdata(), sizeof(float) * n * d);
+}
+uint64_t ref_tpar_query(void *h, int impl, uint64_t k, uint8_t qq, float *weights, uint8_t *attr, uint64_t *ids,
+                        float *scores, uint64_t cap, float *thres, double *ms) {
+  return run_query(static_cast<RefTPAr *>(h), impl, k, qq, weights, attr, ids, scores, cap, thres, ms);
+}
 
 }  // extern "C"

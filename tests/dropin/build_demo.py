@@ -1,5 +1,6 @@
-"""Build tests/dropin/_build/tpac_dropin_demo (needs the reference tree for cpu/AA.h,
-cpu/TPAc.h and time/Time.h; TOPK_REFERENCE, default /root/reference).  The binary
+"""Build tests/dropin/_build/tpac_dropin_demo and tpar_dropin_demo (need the reference
+tree for cpu/AA.h, cpu/TPAc.h, cpu/TPAr.h and time/Time.h; TOPK_REFERENCE, default
+/root/reference).  The binary
 then travels with the working tree; without the reference tree nothing is built and
 the GPU test that runs it skips."""
 import os
@@ -11,25 +12,31 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 OUT = os.path.join(HERE, "_build", "tpac_dropin_demo")
 
 
-def build(verbose=False):
-    ref = os.environ.get("TOPK_REFERENCE", "/root/reference")
-    if not os.path.exists(os.path.join(ref, "cpu", "TPAc.h")):
-        return OUT if os.path.exists(OUT) else None
-    src = os.path.join(HERE, "tpac_dropin_demo.cpp")
-    hdr = os.path.join(ROOT, "include", "topk_b200", "TPAcGPU.h")
+def _build_one(name, header, ref, verbose):
+    out = os.path.join(HERE, "_build", name)
+    src = os.path.join(HERE, name + ".cpp")
+    hdrs = [os.path.join(ROOT, "include", "topk_b200", h) for h in header]
     lib = os.path.join(ROOT, "topk_b200", "_lib", "libtopk_b200.so")
-    if os.path.exists(OUT) and os.path.getmtime(OUT) > max(os.path.getmtime(src), os.path.getmtime(hdr),
-                                                             os.path.getmtime(lib)):
-        return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    if os.path.exists(out) and os.path.getmtime(out) > max(os.path.getmtime(p) for p in [src, lib] + hdrs):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     cmd = ["g++", "-std=c++14", "-O2", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-w",
            "-I", ref, "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "oracle", "stub"),
-           src, "-o", OUT, "-L", os.path.dirname(lib), "-ltopk_b200",
+           src, "-o", out, "-L", os.path.dirname(lib), "-ltopk_b200",
            "-Wl,-rpath,$ORIGIN/../../../topk_b200/_lib"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    return OUT
+    return out
+
+
+def build(verbose=False):
+    """Builds both demos (TPAc and TPAr); returns the TPAc demo's path."""
+    ref = os.environ.get("TOPK_REFERENCE", "/root/reference")
+    if not os.path.exists(os.path.join(ref, "cpu", "TPAc.h")):
+        return OUT if os.path.exists(OUT) else None
+    _build_one("tpar_dropin_demo", ["TPAcGPU.h", "TPArGPU.h"], ref, verbose)
+    return _build_one("tpac_dropin_demo", ["TPAcGPU.h"], ref, verbose)
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dropin", "_build", "tpac_dropin_demo")
+BIN_TPAR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dropin", "_build", "tpar_dropin_demo")
 
 
 @pytest.mark.parametrize("n,d,seed", [(1 << 20, 8, 1), ((1 << 18) + 48, 16, 7)])
@@ -21,6 +22,18 @@ def test_tpacgpu_agrees_with_reference_tpac(n, d, seed):
     if not os.path.exists(BIN):
         pytest.skip("drop-in demo not built (needs the reference headers at build time)")
     r = subprocess.run([BIN, str(n), str(d), str(seed)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "normalize ok" in r.stdout
+    assert r.stdout.strip().endswith("PASS"), r.stdout
+
+
+@pytest.mark.parametrize("n,d,seed", [(1 << 20, 8, 3), ((1 << 18) + 256, 16, 9)])
+def test_tpargpu_agrees_with_reference_tpar(n, d, seed):
+    """TPArGPU (row-major cdata, include/topk_b200/TPArGPU.h) against the reference's
+    TPAr, all three of its query entries."""
+    if not os.path.exists(BIN_TPAR):
+        pytest.skip("drop-in demo not built (needs the reference headers at build time)")
+    r = subprocess.run([BIN_TPAR, str(n), str(d), str(seed)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "normalize ok" in r.stdout
     assert r.stdout.strip().endswith("PASS"), r.stdout

@@ -51,6 +51,8 @@ SIGNATURES = [
     ("topk_create", C.c_int, [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
     ("topk_destroy", C.c_int, [_H]),
     ("topk_upload_colmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_upload_rowmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_download_rowmajor", C.c_int, [_H, _f32p, C.c_uint64]),
     ("topk_csv_shape", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("topk_load_csv", C.c_int, [_H, C.c_char_p, C.c_uint64, _u64p]),
     ("topk_save_csv", C.c_int, [_H, C.c_char_p]),

@@ -256,6 +256,47 @@ __global__ void scatter_values_kernel(const uint64_t *__restrict__ idx, const fl
     table[idx[i]] = vals[i];
 }
 
+// Row-major <-> column-major through 32 x 32 shared-memory tiles (block 32 x 8):
+// reads and writes are both coalesced.  Rows on grid.x (chunks can hold millions),
+// attributes on grid.y (d <= 255).
+__global__ void __launch_bounds__(256)
+    rows_to_cols_kernel(const float *__restrict__ src, uint32_t d, uint64_t nrows, float *__restrict__ dst,
+                        uint64_t ld, uint64_t row0) {
+  __shared__ float tile[32][33];
+  const uint64_t r0 = (uint64_t)blockIdx.x * 32;
+  const uint32_t m0 = blockIdx.y * 32;
+  for (uint32_t j = threadIdx.y; j < 32; j += 8) {
+    const uint64_t r = r0 + j;
+    const uint32_t m = m0 + threadIdx.x;
+    if (r < nrows && m < d) tile[j][threadIdx.x] = src[r * d + m];
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.y; j < 32; j += 8) {
+    const uint32_t m = m0 + j;
+    const uint64_t r = r0 + threadIdx.x;
+    if (r < nrows && m < d) dst[(uint64_t)m * ld + row0 + r] = tile[threadIdx.x][j];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    cols_to_rows_kernel(const float *__restrict__ src, uint64_t ld, uint64_t row0, uint32_t d, uint64_t nrows,
+                        float *__restrict__ dst) {
+  __shared__ float tile[32][33];
+  const uint64_t r0 = (uint64_t)blockIdx.x * 32;
+  const uint32_t m0 = blockIdx.y * 32;
+  for (uint32_t j = threadIdx.y; j < 32; j += 8) {
+    const uint32_t m = m0 + j;
+    const uint64_t r = r0 + threadIdx.x;
+    if (r < nrows && m < d) tile[j][threadIdx.x] = src[(uint64_t)m * ld + row0 + r];
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.y; j < 32; j += 8) {
+    const uint64_t r = r0 + j;
+    const uint32_t m = m0 + threadIdx.x;
+    if (r < nrows && m < d) dst[r * d + m] = tile[threadIdx.x][j];
+  }
+}
+
 }  // namespace
 
 // The loader's buffers, kept by the table handle between loads: two pinned host
@@ -807,6 +848,130 @@ int load_binary_device(LoaderState *L, const char *path, float *table, uint64_t 
   if (e == cudaSuccess) e = cudaStreamSynchronize(B.copy);
   if (e != cudaSuccess) {
     *msg = cuda_msg(e, "load_binary");
+    return TOPK_ERR_CUDA;
+  }
+  return TOPK_OK;
+}
+
+// ------------------------------------------------------------ row-major tables
+// The reference's TPAr keeps the table row-major (cpu/TPAr.h, cdata[i*d + m]) and
+// normalises it in place (common/common.h:63-92, the same arithmetic per attribute as
+// normalize_transpose).  Row-major host tables go through the pipeline buffers: a
+// strided 2D copy of a block of rows into a device buffer, then a tiled transpose
+// into the column-major table; the next block's copy overlaps this block's transpose.
+namespace {
+int rowmajor_prepare(LoaderState &B, std::string *msg) {
+  cudaError_t e = B.chunk >= kDefaultChunk ? cudaSuccess : B.reserve(kDefaultChunk, std::max<uint64_t>(B.max_rows, 2));
+  if (e != cudaSuccess) {
+    *msg = cuda_msg(e, "row-major staging");
+    return e == cudaErrorMemoryAllocation ? TOPK_ERR_OOM : TOPK_ERR_CUDA;
+  }
+  return TOPK_OK;
+}
+}  // namespace
+
+namespace {
+// rows x width floats between strided host arrays, split over up to 8 threads
+void copy_rows(float *dst, uint64_t dst_stride, const float *src, uint64_t src_stride, uint64_t rows,
+               uint64_t width) {
+  const unsigned nt = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>({8, rows * width / (1u << 18) + 1, std::max(1u, std::thread::hardware_concurrency())}));
+  auto part = [&](uint64_t a, uint64_t b) {
+    if (dst_stride == width && src_stride == width) {
+      memcpy(dst + a * width, src + a * width, (b - a) * width * sizeof(float));
+      return;
+    }
+    for (uint64_t r = a; r < b; ++r) memcpy(dst + r * dst_stride, src + r * src_stride, width * sizeof(float));
+  };
+  if (nt == 1) {
+    part(0, rows);
+    return;
+  }
+  std::vector<std::thread> th;
+  const uint64_t per = (rows + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const uint64_t a = std::min<uint64_t>(rows, t * per), b = std::min<uint64_t>(rows, a + per);
+    th.emplace_back(part, a, b);
+  }
+  for (auto &x : th) x.join();
+}
+}  // namespace
+
+// Upload: block i's rows are packed into pinned buffer i % 2 by host threads while
+// block i-1 is copied and transposed; download runs the same pipeline backwards.
+int upload_rowmajor_device(LoaderState *L, const float *host, uint64_t row_stride, float *table, uint64_t ld,
+                           uint32_t d, uint64_t n, std::string *msg) {
+  LoaderState &B = *L;
+  Drain drain{B};
+  int rc = rowmajor_prepare(B, msg);
+  if (rc != TOPK_OK) return rc;
+  const uint64_t per = B.chunk / (4ull * d);  // rows per buffer
+  bool used[2] = {false, false};
+  cudaError_t e = cudaSuccess;
+  int b = 0;
+  for (uint64_t r0 = 0; r0 < n && e == cudaSuccess; r0 += per, b ^= 1) {
+    const uint64_t rows = std::min(per, n - r0);
+    float *hb = reinterpret_cast<float *>(B.h[b]), *stage = reinterpret_cast<float *>(B.dbuf[b]);
+    if (used[b]) e = cudaEventSynchronize(B.copied[b]);  // pinned buffer b copied out
+    if (e != cudaSuccess) break;
+    copy_rows(hb, d, host + r0 * row_stride, row_stride, rows, d);
+    if (used[b]) e = cudaStreamWaitEvent(B.copy, B.parsed[b], 0);  // device buffer b transposed
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stage, hb, rows * d * sizeof(float), cudaMemcpyHostToDevice, B.copy);
+    if (e == cudaSuccess) e = cudaEventRecord(B.copied[b], B.copy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(B.comp, B.copied[b], 0);
+    if (e == cudaSuccess) {
+      rows_to_cols_kernel<<<dim3((unsigned)((rows + 31) / 32), (d + 31) / 32), dim3(32, 8), 0, B.comp>>>(
+          stage, d, rows, table, ld, r0);
+      e = cudaEventRecord(B.parsed[b], B.comp);
+    }
+    used[b] = true;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(B.comp);
+  if (e != cudaSuccess) {
+    *msg = cuda_msg(e, "upload_rowmajor");
+    return TOPK_ERR_CUDA;
+  }
+  return TOPK_OK;
+}
+
+int download_rowmajor_device(LoaderState *L, float *host, uint64_t row_stride, const float *table, uint64_t ld,
+                             uint32_t d, uint64_t n, std::string *msg) {
+  LoaderState &B = *L;
+  Drain drain{B};
+  int rc = rowmajor_prepare(B, msg);
+  if (rc != TOPK_OK) return rc;
+  const uint64_t per = B.chunk / (4ull * d);
+  cudaError_t e = cudaSuccess;
+  int64_t pending = -1;  // block waiting in its pinned buffer to be unpacked
+  int pb = 0;
+  auto unpack = [&]() -> cudaError_t {
+    if (pending < 0) return cudaSuccess;
+    cudaError_t r = cudaEventSynchronize(B.copied[pb]);
+    if (r != cudaSuccess) return r;
+    const uint64_t r0 = (uint64_t)pending * per, rows = std::min(per, n - r0);
+    copy_rows(host + r0 * row_stride, row_stride, reinterpret_cast<const float *>(B.h[pb]), d, rows, d);
+    pending = -1;
+    return cudaSuccess;
+  };
+  int b = 0;
+  for (uint64_t r0 = 0, blk = 0; r0 < n && e == cudaSuccess; r0 += per, ++blk, b ^= 1) {
+    const uint64_t rows = std::min(per, n - r0);
+    float *stage = reinterpret_cast<float *>(B.dbuf[b]);
+    // buffers b were last used by block blk - 2, unpacked before block blk - 1 was queued
+    cols_to_rows_kernel<<<dim3((unsigned)((rows + 31) / 32), (d + 31) / 32), dim3(32, 8), 0, B.comp>>>(
+        table, ld, r0, d, rows, stage);
+    e = cudaEventRecord(B.parsed[b], B.comp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(B.copy, B.parsed[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(B.h[b], stage, rows * d * sizeof(float), cudaMemcpyDeviceToHost, B.copy);
+    if (e == cudaSuccess) e = cudaEventRecord(B.copied[b], B.copy);
+    if (e == cudaSuccess) e = unpack();  // the previous block, while this one is in flight
+    pending = (int64_t)blk;
+    pb = b;
+  }
+  if (e == cudaSuccess) e = unpack();
+  if (e != cudaSuccess) {
+    *msg = cuda_msg(e, "download_rowmajor");
     return TOPK_ERR_CUDA;
   }
   return TOPK_OK;

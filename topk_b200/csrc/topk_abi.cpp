@@ -1118,6 +1118,32 @@ int topk_upload_colmajor(topk_table_t h, const float *host, uint64_t ld_host) {
   return TOPK_OK;
 }
 
+int topk_upload_rowmajor(topk_table_t h, const float *host, uint64_t row_stride) {
+  g_last_error.clear();
+  if (!h || !host) return fail(TOPK_ERR_ARG, "null argument");
+  if (row_stride < h->d) return fail(TOPK_ERR_ARG, "row_stride=%llu < d=%u", (unsigned long long)row_stride, h->d);
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  table_changed(h);
+  if (!h->loader) h->loader = loader_state_new();
+  std::string msg;
+  const int rc = upload_rowmajor_device(h->loader, host, row_stride, h->table, h->ld, h->d, h->n, &msg);
+  h->has_data = rc == TOPK_OK;
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride) {
+  g_last_error.clear();
+  if (!h || !host) return fail(TOPK_ERR_ARG, "null argument");
+  if (row_stride < h->d) return fail(TOPK_ERR_ARG, "row_stride=%llu < d=%u", (unsigned long long)row_stride, h->d);
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  if (!h->loader) h->loader = loader_state_new();
+  std::string msg;
+  const int rc = download_rowmajor_device(h->loader, host, row_stride, h->table, h->ld, h->d, h->n, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
 int topk_csv_shape(const char *path, uint64_t *n, uint64_t *d) {
   g_last_error.clear();
   if (!path || !n || !d) return fail(TOPK_ERR_ARG, "null argument");

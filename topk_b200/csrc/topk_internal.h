@@ -167,5 +167,11 @@ int binary_shape(const char *path, uint64_t *n, uint64_t *d, std::string *msg);
 int save_binary(const char *path, const float *table, uint64_t ld, uint32_t d, uint64_t n, std::string *msg);
 int load_binary_device(LoaderState *L, const char *path, float *table, uint64_t ld, uint32_t d, uint64_t n,
                        std::string *msg);
+// Row-major host tables (row i at host + i*row_stride) to and from the column-major
+// device table, through the loader's buffers and a tiled transpose.
+int upload_rowmajor_device(LoaderState *L, const float *host, uint64_t row_stride, float *table, uint64_t ld,
+                           uint32_t d, uint64_t n, std::string *msg);
+int download_rowmajor_device(LoaderState *L, float *host, uint64_t row_stride, const float *table, uint64_t ld,
+                             uint32_t d, uint64_t n, std::string *msg);
 
 }  // namespace topk

@@ -43,6 +43,18 @@ class Table:
             raise ValueError(f"expected a ({self.d}, >= {self.n}) array, got {t.shape}")
         check(_lib.load().topk_upload_colmajor(self._h, t.reshape(-1), t.shape[1]))
 
+    def upload_rowmajor(self, rows):
+        """rows: (n, row_stride >= d) float32, object i in row i (TPAr's layout)."""
+        r = np.ascontiguousarray(rows, np.float32)
+        if r.ndim != 2 or r.shape[0] != self.n or r.shape[1] < self.d:
+            raise ValueError(f"expected a ({self.n}, >= {self.d}) array, got {r.shape}")
+        check(_lib.load().topk_upload_rowmajor(self._h, r.reshape(-1), r.shape[1]))
+
+    def download_rowmajor(self):
+        out = np.empty((self.n, self.d), np.float32)
+        check(_lib.load().topk_download_rowmajor(self._h, out.reshape(-1), self.d))
+        return out
+
     def load_csv(self, path, chunk_bytes=0):
         """The first n rows of a comma-separated file, parsed on the device (File<float>::load
         with transpose, input/File.h:233-265).  Returns the loader's counters."""

@@ -170,3 +170,34 @@ class TPAc(AA):
 
     def close(self):
         self._table.close()
+
+
+class TPAr(TPAc):
+    """Row-major full-table evaluation (cpu/TPAr.h:6-33): cdata holds the table
+    row-major, (n, d) with object i in row i, and init() normalises it
+    (common/common.h:63-92, the same arithmetic per attribute as TPAc's).  On the GPU
+    the rows are transposed into the column-major table on upload, so the queries are
+    TPAc's exact kernel; results equal the reference TPAr's."""
+
+    def __init__(self, n, d, device=0, mqthreads=256):
+        super().__init__(n, d, device, mqthreads)
+        self.algo = "TPAr"
+
+    def get_cdata(self):
+        if self.cdata is None:
+            self.cdata = np.zeros((self.n, self.d), np.float32)
+        return self.cdata
+
+    def set_cdata(self, cdata):
+        c = np.ascontiguousarray(cdata, np.float32)
+        if c.shape != (self.n, self.d):
+            raise ValueError(f"cdata must be ({self.n}, {self.d}) row-major, got {c.shape}")
+        self.cdata = c
+
+    def init(self):
+        """Upload cdata (if the caller filled it) row-major, transposed on the device,
+        and normalise there (TPAr::init -> normalize, cpu/TPAr.h:28-33)."""
+        if self.cdata is not None:
+            self._table.upload_rowmajor(self.cdata)
+        self._table.normalize()
+        self.tt_init = 0.0

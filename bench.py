@@ -510,7 +510,7 @@ def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
                        "load_GBps": os.path.getsize(pb) / min(btimes) / 1e9},
             "rowmajor_upload": {"bytes": rows.nbytes, "s": min(rtimes), "GBps": rows.nbytes / min(rtimes) / 1e9,
                                 "round_trip_identical": rows_ok,
-                                "note": "pageable host rows, strided copies + device transpose"},
+                                "note": "pageable host rows packed into pinned buffers by host threads, device transpose"},
             "timing": "host wall clock of the whole call (file read, copies, parse, sync)",
         }
         if ref is not None:

@@ -29,6 +29,9 @@ flush is needed between queries.
   loader   table files: a 2^22 x 16 table as the reference's '%f' CSV read by the
           device loader (GB/s, rows/s) against the reference's fscanf loader on a
           2^18-row sample (bit-identical check), and the binary format.
+  ta       the threshold algorithm over device-built sorted lists against the full
+          scan on correlated and independent 2^26 x 8 tables (identical results
+          checked), and the reference's TA on a 2^20-row sample.
   c5       (with --c5, or alone with --only c5) the full chosen form: 16384 queries
           (k log-uniform in [1, 1024]) over a 2^28 x 16 table mixed 1/3 each
           independent/correlated/anticorrelated, plain batched FP32 against the
@@ -525,6 +528,70 @@ def run_loader(T, device, n=1 << 22, d=16, sample_rows=1 << 18):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def run_ta(T, device, n=1 << 26, d=8, n_test=200, sample_rows=1 << 20, seed=8):
+    """The threshold algorithm (cpu/TA.h) on the device: an n x d table per distribution
+    (correlated, where the walk stops early, and independent), sorted lists built on the
+    device (timed), n_test queries (attribute subsets of size U{2..d}, weights U(0,1],
+    k log-uniform in [16, 1024]) answered by the full scan and by TA, results checked
+    identical; host wall time per synchronous call.  The reference's TA (oracle/_ref,
+    its own init and findTopK, one core) on a sample_rows sample with equal weights
+    (its scores are right only then)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    ks = np.exp(rng.uniform(np.log(16), np.log(1025), n_test)).astype(np.uint64).clip(16, 1024)
+    W = ((rng.integers(0, 1 << 24, size=(n_test, d)) + 1) * 2.0 ** -24).astype(np.float32)
+    attrs = [np.sort(rng.choice(d, size=int(rng.integers(2, d + 1)), replace=False)).astype(np.uint8)
+             for _ in range(n_test)]
+    out = {"workload": f"n={n} x d={d}; {n_test} queries, |attrs| U{{2..{d}}}, k log-uniform [16, 1024]",
+           "timing": "host wall clock per synchronous query call"}
+    for name, dist in (("correlated", T.DIST_CORRELATED), ("independent", T.DIST_INDEPENDENT)):
+        with T.Table(n, d, device=device) as t:
+            t.generate(dist, seed)
+            t.normalize()
+            t.build_lists()
+            b0 = time.perf_counter()
+            t.build_lists()
+            build_s = time.perf_counter() - b0
+            for j in range(3):
+                t.query(int(ks[j]), W[j], attrs[j])
+                t.query_ta(int(ks[j]), W[j], attrs[j])
+            full = ta = 0.0
+            depth = scored = 0
+            same = True
+            for j in range(n_test):
+                k, w, a = int(ks[j]), W[j], attrs[j]
+                t0 = time.perf_counter()
+                r0 = t.query(k, w, a)
+                t1 = time.perf_counter()
+                r1 = t.query_ta(k, w, a)
+                t2 = time.perf_counter()
+                full += t1 - t0
+                ta += t2 - t1
+                depth += r1[3][0]
+                scored += r1[3][1]
+                same &= all(np.asarray(x).tobytes() == np.asarray(y).tobytes() for x, y in zip(r0, r1[:3]))
+        out[name] = {"full_scan_queries_per_s": n_test / full, "ta_queries_per_s": n_test / ta,
+                     "ta_vs_full_scan": full / ta, "mean_depth_fraction": depth / (n_test * n),
+                     "mean_objects_scored_fraction": scored / (n_test * n), "lists_build_s": build_s,
+                     "identical_results": bool(same)}
+    if O.RefTPAc.available():
+        cols = O.generate(sample_rows, d, T.DIST_CORRELATED, seed)
+        ref = O.RefTA(np.ascontiguousarray(cols.T))
+        del cols
+        b0 = time.perf_counter()
+        ref.init()
+        init_s = time.perf_counter() - b0
+        tot = 0.0
+        for j in range(min(n_test, 50)):
+            tot += ref.query(int(ks[j]), np.full(d, 0.5, np.float32), attrs[j])[3]
+        ref.close()
+        out["cpu_reference"] = {"kind": "reference", "cores": 1, "sample_rows": sample_rows,
+                                "sample": f"TA::init + findTopK on a correlated {sample_rows} x {d} sample, "
+                                          "equal weights, first 50 queries",
+                                "init_s": init_s, "queries_per_s": min(n_test, 50) / (tot / 1e3)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -535,7 +602,7 @@ def main():
     ap.add_argument("--d", type=int, default=D_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--only", choices=["batched", "pruned", "c5", "loader"], default=None,
+    ap.add_argument("--only", choices=["batched", "pruned", "c5", "loader", "ta"], default=None,
                     help="run one secondary workload alone (no JSON line; for profiling)")
     ap.add_argument("--c5", action="store_true",
                     help="add the full-form workload: 16384 queries over a mixed 2^28 x 16 table")
@@ -545,6 +612,7 @@ def main():
     ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--no-pruned", action="store_true")
     ap.add_argument("--no-loader", action="store_true")
+    ap.add_argument("--no-ta", action="store_true")
     ap.add_argument("--pruned-n", type=int, default=1 << 27)
     ap.add_argument("--pruned-queries", type=int, default=2000)
     ap.add_argument("--batched-n", type=int, default=BATCH_N)
@@ -564,6 +632,8 @@ def main():
             out = run_c5(T, torch, None, 0, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
         elif args.only == "loader":
             out = run_loader(T, 0)
+        elif args.only == "ta":
+            out = run_ta(T, 0)
         else:
             out = run_pruned(T, 0, args.pruned_n, n_test=args.pruned_queries)
         print(json.dumps(out))
@@ -716,6 +786,8 @@ def main():
         result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
     if not args.no_loader and rank == 0:
         result["loader"] = run_loader(T, local)
+    if not args.no_ta and rank == 0:
+        result["ta"] = run_ta(T, local)
     if args.c5:
         result["c5"] = run_c5(T, torch, dist, local, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
     if dist:

@@ -15,6 +15,7 @@
  *   TPAr<T,Z> (row-major cdata), normalize    cpu/TPAr.h:6-33,
  *                                             common/common.h:63-92 -> topk_upload_rowmajor,
  *                                                                      topk_download_rowmajor
+ *   TA<T,Z>::init, findTopK                   cpu/TA.h:40-96        -> topk_build_lists, topk_query_ta
  *   File<T>::count, load (transpose), store   input/File.h:108-132,
  *                                             233-330, 405-431      -> topk_csv_shape, topk_load_csv,
  *                                                                      topk_save_csv
@@ -96,6 +97,25 @@ int topk_normalize(topk_table_t h, float *mins, float *maxs);
 
 /* Copy the device table back (column-major, host stride ld_host >= n). */
 int topk_download_colmajor(topk_table_t h, float *host, uint64_t ld_host);
+
+/* The threshold algorithm (cpu/TA.h).  topk_build_lists: TA::init's sorted lists
+ * (:40-58), one per attribute, ids by value descending (ties by the lower id) with the
+ * values in that order, built on the device (radix sorts, n < 2^31; 8*d*n bytes plus
+ * ~70 MB of query scratch); rebuild after the table changes.  topk_read_list: list m's
+ * ids and values (n each, either may be NULL).  topk_query_ta: TA::findTopK (:61-96)
+ * on the device, exact: the queried lists are walked in blocks of growing depth,
+ * every object met is scored once in the query's order, and the walk stops when the
+ * k-th score is strictly above the threshold of the unseen objects (sum of
+ * w * list value at the depth reached; the attribute's minimum for w < 0), so the
+ * result equals topk_query's, ties to the lower id.  The reference scores every
+ * attribute of an object with the weight of the list it was found in (cpu/TA.h:83),
+ * which is wrong unless all weights are equal; here each attribute has its own weight.
+ * stats (3 entries, may be NULL): depth walked, objects scored, blocks.  TA queries on
+ * one handle run one at a time. */
+int topk_build_lists(topk_table_t h);
+int topk_read_list(topk_table_t h, uint32_t m, uint32_t *ids, float *values);
+int topk_query_ta(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, uint64_t *ids,
+                  float *scores, uint64_t *count, float *threshold, uint64_t *stats);
 
 /* Row-major host tables (row i at host + i*row_stride floats, row_stride >= d), the
  * layout of the reference's TPAr (cpu/TPAr.h: cdata[i*d + m]).  The rows are copied in

@@ -56,8 +56,8 @@ def build_oracle(verbose=False, force=False):
 def build_ref(verbose=False, force=False):
     """Compile the reference TPAc through the shim. Returns the .so path or None."""
     root = reference_root()
-    hdrs = [os.path.join(root, p) for p in ("cpu/TPAc.h", "cpu/TPAr.h", "cpu/AA.h", "common/common.h",
-                                            "time/Time.h")]
+    hdrs = [os.path.join(root, p) for p in ("cpu/TPAc.h", "cpu/TPAr.h", "cpu/TA.h", "cpu/AA.h",
+                                            "common/common.h", "time/Time.h")]
     if not all(os.path.exists(h) for h in hdrs):
         return REF_SO if os.path.exists(REF_SO) else None
     os.makedirs(REF_OUT, exist_ok=True)

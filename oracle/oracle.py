@@ -7,6 +7,7 @@ reference legs.  The product package never imports this module.
   RefTPAc - the reference's own TPAc<float,uint64_t> (cpu/TPAc.h) compiled strict
             into oracle/_ref/libref_tpac.so by oracle/build.py.
   RefTPAr - the reference's row-major TPAr<float,uint64_t> (cpu/TPAr.h), same library.
+  RefTA   - the reference's TA<float,uint64_t> (cpu/TA.h), same library.
 """
 import ctypes as C
 import os
@@ -283,6 +284,63 @@ class RefTPAr:
     def close(self):
         if self.h:
             self.lib().ref_tpar_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefTA:
+    """The reference TA<float,uint64_t> (cpu/TA.h) through oracle/_ref/libref_tpac.so:
+    sorted lists over a row-major table, findTopK."""
+
+    _L = None
+
+    @classmethod
+    def lib(cls):
+        if cls._L is None:
+            L = RefTPAc.lib()
+            L.ref_ta_create.argtypes = [C.c_uint64, C.c_uint64]
+            L.ref_ta_create.restype = C.c_void_p
+            L.ref_ta_destroy.argtypes = [C.c_void_p]
+            L.ref_ta_load.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_uint64]
+            L.ref_ta_init.argtypes = [C.c_void_p]
+            L.ref_ta_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint8, _f32p, _u8p, _u64p, _f32p, C.c_uint64,
+                                       C.POINTER(C.c_float), C.POINTER(C.c_double)]
+            L.ref_ta_query.restype = C.c_uint64
+            cls._L = L
+        return cls._L
+
+    def __init__(self, rows):
+        self.n, self.d = rows.shape
+        L = self.lib()
+        self.h = L.ref_ta_create(self.n, self.d)
+        if L.ref_ta_load(self.h, np.ascontiguousarray(rows, np.float32).reshape(-1), self.n, self.d):
+            raise MemoryError("reference table allocation failed")
+
+    def init(self):
+        self.lib().ref_ta_init(self.h)
+
+    def query(self, k, weights, attr):
+        """Returns (ids, scores, threshold, ms)."""
+        w = np.zeros(max(self.d, len(weights)), np.float32)
+        w[: len(weights)] = weights
+        a = np.ascontiguousarray(attr, np.uint8)
+        cap = max(1, min(k, self.n))
+        ids = np.zeros(cap, np.uint64)
+        sc = np.zeros(cap, np.float32)
+        th = C.c_float(0)
+        ms = C.c_double(0)
+        c = self.lib().ref_ta_query(self.h, k, len(a), w, a, ids, sc, cap, C.byref(th), C.byref(ms))
+        c = min(c, cap)
+        return ids[:c], sc[:c], th.value, ms.value
+
+    def close(self):
+        if self.h:
+            self.lib().ref_ta_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -45,6 +45,7 @@
 #include "time/Time.h"
 #include "cpu/TPAc.h"
 #include "cpu/TPAr.h"
+#include "cpu/TA.h"
 
 namespace {
 
@@ -168,6 +169,33 @@ void ref_normalize_transpose(float *data, uint64_t n, uint64_t d) {
 }
 
 int ref_threads_constant(void) { return THREADS; }
+
+/* TA<float,uint64_t> (cpu/TA.h): sorted lists over a row-major table (load as for
+ * TPAr); query = findTopK.  Returns the result count; ids/scores in res order. */
+void *ref_ta_create(uint64_t n, uint64_t d) { return new TA<float, uint64_t>(n, d); }
+void ref_ta_destroy(void *h) { delete static_cast<TA<float, uint64_t> *>(h); }
+int ref_ta_load(void *h, const float *rows, uint64_t n, uint64_t d) {
+  return load_table(static_cast<TA<float, uint64_t> *>(h), rows, n, d);
+}
+void ref_ta_init(void *h) {
+  Quiet q;
+  static_cast<TA<float, uint64_t> *>(h)->init();
+}
+uint64_t ref_ta_query(void *h, uint64_t k, uint8_t qq, float *weights, uint8_t *attr, uint64_t *ids, float *scores,
+                      uint64_t cap, float *thres, double *ms) {
+  TA<float, uint64_t> *t = static_cast<TA<float, uint64_t> *>(h);
+  Quiet q;
+  t->reset_clocks();
+  double t0 = omp_get_wtime();
+  t->findTopK(k, qq, weights, attr);
+  double t1 = omp_get_wtime();
+  std::vector<tuple_<float, uint64_t>> res = t->get_res();
+  uint64_t c = res.size() < cap ? res.size() : cap;
+  for (uint64_t j = 0; j < c; j++) { ids[j] = res[j].tid; scores[j] = res[j].score; }
+  if (thres) *thres = t->get_thres();
+  if (ms) *ms = (t1 - t0) * 1e3;
+  return res.size();
+}
 
 /* TPAr<float,uint64_t> (cpu/TPAr.h): the row-major variant.  load copies an n x d
  * row-major table (object i at src + i*d); init normalises it (common/common.h:63-92);

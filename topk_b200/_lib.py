@@ -51,6 +51,10 @@ SIGNATURES = [
     ("topk_create", C.c_int, [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
     ("topk_destroy", C.c_int, [_H]),
     ("topk_upload_colmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_build_lists", C.c_int, [_H]),
+    ("topk_read_list", C.c_int, [_H, C.c_uint32, _u32p, _f32p]),
+    ("topk_query_ta", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, _u64p, _f32p, C.POINTER(C.c_uint64),
+                                C.POINTER(C.c_float), _u64p]),
     ("topk_upload_rowmajor", C.c_int, [_H, _f32p, C.c_uint64]),
     ("topk_download_rowmajor", C.c_int, [_H, _f32p, C.c_uint64]),
     ("topk_csv_shape", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

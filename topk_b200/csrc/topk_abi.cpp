@@ -142,6 +142,9 @@ struct topk_table_s {
   // original ids, per-partition [P][d] min / max / mean (device and host copies)
   float *ptable = nullptr;
   LoaderState *loader = nullptr;  // table-file pipeline buffers, made on the first load
+  TaLists *ta = nullptr;          // sorted lists of the threshold algorithm
+  uint64_t ta_version = 0;
+  std::mutex ta_mu;               // TA queries share the lists' scratch
   uint32_t *pids = nullptr;
   float *pstats = nullptr;
   uint32_t part_log2 = 0, num_parts = 0;
@@ -1087,6 +1090,7 @@ int topk_destroy(topk_table_t h) {
   cudaFree(h->pstats);
   cudaFree(h->table);
   loader_state_free(h->loader);
+  ta_lists_free(h->ta);
   cudaFree(h->d_minmax);
   cudaFree(h->d_norm);
   delete h;
@@ -1141,6 +1145,52 @@ int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride) {
   if (!h->loader) h->loader = loader_state_new();
   std::string msg;
   const int rc = download_rowmajor_device(h->loader, host, row_stride, h->table, h->ld, h->d, h->n, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_build_lists(topk_table_t h) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::lock_guard<std::mutex> lk(h->ta_mu);
+  ta_lists_free(h->ta);
+  h->ta = nullptr;
+  std::string msg;
+  const int rc = ta_lists_build(&h->ta, h->table, h->ld, h->d, h->n, h->num_sms, &msg);
+  if (rc != TOPK_OK) return fail(rc, "%s", msg.c_str());
+  h->ta_version = h->data_version;
+  return TOPK_OK;
+}
+
+int topk_read_list(topk_table_t h, uint32_t m, uint32_t *ids, float *values) {
+  g_last_error.clear();
+  if (!h) return fail(TOPK_ERR_ARG, "null handle");
+  if (!h->ta || h->ta_version != h->data_version) return fail(TOPK_ERR_STATE, "no sorted lists of the current table");
+  if (m >= h->d) return fail(TOPK_ERR_ARG, "attribute %u >= d", m);
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::lock_guard<std::mutex> lk(h->ta_mu);
+  std::string msg;
+  const int rc = ta_lists_read(h->ta, m, ids, values, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
+int topk_query_ta(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, uint64_t *ids,
+                  float *scores, uint64_t *count, float *threshold, uint64_t *stats) {
+  g_last_error.clear();
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (!ids || !scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  if (!h->ta || h->ta_version != h->data_version)
+    return fail(TOPK_ERR_STATE, "no sorted lists for the current table: call topk_build_lists");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::lock_guard<std::mutex> lk(h->ta_mu);
+  std::string msg;
+  const int rc = ta_query(h->ta, h->table, h->ld, k, qq, weights, attr, h->num_sms, ids, scores, count, threshold,
+                          stats, &msg);
   return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
 }
 

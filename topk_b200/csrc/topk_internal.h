@@ -174,4 +174,18 @@ int upload_rowmajor_device(LoaderState *L, const float *host, uint64_t row_strid
 int download_rowmajor_device(LoaderState *L, float *host, uint64_t row_stride, const float *table, uint64_t ld,
                              uint32_t d, uint64_t n, std::string *msg);
 
+// Threshold algorithm over sorted lists (ta.cu; cpu/TA.h).  ta_lists_build: per
+// attribute the ids by value descending (ties by the lower id) and the sorted values,
+// plus query scratch.  ta_query: exact top-k by walking the queried lists (results of
+// the full scan); stats: depth walked, objects scored, blocks.  One query at a time
+// per TaLists.
+struct TaLists;
+int ta_lists_build(TaLists **out, const float *table, uint64_t ld, uint32_t d, uint64_t n, int num_sms,
+                   std::string *msg);
+void ta_lists_free(TaLists *L);
+int ta_lists_read(const TaLists *L, uint32_t m, uint32_t *ids, float *vals, std::string *msg);
+int ta_query(TaLists *L, const float *table, uint64_t ld, uint64_t k, uint32_t qq, const float *weights,
+             const uint8_t *attr, int num_sms, uint64_t *ids, float *scores, uint64_t *count, float *threshold,
+             uint64_t *stats, std::string *msg);
+
 }  // namespace topk

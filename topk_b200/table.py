@@ -125,6 +125,32 @@ class Table:
         c = cnt.value
         return ids[:c], sc[:c], th.value
 
+    # -- threshold algorithm over sorted lists -----------------------------
+    def build_lists(self):
+        """TA::init's sorted lists (cpu/TA.h:40-58), built on the device."""
+        check(_lib.load().topk_build_lists(self._h))
+
+    def read_list(self, m):
+        """(ids uint32, values float32) of attribute m's list, value descending."""
+        ids = np.empty(self.n, np.uint32)
+        vals = np.empty(self.n, np.float32)
+        check(_lib.load().topk_read_list(self._h, int(m), ids, vals))
+        return ids, vals
+
+    def query_ta(self, k, weights, attr):
+        """Exact top-k by the threshold algorithm (cpu/TA.h:61-96); returns (ids, scores,
+        threshold, stats) with stats = (depth walked, objects scored, blocks)."""
+        w, a = _weights(weights, self.d), _attr(attr)
+        cap = max(1, min(int(k), self.n))
+        ids = np.empty(cap, np.uint64)
+        sc = np.empty(cap, np.float32)
+        cnt = C.c_uint64()
+        th = C.c_float()
+        st = np.zeros(3, np.uint64)
+        check(_lib.load().topk_query_ta(self._h, int(k), len(a), w, a, ids, sc, C.byref(cnt), C.byref(th), st))
+        c = cnt.value
+        return ids[:c], sc[:c], th.value, tuple(int(x) for x in st)
+
     def query_device(self, k, weights, attr, d_ids, d_scores, d_threshold=0, stream=0):
         """Asynchronous query writing into device pointers (ints) on a stream (int handle)."""
         w, a = _weights(weights, self.d), _attr(attr)

@@ -201,3 +201,55 @@ class TPAr(TPAc):
             self._table.upload_rowmajor(self.cdata)
         self._table.normalize()
         self.tt_init = 0.0
+
+
+class TA(AA):
+    """The threshold algorithm over sorted lists (cpu/TA.h:10-96).  Like the reference,
+    cdata holds the table row-major, (n, d); init() normalises it
+    (common/common.h:63-92) and builds the sorted lists, on the device; findTopK walks
+    them there.  Results are the exact top-k (each attribute scored with its own
+    weight; the reference reuses the weight of the list an object was found in,
+    cpu/TA.h:83)."""
+
+    def __init__(self, n, d, device=0, mqthreads=256):
+        super().__init__(n, d, device, mqthreads)
+        self.algo = "TA"
+        self._table = Table(n, d, device)
+        self.last_stats = None
+
+    @property
+    def table(self):
+        return self._table
+
+    def get_cdata(self):
+        if self.cdata is None:
+            self.cdata = np.zeros((self.n, self.d), np.float32)
+        return self.cdata
+
+    def set_cdata(self, cdata):
+        c = np.ascontiguousarray(cdata, np.float32)
+        if c.shape != (self.n, self.d):
+            raise ValueError(f"cdata must be ({self.n}, {self.d}) row-major, got {c.shape}")
+        self.cdata = c
+
+    def init(self):
+        t0 = time.perf_counter()
+        if self.cdata is not None:
+            self._table.upload_rowmajor(self.cdata)
+        self._table.normalize()
+        self._table.build_lists()
+        self.tt_init = (time.perf_counter() - t0) * 1e3
+
+    def findTopK(self, k, qq, weights, attr):
+        a = np.ascontiguousarray(attr, np.uint8)[: int(qq)]
+        t0 = time.perf_counter()
+        ids, sc, th, st = self._table.query_ta(int(k), weights, a)
+        self.tt_processing += (time.perf_counter() - t0) * 1e3
+        self.res = list(zip(ids.tolist(), sc.tolist()))
+        self.res_ids, self.res_scores = ids, sc
+        self.threshold = th
+        self.last_stats = st
+        self.tuple_count = st[1]
+
+    def close(self):
+        self._table.close()

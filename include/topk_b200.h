@@ -144,8 +144,8 @@ int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride);
  * numbers, or fewer than n rows return TOPK_ERR_ARG naming the row, and leave the table
  * without data.  stats (4 entries, may be NULL): bytes parsed, rows found, values
  * converted on the host, chunks.  The handle keeps the pipeline's buffers (two pinned
- * and two device chunk buffers with their row arrays) for later loads; loads on one
- * handle must not overlap.
+ * and two device chunk buffers with their row arrays) for later loads; loads and
+ * row-major transfers on one handle take turns on them.
  *
  * topk_save_csv: the table as File<T>::store writes it (input/File.h:405-431): one
  * line per object, "%f" fields separated by ','.

@@ -142,6 +142,7 @@ struct topk_table_s {
   // original ids, per-partition [P][d] min / max / mean (device and host copies)
   float *ptable = nullptr;
   LoaderState *loader = nullptr;  // table-file pipeline buffers, made on the first load
+  std::mutex loader_mu;           // one load / row-major transfer at a time uses them
   TaLists *ta = nullptr;          // sorted lists of the threshold algorithm
   uint64_t ta_version = 0;
   std::mutex ta_mu;               // TA queries share the lists' scratch
@@ -1129,6 +1130,7 @@ int topk_upload_rowmajor(topk_table_t h, const float *host, uint64_t row_stride)
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   table_changed(h);
+  std::lock_guard<std::mutex> lk(h->loader_mu);
   if (!h->loader) h->loader = loader_state_new();
   std::string msg;
   const int rc = upload_rowmajor_device(h->loader, host, row_stride, h->table, h->ld, h->d, h->n, &msg);
@@ -1142,6 +1144,7 @@ int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride) {
   if (row_stride < h->d) return fail(TOPK_ERR_ARG, "row_stride=%llu < d=%u", (unsigned long long)row_stride, h->d);
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::lock_guard<std::mutex> lk(h->loader_mu);
   if (!h->loader) h->loader = loader_state_new();
   std::string msg;
   const int rc = download_rowmajor_device(h->loader, host, row_stride, h->table, h->ld, h->d, h->n, &msg);
@@ -1209,6 +1212,7 @@ int topk_load_csv(topk_table_t h, const char *path, uint64_t chunk_bytes, uint64
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   table_changed(h);
   std::string msg;
+  std::lock_guard<std::mutex> lk(h->loader_mu);
   if (!h->loader) h->loader = loader_state_new();
   const int rc = load_csv_device(h->loader, path, h->table, h->ld, h->d, h->n, h->num_sms, chunk_bytes, stats, &msg);
   h->has_data = rc == TOPK_OK;  // a failed load leaves the table undefined
@@ -1241,6 +1245,7 @@ int topk_load_binary(topk_table_t h, const char *path) {
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   table_changed(h);
   std::string msg;
+  std::lock_guard<std::mutex> lk(h->loader_mu);
   if (!h->loader) h->loader = loader_state_new();
   const int rc = load_binary_device(h->loader, path, h->table, h->ld, h->d, h->n, &msg);
   h->has_data = rc == TOPK_OK;

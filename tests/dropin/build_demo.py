@@ -1,6 +1,6 @@
-"""Build tests/dropin/_build/tpac_dropin_demo and tpar_dropin_demo (need the reference
-tree for cpu/AA.h, cpu/TPAc.h, cpu/TPAr.h and time/Time.h; TOPK_REFERENCE, default
-/root/reference).  The binary
+"""Build tests/dropin/_build/tpac_dropin_demo, tpar_dropin_demo and ta_dropin_demo (need
+the reference tree for cpu/AA.h, cpu/TPAc.h, cpu/TPAr.h, cpu/TA.h and time/Time.h;
+TOPK_REFERENCE, default /root/reference).  The binary
 then travels with the working tree; without the reference tree nothing is built and
 the GPU test that runs it skips."""
 import os
@@ -31,11 +31,12 @@ def _build_one(name, header, ref, verbose):
 
 
 def build(verbose=False):
-    """Builds both demos (TPAc and TPAr); returns the TPAc demo's path."""
+    """Builds the demos (TPAc, TPAr, TA); returns the TPAc demo's path."""
     ref = os.environ.get("TOPK_REFERENCE", "/root/reference")
     if not os.path.exists(os.path.join(ref, "cpu", "TPAc.h")):
         return OUT if os.path.exists(OUT) else None
     _build_one("tpar_dropin_demo", ["TPAcGPU.h", "TPArGPU.h"], ref, verbose)
+    _build_one("ta_dropin_demo", ["TPAcGPU.h", "TAGPU.h"], ref, verbose)
     return _build_one("tpac_dropin_demo", ["TPAcGPU.h"], ref, verbose)
 
 

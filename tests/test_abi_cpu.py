@@ -70,3 +70,32 @@ def test_create_without_gpu_reports_cuda_error(gpu_available):
     with pytest.raises(T.TopKError) as ei:
         T.Table(1024, 4)
     assert ei.value.status == _lib.ERR_CUDA
+
+
+def test_null_handle_calls_of_the_file_index_and_ta_entries():
+    """The table-file, row-major, index-order and TA entries reject a null handle (or
+    null arguments) before any device work."""
+    import numpy as np
+    L = T.load()
+    w = np.ones(4, np.float32)
+    a = np.zeros(2, np.uint8)
+    ids = np.zeros(4, np.uint64)
+    sc = np.zeros(4, np.float32)
+    st = np.zeros(4, np.uint64)
+    rows = np.zeros(16, np.float32)
+    u32 = np.zeros(4, np.uint32)
+    assert L.topk_load_csv(None, b"/nonexistent.csv", 0, st) == _lib.ERR_ARG
+    assert L.topk_save_csv(None, b"x.csv") == _lib.ERR_ARG
+    assert L.topk_load_binary(None, b"x.bin") == _lib.ERR_ARG
+    assert L.topk_save_binary(None, b"x.bin") == _lib.ERR_ARG
+    assert L.topk_upload_rowmajor(None, rows, 4) == _lib.ERR_ARG
+    assert L.topk_download_rowmajor(None, rows, 4) == _lib.ERR_ARG
+    assert L.topk_build_partitions_ordered(None, 1024, 1) == _lib.ERR_ARG
+    assert L.topk_build_partitions_ordered(None, 1024, 9) == _lib.ERR_ARG  # unknown order
+    assert L.topk_partition_ids(None, u32) == _lib.ERR_ARG
+    assert L.topk_build_lists(None) == _lib.ERR_ARG
+    assert L.topk_read_list(None, 0, u32, np.zeros(4, np.float32)) == _lib.ERR_ARG
+    assert L.topk_query_ta(None, 4, 2, w, a, ids, sc, None, None, st) == _lib.ERR_ARG
+    n, d = C.c_uint64(), C.c_uint64()
+    assert L.topk_csv_shape(None, C.byref(n), C.byref(d)) == _lib.ERR_ARG
+    assert L.topk_binary_shape(b"/nonexistent.bin", C.byref(n), C.byref(d)) == _lib.ERR_ARG

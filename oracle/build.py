@@ -10,6 +10,8 @@ Products:
     builds (cpu/VTA.h, cpu/PTA.h) through ref_index_shim.cpp, likewise.
   * oracle/_ref/libref_file.so - the reference's table loader (input/File.h) through
     ref_file_shim.cpp, likewise.
+  * oracle/_ref/libref_sla_d{D}.so - the reference's SLA layer build (cpu/SLA.h and
+    its vendored skyline library) through ref_sla_shim.cpp, likewise.
 
 Strict flags for both: -O3 -ffp-contract=off, never -ffast-math.  The reference's
 own Makefile:60 adds -ffast-math, which changes the normalised table and the
@@ -98,6 +100,36 @@ def build_ref_index(verbose=False, force=False):
     return outs
 
 
+SLA_DIMS = (4, 6)
+
+
+def ref_sla_so(num_dims):
+    return os.path.join(REF_OUT, f"libref_sla_d{num_dims}.so")
+
+
+def build_ref_sla(verbose=False, force=False):
+    """Compile the reference SLA layer build (cpu/SLA.h with the skyline library it
+    vendors under skyline/) through ref_sla_shim.cpp, one library per NUM_DIMS.
+    Returns the list of built paths (those present when the reference is absent)."""
+    root = reference_root()
+    srcs = [os.path.join(root, p) for p in ("skyline/hybrid/hybrid.cpp", "skyline/common/common.cpp",
+                                            "skyline/common/skyline_i.cpp", "skyline/util/timing.cpp")]
+    hdrs = [os.path.join(root, p) for p in ("cpu/SLA.h", "cpu/VTA.h", "cpu/AA.h", "common/common.h",
+                                            "skyline/hybrid/hybrid.h", "time/Time.h")]
+    outs = [ref_sla_so(dd) for dd in SLA_DIMS]
+    if not all(os.path.exists(f) for f in srcs + hdrs):
+        return [o for o in outs if os.path.exists(o)]
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_sla_shim.cpp")
+    for dd, out in zip(SLA_DIMS, outs):
+        if force or _stale(out, [shim] + srcs + hdrs):
+            _run(["g++", "-std=c++14", "-O2", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math",
+                  "-fopenmp", "-fPIC", "-shared", "-w", f"-DNUM_DIMS={dd}", "-I", root,
+                  "-I", os.path.join(HERE, "stub"), "-I", os.path.join(root, "skyline"), shim] + srcs + ["-o", out],
+                 verbose)
+    return outs
+
+
 REF_FILE_SO = os.path.join(REF_OUT, "libref_file.so")
 
 
@@ -123,3 +155,4 @@ if __name__ == "__main__":
     print(build_ref(v, force="-f" in sys.argv))
     print(build_ref_index(v, force="-f" in sys.argv))
     print(build_ref_file(v, force="-f" in sys.argv))
+    print(build_ref_sla(v, force="-f" in sys.argv))

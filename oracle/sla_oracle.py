@@ -11,9 +11,10 @@ blocks of 1024 rows.
 
 `skyline_layers` restates the peeling.  `layer_depths` computes the same layers the way
 a parallel build would: a row's depth is 1 + the largest depth of the rows that
-dominate it (0 for the skyline), every dominator of a row has a smaller coordinate sum
-(computed in FP32 with one rounding per addition, monotone), so rows processed in
-ascending sum order see their dominators first; the stop rule then merges every depth
+dominate it (0 for the skyline), every dominator of a row has a coordinate sum no
+larger (computed in FP32 with one rounding per addition, monotone) and, at an equal
+sum, comes first in the lexicographic order of its values, so rows processed in that
+order see their dominators first; the stop rule then merges every depth
 from the first one with at most 100 rows at or beyond it.  `sla_order` is the index
 order with ties by the lower id (the reference's unstable sorts and its skyline
 library's output order leave them open).  Pinned against the reference itself
@@ -64,14 +65,17 @@ def skyline_layers(table, stop=STOP_ROWS):
 
 
 def layer_depths(table, stop=STOP_ROWS):
-    """The same layers by depth: rows in ascending FP32 coordinate-sum order, depth =
-    1 + max depth of the dominators (all earlier in that order), then the stop rule."""
+    """The same layers by depth: rows in ascending FP32 coordinate-sum order (ties by
+    the values, lexicographically), depth = 1 + max depth of the dominators (all earlier
+    in that order), then the stop rule."""
     x = sky_values(table)
     n, d = x.shape
     s = np.zeros(n, np.float32)
     for m in range(d):
         s = (s + x[:, m]).astype(np.float32)
-    order = np.argsort(s, kind="stable")
+    # rounding can give a dominator the same FP32 sum as the row it dominates; among
+    # equal sums the lexicographic order of the values still puts the dominator first
+    order = np.lexsort(tuple(x[:, m] for m in range(d - 1, -1, -1)) + (s,))
     depth = np.zeros(n, np.int64)
     xs = x[order]
     for j in range(n):

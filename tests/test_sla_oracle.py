@@ -54,3 +54,17 @@ def test_index_order_matches_reference(n, d):
     layers = S.skyline_layers(tn)
     ref_perm = V.rows_to_ids(tn, rows)
     assert V.same_order_up_to_ties(tn, layers, ref_perm, S.sla_order(tn, layers))
+
+
+def test_depth_order_puts_dominators_first_at_equal_sums():
+    """Rows whose FP32 sums round to the same value while one dominates the other: the
+    lexicographic tie-break keeps the dominator first."""
+    # table values t, sky values 1 - t: row 0 -> (1, 2^-24), row 1 -> (1, 0); row 1
+    # dominates row 0, and both sums are 1.0 in FP32 (1 + 2^-24 rounds to even)
+    t_small = np.float32(1.0) - np.float32(2.0 ** -24)
+    tn = np.array([[0.0, 0.0], [t_small, 1.0]], np.float32)  # (d, n)
+    x = S.sky_values(tn)
+    assert x[0, 1] == np.float32(2.0 ** -24) and x[1, 1] == 0.0
+    assert np.float32(x[0, 0] + x[0, 1]) == np.float32(x[1, 0] + x[1, 1])
+    assert list(S.skyline_layers(tn, stop=0)) == [1, 0]
+    assert np.array_equal(S.layer_depths(tn, stop=0), S.skyline_layers(tn, stop=0))

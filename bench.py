@@ -38,7 +38,8 @@ flush is needed between queries.
           learned start with the BF16 filter, identical results checked.
 
 Multi-GPU (torchrun): every rank holds its own replica and runs the same query
-steps (weak scaling, no collective on the data path); time = max over ranks.
+steps (weak scaling, no collective on the data path); time = max over ranks.  The
+one-GPU secondary sections (pruned, loader, ta) run only when the job has one rank.
 
 `--impl reference` runs the reference's own CPU TPAc on the host (rank 0 only).
 """
@@ -782,11 +783,14 @@ def main():
     if not args.no_batched:
         result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q,
                                         methods=tuple(args.batched_methods.split(",")))
-    if not args.no_pruned and rank == 0:
+    # one-GPU secondary workloads: under torchrun the other ranks would idle at the
+    # final barrier (process-group timeout 120 s) while rank 0 ran them, so they run
+    # only when the job has one rank
+    if not args.no_pruned and world == 1:
         result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
-    if not args.no_loader and rank == 0:
+    if not args.no_loader and world == 1:
         result["loader"] = run_loader(T, local)
-    if not args.no_ta and rank == 0:
+    if not args.no_ta and world == 1:
         result["ta"] = run_ta(T, local)
     if args.c5:
         result["c5"] = run_c5(T, torch, dist, local, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))

@@ -74,6 +74,9 @@ class Table:
 
     @classmethod
     def from_csv(cls, path, device=0, chunk_bytes=0):
+        """A table of the file's shape as File<T>::count reads it (n = newlines), loaded
+        on the device.  Blank lines count in n but hold no row, so a file with blank
+        lines needs Table(rows, d).load_csv(path) instead."""
         n, d = csv_shape(path)
         t = cls(n, d, device)
         t.load_csv(path, chunk_bytes)

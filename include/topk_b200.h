@@ -16,6 +16,8 @@
  *                                             common/common.h:63-92 -> topk_upload_rowmajor,
  *                                                                      topk_download_rowmajor
  *   TA<T,Z>::init, findTopK                   cpu/TA.h:40-96        -> topk_build_lists, topk_query_ta
+ *   SLA<T,Z>::build_layers, create_lists      cpu/SLA.h:102-251     -> topk_skyline_layers,
+ *                                                                      topk_build_partitions_ordered(SLA)
  *   File<T>::count, load (transpose), store   input/File.h:108-132,
  *                                             233-330, 405-431      -> topk_csv_shape, topk_load_csv,
  *                                                                      topk_save_csv
@@ -238,6 +240,11 @@ int topk_build_partitions(topk_table_t h, uint32_t part_rows);
 #define TOPK_ORDER_VTA_THREADS 3 /* VTA's order as its threaded build makes it (IMP 2, the
                                   * reference's default): 16 ranges of ceil(n/16) rows,
                                   * each in VTA's order on its own (cpu/VTA.h:13,78-85). */
+#define TOPK_ORDER_SLA 4    /* SLA's order (cpu/SLA.h:102-139, 199-251): rows grouped by
+                             * skyline layer (the skyline of 1 - x, peeled while more than
+                             * 100 rows remain; see topk_skyline_layers), each layer in
+                             * VTA's order, layers by number.  Needs d <= 32; the layer
+                             * build compares O(n^2 d) pairs. */
 /* In the VTA and PTA orders ties go to the lower row id (the reference's sorts are not
  * stable and leave them unspecified: rows sharing a minimum position, equal values);
  * PTA's angles order as their tangents, which are compared. */
@@ -246,6 +253,13 @@ int topk_build_partitions(topk_table_t h, uint32_t part_rows);
  * device (radix sorts, n < 2^31) and need about 20*n (VTA) or 32*n (VTA_THREADS, PTA)
  * bytes of scratch while they run. */
 int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order);
+
+/* SLA's skyline layers (cpu/SLA.h:102-139), built on the device: layers[i] = the layer
+ * of row i (0 = the skyline of the values 1 - x: no other row is <= in every attribute
+ * and < in one); each next layer is the skyline of the rows left, and once at most 100
+ * rows are left they form the last layer, as in the reference.  num_layers = the
+ * count.  d <= 32, n < 2^31; O(n^2 d) compares. */
+int topk_skyline_layers(topk_table_t h, uint32_t *layers, uint64_t *num_layers);
 
 /* The partitioned copy's row ids (n entries): row i of the copy is row ids[i] of the
  * table. */

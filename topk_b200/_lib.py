@@ -28,7 +28,7 @@ DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
 
 # topk_query_batch methods (TOPK_BATCH_* in include/topk_b200.h)
 BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16, BATCH_LEARNED = 0, 1, 2, 3, 4
-ORDER_MORTON, ORDER_VTA, ORDER_PTA, ORDER_VTA_THREADS = 0, 1, 2, 3
+ORDER_MORTON, ORDER_VTA, ORDER_PTA, ORDER_VTA_THREADS, ORDER_SLA = 0, 1, 2, 3, 4
 
 
 class TopKError(RuntimeError):
@@ -51,6 +51,7 @@ SIGNATURES = [
     ("topk_create", C.c_int, [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]),
     ("topk_destroy", C.c_int, [_H]),
     ("topk_upload_colmajor", C.c_int, [_H, _f32p, C.c_uint64]),
+    ("topk_skyline_layers", C.c_int, [_H, _u32p, C.POINTER(C.c_uint64)]),
     ("topk_build_lists", C.c_int, [_H]),
     ("topk_read_list", C.c_int, [_H, C.c_uint32, _u32p, _f32p]),
     ("topk_query_ta", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, _u64p, _f32p, C.POINTER(C.c_uint64),

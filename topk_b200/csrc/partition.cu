@@ -241,16 +241,18 @@ uint64_t index_order_work_words(uint64_t n, IndexOrder kind) { return (kind == I
 
 cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, IndexOrder kind,
                                uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
-                               cudaStream_t s) {
+                               cudaStream_t s, const uint32_t *groups, uint32_t group_bits) {
   const bool pta = kind == IndexOrder::kPta, grouped = kind != IndexOrder::kVta;
   if (n > 0x7FFFFFFFull || (pta && (n < 2 || d > 32))) return cudaErrorInvalidValue;
+  if (kind == IndexOrder::kGroups && (!groups || group_bits > 31)) return cudaErrorInvalidValue;
   // work, VTA: keys in/out, ids in/out, min ranks (n words each); grouped orders:
   // 64-bit keys in/out (2n words each, the angle sorts use their first halves), ids
   // in/out, min ranks, groups
   uint32_t *kin = work, *kout = work + (grouped ? 2 * n : n);
   uint32_t *iin = work + (grouped ? 4 * n : 2 * n), *iout = iin + n, *rank = iout + n, *part = rank + n;
   uint64_t *kin64 = reinterpret_cast<uint64_t *>(kin), *kout64 = reinterpret_cast<uint64_t *>(kout);
-  const uint32_t gbits = pta ? d - 1 : (grouped ? 4 : 0);  // groups < 2^gbits
+  // groups < 2^gbits
+  const uint32_t gbits = pta ? d - 1 : kind == IndexOrder::kGroups ? group_bits : (grouped ? 4 : 0);
   const int nn = (int)n;
   if (!temp) {  // size query
     size_t a = 0, b = 0, c = 0;
@@ -271,6 +273,8 @@ cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint
       e = cub::DeviceRadixSort::SortPairs(temp, tb, kin, kout, iin, iout, nn, 0, 32, s);
       if (e == cudaSuccess) pta_part_add_kernel<<<g, 256, 0, s>>>(iout, n, n / 2, 1u << c, part);
     }
+  } else if (kind == IndexOrder::kGroups) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(part, groups, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
   } else if (grouped) {
     range_part_kernel<<<g, 256, 0, s>>>(n, (n - 1) / kVtaThreadRanges + 1, part);
   }

@@ -1151,6 +1151,17 @@ int topk_download_rowmajor(topk_table_t h, float *host, uint64_t row_stride) {
   return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
 }
 
+int topk_skyline_layers(topk_table_t h, uint32_t *layers, uint64_t *num_layers) {
+  g_last_error.clear();
+  if (!h || !layers || !num_layers) return fail(TOPK_ERR_ARG, "null argument");
+  if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  std::string msg;
+  const int rc = skyline_layers_device(h->table, h->ld, h->d, h->n, h->num_sms, layers, num_layers, &msg);
+  return rc == TOPK_OK ? rc : fail(rc, "%s", msg.c_str());
+}
+
 int topk_build_lists(topk_table_t h) {
   g_last_error.clear();
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
@@ -1506,7 +1517,7 @@ int topk_partition_ids(topk_table_t h, uint32_t *ids) {
 int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order) {
   g_last_error.clear();
   if (order != TOPK_ORDER_MORTON && order != TOPK_ORDER_VTA && order != TOPK_ORDER_PTA &&
-      order != TOPK_ORDER_VTA_THREADS)
+      order != TOPK_ORDER_VTA_THREADS && order != TOPK_ORDER_SLA)
     return fail(TOPK_ERR_ARG, "unknown order %d", order);
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
@@ -1514,6 +1525,7 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
     return fail(TOPK_ERR_UNSUPPORTED, "VTA and PTA orders need n < 2^31 rows");
   if (order == TOPK_ORDER_PTA && (h->n < 2 || h->d > 32))
     return fail(TOPK_ERR_UNSUPPORTED, "PTA order needs n >= 2 and d <= 32");
+  if (order == TOPK_ORDER_SLA && h->d > 32) return fail(TOPK_ERR_UNSUPPORTED, "SLA order needs d <= 32");
   if (part_rows < 1024 || part_rows > (1u << 24) || (part_rows & (part_rows - 1)))
     return fail(TOPK_ERR_ARG, "part_rows must be a power of two in [1024, 2^24]");
   uint32_t lg = 0;
@@ -1523,6 +1535,17 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   cudaStream_t s = h->primary->stream;
+  // SLA: the skyline layers first (they are the groups of the order)
+  std::vector<uint32_t> sla_layers;
+  uint32_t sla_bits = 0;
+  if (order == TOPK_ORDER_SLA) {
+    sla_layers.resize(h->n);
+    uint64_t nl = 0;
+    std::string msg;
+    const int rc = skyline_layers_device(h->table, h->ld, h->d, h->n, h->num_sms, sla_layers.data(), &nl, &msg);
+    if (rc != TOPK_OK) return fail(rc, "%s", msg.c_str());
+    while (sla_bits < 31 && (1ull << sla_bits) < nl) ++sla_bits;
+  }
   // column extremes: the Morton code quantises each attribute over [min, max]
   CK(launch_minmax(h->table, h->ld, h->d, h->n, h->d_minmax, s));
   std::vector<uint32_t> w((size_t)h->d * kMinmaxWords);
@@ -1573,19 +1596,29 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
   if (e == cudaSuccess && order != TOPK_ORDER_MORTON) {
     const IndexOrder kind = order == TOPK_ORDER_PTA           ? IndexOrder::kPta
                             : order == TOPK_ORDER_VTA_THREADS ? IndexOrder::kVtaThreads
+                            : order == TOPK_ORDER_SLA         ? IndexOrder::kGroups
                                                               : IndexOrder::kVta;
-    uint32_t *work = nullptr;
+    uint32_t *work = nullptr, *groups = nullptr;
     void *temp = nullptr;
     size_t temp_bytes = 0;
-    e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, nullptr, nullptr, &temp_bytes, h->num_sms, s);
+    if (kind == IndexOrder::kGroups) {
+      e = cudaMalloc(&groups, h->n * sizeof(uint32_t));
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(groups, sla_layers.data(), h->n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess)
+      e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, nullptr, nullptr, &temp_bytes, h->num_sms, s,
+                             groups, sla_bits);
     if (e == cudaSuccess) e = cudaMalloc(&work, index_order_work_words(h->n, kind) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc(&temp, std::max<size_t>(temp_bytes, 16));
     if (e == cudaSuccess)
-      e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, work, temp, &temp_bytes, h->num_sms, s);
+      e = launch_index_order(h->table, h->ld, h->d, h->n, kind, h->pids, work, temp, &temp_bytes, h->num_sms, s,
+                             groups, sla_bits);
     if (e == cudaSuccess) e = launch_gather_rows(h->table, h->ld, h->d, h->n, h->pids, h->ptable, h->num_sms, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // before the scratch goes
     cudaFree(work);
     cudaFree(temp);
+    cudaFree(groups);
   }
   float *pmin = h->pstats, *pmax = h->pstats + P * h->d, *pmean = h->pstats + 2 * P * h->d;
   if (e == cudaSuccess) e = launch_partition_stats(h->ptable, h->ld, h->d, h->n, lg, (uint32_t)P, pmin, pmax, pmean, s);

@@ -137,12 +137,20 @@ cudaError_t launch_partition_build(const float *table, uint64_t ld, uint32_t d, 
 // work holds index_order_work_words(n, kind) words; temp is the radix sorts' scratch
 // (first call with temp == nullptr to size it).  n < 2^31; PTA also needs n >= 2 and
 // d <= 32.
-enum class IndexOrder { kVta, kVtaThreads, kPta };
+// kGroups: VTA's order inside caller-given groups (device array `groups`, each value
+// < 2^group_bits, group_bits <= 31), groups by number: SLA's index with the skyline
+// layer as the group (cpu/SLA.h:199-251).
+enum class IndexOrder { kVta, kVtaThreads, kPta, kGroups };
 constexpr uint32_t kVtaThreadRanges = 16;
 uint64_t index_order_work_words(uint64_t n, IndexOrder kind);
 cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, IndexOrder kind,
                                uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
-                               cudaStream_t s);
+                               cudaStream_t s, const uint32_t *groups = nullptr, uint32_t group_bits = 0);
+// SLA's skyline layers (skyline.cu; cpu/SLA.h:102-139): the layer of every row, 0 = the
+// first skyline, with the reference's stop rule (the last <= 100 rows form one layer).
+// d <= 32, n < 2^31.  layers: n entries on the host.
+int skyline_layers_device(const float *table, uint64_t ld, uint32_t d, uint64_t n, int num_sms, uint32_t *layers,
+                          uint64_t *num_layers, std::string *msg);
 cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
                                float *ptable, int num_sms, cudaStream_t s);
 // Per-partition min / max / mean of each attribute, [num_parts][d] each.

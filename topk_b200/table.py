@@ -201,9 +201,16 @@ class Table:
 
     # -- partitions and pruned queries -------------------------------------
     def build_partitions(self, part_rows=1 << 16, order=0):
-        """order: ORDER_MORTON (0), ORDER_VTA (1), ORDER_PTA (2) or ORDER_VTA_THREADS (3),
-        see topk_build_partitions_ordered."""
+        """order: ORDER_MORTON (0), ORDER_VTA (1), ORDER_PTA (2), ORDER_VTA_THREADS (3) or
+        ORDER_SLA (4), see topk_build_partitions_ordered."""
         check(_lib.load().topk_build_partitions_ordered(self._h, int(part_rows), int(order)))
+
+    def skyline_layers(self):
+        """(layer of every row, number of layers): SLA's skyline layers (cpu/SLA.h:102-139)."""
+        out = np.empty(self.n, np.uint32)
+        nl = C.c_uint64()
+        check(_lib.load().topk_skyline_layers(self._h, out, C.byref(nl)))
+        return out, nl.value
 
     def partition_ids(self):
         """Row ids of the partitioned copy (row i of the copy is table row ids[i])."""

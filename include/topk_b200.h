@@ -199,8 +199,11 @@ int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
  * it, held until the process exits): k is limited to 1024 (TOPK_ERR_UNSUPPORTED
  * above), and calls whose work overlaps on the GPU share that array and race, so
  * serialise them.  The first call on each device performs a one-time set-up on
- * that device; make it before capturing work on that device.  Errors: the usual
- * status codes, message from topk_last_error(). */
+ * that device; make it before capturing work on that device.  The scan behind this
+ * entry has no device-side wait that can give up, so a call that returns TOPK_OK
+ * has enqueued work that always writes all its outputs; a kernel failure shows as a
+ * CUDA error on `stream`.  Errors: the usual status codes, message from
+ * topk_last_error(). */
 int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld, uint32_t d, uint64_t k, uint32_t qq,
                        const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores,
                        float *d_threshold, void *stream);
@@ -243,8 +246,9 @@ int topk_build_partitions(topk_table_t h, uint32_t part_rows);
 #define TOPK_ORDER_SLA 4    /* SLA's order (cpu/SLA.h:102-139, 199-251): rows grouped by
                              * skyline layer (the skyline of 1 - x, peeled while more than
                              * 100 rows remain; see topk_skyline_layers), each layer in
-                             * VTA's order, layers by number.  Needs d <= 32; the layer
-                             * build compares O(n^2 d) pairs. */
+                             * VTA's order, layers by number.  Needs d <= 32 and
+                             * n <= TOPK_SKYLINE_MAX_ROWS; the layer build compares
+                             * O(n^2 d) pairs. */
 /* In the VTA and PTA orders ties go to the lower row id (the reference's sorts are not
  * stable and leave them unspecified: rows sharing a minimum position, equal values);
  * PTA's angles order as their tangents, which are compared. */
@@ -258,7 +262,9 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
  * of row i (0 = the skyline of the values 1 - x: no other row is <= in every attribute
  * and < in one); each next layer is the skyline of the rows left, and once at most 100
  * rows are left they form the last layer, as in the reference.  num_layers = the
- * count.  d <= 32, n < 2^31; O(n^2 d) compares. */
+ * count.  d <= 32 and n <= TOPK_SKYLINE_MAX_ROWS (2^22): the build compares
+ * O(n^2 d) pairs, so larger tables return TOPK_ERR_UNSUPPORTED. */
+#define TOPK_SKYLINE_MAX_ROWS (1ull << 22)
 int topk_skyline_layers(topk_table_t h, uint32_t *layers, uint64_t *num_layers);
 
 /* The partitioned copy's row ids (n entries): row i of the copy is row ids[i] of the

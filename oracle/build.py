@@ -5,7 +5,7 @@ Products:
   * oracle/_ref/libref_tpac.so  - the reference's own TPAc (cpu/TPAc.h, cpu/AA.h,
     common/common.h, time/Time.h) compiled from where its sources lie, through the
     forwarding shim ref_tpac_shim.cpp.  Built only when the reference tree is present
-    (TOPK_REFERENCE, default /root/reference); the .so then travels with the repo.
+    (see reference_root()); the .so then travels with the repo.
   * oracle/_ref/libref_index_d{D}_imp{I}.so - the reference's VTA and PTA index
     builds (cpu/VTA.h, cpu/PTA.h) through ref_index_shim.cpp, likewise.
   * oracle/_ref/libref_file.so - the reference's table loader (input/File.h) through
@@ -29,8 +29,16 @@ ORACLE_SO = os.path.join(BUILD, "liboracle.so")
 REF_SO = os.path.join(REF_OUT, "libref_tpac.so")
 
 
+# Where the build container mounts the reference tree (read-only).  This recipe is
+# the one place that names it; set TOPK_REFERENCE to build from another checkout.
+CONTAINER_REFERENCE = "/root/reference"
+
+
 def reference_root():
-    return os.environ.get("TOPK_REFERENCE", "/root/reference")
+    """The reference tree this recipe compiles from: $TOPK_REFERENCE when set, else the
+    build container's mount.  Callers check that it exists (it does not on GPU boxes,
+    which use the prebuilt libraries under oracle/_ref)."""
+    return os.environ.get("TOPK_REFERENCE") or CONTAINER_REFERENCE
 
 
 def _run(cmd, verbose):

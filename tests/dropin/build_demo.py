@@ -1,6 +1,6 @@
 """Build tests/dropin/_build/tpac_dropin_demo, tpar_dropin_demo and ta_dropin_demo (need
-the reference tree for cpu/AA.h, cpu/TPAc.h, cpu/TPAr.h, cpu/TA.h and time/Time.h;
-TOPK_REFERENCE, default /root/reference).  The binary
+the reference tree for cpu/AA.h, cpu/TPAc.h, cpu/TPAr.h, cpu/TA.h and time/Time.h,
+located by the oracle's build recipe, oracle.build.reference_root()).  The binary
 then travels with the working tree; without the reference tree nothing is built and
 the GPU test that runs it skips."""
 import os
@@ -9,6 +9,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from oracle.build import reference_root  # noqa: E402
+
 OUT = os.path.join(HERE, "_build", "tpac_dropin_demo")
 
 
@@ -32,7 +35,7 @@ def _build_one(name, header, ref, verbose):
 
 def build(verbose=False):
     """Builds the demos (TPAc, TPAr, TA); returns the TPAc demo's path."""
-    ref = os.environ.get("TOPK_REFERENCE", "/root/reference")
+    ref = reference_root()
     if not os.path.exists(os.path.join(ref, "cpu", "TPAc.h")):
         return OUT if os.path.exists(OUT) else None
     _build_one("tpar_dropin_demo", ["TPAcGPU.h", "TPArGPU.h"], ref, verbose)

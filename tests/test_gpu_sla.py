@@ -59,3 +59,10 @@ def test_sla_limits():
             t.skyline_layers()
         with pytest.raises(T.TopKError):
             t.build_partitions(1024, order=T.ORDER_SLA)
+    # the O(n^2 d) build refuses tables above 2^22 rows before any device work
+    with T.Table((1 << 22) + 1, 1) as t:
+        t.generate(1, 1)
+        with pytest.raises(T.TopKError, match="2\\^22"):
+            t.skyline_layers()
+        with pytest.raises(T.TopKError, match="2\\^22"):
+            t.build_partitions(1024, order=T.ORDER_SLA)

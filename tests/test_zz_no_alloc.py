@@ -58,6 +58,28 @@ def test_noalloc_matches_regular_entry_point_twice():
             H.assert_same_result(got, t.query(k, w, a))
 
 
+def test_noalloc_k_above_n_matches_regular_entry_point():
+    torch = pytest.importorskip("torch")
+    L = T.load()
+    n, d = 300, 5  # k > n: min(k, n) objects, like topk_query
+    raw = O.generate(n, d, O.INDEPENDENT, 5)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        dt = torch.from_numpy(np.ascontiguousarray(t.download())).cuda()
+        ids = torch.full((1024,), -1, dtype=torch.int64, device="cuda")
+        sc = torch.empty(1024, dtype=torch.float32, device="cuda")
+        th = torch.empty(1, dtype=torch.float32, device="cuda")
+        w = np.linspace(0.2, 1.0, d).astype(np.float32)
+        a = np.array([4, 1, 2], np.uint8)
+        st = _noalloc(L, dt, n, n, d, 1000, w, a, ids, sc, th, torch.cuda.current_stream().cuda_stream)
+        assert st == _lib.OK, L.topk_last_error()
+        torch.cuda.synchronize()
+        got = (ids[:n].cpu().numpy().astype(np.uint64), sc[:n].cpu().numpy(), float(th.cpu()[0]))
+        H.assert_same_result(got, t.query(1000, w, a))
+        assert int(ids[n].cpu()) == -1  # nothing written past min(k, n)
+
+
 def test_noalloc_rejects_k_above_its_limit():
     torch = pytest.importorskip("torch")
     L = T.load()

@@ -24,6 +24,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -50,7 +52,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+// Per device: the SM count and shared-memory limit are written first, then the
+// scratch address is published with a release store; a call that loads the address
+// with acquire order and finds it set also sees the other two.
+std::atomic<unsigned char *> g_scratch_ptr[kMaxDevices] = {};
 int g_num_sms[kMaxDevices] = {};
 size_t g_smem_optin[kMaxDevices] = {};
 
@@ -70,7 +75,7 @@ int fail(int code, const char *fmt, ...) {
 // shared-memory attribute.
 int setup_current_device(int dev) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (g_scratch_ptr[dev]) return TOPK_OK;
+  if (g_scratch_ptr[dev].load(std::memory_order_acquire)) return TOPK_OK;
   void *ptr = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
   if (e != cudaSuccess || !ptr) return fail(TOPK_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
@@ -83,7 +88,7 @@ int setup_current_device(int dev) {
   g_smem_optin[dev] = (size_t)v;
   if ((e = scan_set_attributes(g_smem_optin[dev])) != cudaSuccess)
     return fail(TOPK_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-  g_scratch_ptr[dev] = static_cast<unsigned char *>(ptr);
+  g_scratch_ptr[dev].store(static_cast<unsigned char *>(ptr), std::memory_order_release);
   return TOPK_OK;
 }
 
@@ -111,15 +116,18 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(TOPK_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fail(TOPK_ERR_UNSUPPORTED, "device %d out of range", dev);
-  if (!g_scratch_ptr[dev]) {
+  unsigned char *blk = g_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!blk) {
     const int st = setup_current_device(dev);
     if (st != TOPK_OK) return st;
+    blk = g_scratch_ptr[dev].load(std::memory_order_acquire);
   }
-  unsigned char *blk = g_scratch_ptr[dev];
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the result holds min(k, n) objects, as topk_query's does
+  const uint64_t kk = std::min<uint64_t>(k, n);
 
-  ScanPlan pl = plan_scan(qq, (uint32_t)k, n, g_num_sms[dev], g_smem_optin[dev]);
-  if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)k);
+  ScanPlan pl = plan_scan(qq, (uint32_t)kk, n, g_num_sms[dev], g_smem_optin[dev]);
+  if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)kk);
   ScanParams p{};
   p.table = d_table;
   p.ld = ld;
@@ -132,13 +140,17 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;
   if ((uint32_t)pl.grid > kNoAllocMaxGrid) pl.grid = (int)kNoAllocMaxGrid;
   p.qq = qq;
-  p.k = (uint32_t)k;
+  p.k = (uint32_t)kk;
   p.cap = pl.cap;
   p.mcap = pl.mcap;
   uint32_t tree_slots = 0, tree_groups = 0;
   plan_merge_tree(p, (uint32_t)pl.grid, pl.fanin, &tree_slots, &tree_groups);
   if (tree_slots > kNoAllocMaxSlots || tree_groups > kNoAllocMaxGroups || p.nslots[p.levels] != 1)
     return fail(TOPK_ERR_UNSUPPORTED, "merge tree of %d CTAs does not fit the fixed scratch", pl.grid);
+  // No wait hook: with fault_mode 0 the scan has no device-side wait that can give
+  // up (its only bounded wait is the fault-injection barrier of the handle-based
+  // path), so a launch that succeeds always runs to the root and writes ids, scores
+  // and the threshold; a failure shows as a CUDA error on the stream.
   p.wait_limit = 1ull << 26;
   p.fault_mode = 0;
   p.scratch = reinterpret_cast<ScanScratch *>(blk);

@@ -34,6 +34,10 @@ namespace {
 
 constexpr uint32_t kSkyBlock = 256;   // rows per block (= threads of the block kernels)
 constexpr uint32_t kSkyMaxD = 32;
+// Largest table the layer build accepts.  The build compares O(n^2 d / 2) pairs in
+// n / 256 sequential settle + panel launch pairs: 2^22 rows are about 1.4e14 compares
+// (seconds to minutes on one B200); 2^26 rows would be 256 times that.
+constexpr uint64_t kSkyMaxRows = 1ull << 22;
 constexpr uint64_t kSkyStopRows = 100;  // cpu/SLA.h:110
 
 // key of column m of the sky values (m == d: the FP32 sum of all of them)
@@ -146,8 +150,8 @@ int grid_n(uint64_t work, int num_sms) {
 
 int skyline_layers_device(const float *table, uint64_t ld, uint32_t d, uint64_t n, int num_sms, uint32_t *layers,
                           uint64_t *num_layers, std::string *msg) {
-  if (d == 0 || d > kSkyMaxD || n == 0 || n > 0x7FFFFFFFull) {
-    *msg = "skyline layers need 1 <= d <= 32 and 1 <= n < 2^31";
+  if (d == 0 || d > kSkyMaxD || n == 0 || n > kSkyMaxRows) {
+    *msg = "skyline layers need 1 <= d <= 32 and 1 <= n <= 2^22 (the build compares O(n^2 d) pairs)";
     return TOPK_ERR_UNSUPPORTED;
   }
   cudaStream_t s = nullptr;

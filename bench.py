@@ -12,7 +12,9 @@ flush is needed between queries.
   e2e     the same queries through topk_query (the C-ABI call a caller makes) with
           host weights/attrs and host result buffers; host wall time per step.
   roofline  the fused scan kernel: algorithmic bytes 4*n*q per launch over its mean
-          launch time (per-launch CUDA events), against MEASURED_PEAKS.json hbm_gbs.
+          launch time (per-launch CUDA events), against MEASURED_PEAKS.json hbm_gbs;
+          traffic from ncu captures of 2^25-row launches scaled x8 (labelled); per_dist
+          the same step on the correlated and anticorrelated tables of the workload.
   cpu_baseline  the reference's TPAc::findTopKthreads (compiled strict into
           oracle/_ref) on this host, timed on a 2^25-row sample, scaled to n.
   batched  the multi-query workload: 4096 queries (attribute subsets of size
@@ -32,10 +34,14 @@ flush is needed between queries.
   ta       the threshold algorithm over device-built sorted lists against the full
           scan on correlated and independent 2^26 x 8 tables (identical results
           checked), and the reference's TA on a 2^20-row sample.
-  c5       (with --c5, or alone with --only c5) the full chosen form: 16384 queries
-          (k log-uniform in [1, 1024]) over a 2^28 x 16 table mixed 1/3 each
-          independent/correlated/anticorrelated, plain batched FP32 against the
-          learned start with the BF16 filter, identical results checked.
+  c5       the full chosen form: 16384 queries (k log-uniform in [1, 1024]) over a
+          2^28 x 16 table mixed 1/3 each independent/correlated/anticorrelated, plain
+          batched FP32 full evaluation against the BF16 filter (with retirement of
+          queries whose k-th score reaches their bound), without and with the learned
+          start; identical results checked.  (--no-c5 leaves it out.)
+
+The secondary sections come after the headline keys and the batched ones last, so the
+end of the line holds batched and c5.
 
 Multi-GPU (torchrun): every rank holds its own replica and runs the same query
 steps (weak scaling, no collective on the data path); time = max over ranks.  The
@@ -97,18 +103,11 @@ def measured_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the scan kernel by q, from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "scan_select_n2e28_d16.md")
-    out = {}
-    try:
-        for line in open(p):
-            m = re.match(r"\s*traffic_bytes_per_launch\[q=(\d+)\]:\s*([0-9.eE+]+)", line)
-            if m:
-                out[int(m.group(1))] = float(m.group(2))
-    except OSError:
-        pass
-    return out
+# DRAM bytes (read + write) per launch of the fused scan at n = 2^28, by q: dram__bytes
+# of 2^25-row captures (every object is read once, so traffic grows with the rows
+# scanned) scaled x8, the mean over k in {16, 64, 256, 1024}.
+TRAFFIC_PER_LAUNCH = {2: 2.1567e9, 4: 4.2988e9, 8: 8.6041e9, 16: 1.7183e10}
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of 2^25-row launches, scaled x8 to 2^28 rows"
 
 
 class Clocks:
@@ -187,7 +186,41 @@ def cpu_baseline(n_full, d, queries, sample_rows=1 << 25, reps=2):
     }
 
 
+def host_available_bytes():
+    """MemAvailable from /proc/meminfo (0 when unreadable)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def generate_parallel(O, n, d, dist, seed, threads=None):
+    """The oracle's seeded table, rows generated by host threads (ctypes releases the
+    GIL); identical to one O.generate call."""
+    from concurrent.futures import ThreadPoolExecutor
+    t = np.zeros((d, n), np.float32)
+    threads = threads or os.cpu_count() or 1
+    step = (n + threads - 1) // threads
+    flat = t.reshape(-1)
+
+    def part(r0):
+        O.lib().orc_generate(flat, n, d, r0, min(step, n - r0), dist, seed)
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(part, range(0, n, step)))
+    return t
+
+
 def run_reference(args):
+    """The reference's own TPAc::findTopKthreads (compiled strict into oracle/_ref) on
+    this host's cores, on the same 2^28 x 16 table and 16-query step as the GPU arm.
+    The full table needs about 2 x 16 GiB of host memory (the generated table and the
+    reference's own copy); with less available the step runs on a 2^25-row sample and
+    the line says so ("scaled")."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -196,8 +229,9 @@ def run_reference(args):
     if not O.RefTPAc.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference TPAc library oracle/_ref not built"}))
         return 0
-    sample = 1 << 25
-    t = O.generate(sample, D_FULL, 1, 0)
+    need = 2 * N_FULL * D_FULL * 4 + (8 << 30)
+    rows = N_FULL if host_available_bytes() >= need else 1 << 25
+    t = generate_parallel(O, rows, D_FULL, 1, 0)
     ref = O.RefTPAc(t)
     del t
     ref.init()
@@ -208,19 +242,25 @@ def run_reference(args):
         tot = 0.0
         for k, q, w, a in queries:
             tot += ref.query(2, k, w, a)[3]
-        times.append(tot * (N_FULL / sample))
+        times.append(tot * (N_FULL / rows))
     ref.close()
     ms = statistics.mean(times)
     qps = len(queries) * 1000.0 / ms
     cores = int(O.RefTPAc.lib().ref_threads_constant())
+    scaled = N_FULL // rows
+    sample = (f"TPAc::findTopKthreads (THREADS={cores} as shipped) on the full {rows} x {D_FULL} table, "
+              f"the {len(queries)}-query step, mean of {args.steps} steps" if scaled == 1 else
+              f"TPAc::findTopKthreads (THREADS={cores}) on a {rows}-row sample (host memory below "
+              f"{need >> 30} GiB), per-query time scaled by {scaled}")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "single-query exact top-k, n=2^28 x d=16, 16 queries/step", "n": N_FULL, "d": D_FULL},
+        "config": {"workload": "single-query exact top-k (TPAc), n=2^28 x d=16 column-major FP32, 16 queries/step: "
+                               "q in {2,4,8,16} (last q attributes) x k in {16,64,256,1024}", "n": N_FULL, "d": D_FULL,
+                   "rows_run": rows, "scaled": scaled},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "host_cpus": os.cpu_count(),
-                         "kind": "reference",
-                         "sample": f"TPAc::findTopKthreads on {sample} rows x {D_FULL}, scaled by n/{sample}"},
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -324,7 +364,7 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
     return out
 
 
-def run_c5(T, torch, dist, device, n, nq, methods=("fp32", "learned_bf16")):
+def run_c5(T, torch, dist, device, n, nq, methods=("fp32", "bf16", "learned_bf16")):
     """Full chosen form against plain: an n x 16 table whose objects are 1/3 each
     independent, correlated and anticorrelated (object i takes distribution i mod 3),
     a stream of nq queries (attribute subsets of size U{2..16}, weights U(0,1], k
@@ -439,6 +479,7 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000
         "workload": f"anticorrelated n={n} x {d}, {P} partitions of {part_rows} rows; {n_test} test queries, "
                     f"|attrs| U{{2..{d}}}, k log-uniform [16, 1024]; model fitted on {n_train} queries",
         "queries_per_s": qps,
+        "speedup_pruned_vs_full_scan": qps["pruned"] / qps["full_scan"],
         "speedup_learned_vs_full_scan": qps["learned_pruned"] / qps["full_scan"],
         "speedup_learned_vs_pruned": qps["learned_pruned"] / qps["pruned"],
         "partitions_scanned_fraction": {"pruned": scanned_p / (n_test * P), "learned_pruned": scanned_l / (n_test * P)},
@@ -605,11 +646,11 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--only", choices=["batched", "pruned", "c5", "loader", "ta"], default=None,
                     help="run one secondary workload alone (no JSON line; for profiling)")
-    ap.add_argument("--c5", action="store_true",
-                    help="add the full-form workload: 16384 queries over a mixed 2^28 x 16 table")
+    ap.add_argument("--no-c5", action="store_true",
+                    help="leave out the full-form workload (16384 queries over a mixed 2^28 x 16 table)")
     ap.add_argument("--c5-n", type=int, default=C5_N)
     ap.add_argument("--c5-q", type=int, default=C5_Q)
-    ap.add_argument("--c5-methods", default="fp32,learned_bf16")
+    ap.add_argument("--c5-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--no-pruned", action="store_true")
     ap.add_argument("--no-loader", action="store_true")
@@ -713,11 +754,44 @@ def main():
     tot_ms = sum(time_by_q.values())
     achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic()
     launches = args.steps * len(queries)
-    traffic_per_launch = None
-    if traffic and all(q in traffic for q in QS):
-        traffic_per_launch = sum(traffic[q] * (n / N_FULL) for (_, q, _, _) in queries) / len(queries)
+    traffic_per_launch = sum(TRAFFIC_PER_LAUNCH[q] * (n / N_FULL) for (_, q, _, _) in queries) / len(queries)
+
+    # the same step on the other two distributions of the workload (correlated,
+    # anticorrelated), each table generated in place of the last
+    per_dist = {"independent": {"queries_per_s": world * len(queries) * 1000.0 / (elapsed_ms / args.steps),
+                                "scan_gbs": achieved}}
+    for dname, dcode in (("correlated", T.DIST_CORRELATED), ("anticorrelated", T.DIST_ANTICORRELATED)):
+        table.generate(dcode, 0)
+        table.normalize()
+        for _ in range(args.warmup):
+            run_step()
+        ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in queries]
+              for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        d0 = torch.cuda.Event(enable_timing=True)
+        d1 = torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        for st_ in range(args.steps):
+            run_step(ev[st_])
+        d1.record(stream)
+        torch.cuda.synchronize()
+        dms = d0.elapsed_time(d1)
+        if dist:
+            tt = torch.tensor([dms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dms = float(tt.item())
+        dbytes = sum(4.0 * n * q for (_, q, _, _) in queries) * args.steps
+        dlaunch = sum(ev[a][b][0].elapsed_time(ev[a][b][1]) for a in range(args.steps) for b in range(len(queries)))
+        per_dist[dname] = {"queries_per_s": world * len(queries) * 1000.0 / (dms / args.steps),
+                           "scan_gbs": dbytes / (dlaunch * 1e-3) / 1e9,
+                           "ms_per_query": {f"q{q}_k{k}": round(sum(ev[a][j][0].elapsed_time(ev[a][j][1])
+                                                                    for a in range(args.steps)) / args.steps, 4)
+                                            for j, (k, q, _, _) in enumerate(queries)}}
+    table.generate(T.DIST_INDEPENDENT, 0)
+    table.normalize()
 
     # e2e: the host-buffer C-ABI call, host wall time per step
     if dist:
@@ -764,6 +838,8 @@ def main():
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind,
             "traffic": traffic_per_launch,
+            "traffic_source": TRAFFIC_SOURCE,
+            "per_dist": per_dist,
             "per_q": {str(q): {"gbs": bytes_by_q[q] / (time_by_q[q] * 1e-3) / 1e9,
                                "ms_per_launch": time_by_q[q] / (args.steps * len(KS))} for q in QS},
             "ms_per_query": {key: round(v, 4) for key, v in time_by_qk.items()},
@@ -780,9 +856,6 @@ def main():
         except Exception as e:  # the baseline is reported, never the product
             result["cpu_baseline"] = {"error": str(e)}
     table.close()
-    if not args.no_batched:
-        result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q,
-                                        methods=tuple(args.batched_methods.split(",")))
     # one-GPU secondary workloads: under torchrun the other ranks would idle at the
     # final barrier (process-group timeout 120 s) while rank 0 ran them, so they run
     # only when the job has one rank
@@ -792,7 +865,11 @@ def main():
         result["loader"] = run_loader(T, local)
     if not args.no_ta and world == 1:
         result["ta"] = run_ta(T, local)
-    if args.c5:
+    # the batched workloads last, so that the end of the line holds them
+    if not args.no_batched:
+        result["batched"] = run_batched(T, torch, dist, local, args.batched_n, args.batched_q,
+                                        methods=tuple(args.batched_methods.split(",")))
+    if not args.no_c5:
         result["c5"] = run_c5(T, torch, dist, local, args.c5_n, args.c5_q, tuple(args.c5_methods.split(",")))
     if dist:
         dist.barrier()

@@ -195,7 +195,7 @@ int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
  * the query (host weights indexed by attribute id, host attr), and device outputs
  * for min(k, n) ids / scores (d_threshold may be NULL); work is enqueued on
  * `stream` (a cudaStream_t, NULL = the legacy default stream).  The scan's scratch
- * is a fixed array compiled into the library (about 2.7 MB on each GPU that loads
+ * is a fixed array compiled into the library (about 8.4 MB on each GPU that loads
  * it, held until the process exits): k is limited to 1024 (TOPK_ERR_UNSUPPORTED
  * above), and calls whose work overlaps on the GPU share that array and race, so
  * serialise them.  The first call on each device performs a one-time set-up on
@@ -428,6 +428,14 @@ int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uin
 /* How many queries of the last topk_query_batch the hybrid BF16 batch moved to the
  * exact FP32 scorer (0 for the other methods). */
 int topk_last_batch_switched(topk_table_t h, uint64_t *switched);
+
+/* How many queries of the last topk_query_batch the BF16 filter retired before the
+ * table's end: their k-th score had reached the largest score any object can have
+ * (the reference-order sum over the column extremes), so no later object could enter
+ * their top-k and the filter stopped serving them -- the reference's stop rule
+ * (cpu/VTA.h:210-216, cpu/PTA.h:636-641) with the whole table as the block.  0 for the
+ * other methods. */
+int topk_last_batch_retired(topk_table_t h, uint64_t *retired);
 
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */

@@ -314,3 +314,68 @@ def test_batch_tune_keeps_results():
         check_batch(t, tn, ks, W, A, qqs)
         with pytest.raises(T.TopKError):
             t.set_batch_tiles(4, 1000)
+
+
+def test_batch_bf16_retires_queries_tied_at_the_maximum():
+    """Many rows hold the largest possible score (every queried value at its column
+    maximum): once k of them are found the k-th score equals the bound over the
+    column extremes, so the filter retires the query instead of passing every later
+    tied row (which would overflow its candidates).  Results exact, lowest ids."""
+    n, d = 300001, 6
+    rng = np.random.default_rng(31)
+    raw = (rng.integers(0, 1 << 22, size=(d, n)) * 2.0 ** -23).astype(np.float32)  # [0, 0.5)
+    raw[:, ::37] = 1.0  # ~8100 rows at the top in every attribute
+    raw[0, 5] = 0.0     # one column minimum of 0 (normalisation keeps the range)
+    tn = raw.copy()
+    O.normalize(tn)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        t.set_batch_method(BF16)
+        nq = 300
+        ks = rng.integers(1, 1025, size=nq).astype(np.uint64)
+        W = ((rng.integers(0, 1 << 24, size=(nq, d)) + 1) * 2.0 ** -24).astype(np.float32)
+        A = np.zeros((nq, d), np.uint8)
+        qqs = np.zeros(nq, np.uint32)
+        for j in range(nq):
+            q = int(rng.integers(1, d + 1))
+            A[j, :q] = rng.choice(d, size=q, replace=False)
+            qqs[j] = q
+        check_batch(t, tn, ks, W, A, qqs)
+        st = bf16_ran(t)
+        assert st["retired"] == nq and st["switched_fp32"] == 0, st
+
+
+def test_batch_c5_shaped_mixed_table():
+    """The full chosen form's shape at 2^22 rows: a table mixed 1/3 each independent,
+    correlated and anticorrelated, 2048 queries with 2-16 attributes and k log-uniform
+    in [1, 1024].  The clipped correlated rows tie at the maximum for most small
+    queries; those retire, and few queries move to the FP32 scorer.  Every method
+    returns the plain FP32 batch's results; a sample is checked against the oracle."""
+    n, d, nq = 1 << 22, 16, 2048
+    rng = np.random.default_rng(55)
+    ks = np.exp(rng.uniform(0.0, np.log(1025.0), nq)).astype(np.uint64).clip(1, 1024)
+    W = ((rng.integers(0, 1 << 24, size=(nq, d)) + 1) * 2.0 ** -24).astype(np.float32)
+    A = np.zeros((nq, 16), np.uint8)
+    qqs = np.zeros(nq, np.uint32)
+    for j in range(nq):
+        q = int(rng.integers(2, 17))
+        A[j, :q] = np.sort(rng.choice(d, size=q, replace=False))
+        qqs[j] = q
+    with T.Table(n, d) as t:
+        t.generate(3, 12)
+        t.normalize()
+        tn = t.download()
+        t.set_batch_method(FP32)
+        base = t.query_batch(ks, W, A, qqs)
+        t.set_batch_method(BF16)
+        got = t.query_batch(ks, W, A, qqs)
+        st = bf16_ran(t)
+        for x, y in zip(base, got):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
+        assert st["switched_fp32"] < nq // 4, st
+        assert st["retired"] > nq // 4, st
+        for j in rng.choice(nq, size=24, replace=False):
+            c = int(got[2][j])
+            want = O.topk_numpy(tn, int(ks[j]), W[j], A[j, : qqs[j]])
+            H.assert_same_result((got[0][j, :c], got[1][j, :c], got[3][j]), want)

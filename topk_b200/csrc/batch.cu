@@ -21,6 +21,7 @@
 // Two scorers share this schedule: the plain FP32 one here (exact keys), and the
 // BF16 tensor-core filter (bf16_filter.cu), whose candidates carry approximate
 // keys that the reduce makes exact by rescoring them in the reference order.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -46,6 +47,10 @@ __device__ __forceinline__ float score_row(const float *table, uint64_t ld, uint
   for (uint32_t m = 0; m < qq; ++m) s = __fadd_rn(s, __fmul_rn(__ldg(table + (uint64_t)attr[m] * ld + row), w[m]));
   return s;
 }
+
+// A query's m-th weight and attribute (m < kBatchMaxQ; entries past qq are unused).
+__device__ __forceinline__ float bq_w(const BatchQuery *qs, uint32_t q, int m) { return qs[q].w[m]; }
+__device__ __forceinline__ uint32_t bq_attr(const BatchQuery *qs, uint32_t q, int m) { return qs[q].attr[m]; }
 
 // ---------------------------------------------------------------- bootstrap
 // One block per query: exact top-k of rows [0, rows).  Shared: entries[rows] and
@@ -86,36 +91,43 @@ __global__ void __launch_bounds__(kBT) batch_bootstrap_kernel(const float *__res
 }
 
 // ---------------------------------------------------------------- FP32 scorer
-// Block (query group g, tile): rows [row0, row0 + OPT*256) of the chunk, all d
-// columns staged in shared memory once, scored for the group's queries.  With a
-// query list the groups are formed from qlist[0..nq) (the queries a hybrid batch has
-// moved to this scorer), else from queries 0..nq-1.  With `list_end` the list is
+// One thread per query, one block per (group of 256 queries, tile of `to` rows).  The
+// tile's d columns are staged once in shared memory (row stride to + 4 floats, so the
+// 16-byte pieces of different attributes at one row fall in different banks), with
+// one extra row of zeros; each thread then walks the tile 16 rows at a time and
+// scores them for its own query in that query's attribute order (four 16-byte shared
+// loads per attribute; weights and row offsets in registers).  A warp runs as many
+// steps as its longest query; a shorter query's extra steps add 0 * 0 = +0, which
+// leaves every sum as it is (no sum is ever -0: it starts at +0, and +0 + -0 = +0).
+// Lanes of a warp read at most d distinct pieces per load -- few when the queries are
+// ordered by attribute list, as the host orders them -- so one shared-memory wavefront
+// serves up to 32 queries x 4 rows, and the kernel runs near the FP32 pipe's rate of
+// one separately rounded multiply and add per product.  Groups are formed from
+// qlist[0..nq), or from queries 0..nq-1.  With `list_end` the list is
 // qlist[*list_begin .. *list_end) as the device holds it when the kernel starts (a
 // hybrid batch's lists grow in its reduce, which the host does not wait for): the grid
 // is then a fixed set of blocks taking (group, tile) items in order from the counter
-// `work` (zero at launch; in order, so the groups reading one tile run together and
-// find it in L2), and an empty list costs one read.
-template <int OPT>
+// `work` (zero at launch), so the groups reading one tile run together and find it in
+// L2, and an empty list costs one read.  With `retire` a query whose threshold is
+// above its largest possible score (BatchQuery::maxkey) is skipped: no row can still
+// enter its top-k.
+constexpr uint32_t kScoreRows = 16;  // rows per step of a thread
+
+template <int QM>
 __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__restrict__ table, uint64_t ld,
-                                                               uint32_t d, uint64_t r0, uint64_t r1,
+                                                               uint32_t d, uint32_t to, uint64_t r0, uint64_t r1,
                                                                const BatchQuery *__restrict__ qs, uint32_t nq,
                                                                BatchState *__restrict__ st,
                                                                uint2 *__restrict__ cand,
                                                                const uint32_t *__restrict__ qlist,
                                                                const uint32_t *__restrict__ list_end,
                                                                const uint32_t *__restrict__ list_begin,
-                                                               uint32_t *__restrict__ work) {
+                                                               uint32_t *__restrict__ work, int retire) {
   __shared__ uint32_t next_item;
-  constexpr uint32_t TO = kBT * OPT;
-  extern __shared__ __align__(16) unsigned char smem[];
-  float *xs = reinterpret_cast<float *>(smem);                       // d x TO
-  uint8_t *gattr = smem + (size_t)d * TO * 4;                        // kBatchGroup x kBatchMaxQ
-  float *gw = reinterpret_cast<float *>(gattr + kBatchGroup * kBatchMaxQ);  // kBatchGroup x kBatchMaxQ
-  uint32_t *gthr = reinterpret_cast<uint32_t *>(gw + kBatchGroup * kBatchMaxQ);
-  uint32_t *gqq = gthr + kBatchGroup;
-  uint32_t *gq = gqq + kBatchGroup;  // query of each group slot
-
+  extern __shared__ __align__(16) float xs[];  // d + 1 rows of `xstride` floats; row d is zero
+  const uint32_t xstride = to + 4;
   const int t = threadIdx.x;
+  for (uint32_t i = t; i < xstride; i += kBT) xs[d * xstride + i] = 0.0f;
   if (list_end) {
     const uint32_t b = list_begin ? *list_begin : 0u;
     nq = *list_end - b;
@@ -123,93 +135,121 @@ __global__ void __launch_bounds__(kBT) batch_score_fp32_kernel(const float *__re
   }
   // item -> (query group, tile), groups fastest: the items of one tile run together
   // and its second and later reads come from L2
-  const uint32_t ngroups = (nq + kBatchGroup - 1) / kBatchGroup;
-  const uint64_t items = (uint64_t)ngroups * ((r1 - r0 + TO - 1) / TO);
+  const uint32_t ngroups = (nq + kBT - 1) / kBT;
+  const uint64_t items = (uint64_t)ngroups * ((r1 - r0 + to - 1) / to);
   uint64_t item = blockIdx.x;  // without a list: one item per block
   if (list_end) {
     if (t == 0) next_item = atomicAdd(work, 1u);
     __syncthreads();
     item = next_item;
   }
+  uint32_t group = 0xFFFFFFFFu;
+  // this thread's query: weights and row offsets (attr * xstride) in registers;
+  // steps past its attribute count read the zero row with weight 0
+  float w[QM];
+  uint32_t off[QM];
+  uint32_t qq = 0, q = 0, ccap = 0, coff = 0;
+  float thr_f = 0.0f;
+  bool take_all = false;
   while (item < items) {
-  const uint32_t q0 = (uint32_t)(item % ngroups) * kBatchGroup;
-  const uint64_t tile = item / ngroups;
-  const uint32_t nqg = min(kBatchGroup, nq - q0);
-  const uint64_t base = r0 + tile * TO;
-  const uint32_t valid = (uint32_t)min((uint64_t)TO, r1 - base);
-  // stage the tile (rows beyond r1 read as 0 and are never appended)
-  for (uint32_t m = 0; m < d; ++m) {
-    const float *col = table + (uint64_t)m * ld + base;
-    for (uint32_t i = t; i < TO; i += kBT) xs[m * TO + i] = i < valid ? __ldcs(col + i) : 0.0f;
-  }
-  for (uint32_t j = t; j < nqg; j += kBT) gq[j] = qlist ? qlist[q0 + j] : q0 + j;
-  __syncthreads();
-  for (uint32_t j = t; j < nqg * kBatchMaxQ; j += kBT) {
-    const uint32_t qj = j / kBatchMaxQ, m = j % kBatchMaxQ;
-    gattr[j] = qs[gq[qj]].attr[m];
-    gw[j] = qs[gq[qj]].w[m];
-  }
-  for (uint32_t j = t; j < nqg; j += kBT) {
-    gthr[j] = st[gq[j]].thr;
-    gqq[j] = qs[gq[j]].qq;
-  }
-  __syncthreads();
-
-  const int lane = t & 31;
-  for (uint32_t j = 0; j < nqg; ++j) {
-    const uint32_t qq = gqq[j];
-    const uint8_t *a = gattr + j * kBatchMaxQ;
-    const float *w = gw + j * kBatchMaxQ;
-    float acc[OPT];
-#pragma unroll
-    for (int v = 0; v < OPT; ++v) acc[v] = 0.0f;
-    for (uint32_t m = 0; m < qq; ++m) {
-      const float *row = xs + (uint32_t)a[m] * TO + t * OPT;
-      const float wm = w[m];
-      if constexpr (OPT == 4) {
-        const float4 x = *reinterpret_cast<const float4 *>(row);
-        acc[0] = __fadd_rn(acc[0], __fmul_rn(x.x, wm));
-        acc[1] = __fadd_rn(acc[1], __fmul_rn(x.y, wm));
-        acc[2] = __fadd_rn(acc[2], __fmul_rn(x.z, wm));
-        acc[3] = __fadd_rn(acc[3], __fmul_rn(x.w, wm));
-      } else {
-#pragma unroll
-        for (int v = 0; v < OPT; ++v) acc[v] = __fadd_rn(acc[v], __fmul_rn(row[v], wm));
-      }
-    }
-    const uint32_t thr = gthr[j];
-    const bool take_all = thr == 0u;
-    const float thr_f = thr_float(thr);
-    unsigned pass = 0;
-#pragma unroll
-    for (int v = 0; v < OPT; ++v)
-      pass |= (unsigned)((take_all || acc[v] >= thr_f) && (uint32_t)(t * OPT + v) < valid) << v;
-    if (__ballot_sync(0xFFFFFFFFu, pass != 0u)) {  // warp-uniform
-      const uint32_t np = __popc(pass);
-      uint32_t incl = np;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const uint32_t wtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-      const BatchQuery &q = qs[gq[j]];
-      uint32_t pos = 0;
-      if (lane == 31) pos = atomicAdd(&st[gq[j]].ccount, wtot);
-      pos = __shfl_sync(0xFFFFFFFFu, pos, 31) + incl - np;
-#pragma unroll
-      for (int v = 0; v < OPT; ++v)
-        if (pass & (1u << v)) {
-          if (pos < q.cand_cap) cand[q.cand_off + pos] = make_uint2(f2key(acc[v]), (uint32_t)(base + t * OPT + v));
-          ++pos;
+    const uint32_t g = (uint32_t)(item % ngroups);
+    const uint64_t tile = item / ngroups;
+    const uint64_t base = r0 + tile * to;
+    const uint32_t valid = (uint32_t)min((uint64_t)to, r1 - base);
+    // stage the tile (rows beyond r1 read as 0 and are never appended); 16-byte
+    // loads where the columns allow them
+    if ((ld & 3u) == 0 && (base & 3u) == 0) {
+      const uint32_t v4 = (valid + 3) / 4, per = to / 4;
+      for (uint32_t e = t; e < d * per; e += kBT) {
+        const uint32_t m = e / per, i = e % per;
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < v4) {
+          if (4 * i + 4 <= valid) {
+            x = __ldcs(reinterpret_cast<const float4 *>(table + (uint64_t)m * ld + base) + i);
+          } else {
+            const float *c = table + (uint64_t)m * ld + base + 4 * i;
+            const uint32_t left = valid - 4 * i;
+            x.x = __ldcs(c);
+            if (left > 1) x.y = __ldcs(c + 1);
+            if (left > 2) x.z = __ldcs(c + 2);
+          }
         }
+        *reinterpret_cast<float4 *>(xs + m * xstride + 4 * i) = x;
+      }
+    } else {
+      for (uint32_t e = t; e < d * to; e += kBT) {
+        const uint32_t m = e / to, i = e % to;
+        xs[m * xstride + i] = i < valid ? __ldcs(table + (uint64_t)m * ld + base + i) : 0.0f;
+      }
     }
-  }
-  __syncthreads();  // the next item restages the shared tile
-  if (!list_end) break;
-  if (t == 0) next_item = atomicAdd(work, 1u);
-  __syncthreads();
-  item = next_item;
+    if (g != group) {
+      group = g;
+      const uint32_t slot = g * kBT + (uint32_t)t;
+      qq = 0;
+      if (slot < nq) {
+        q = qlist ? qlist[slot] : slot;
+        const BatchQuery &bq = qs[q];
+        const uint32_t thr = st[q].thr;
+        qq = bq.qq;
+        if (retire && thr != 0u && thr > bq.maxkey) qq = 0;  // nothing left that can enter
+        take_all = thr == 0u;
+        thr_f = thr_float(thr);
+        ccap = bq.cand_cap;
+        coff = bq.cand_off;
+      }
+#pragma unroll
+      for (int m = 0; m < QM; ++m) {
+        w[m] = (uint32_t)m < qq ? bq_w(qs, q, m) : 0.0f;
+        off[m] = ((uint32_t)m < qq ? (uint32_t)bq_attr(qs, q, m) : d) * xstride;
+      }
+    }
+    __syncthreads();  // tile staged
+    const uint32_t qmax = __reduce_max_sync(0xFFFFFFFFu, qq);  // warp-uniform step count
+    if (qmax) {
+      for (uint32_t o = 0; o < valid; o += kScoreRows) {
+        float a[kScoreRows];
+#pragma unroll
+        for (int v = 0; v < (int)kScoreRows; ++v) a[v] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < QM; ++m) {
+          if ((uint32_t)m >= qmax) break;
+          const float4 *row = reinterpret_cast<const float4 *>(xs + off[m] + o);
+          const float wm = w[m];
+#pragma unroll
+          for (int c = 0; c < (int)kScoreRows / 4; ++c) {
+            const float4 x = row[c];
+            a[4 * c + 0] = __fadd_rn(a[4 * c + 0], __fmul_rn(x.x, wm));
+            a[4 * c + 1] = __fadd_rn(a[4 * c + 1], __fmul_rn(x.y, wm));
+            a[4 * c + 2] = __fadd_rn(a[4 * c + 2], __fmul_rn(x.z, wm));
+            a[4 * c + 3] = __fadd_rn(a[4 * c + 3], __fmul_rn(x.w, wm));
+          }
+        }
+        // the largest of the 16 against the threshold first (NaN never passes it)
+        float mx = a[0];
+#pragma unroll
+        for (int v = 1; v < (int)kScoreRows; ++v) mx = fmaxf(mx, a[v]);
+        if (qq && (take_all || mx >= thr_f)) {  // rare once a threshold is known
+          unsigned pass = 0;
+#pragma unroll
+          for (int v = 0; v < (int)kScoreRows; ++v)
+            pass |= (unsigned)((take_all || a[v] >= thr_f) && o + v < valid) << v;
+          if (pass) {
+            uint32_t pos = atomicAdd(&st[q].ccount, (uint32_t)__popc(pass));
+#pragma unroll
+            for (int v = 0; v < (int)kScoreRows; ++v)
+              if (pass & (1u << v)) {
+                if (pos < ccap) cand[coff + pos] = make_uint2(f2key(a[v]), (uint32_t)(base + o + v));
+                ++pos;
+              }
+          }
+        }
+      }
+    }
+    __syncthreads();  // the next item restages the shared tile
+    if (!list_end) break;
+    if (t == 0) next_item = atomicAdd(work, 1u);
+    __syncthreads();
+    item = next_item;
   }
 }
 
@@ -363,59 +403,49 @@ cudaError_t launch_batch_bootstrap(const float *table, uint64_t ld, uint32_t row
   return cudaGetLastError();
 }
 
-size_t batch_score_smem(uint32_t d) {
-  const uint32_t to = (d <= 16 ? 4u : 1u) * kBT;
-  return (size_t)d * to * 4 + kBatchGroup * kBatchMaxQ * 5 + kBatchGroup * 12;
+uint32_t batch_score_rows(uint32_t d) { return d <= 16 ? 1024u : d <= 32 ? 512u : 256u; }
+
+size_t batch_score_smem(uint32_t d) { return (size_t)(d + 1) * (batch_score_rows(d) + 4) * 4; }
+
+namespace {
+using ScoreKernel = void (*)(const float *, uint64_t, uint32_t, uint32_t, uint64_t, uint64_t, const BatchQuery *, uint32_t,
+                             BatchState *, uint2 *, const uint32_t *, const uint32_t *, const uint32_t *, uint32_t *, int);
+ScoreKernel score_kernel(uint32_t qmax) {
+  return qmax <= 16 ? batch_score_fp32_kernel<16> : batch_score_fp32_kernel<(int)kBatchMaxQ>;
 }
+}  // namespace
 
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                     const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand,
-                                    const uint32_t *qlist, cudaStream_t s) {
+                                    const uint32_t *qlist, uint32_t qmax, bool retire, cudaStream_t s) {
   if (nq == 0 || r1 <= r0) return cudaSuccess;
   const size_t smem = batch_score_smem(d);
-  const uint32_t opt = d <= 16 ? 4u : 1u;
-  const uint64_t to = (uint64_t)opt * kBT;
-  const uint64_t blocks = (uint64_t)((nq + kBatchGroup - 1) / kBatchGroup) * ((r1 - r0 + to - 1) / to);
+  const uint64_t to = batch_score_rows(d);
+  const uint64_t blocks = (uint64_t)((nq + kBT - 1) / kBT) * ((r1 - r0 + to - 1) / to);
   if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
-  const dim3 grid((unsigned)blocks);
-  cudaError_t e;
-  if (opt == 4) {
-    if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-      return e;
-    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist, nullptr, nullptr,
-                                                        nullptr);
-  } else {
-    if ((e = cudaFuncSetAttribute(batch_score_fp32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-      return e;
-    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, nq, st, cand, qlist, nullptr, nullptr,
-                                                        nullptr);
-  }
+  const ScoreKernel fn = score_kernel(qmax);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<(unsigned)blocks, kBT, smem, s>>>(table, ld, d, (uint32_t)to, r0, r1, qs, nq, st, cand, qlist, nullptr, nullptr,
+                                         nullptr, retire ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_score_fp32_list(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                          const BatchQuery *qs, BatchState *st, uint2 *cand, const uint32_t *qlist,
                                          const uint32_t *list_end, const uint32_t *list_begin, uint32_t *work,
-                                         int num_sms, cudaStream_t s) {
+                                         uint32_t qmax, bool retire, int num_sms, cudaStream_t s) {
   if (r1 <= r0) return cudaSuccess;
   const size_t smem = batch_score_smem(d);
-  const bool four = d <= 16;
-  const void *fn = four ? reinterpret_cast<const void *>(batch_score_fp32_kernel<4>)
-                        : reinterpret_cast<const void *>(batch_score_fp32_kernel<1>);
+  const ScoreKernel fn = score_kernel(qmax);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBT, smem)) != cudaSuccess) return e;
   const dim3 grid((unsigned)(std::max(1, per_sm) * std::max(1, num_sms)));
   if ((e = cudaMemsetAsync(work, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
-  if (four)
-    batch_score_fp32_kernel<4><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, 0, st, cand, qlist, list_end, list_begin,
-                                                        work);
-  else
-    batch_score_fp32_kernel<1><<<grid, kBT, smem, s>>>(table, ld, d, r0, r1, qs, 0, st, cand, qlist, list_end, list_begin,
-                                                        work);
+  fn<<<grid, kBT, smem, s>>>(table, ld, d, batch_score_rows(d), r0, r1, qs, 0, st, cand, qlist, list_end, list_begin,
+                             work, retire ? 1 : 0);
   return cudaGetLastError();
 }
 

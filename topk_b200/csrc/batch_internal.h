@@ -7,7 +7,6 @@
 namespace topk {
 
 constexpr uint32_t kBatchMaxQ = 32;    // attributes per query on the batched path
-constexpr uint32_t kBatchGroup = 64;   // queries scored per staged table tile (FP32 scorer)
 constexpr uint32_t kBatchMaxD = 64;    // table width the FP32 scorer stages
 constexpr uint32_t kBatchBootRows = 8192;  // rows of the exact bootstrap (default)
 constexpr uint32_t kBatchBootMax = 16384;  // its shared-memory limit
@@ -22,7 +21,8 @@ struct BatchQuery {
   uint32_t cand_cap;   // entries of the candidate region
   float err;           // BF16 filter: bound on |filter score - exact score|
   float thr0;          // learned start: candidates below it are not kept (0: none)
-  uint32_t pad;
+  uint32_t maxkey;     // key of an upper bound of every score over the table (the
+                       // reference-order FP32 sum over column extremes); 0xFFFFFFFF: none
   uint8_t attr[kBatchMaxQ];
   float w[kBatchMaxQ];  // weights[attr[m]]
 };
@@ -47,16 +47,19 @@ size_t batch_bootstrap_smem(uint32_t rows, uint32_t kmax);
 cudaError_t launch_batch_bootstrap(const float *table, uint64_t ld, uint32_t rows, uint32_t kmax,
                                    const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *best, cudaStream_t s);
 size_t batch_score_smem(uint32_t d);
+// Exact FP32 scorer over rows [r0, r1) for queries qlist[0..nq) (qlist null: 0..nq-1);
+// qmax = the largest attribute count among them.  retire: skip queries whose threshold
+// is above BatchQuery::maxkey.
 cudaError_t launch_batch_score_fp32(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                     const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand,
-                                    const uint32_t *qlist, cudaStream_t s);
+                                    const uint32_t *qlist, uint32_t qmax, bool retire, cudaStream_t s);
 // The same scorer over the queries qlist[*list_begin .. *list_end) (list_begin may be
 // null: from 0), read from device memory when the kernel starts; a fixed grid of
 // blocks takes the work items from the counter `work` (zeroed here, in stream order).
 cudaError_t launch_batch_score_fp32_list(const float *table, uint64_t ld, uint32_t d, uint64_t r0, uint64_t r1,
                                          const BatchQuery *qs, BatchState *st, uint2 *cand, const uint32_t *qlist,
                                          const uint32_t *list_end, const uint32_t *list_begin, uint32_t *work,
-                                         int num_sms, cudaStream_t s);
+                                         uint32_t qmax, bool retire, int num_sms, cudaStream_t s);
 cudaError_t launch_copy_word(uint32_t *dst, const uint32_t *src, cudaStream_t s);  // *dst = *src, in stream order
 size_t batch_reduce_smem(uint32_t kmax, uint32_t capmax);
 cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuery *qs, uint32_t nq, BatchState *st,
@@ -64,24 +67,34 @@ cudaError_t launch_batch_reduce(const float *table, uint64_t ld, const BatchQuer
                                 uint32_t *sw, cudaStream_t s);
 // BF16 tensor-core filter (bf16_filter.cu).
 uint64_t bf16_table_bytes(uint64_t n);
-cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,
+// Also the column extremes: ext[m] = largest |x| bits, ext[d + m] = largest order key,
+// ext[2d + m] = smallest order key (NaN left out) of column m.
+cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *ext,
                              int num_sms, cudaStream_t s);
 size_t bf16_query_bytes(uint32_t nq);
 // Host: write query j's 16-wide row a[] (hi and lo) into the tiled query buffer.
 void bf16_pack_query(const float *a, uint32_t j, uint8_t *abf);
-// Work split of one filter launch over rows [r0, r1): query tiles of 256 in groups
-// of up to 8 per CTA, the chunk's object tiles of 128 split among cpg CTAs per group.
+// One filter launch over rows [r0, r1): its object tiles, the most query tiles of 128
+// one CTA takes (qt_cap) and the grid (the work split itself is made on the device
+// from the active count, see launch_bf16_filter).
 struct FilterPlan {
   uint64_t tile0, tile1;
-  uint32_t nqt, qt_per_cta, ngroups, cpg;
+  uint32_t qt_cap;
   uint64_t grid;
 };
-// qt_cap: query tiles of 128 per CTA at most (0: the kernel's maximum)
+// nq: queries of the batch (the most that can be active); qt_cap 0: the kernel's maximum
 FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms, uint32_t qt_cap = 0);
-// r0 must be a multiple of 128; log/log_q hold grid * log_cap entries.
-cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
-                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *recv,
-                               uint2 *rech, uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s);
+// r0 must be a multiple of 256.  The filter serves the *nact active queries in the
+// compact tiles abf (slot -> query: amap); recv/rech hold grid * rec_cap records.
+cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, const uint32_t *amap,
+                               const uint32_t *nact, uint64_t r0, uint64_t r1, const BatchQuery *qs, BatchState *st,
+                               uint2 *cand, uint4 *recv, uint2 *rech, uint32_t rec_cap, uint64_t wait_limit,
+                               uint32_t *err, cudaStream_t s);
+// Before each chunk: the queries the filter still serves (neither moved to the FP32
+// scorer nor retired by BatchQuery::maxkey), their rows of abf copied into compact
+// tiles abf_act (same size as abf), amap[slot] = query, *nact = count.
+cudaError_t launch_batch_active(const BatchQuery *qs, const BatchState *st, uint32_t nq, const uint8_t *abf,
+                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, cudaStream_t s);
 // Learned k-th-score model (mlp.cu): in -> 64 -> 64 -> 1 ReLU MLP, features of
 // feature_dim(d) values per query from the partition statistics ([P][d] each).
 constexpr uint32_t kHid = 64;
@@ -108,6 +121,10 @@ __host__ __device__ inline float learned_cut(float u, float b1s, float S, float 
 // Start each query's state at its learned cut (pred: model outputs; X: features).
 cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
                                 BatchState *st, uint32_t nq, cudaStream_t s);
+// One query (device descriptor q): *seed = key of its learned cut (0: none), *cut = the
+// cut (NaN when not finite).
+cudaError_t launch_learned_seed_one(const float *pred, const float *X, uint32_t d, const BatchQuery *q, float margin,
+                                    uint32_t *seed, float *cut, cudaStream_t s);
 cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
                                 uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
                                 uint32_t *out_count, float *out_thr, cudaStream_t s);

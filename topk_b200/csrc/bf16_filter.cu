@@ -157,8 +157,9 @@ struct FilterArgs {
                        // (8 x uint4) of one query over 32 consecutive objects
   uint2 *rech;         // and their headers: (first object, CTA-relative query)
   uint32_t rec_cap;
-  uint32_t nq, nqt;    // queries, query tiles
-  uint32_t qt_per_cta, ngroups, cpg;
+  const uint32_t *amap;  // compact query slot -> query (batch_active_kernel)
+  const uint32_t *nact;  // active queries (slots 0..*nact-1), read when the kernel starts
+  uint32_t qt_cap;       // query tiles of 128 per CTA at most
   uint64_t tile0, tile1;  // object tiles of the chunk
   uint64_t r1;            // rows >= r1 are never appended
   uint64_t wait_limit;
@@ -167,21 +168,32 @@ struct FilterArgs {
 
 __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterArgs p) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  const uint32_t g = blockIdx.x % p.ngroups, c = blockIdx.x / p.ngroups;
-  const uint32_t QT = p.qt_per_cta;
-  const uint32_t qt0 = g * QT;
-  const uint32_t nqt = min(QT, p.nqt - qt0);
+  // Work split from the active query count: the chunk's active queries in tiles of
+  // 128, the tiles in groups of at most qt_cap per CTA (balanced), each group's object
+  // tiles split among cpg CTAs.  Every thread reads the same count, so the early
+  // returns below are uniform over the block (no barrier or TMEM touched yet).
+  const uint32_t nact = *p.nact;
+  const uint32_t nqt_all = (nact + kQTile - 1) / kQTile;
+  if (nqt_all == 0) return;
+  const uint32_t ngroups = (nqt_all + p.qt_cap - 1) / p.qt_cap;
+  const uint32_t QT = (nqt_all + ngroups - 1) / ngroups;
   const uint64_t ntiles = p.tile1 - p.tile0;
-  const uint64_t per = (ntiles + p.cpg - 1) / p.cpg;
+  const uint32_t cpg = (uint32_t)max((uint64_t)1, min(ntiles, (uint64_t)(gridDim.x / ngroups)));
+  if (blockIdx.x >= ngroups * cpg) return;
+  const uint32_t g = blockIdx.x % ngroups, c = blockIdx.x / ngroups;
+  const uint32_t qt0 = g * QT;
+  if (qt0 >= nqt_all) return;
+  const uint32_t nqt = min(QT, nqt_all - qt0);
+  const uint64_t per = (ntiles + cpg - 1) / cpg;
   const uint64_t tb = p.tile0 + (uint64_t)c * per;
   const uint64_t te = min(p.tile1, tb + per);
-  if (tb >= te) return;  // uniform over the block: no barrier or TMEM touched yet
+  if (tb >= te) return;
 
   // shared layout: query tiles | object ring | cut[QT*kQTile] | barriers and words
   unsigned char *sq = smem;
-  unsigned char *so = smem + (size_t)QT * kQTileBytes;
+  unsigned char *so = smem + (size_t)p.qt_cap * kQTileBytes;
   float *scut = reinterpret_cast<float *>(so + (size_t)kStages * kOTileBytes);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(scut + QT * kQTile);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(scut + p.qt_cap * kQTile);
   uint64_t *full = bars, *empty = bars + kStages, *accf = bars + 2 * kStages, *acce = accf + kAcc;
   uint64_t *qfull = acce + kAcc, *mdone = qfull + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 1);
@@ -190,7 +202,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
   const uint32_t seg_cap = p.rec_cap / kEpiWarps;
   uint4 *recv = p.recv + (size_t)blockIdx.x * p.rec_cap * 8u;
   uint2 *rech = p.rech + (size_t)blockIdx.x * p.rec_cap;
-  const uint32_t q0 = qt0 * kQTile;  // first query of this CTA
+  const uint32_t q0 = qt0 * kQTile;  // first query slot of this CTA
 
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t limit = p.wait_limit;
@@ -209,14 +221,16 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     for (uint32_t w = 0; w < kEpiWarps; ++w) wrec_n[w] = 0u;
     fence_barrier_init();
   }
-  // per-query cut: threshold float minus the bound, rounded down; +inf for columns
-  // past the last query, -inf while best[] is not full (every object is a candidate)
+  // per-slot cut: threshold float minus the bound, rounded down; +inf for slots past
+  // the last active query, -inf while best[] is not full (every object is a candidate)
   for (uint32_t j = threadIdx.x; j < QT * kQTile; j += kFThreads) {
-    const uint32_t q = q0 + j;
+    const uint32_t sl = q0 + j;
     float cut = __int_as_float(0x7F800000);
-    if (j < nqt * kQTile && q < p.nq) {
+    if (j < nqt * kQTile && sl < nact) {
+      const uint32_t q = p.amap[sl];
       const BatchState sq_st = p.st[q];
-      // a query moved to the exact FP32 scorer keeps +inf: nothing passes for it
+      // the active list holds neither moved nor retired queries; a query moved to the
+      // exact FP32 scorer since keeps +inf: nothing passes for it
       if (!(sq_st.flags & kFlagFp32))
         cut = sq_st.thr == 0u ? __int_as_float(0xFF800000) : __fsub_rd(thr_float(sq_st.thr), p.qs[q].err);
     }
@@ -298,7 +312,6 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     // this warp's record segment and its fill, the same in every lane (no atomics)
     uint4 *wrecv = recv + (size_t)warp * seg_cap * 8u;
     uint2 *wrech = rech + (size_t)warp * seg_cap;
-    BatchState *st0 = p.st + q0;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t wcnt = 0;
     const uint64_t npairs = (te - tb) * nqt;
@@ -339,7 +352,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
             for (int c = 0; c < 8; ++c) dst[c] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
             wrech[e] = make_uint2((uint32_t)(obj0 + rt * 32u), ql);
           } else {
-            atomicOr(&st0[ql].flags, kFlagOverflow);  // lost: the query moves to the exact scorer
+            atomicOr(&p.st[p.amap[q0 + ql]].flags, kFlagOverflow);  // lost: the query moves to the exact scorer
           }
         }
       }
@@ -390,7 +403,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
       const uint32_t nvalid = h.x >= p.r1 ? 0u : p.r1 - h.x >= 32u ? 32u : (uint32_t)(p.r1 - h.x);
       if (nvalid < 32u) mask &= (1u << nvalid) - 1u;
       if (!mask) continue;
-      const uint32_t q = q0 + h.y;
+      const uint32_t q = p.amap[q0 + h.y];
       uint32_t at = atomicAdd(&p.st[q].ccount, (uint32_t)__popc(mask));
       const BatchQuery &bq = p.qs[q];
 #pragma unroll
@@ -405,14 +418,19 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
 
 // ---------------------------------------------------------------- table split
 // One thread per object (grid-stride): reads its 16 attributes (columns >= d and
-// rows >= n are zero), writes hi and lo in the tiled core-matrix layout, and
-// keeps the largest |x| bit pattern per column (NaN and inf show as >= 0x7F800000).
+// rows >= n are zero), writes hi and lo in the tiled core-matrix layout, and keeps
+// per column the largest |x| bit pattern (NaN and inf show as >= 0x7F800000) and the
+// largest and smallest order keys (NaN left out of both).
 __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict__ table, uint64_t ld, uint32_t d,
                                                         uint64_t n, uint64_t nobj, uint8_t *__restrict__ xbf,
-                                                        uint32_t *__restrict__ absmax) {
-  uint32_t amax[16];
+                                                        uint32_t *__restrict__ ext) {
+  uint32_t amax[16], kmax[16], kmin[16];
 #pragma unroll
-  for (int m = 0; m < 16; ++m) amax[m] = 0u;
+  for (int m = 0; m < 16; ++m) {
+    amax[m] = 0u;
+    kmax[m] = 0u;
+    kmin[m] = 0xFFFFFFFFu;
+  }
   for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nobj; o += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t hi[8], lo[8];
 #pragma unroll
@@ -420,8 +438,14 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict_
       float x[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        x[e] = ((uint32_t)(m + e) < d && o < n) ? __ldg(table + (uint64_t)(m + e) * ld + o) : 0.0f;
+        const bool in = (uint32_t)(m + e) < d && o < n;
+        x[e] = in ? __ldg(table + (uint64_t)(m + e) * ld + o) : 0.0f;
         amax[m + e] = max(amax[m + e], __float_as_uint(x[e]) & 0x7FFFFFFFu);
+        if (in && x[e] == x[e]) {
+          const uint32_t k = f2key(x[e]);
+          kmax[m + e] = max(kmax[m + e], k);
+          kmin[m + e] = min(kmin[m + e], k);
+        }
       }
       const __nv_bfloat16 h0 = __float2bfloat16_rn(x[0]), h1 = __float2bfloat16_rn(x[1]);
       const __nv_bfloat16 l0 = __float2bfloat16_rn(x[0] - __bfloat162float(h0));
@@ -439,11 +463,94 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(const float *__restrict_
   }
 #pragma unroll
   for (int m = 0; m < 16; ++m) {
-    uint32_t a = amax[m];
+    uint32_t a = amax[m], hk = kmax[m], lk = kmin[m];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) a = max(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
-    if ((threadIdx.x & 31) == 0 && (uint32_t)m < d) atomicMax(absmax + m, a);
+    for (int o = 16; o > 0; o >>= 1) {
+      a = max(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
+      hk = max(hk, __shfl_xor_sync(0xFFFFFFFFu, hk, o));
+      lk = min(lk, __shfl_xor_sync(0xFFFFFFFFu, lk, o));
+    }
+    if ((threadIdx.x & 31) == 0 && (uint32_t)m < d) {
+      atomicMax(ext + m, a);
+      atomicMax(ext + d + m, hk);
+      atomicMin(ext + 2 * d + m, lk);
+    }
   }
+}
+
+// ---------------------------------------------------------------- active queries
+// One block, before each chunk's filter: lists the queries the filter still has to
+// serve, in query order, as compact slots (amap[slot] = query, *nact = count), and
+// copies each one's operand row (hi and lo, 64 bytes) from the batch's query tiles to
+// its slot in the compact tiles.  A query is left out once it has moved to the exact
+// FP32 scorer, or once its threshold is above the largest score any row can have
+// (BatchQuery::maxkey: the reference-order FP32 sum over the column extremes, an
+// exact upper bound because rounding is monotone) -- then no later row can enter its
+// top-k.  This is the reference's stop rule (cpu/VTA.h:210-216, cpu/PTA.h:636-641:
+// stop once the k-th score reaches the bound of what is left) with the whole table as
+// the block.  The rows of the last tile past the count are zeroed.
+constexpr uint32_t kActThreads = 1024;
+
+__device__ __forceinline__ size_t qrow_off(uint32_t j) {  // query j's hi row in the tile layout
+  return (size_t)(j / kQTile) * kQTileBytes + ((j % kQTile) >> 3) * 256u + (j & 7u) * 16u;
+}
+
+__global__ void __launch_bounds__(kActThreads) batch_active_kernel(const BatchQuery *__restrict__ qs,
+                                                                 const BatchState *__restrict__ st, uint32_t nq,
+                                                                 const uint8_t *__restrict__ abf,
+                                                                 uint8_t *__restrict__ abf_act,
+                                                                 uint32_t *__restrict__ amap,
+                                                                 uint32_t *__restrict__ nact) {
+  __shared__ uint32_t wsum[kActThreads / 32];
+  __shared__ uint32_t base;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  if (t == 0) base = 0;
+  __syncthreads();
+  for (uint32_t j0 = 0; j0 < nq; j0 += kActThreads) {
+    const uint32_t j = j0 + t;
+    bool act = false;
+    if (j < nq) {
+      const BatchState s = st[j];
+      act = !(s.flags & kFlagFp32) && !(s.thr != 0u && s.thr > qs[j].maxkey);
+    }
+    const unsigned b = __ballot_sync(0xFFFFFFFFu, act);
+    if (lane == 0) wsum[warp] = __popc(b);
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of the 32 warp counts
+      const uint32_t v = wsum[lane];
+      uint32_t incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      wsum[lane] = incl - v;
+    }
+    __syncthreads();
+    const uint32_t slot = base + wsum[warp] + __popc(b & ((1u << lane) - 1u));
+    if (act) {
+      amap[slot] = j;
+      const uint4 *src = reinterpret_cast<const uint4 *>(abf + qrow_off(j));
+      uint4 *dst = reinterpret_cast<uint4 *>(abf_act + qrow_off(slot));
+      dst[0] = src[0];                      // hi, attributes 0-7
+      dst[8] = src[8];                      // hi, attributes 8-15 (128 bytes on)
+      dst[kQTileBytes / 32] = src[kQTileBytes / 32];          // lo
+      dst[kQTileBytes / 32 + 8] = src[kQTileBytes / 32 + 8];
+    }
+    __syncthreads();
+    if (t == kActThreads - 1) base = slot + (act ? 1u : 0u);
+    __syncthreads();
+  }
+  const uint32_t total = base;
+  for (uint32_t sl = total + t; sl < (total + kQTile - 1) / kQTile * kQTile; sl += kActThreads) {
+    uint4 *dst = reinterpret_cast<uint4 *>(abf_act + qrow_off(sl));
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    dst[0] = z;
+    dst[8] = z;
+    dst[kQTileBytes / 32] = z;
+    dst[kQTileBytes / 32 + 8] = z;
+  }
+  if (t == 0) *nact = total;
 }
 
 }  // namespace
@@ -456,14 +563,15 @@ size_t filter_smem_bytes(uint32_t qt) {
 
 uint64_t bf16_table_bytes(uint64_t n) { return (n + kOTile - 1) / kOTile * kOTileBytes; }
 
-cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *absmax,
+cudaError_t launch_bf16_pack(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint8_t *xbf, uint32_t *ext,
                              int num_sms, cudaStream_t s) {
   if (d > kBf16MaxD) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(absmax, 0, d * sizeof(uint32_t), s);
+  cudaError_t e = cudaMemsetAsync(ext, 0, 2 * d * sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ext + 2 * d, 0xFF, d * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   const uint64_t nobj = (n + kOTile - 1) / kOTile * kOTile;
   const uint64_t blocks = std::min<uint64_t>((nobj + 255) / 256, (uint64_t)num_sms * 8);
-  bf16_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(table, ld, d, n, nobj, xbf, absmax);
+  bf16_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(table, ld, d, n, nobj, xbf, ext);
   return cudaGetLastError();
 }
 
@@ -498,18 +606,18 @@ FilterPlan plan_bf16_filter(uint32_t nq, uint64_t r0, uint64_t r1, int num_sms, 
   FilterPlan f{};
   f.tile0 = r0 / kOTile;
   f.tile1 = (r1 + kOTile - 1) / kOTile;
-  f.nqt = (nq + kQTile - 1) / kQTile;
-  f.qt_per_cta = std::min<uint32_t>(f.nqt, (qt_cap >= 1 && qt_cap < kMaxQTPerCta) ? qt_cap : kMaxQTPerCta);
-  f.ngroups = (f.nqt + f.qt_per_cta - 1) / f.qt_per_cta;
-  const uint64_t ntiles = f.tile1 - f.tile0;
-  f.cpg = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)std::max(1, num_sms / (int)f.ngroups)));
-  f.grid = (uint64_t)f.ngroups * f.cpg;
+  const uint32_t nqt = (nq + kQTile - 1) / kQTile;
+  f.qt_cap = (qt_cap >= 1 && qt_cap < kMaxQTPerCta) ? qt_cap : kMaxQTPerCta;
+  // enough CTAs for every group the active count can need, and at least one per SM
+  const uint64_t groups = (nqt + f.qt_cap - 1) / f.qt_cap;
+  f.grid = std::max<uint64_t>((uint64_t)std::max(1, num_sms), groups);
   return f;
 }
 
-cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, uint64_t r0, uint64_t r1,
-                               const BatchQuery *qs, uint32_t nq, BatchState *st, uint2 *cand, uint4 *recv,
-                               uint2 *rech, uint32_t rec_cap, uint64_t wait_limit, uint32_t *err, cudaStream_t s) {
+cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const uint8_t *abf, const uint32_t *amap,
+                               const uint32_t *nact, uint64_t r0, uint64_t r1, const BatchQuery *qs, BatchState *st,
+                               uint2 *cand, uint4 *recv, uint2 *rech, uint32_t rec_cap, uint64_t wait_limit,
+                               uint32_t *err, cudaStream_t s) {
   if (r0 % kOTile || f.grid == 0 || f.grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
   FilterArgs p{};
   p.xbf = xbf;
@@ -520,20 +628,24 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
   p.recv = recv;
   p.rech = rech;
   p.rec_cap = rec_cap;
-  p.nq = nq;
-  p.nqt = f.nqt;
-  p.qt_per_cta = f.qt_per_cta;
-  p.ngroups = f.ngroups;
-  p.cpg = f.cpg;
+  p.amap = amap;
+  p.nact = nact;
+  p.qt_cap = f.qt_cap;
   p.tile0 = f.tile0;
   p.tile1 = f.tile1;
   p.r1 = r1;
   p.wait_limit = wait_limit;
   p.err = err;
-  const size_t smem = std::max(kMinFilterSmem, filter_smem_bytes(f.qt_per_cta));
+  const size_t smem = std::max(kMinFilterSmem, filter_smem_bytes(f.qt_cap));
   cudaError_t e = cudaFuncSetAttribute(bf16_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   bf16_filter_kernel<<<(unsigned)f.grid, kFThreads, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_active(const BatchQuery *qs, const BatchState *st, uint32_t nq, const uint8_t *abf,
+                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, cudaStream_t s) {
+  batch_active_kernel<<<1, kActThreads, 0, s>>>(qs, st, nq, abf, abf_act, amap, nact);
   return cudaGetLastError();
 }
 

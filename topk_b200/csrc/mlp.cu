@@ -385,9 +385,27 @@ __global__ void learned_seed_kernel(const float *__restrict__ pred, const float 
   st[j] = s;
 }
 
+// One query (a pruned single query): its seed key (0: none) and the cut itself.
+__global__ void learned_seed_one_kernel(const float *__restrict__ pred, const float *__restrict__ X, uint32_t bcol,
+                                        const BatchQuery *__restrict__ q, float margin, uint32_t *__restrict__ seed,
+                                        float *__restrict__ cut_out) {
+  float S = 0.0f;
+  for (uint32_t m = 0; m < q->qq; ++m) S += fabsf(q->w[m]);
+  if (S == 0.0f) S = 1.0f;
+  const float cut = learned_cut(pred[0], X[bcol], S, (float)q->qq, margin);
+  *seed = isfinite(cut) ? f2key(cut) : 0u;
+  *cut_out = isfinite(cut) ? cut : __int_as_float(0x7FC00000);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
+cudaError_t launch_learned_seed_one(const float *pred, const float *X, uint32_t d, const BatchQuery *q, float margin,
+                                    uint32_t *seed, float *cut, cudaStream_t s) {
+  learned_seed_one_kernel<<<1, 1, 0, s>>>(pred, X, feature_bound_col(d), q, margin, seed, cut);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
                                 BatchState *st, uint32_t nq, cudaStream_t s) {
   if (nq)

@@ -10,9 +10,9 @@
 // array compiled into this library.
 //
 // Limits and sharing:
-//   * k <= kNoAllocMaxK (1024); the launch uses at most kNoAllocMaxGrid CTAs
-//     (fewer CTAs per SM than topk_query may use on large GPUs).
-//   * The array takes kNoAllocScratchBytes (about 2.7 MB) of device memory on every
+//   * k <= kNoAllocMaxK (1024); the launch uses at most kNoAllocMaxGrid CTAs, and for
+//     k above 256 fewer CTAs per SM than topk_query may use (the slots are fixed).
+//   * The array takes kNoAllocScratchBytes (about 8.4 MB) of device memory on every
 //     GPU that loads this library, for as long as the process lives.
 //   * Every call on a device uses the same array.  Calls whose kernels overlap on
 //     the GPU (different streams, or different host threads without ordering)
@@ -38,13 +38,18 @@ using namespace topk;
 namespace {
 
 constexpr uint32_t kNoAllocMaxK = 1024;
-constexpr uint32_t kNoAllocMaxGrid = 160;  // >= SM count of a B200 (148)
+// CTAs of one scan at most: 8 per SM of a B200 (148 SMs), as many as the scan's
+// occupancy allows.  The merge-tree slots hold kNoAllocSlotEntries (key, id) entries
+// in all; a scan with k entries per slot gets at most (entries / k - levels) / 2 CTAs
+// (every CTA for k <= 256; about 3.4 per SM at k = 1024).
+constexpr uint32_t kNoAllocMaxGrid = 8 * 148;
+constexpr uint32_t kNoAllocSlotEntries = 1u << 20;  // 8 MiB
 constexpr uint32_t kNoAllocMaxSlots = 2 * kNoAllocMaxGrid + kMaxLevels;
 constexpr uint32_t kNoAllocMaxGroups = kNoAllocMaxGrid + kMaxLevels;
-// layout: ScanScratch | done[groups] | slot_count[slots] | pad | slots[slots * k]
+// layout: ScanScratch | done[groups] | slot_count[slots] | pad | slots[entries]
 constexpr size_t kMetaBytes = sizeof(ScanScratch) + (size_t)kNoAllocMaxGroups * 4;
 constexpr size_t kSlotsOff = (kMetaBytes + (size_t)kNoAllocMaxSlots * 4 + 255) / 256 * 256;
-constexpr size_t kNoAllocScratchBytes = kSlotsOff + (size_t)kNoAllocMaxSlots * kNoAllocMaxK * sizeof(uint2);
+constexpr size_t kNoAllocScratchBytes = kSlotsOff + (size_t)kNoAllocSlotEntries * sizeof(uint2);
 
 // The scratch.  In host code this name is only a stand-in for the symbol: its
 // device address comes from cudaGetSymbolAddress below, once per device.
@@ -139,13 +144,17 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   p.num_tiles = (uint32_t)tiles;
   if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;
   if ((uint32_t)pl.grid > kNoAllocMaxGrid) pl.grid = (int)kNoAllocMaxGrid;
+  // the merge tree's slots (< (2 * grid + levels) * k entries) within the fixed array
+  const uint64_t max_grid_k = (kNoAllocSlotEntries / kk - (uint64_t)kMaxLevels) / 2;
+  if ((uint64_t)pl.grid > max_grid_k) pl.grid = (int)max_grid_k;
   p.qq = qq;
   p.k = (uint32_t)kk;
   p.cap = pl.cap;
   p.mcap = pl.mcap;
   uint32_t tree_slots = 0, tree_groups = 0;
   plan_merge_tree(p, (uint32_t)pl.grid, pl.fanin, &tree_slots, &tree_groups);
-  if (tree_slots > kNoAllocMaxSlots || tree_groups > kNoAllocMaxGroups || p.nslots[p.levels] != 1)
+  if (tree_slots > kNoAllocMaxSlots || tree_groups > kNoAllocMaxGroups || p.nslots[p.levels] != 1 ||
+      (uint64_t)tree_slots * kk > kNoAllocSlotEntries)
     return fail(TOPK_ERR_UNSUPPORTED, "merge tree of %d CTAs does not fit the fixed scratch", pl.grid);
   // No wait hook: with fault_mode 0 the scan has no device-side wait that can give
   // up (its only bounded wait is the fault-injection barrier of the handle-based

@@ -98,20 +98,19 @@ __global__ void gather_rows_kernel(const float *__restrict__ table, uint64_t ld,
 __global__ void __launch_bounds__(256) part_stats_kernel(const float *__restrict__ ptable, uint64_t ld, uint32_t d,
                                                          uint64_t n, uint32_t rows_log2, float *__restrict__ mins,
                                                          float *__restrict__ maxs, float *__restrict__ means) {
-  __shared__ float smn[8], smx[8];
-  __shared__ double ssum[8];
+  __shared__ float smn[8], smx[8], ssum[8];
   const uint64_t r0 = (uint64_t)blockIdx.x << rows_log2;
   const uint64_t r1 = min((uint64_t)n, r0 + (uint64_t)(1ull << rows_log2));
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint32_t m = 0; m < d; ++m) {
     const float *col = ptable + (uint64_t)m * ld;
     float mn = __int_as_float(0x7F800000), mx = __int_as_float(0xFF800000);
-    double sum = 0.0;
+    float sum = 0.0f;  // the mean is a model feature only: FP32 partial sums suffice
     for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
       const float x = col[r];
       mn = fminf(mn, x);
       mx = fmaxf(mx, x);
-      sum += (double)x;
+      sum += x;
     }
     for (int o = 16; o > 0; o >>= 1) {
       mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
@@ -133,7 +132,7 @@ __global__ void __launch_bounds__(256) part_stats_kernel(const float *__restrict
       const size_t o = (size_t)blockIdx.x * d + m;
       mins[o] = mn;
       maxs[o] = mx;
-      means[o] = r1 > r0 ? (float)(sum / (double)(r1 - r0)) : 0.0f;
+      means[o] = r1 > r0 ? sum / (float)(r1 - r0) : 0.0f;
     }
     __syncthreads();
   }
@@ -221,6 +220,72 @@ int grid_for(uint64_t n, int num_sms) {
   return (int)(b < (uint64_t)num_sms * 16 ? (b ? b : 1) : (uint64_t)num_sms * 16);
 }
 
+// ---------------------------------------------------------------- partition order of a query
+// The bound of partition p for one query: the reference-order FP32 sum of
+// w[attr[m]] * (w >= 0 ? max : min of column attr[m] in p).  IEEE multiplication and
+// addition round monotonically, so no row of p scores above it (no slack needed, and
+// a partition whose every queried value sits at its maximum scores exactly it).  The
+// order key of the bound, or 0xFFFFFFFF (keep) when it is NaN.
+__device__ __forceinline__ uint32_t part_bound_key(const float *__restrict__ pmin, const float *__restrict__ pmax,
+                                                   uint32_t d, uint32_t p, const PartQuery &q) {
+  float sacc = 0.0f;
+  for (uint32_t m = 0; m < q.qq; ++m) {
+    const float w = q.w[m];
+    const size_t o = (size_t)p * d + q.attr[m];
+    const float x = w >= 0.0f ? __ldg(pmax + o) : __ldg(pmin + o);
+    sacc = __fadd_rn(sacc, __fmul_rn(x, w));
+  }
+  return sacc != sacc ? 0xFFFFFFFFu : f2key(sacc);
+}
+
+// One block: every partition's bound key, sorted descending (ties by the lower
+// partition number) in shared memory by a bitonic network; plist[i] = partition of
+// rank i, pkey[i] = its bound key.
+constexpr uint32_t kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *__restrict__ pmin,
+                                                                  const float *__restrict__ pmax, uint32_t P,
+                                                                  uint32_t Ppad, uint32_t d, const PartQuery q,
+                                                                  uint32_t *__restrict__ plist,
+                                                                  uint32_t *__restrict__ pkey) {
+  extern __shared__ unsigned long long ent[];
+  const uint32_t t = threadIdx.x;
+  // (key, ~partition): descending composite = key descending, then partition ascending;
+  // padding entries are 0, below every real one
+  for (uint32_t i = t; i < Ppad; i += kOrderThreads)
+    ent[i] = i < P ? ((unsigned long long)part_bound_key(pmin, pmax, d, i, q) << 32) | (0xFFFFFFFFu - i) : 0ull;
+  __syncthreads();
+  for (uint32_t size = 2; size <= Ppad; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t i = t; i < Ppad / 2; i += kOrderThreads) {
+        const uint32_t lo = 2 * i - (i & (stride - 1));
+        const uint32_t hi = lo + stride;
+        const bool desc = (lo & size) == 0;
+        const unsigned long long x = ent[lo], y = ent[hi];
+        if (desc ? (x < y) : (x > y)) {
+          ent[lo] = y;
+          ent[hi] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = t; i < P; i += kOrderThreads) {
+    const unsigned long long e = ent[i];
+    plist[i] = 0xFFFFFFFFu - (uint32_t)e;
+    pkey[i] = (uint32_t)(e >> 32);
+  }
+}
+
+// Many partitions: the keys and partition numbers into arrays for a radix sort.
+__global__ void part_keys_kernel(const float *__restrict__ pmin, const float *__restrict__ pmax, uint32_t P,
+                                 uint32_t d, const PartQuery q, uint32_t *__restrict__ keys,
+                                 uint32_t *__restrict__ ids) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+    keys[i] = part_bound_key(pmin, pmax, d, i, q);
+    ids[i] = i;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_partition_build(const float *table, uint64_t ld, uint32_t d, uint64_t n, const float *lo,
@@ -305,6 +370,41 @@ cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint
 cudaError_t launch_partition_stats(const float *ptable, uint64_t ld, uint32_t d, uint64_t n, uint32_t rows_log2,
                                    uint32_t num_parts, float *mins, float *maxs, float *means, cudaStream_t s) {
   part_stats_kernel<<<num_parts, 256, 0, s>>>(ptable, ld, d, n, rows_log2, mins, maxs, means);
+  return cudaGetLastError();
+}
+
+size_t part_order_temp_bytes(uint32_t P) {
+  if (P <= kPartOrderOneBlock) return 0;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)P, 0, 32);
+  return (tb + 255) / 256 * 256 + 2 * (size_t)P * sizeof(uint32_t);
+}
+
+cudaError_t launch_part_order(const float *pmin, const float *pmax, uint32_t P, uint32_t d, const PartQuery &q,
+                              uint32_t *plist, uint32_t *pkey, void *temp, size_t temp_bytes, int num_sms,
+                              cudaStream_t s) {
+  if (P == 0) return cudaSuccess;
+  if (P <= kPartOrderOneBlock) {
+    uint32_t Ppad = 1;
+    while (Ppad < P) Ppad <<= 1;
+    const size_t smem = (size_t)Ppad * 8;
+    cudaError_t e = cudaFuncSetAttribute(part_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    part_order_kernel<<<1, kOrderThreads, smem, s>>>(pmin, pmax, P, Ppad, d, q, plist, pkey);
+    return cudaGetLastError();
+  }
+  // keys_in | ids_in after the radix sort's own scratch
+  if (temp_bytes < part_order_temp_bytes(P)) return cudaErrorInvalidValue;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)P, 0, 32);
+  uint32_t *kin = reinterpret_cast<uint32_t *>(static_cast<unsigned char *>(temp) + (tb + 255) / 256 * 256);
+  uint32_t *iin = kin + P;
+  part_keys_kernel<<<grid_for(P, num_sms), 256, 0, s>>>(pmin, pmax, P, d, q, kin, iin);
+  // stable: equal keys keep ascending partition numbers
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, kin, pkey, iin, plist, (int)P, 0, 32, s);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

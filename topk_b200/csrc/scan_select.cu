@@ -43,11 +43,12 @@ struct SmemCtl {
   uint32_t count;      // entries in the current candidate buffer
   uint32_t cur;        // which of the two candidate buffers is current
   uint32_t thr_local;  // min key that can still enter (k-th CTA key + 1)
-  uint32_t thr_g;      // CTA copy of the global threshold
+  uint32_t thr_g[2];   // CTA copy of the global threshold: tile i reads [i & 1], thread 0
+                       // writes [(i + 1) & 1] before tile i's barrier, so every thread of
+                       // a tile reads the same value
   uint32_t reductions;
   uint32_t is_last;
   uint32_t red_g;      // threshold snapshot shared by the block
-  uint32_t pad;
   SelShared sel;       // state of the block-wide selects
 };
 
@@ -191,8 +192,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     ctl->count = 0;
     ctl->cur = 0;
     ctl->thr_local = 0;
-    if (p.thr_seed) atomicMax(&p.scratch->g_thr, p.thr_seed);  // every later read includes it
-    ctl->thr_g = max(ld_volatile_u32(&p.scratch->g_thr), p.thr_seed);
+    const uint32_t seed = max(p.thr_seed, p.thr_seed_dev ? *p.thr_seed_dev : 0u);
+    if (seed) atomicMax(&p.scratch->g_thr, seed);  // every later read includes it
+    ctl->thr_g[0] = max(ld_volatile_u32(&p.scratch->g_thr), seed);
     ctl->reductions = 0;
   }
   bsync();
@@ -234,21 +236,31 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     for (int dd = 0; dd < kDepth; ++dd)
       if ((uint32_t)dd < my_tiles) load_tile(dd, xn[dd]);
   }
-  // partition mode: the partition of the next tile is loaded one tile ahead
+  // partition mode: the partition of the next tile (and its bound) is loaded one tile ahead
   const uint32_t pmask = (1u << p.part_shift) - 1u;
   uint32_t part_next = (p.part_list && my_tiles) ? __ldg(p.part_list + (blockIdx.x >> p.part_shift)) : 0u;
+  uint32_t key_next = (p.part_key && my_tiles) ? __ldg(p.part_key + (blockIdx.x >> p.part_shift)) : 0xFFFFFFFFu;
+  uint32_t tiles_done = 0;
   for (uint32_t i = 0; i < my_tiles; ++i) {
     const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
+    // every thread reads the same thresholds here (see SmemCtl::thr_g)
+    const uint32_t thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
     uint64_t tile0;
     if (p.part_list) {
+      // nothing in this partition (nor in any later one of this CTA) can reach thr
+      if (key_next < thr) break;
       tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
-      if (i + 1 < my_tiles) part_next = __ldg(p.part_list + ((tix + gridDim.x) >> p.part_shift));
+      if (i + 1 < my_tiles) {
+        const uint64_t nx = (tix + gridDim.x) >> p.part_shift;
+        part_next = __ldg(p.part_list + nx);
+        if (p.part_key) key_next = __ldg(p.part_key + nx);
+      }
     } else {
       tile0 = p.tile_begin + tix * kTile;
     }
+    ++tiles_done;
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
-    const uint32_t thr = max(ctl->thr_local, ctl->thr_g);
     float4 s;
     if (prefetch) {
       float4 x[kPQ];
@@ -303,6 +315,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
           ++base;
         }
     }
+    // thread 0 hands the next tile its copy of the global threshold (see SmemCtl::thr_g):
+    // it loads the global word every 8 tiles and applies it 7 tiles later, so the L2
+    // round trip is never waited on
+    if (t == 0) {
+      uint32_t g = ctl->thr_g[i & 1u];
+      if ((i & 7u) == 7u) g = max(g, g_pending);
+      ctl->thr_g[(i + 1u) & 1u] = g;
+      if ((i & 7u) == 0u) g_pending = ld_volatile_u32(&p.scratch->g_thr);
+    }
     if (__syncthreads_or(after > cap - kTile)) {
       if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       bsync();
@@ -323,12 +344,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
       }
       bsync();
     }
-    // Thread 0 loads the global threshold every 8 tiles and publishes it to the CTA
-    // 7 tiles later, so the L2 round trip is never waited on.
-    if (t == 0) {
-      if ((i & 7u) == 7u) ctl->thr_g = max(ctl->thr_g, g_pending);
-      if ((i & 7u) == 0u) g_pending = ld_volatile_u32(&p.scratch->g_thr);
-    }
   }
 
   // ---- end of scan: reduce to <= k ----
@@ -348,6 +363,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     bsync();
   }
   if (t == 0 && ctl->reductions) atomicAdd(&p.scratch->acc_reductions, ctl->reductions);
+  if (t == 0 && p.part_list) atomicAdd(&p.scratch->acc_tiles, tiles_done);
 
   // ---- merge tree ----
   const uint32_t k = p.k;
@@ -430,13 +446,16 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     if (p.out_threshold) *p.out_threshold = res_n ? key2f(res[res_n - 1].x) : 0.0f;
     if (p.out_count) *p.out_count = res_n;
     const uint32_t reds = ld_volatile_u32(&p.scratch->acc_reductions);
+    const uint32_t tiles = ld_volatile_u32(&p.scratch->acc_tiles);
     p.scratch->last_cands = merged;
     p.scratch->last_reductions = reds;
     if (p.out_stats) {
       p.out_stats[0] = merged;
       p.out_stats[1] = reds;
+      p.out_stats[2] = tiles;
     }
     p.scratch->acc_reductions = 0;
+    p.scratch->acc_tiles = 0;
     p.scratch->g_thr = 0;
     __threadfence();
   }

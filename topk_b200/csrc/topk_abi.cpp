@@ -72,11 +72,14 @@ struct DeviceGuard {
 struct ResultHeader {
   uint32_t count;
   float threshold;
-  uint32_t stats[2];  // candidates in the final select, block-selects
-  uint32_t pad[12];
+  uint32_t stats[3];  // candidates in the final select, block-selects, tiles scanned
+  float cut;          // a pruned query's learned cut
+  uint32_t pad[10];
 };
 constexpr size_t kHdr = sizeof(ResultHeader);  // 64 bytes
 size_t result_bytes(uint32_t k) { return kHdr + (size_t)k * 8 + (size_t)k * 4; }
+// The pinned result mirror also stages a pruned query's descriptor after the result.
+constexpr size_t kStageBytes = 256;
 
 struct Ctx {
   cudaStream_t stream = nullptr;
@@ -95,8 +98,13 @@ struct Ctx {
   uint64_t *d_ids_scratch = nullptr;  // gather ids
   float *d_rows = nullptr;
   size_t rows_cap = 0;
-  uint32_t *d_plist = nullptr;  // partition list of a pruned scan
+  // pruned queries: partitions by bound and their bound keys, the radix sort's scratch
+  // (many partitions only), the learned start's descriptor, features, prediction, seed
+  uint32_t *d_plist = nullptr, *d_pkey = nullptr;
   size_t plist_cap = 0;
+  void *d_ptemp = nullptr;
+  size_t ptemp_bytes = 0;
+  unsigned char *d_lq = nullptr;
   bool busy = false;
 };
 
@@ -135,8 +143,11 @@ struct topk_table_s {
   // BF16 filter: split copy of the table (rebuilt when the table changed), the
   // per-column max |x| it was built from, the batch's query tiles and error word
   DevBuf xbf, xbf_absmax, b_abf, b_err, b_log, b_logh, b_sw, b_feat, b_pred;
+  // compact active query tiles of the filter, slot -> query map and count; the plain
+  // FP32 scorer's query order (by attribute count)
+  DevBuf b_abf_act, b_amap, b_order;
   uint64_t data_version = 1, xbf_version = 0;
-  std::vector<float> absmax;
+  std::vector<float> absmax, colmax, colmin;  // per column: max |x|, max, min (NaN left out)
   bool xbf_usable = false;
   // partitioned copy for pruned queries (topk_build_partitions): rows reordered,
   // original ids, per-partition [P][d] min / max / mean (device and host copies)
@@ -163,6 +174,7 @@ struct topk_table_s {
   double last_batch_ms = 0, last_batch_err_ratio = 0;
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
   uint64_t last_batch_switched = 0;  // queries a hybrid batch moved from the filter to the FP32 scorer
+  uint64_t last_batch_retired = 0;   // queries the filter retired (threshold above their score bound)
   // pinned host copies of a batch's results (grow-only): copied at full link speed,
   // no page faults on the critical path
   void *hb_res = nullptr;
@@ -219,7 +231,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
   if ((e = cudaMemset(blk, 0, slots_off)) != cudaSuccess) return bail(e, "scratch memset");
   if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
   if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
-  if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK), cudaHostAllocDefault)) != cudaSuccess)
+  if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK) + kStageBytes, cudaHostAllocDefault)) != cudaSuccess)
     return bail(e, "pinned result");
   *out = c;
   return TOPK_OK;
@@ -235,6 +247,9 @@ void ctx_free(Ctx *c) {
   cudaFree(c->d_ids_scratch);
   cudaFree(c->d_rows);
   cudaFree(c->d_plist);
+  cudaFree(c->d_pkey);
+  cudaFree(c->d_ptemp);
+  cudaFree(c->d_lq);
   if (c->h_res) cudaFreeHost(c->h_res);
   delete c;
 }
@@ -289,9 +304,11 @@ int check_query(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, c
 
 // A scan over a list of partitions of the partitioned copy, with a threshold seed.
 struct PartScan {
-  const uint32_t *d_list;  // partition numbers (device)
+  const uint32_t *d_list;  // partition numbers (device), by bound descending
   uint32_t count;
   uint32_t seed;           // objects need key >= seed (0: none)
+  const uint32_t *d_key;   // bound key of each listed partition (null: no stop rule)
+  const uint32_t *d_seed;  // a further seed in device memory (null: none)
 };
 
 // Enqueue one fused scan over rows [r0, r1) (or over the partitions of `ps`)
@@ -330,10 +347,19 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     p.part_rows_log2 = h->part_log2;
     p.row_ids = h->pids;
     p.thr_seed = ps->seed;
+    p.part_key = ps->d_key;
+    p.thr_seed_dev = ps->d_seed;
     tiles = (uint64_t)ps->count << p.part_shift;
     if (tiles > 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "too many tiles");
   }
   p.num_tiles = (uint32_t)tiles;
+  if (ps && ps->d_key) {
+    // With the stop rule, the first wave of CTAs scans its tiles before any threshold
+    // exists; on a small copy keep that wave to about 1/32 of the tiles (one CTA per
+    // SM at least), so most partitions are still decided by the rule.
+    const uint64_t cap = std::max<uint64_t>((uint64_t)h->num_sms, tiles / 32);
+    if ((uint64_t)pl.grid > cap) pl.grid = (int)cap;
+  }
   if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;
   p.qq = qq;
   p.k = (uint32_t)k;
@@ -422,176 +448,145 @@ uint32_t host_f2key(float f) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// A result as (key, id) pairs.
-struct HostResult {
-  std::vector<uint32_t> key;
-  std::vector<uint64_t> id;
-  std::vector<float> score;
-  float threshold = 0.0f;
-};
-
-// One fused scan over a list of partitions with a threshold seed; synchronous.
-// Fewer than min(k, n) results means fewer objects reached the seed.
-int scan_partitions(topk_table_t h, Ctx *c, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr,
-                    const std::vector<uint32_t> &list, uint32_t seed, HostResult *out) {
-  out->key.clear();
-  out->id.clear();
-  out->score.clear();
-  if (list.empty()) return TOPK_OK;
-  if (c->plist_cap < list.size()) {
-    cudaFree(c->d_plist);
-    c->d_plist = nullptr;
-    c->plist_cap = 0;
-    CK(cudaMalloc(&c->d_plist, h->num_parts * sizeof(uint32_t)));
-    c->plist_cap = h->num_parts;
-  }
-  const uint64_t kk = std::min<uint64_t>(k, h->n);
-  unsigned char *dr = c->d_res;
-  ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
-  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
-  float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
-  CK(cudaMemcpyAsync(c->d_plist, list.data(), list.size() * 4, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), c->stream));
-  PartScan ps{c->d_plist, (uint32_t)list.size(), seed};
-  int st = enqueue_scan(h, c, c->stream, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
-                        dh->stats, &ps);
-  if (st != TOPK_OK) return st;
-  CK(cudaMemcpyAsync(c->h_res, dr, kHdr + kk * 12, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
-  if (hh->count > kk) {
-    ScanScratch sc{};
-    cudaMemcpy(&sc, c->scratch, sizeof(sc), cudaMemcpyDeviceToHost);
-    cudaMemset(c->scratch, 0, c->meta_bytes);
-    if (sc.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
-    return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
-  }
-  const uint32_t cnt = hh->count;
-  out->id.assign(reinterpret_cast<const uint64_t *>(c->h_res + kHdr), reinterpret_cast<const uint64_t *>(c->h_res + kHdr) + cnt);
-  const float *sc = reinterpret_cast<const float *>(c->h_res + kHdr + kk * 8);
-  out->score.assign(sc, sc + cnt);
-  for (uint32_t j = 0; j < cnt; j++) out->key.push_back(host_f2key(sc[j]));
-  out->threshold = hh->threshold;
-  return TOPK_OK;
-}
-
-// Upper bound of every reference-order FP32 score in partition p: the bound in
-// double over the partition's extremes, plus the FP32 rounding of qq products and
-// qq additions (each within 2^-24 relative of the running magnitude), rounded up.
-float partition_bound(topk_table_t h, uint32_t p, uint32_t qq, const float *weights, const uint8_t *attr) {
-  double ub = 0.0, mag = 0.0;
-  for (uint32_t m = 0; m < qq; m++) {
-    const double w = weights[attr[m]];
-    const size_t o = (size_t)p * h->d + attr[m];
-    const double x = w >= 0.0 ? h->pmax[o] : h->pmin[o];
-    ub += w * x;
-    mag += std::fabs(w * x);
-  }
-  const double b = ub + mag * std::ldexp((double)(2 * qq + 2), -24) + 1e-37;
-  if (!(b == b) || b > 3.0e38) return INFINITY;
-  float f = (float)b;
-  if ((double)f < b) f = std::nextafter(f, INFINITY);
+float host_key2f(uint32_t k) {
+  const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  float f;
+  std::memcpy(&f, &u, 4);
   return f;
 }
 
-// Exact top-k over the partitioned copy, scanning only partitions whose bound can
-// reach the threshold.  With a finite `cut` (a predicted lower bound of the k-th
-// score): one scan of the partitions with bound >= cut, seeded with cut, accepted
-// when it returns min(k, n) objects (then every object of the true top-k scored
-// >= cut and was scanned); otherwise, and without a cut, two rounds: the
-// highest-bound partitions give an exact k-th score t1 of a subset (a lower bound
-// of the true k-th), then the other partitions with bound >= t1, seeded with t1;
-// the union's top-k is the answer.  stats: partitions scanned, partitions,
-// cut accepted (1/0), scans.
+
+std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs,
+                                     const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride);
+
+// Exact top-k over the partitioned copy in one device pipeline on the context's
+// stream: a kernel orders the partitions by the query's bound (the reference-order
+// FP32 sum over each partition's extremes: an exact upper bound of its scores) and one
+// fused scan walks them in that order, each CTA stopping at its first partition whose
+// bound is below its running threshold -- the reference's stop rule per block
+// (cpu/VTA.h:210-216, cpu/PTA.h:636-641).  The scan's merge tree gives the result;
+// nothing is decided on the host between the launches.  With a seed (a predicted
+// lower bound of the k-th score: `cut`, or the learned model's cut computed on the
+// device), objects and partitions below it are left out from the start; the result
+// is accepted when it holds min(k, n) objects (then the true k-th score is at least
+// the seed, so every object of the true top-k was scanned), otherwise the same scan
+// runs again without the seed.  stats: partitions scanned (tiles scanned / tiles per
+// partition, over both scans), partitions, seed accepted (1/0), scans.
 int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
-               uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats) {
+               bool learned, uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats,
+               float *cut_out) {
   int st = check_query(h, k, qq, weights, attr);
   if (st != TOPK_OK) return st;
   if (!h->ptable || h->part_version != h->data_version)
     return fail(TOPK_ERR_STATE, "no partitions for the current table: call topk_build_partitions");
   const uint64_t kk = std::min<uint64_t>(k, h->n);
   if (!ids || !scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  if (learned && qq > kBatchMaxQ) return fail(TOPK_ERR_UNSUPPORTED, "the learned path supports qq <= %u", kBatchMaxQ);
+  const float *mlp = nullptr;
+  float margin = 0.0f;
+  if (learned) {
+    std::lock_guard<std::mutex> lk(h->learned_mu);
+    if (!h->mlp || h->mlp_part_version != h->part_version || h->part_version != h->data_version)
+      return fail(TOPK_ERR_STATE, "no learned model for the current partitions");
+    mlp = h->mlp;
+    margin = h->mlp_margin;
+  }
   DeviceGuard dg(h->device);
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   CtxLease lease(h);
   if (lease.status != TOPK_OK) return lease.status;
   Ctx *c = lease.c;
   const uint32_t P = h->num_parts;
-  std::vector<float> ub(P);
-  for (uint32_t p = 0; p < P; p++) ub[p] = partition_bound(h, p, qq, weights, attr);
-  uint64_t scanned = 0, scans = 0, accepted = 0;
-  HostResult res;
-  bool done = false;
-  if (std::isfinite(cut)) {
-    std::vector<uint32_t> list;
-    for (uint32_t p = 0; p < P; p++)
-      if (ub[p] >= cut) list.push_back(p);
-    if ((st = scan_partitions(h, c, k, qq, weights, attr, list, host_f2key(cut), &res)) != TOPK_OK) return st;
-    scanned += list.size();
+  cudaStream_t s = c->stream;
+  if (c->plist_cap < P) {
+    cudaFree(c->d_plist);
+    cudaFree(c->d_pkey);
+    cudaFree(c->d_ptemp);
+    c->d_plist = c->d_pkey = nullptr;
+    c->d_ptemp = nullptr;
+    c->plist_cap = 0;
+    c->ptemp_bytes = part_order_temp_bytes(P);
+    CK(cudaMalloc(&c->d_plist, (size_t)P * 4));
+    CK(cudaMalloc(&c->d_pkey, (size_t)P * 4));
+    if (c->ptemp_bytes) CK(cudaMalloc(&c->d_ptemp, c->ptemp_bytes));
+    c->plist_cap = P;
+  }
+  unsigned char *dr = c->d_res;
+  ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
+  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
+  float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
+  const uint32_t *d_seed = nullptr;
+  if (learned) {
+    // descriptor | features (kMlpMaxIn) | prediction | seed word
+    const size_t qb = (sizeof(BatchQuery) + 15) / 16 * 16;
+    if (!c->d_lq) CK(cudaMalloc(&c->d_lq, qb + (kMlpMaxIn + 2) * 4));
+    const uint64_t k1 = k;
+    const std::vector<BatchQuery> bq = pack_queries(h, 1, &k1, &qq, weights, 0, attr, 0);
+    static_assert(sizeof(BatchQuery) <= kStageBytes, "descriptor staging");
+    unsigned char *stage = c->h_res + result_bytes(kMaxK);  // pinned, after the result area
+    std::memcpy(stage, &bq[0], sizeof(BatchQuery));
+    BatchQuery *dq = reinterpret_cast<BatchQuery *>(c->d_lq);
+    float *X = reinterpret_cast<float *>(c->d_lq + qb);
+    uint32_t *seed = reinterpret_cast<uint32_t *>(X + kMlpMaxIn + 1);
+    CK(cudaMemcpyAsync(dq, stage, sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
+    const size_t Pd = (size_t)P * h->d;
+    CK(launch_features(h->pstats, h->pstats + Pd, h->pstats + 2 * Pd, P, h->d, dq, 1, X, mlp, X + kMlpMaxIn, s));
+    CK(launch_learned_seed_one(X + kMlpMaxIn, X, h->d, dq, margin, seed, &dh->cut, s));
+    d_seed = seed;
+  }
+  PartQuery pq{};
+  pq.qq = qq;
+  for (uint32_t m = 0; m < qq; m++) {
+    pq.attr[m] = attr[m];
+    pq.w[m] = weights[attr[m]];
+  }
+  CK(launch_part_order(h->pstats, h->pstats + (size_t)P * h->d, P, h->d, pq, c->d_plist, c->d_pkey, c->d_ptemp,
+                       c->ptemp_bytes, h->num_sms, s));
+  const uint32_t seed_host = std::isfinite(cut) ? host_f2key(cut) : 0u;
+  const bool seeded = learned || seed_host != 0u;
+  const uint64_t tiles_per_part = (1ull << h->part_log2) / 1024u;
+  uint64_t tiles = 0, scans = 0, accepted = 0;
+  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
+  float cut_seen = cut;
+  for (int round = 0; round < 2; round++) {
+    const bool use_seed = seeded && round == 0;
+    CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), s));
+    PartScan ps{c->d_plist, P, use_seed ? seed_host : 0u, c->d_pkey, use_seed ? d_seed : nullptr};
+    st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count, dh->stats,
+                      &ps);
+    if (st != TOPK_OK) return st;
+    CK(cudaMemcpyAsync(c->h_res, dr, kHdr + kk * 12, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hh->count > kk) {
+      ScanScratch sc{};
+      cudaMemcpy(&sc, c->scratch, sizeof(sc), cudaMemcpyDeviceToHost);
+      cudaMemset(c->scratch, 0, c->meta_bytes);
+      if (sc.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
+      return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
+    }
+    if (learned && round == 0) cut_seen = hh->cut;
+    tiles += hh->stats[2];
     scans++;
-    if (res.id.size() == kk) {
-      done = true;
+    if (!use_seed) break;
+    if (hh->count == kk) {
       accepted = 1;
+      break;
     }
   }
-  if (!done) {
-    std::vector<uint32_t> order(P);
-    for (uint32_t p = 0; p < P; p++) order[p] = p;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return ub[a] > ub[b]; });
-    // round 1: enough highest-bound partitions for k objects, and at least 1/32 of them
-    const uint64_t R = 1ull << h->part_log2;
-    uint32_t m1 = (uint32_t)std::min<uint64_t>(P, std::max<uint64_t>((kk + R - 1) / R + 1, (P + 31) / 32));
-    std::vector<uint32_t> l1(order.begin(), order.begin() + m1);
-    HostResult r1;
-    if ((st = scan_partitions(h, c, k, qq, weights, attr, l1, 0u, &r1)) != TOPK_OK) return st;
-    scanned += m1;
-    scans++;
-    if (r1.id.size() < kk) {  // the first round held fewer than k rows: scan everything else too
-      std::vector<uint32_t> rest(order.begin() + m1, order.end());
-      HostResult r2;
-      if ((st = scan_partitions(h, c, k, qq, weights, attr, rest, 0u, &r2)) != TOPK_OK) return st;
-      scanned += rest.size();
-      scans++;
-      res = r1;
-      res.key.insert(res.key.end(), r2.key.begin(), r2.key.end());
-      res.id.insert(res.id.end(), r2.id.begin(), r2.id.end());
-      res.score.insert(res.score.end(), r2.score.begin(), r2.score.end());
-    } else {
-      // k-th key of the first round; compared as keys, so a NaN k-th score (key 0,
-      // below every number) keeps every partition
-      const uint32_t t1 = host_f2key(r1.threshold);
-      std::vector<uint32_t> l2;
-      for (uint32_t j = m1; j < P; j++)
-        if (host_f2key(ub[order[j]]) >= t1) l2.push_back(order[j]);
-      HostResult r2;
-      if ((st = scan_partitions(h, c, k, qq, weights, attr, l2, t1, &r2)) != TOPK_OK) return st;
-      scanned += l2.size();
-      scans += l2.empty() ? 0 : 1;
-      res = r1;
-      res.key.insert(res.key.end(), r2.key.begin(), r2.key.end());
-      res.id.insert(res.id.end(), r2.id.begin(), r2.id.end());
-      res.score.insert(res.score.end(), r2.score.begin(), r2.score.end());
-    }
-  }
-  // top kk of the union by (key desc, id asc), written ascending like topk_query
-  std::vector<uint32_t> idx(res.id.size());
-  for (uint32_t j = 0; j < idx.size(); j++) idx[j] = j;
-  std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
-    return res.key[a] != res.key[b] ? res.key[a] > res.key[b] : res.id[a] < res.id[b];
-  });
-  const uint64_t cnt = std::min<uint64_t>(kk, idx.size());
-  for (uint64_t r = 0; r < cnt; r++) {
-    ids[cnt - 1 - r] = res.id[idx[r]];
-    scores[cnt - 1 - r] = res.score[idx[r]];
-  }
+  const uint32_t cnt = hh->count;
+  std::memcpy(ids, c->h_res + kHdr, (size_t)cnt * 8);
+  std::memcpy(scores, c->h_res + kHdr + kk * 8, (size_t)cnt * 4);
   if (count) *count = cnt;
-  if (threshold) *threshold = cnt ? res.score[idx[cnt - 1]] : 0.0f;
+  if (threshold) *threshold = hh->threshold;
+  if (cut_out) *cut_out = cut_seen;
   if (stats) {
-    stats[0] = scanned;
+    stats[0] = (tiles + tiles_per_part - 1) / tiles_per_part;
     stats[1] = P;
     stats[2] = accepted;
     stats[3] = scans;
   }
+  g_last_cands = hh->stats[0];
+  g_last_reductions = hh->stats[1];
   return TOPK_OK;
 }
 
@@ -609,7 +604,8 @@ int ensure(topk_table_s::DevBuf &b, size_t bytes) {
 void free_batch_buffers(topk_table_t h) {
   for (topk_table_s::DevBuf *b : {&h->b_q, &h->b_st, &h->b_best, &h->b_cand, &h->b_ids, &h->b_scores, &h->b_count,
                                   &h->b_thr, &h->xbf, &h->xbf_absmax, &h->b_abf, &h->b_err, &h->b_log,
-                                  &h->b_logh, &h->b_sw, &h->b_feat, &h->b_pred}) {
+                                  &h->b_logh, &h->b_sw, &h->b_feat, &h->b_pred, &h->b_abf_act, &h->b_amap,
+                                  &h->b_order}) {
     cudaFree(b->p);
     b->p = nullptr;
     b->bytes = 0;
@@ -647,37 +643,58 @@ int ensure_bf16_table(topk_table_t h, cudaStream_t s) {
   }
   int st;
   if ((st = ensure(h->xbf, bf16_table_bytes(h->n))) != TOPK_OK) return st;
-  if ((st = ensure(h->xbf_absmax, (size_t)h->d * 4)) != TOPK_OK) return st;
+  if ((st = ensure(h->xbf_absmax, (size_t)h->d * 12)) != TOPK_OK) return st;
   CK(launch_bf16_pack(h->table, h->ld, h->d, h->n, static_cast<uint8_t *>(h->xbf.p),
                       static_cast<uint32_t *>(h->xbf_absmax.p), h->num_sms, s));
-  std::vector<uint32_t> bits(h->d);
-  CK(cudaMemcpyAsync(bits.data(), h->xbf_absmax.p, (size_t)h->d * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<uint32_t> bits(3 * (size_t)h->d);
+  CK(cudaMemcpyAsync(bits.data(), h->xbf_absmax.p, bits.size() * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   h->absmax.assign(h->d, 0.0f);
+  h->colmax.assign(h->d, 0.0f);
+  h->colmin.assign(h->d, 0.0f);
   bool usable = true;
   for (uint32_t m = 0; m < h->d; m++) {
     float f;
     std::memcpy(&f, &bits[m], 4);
     if (!(f <= kBf16MaxAbs)) usable = false;  // also NaN / inf
     h->absmax[m] = f;
+    h->colmax[m] = host_key2f(bits[h->d + m]);      // NaN when the column holds no number
+    h->colmin[m] = host_key2f(bits[2 * h->d + m]);
   }
   h->xbf_usable = usable;
   h->xbf_version = h->data_version;
   return TOPK_OK;
 }
 
+// Key of an upper bound of every reference-order FP32 score of query b over the table:
+// the same sum, in the same order, over the column extremes (the max where the weight
+// is >= 0, the min where it is negative).  IEEE multiplication and addition round
+// monotonically, so no row's score exceeds it.  0xFFFFFFFF (no bound) when the sum is
+// NaN (an all-NaN column, or inf times a zero weight).
+uint32_t score_bound_key(const BatchQuery &b, const std::vector<float> &cmax, const std::vector<float> &cmin) {
+  float s = 0.0f;
+  for (uint32_t m = 0; m < b.qq; m++) {
+    const float w = b.w[m];
+    const float x = w >= 0.0f ? cmax[b.attr[m]] : cmin[b.attr[m]];
+    const float prod = x * w;
+    s = s + prod;
+  }
+  if (s != s) return 0xFFFFFFFFu;
+  return host_f2key(s);
+}
+
 // Per-query bound of the BF16 filter, rounded up to a float:
 // 2^-13 * sum_m |w_m| * absmax[attr_m] + 2^-100 * sum_m (|w_m| + absmax[attr_m]).
+// Summed in FP32: each sum of at most 32 nonnegative terms is within 33 * 2^-24 of
+// its exact value, so scaling by 1 + 2^-16 and rounding up keeps an upper bound.
 float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
-  double rel = 0, tiny = 0;
+  float rel = 0.0f, tiny = 0.0f;
   for (uint32_t m = 0; m < b.qq; m++) {
-    rel += std::fabs((double)b.w[m]) * (double)absmax[b.attr[m]];
-    tiny += std::fabs((double)b.w[m]) + (double)absmax[b.attr[m]];
+    rel += std::fabs(b.w[m]) * absmax[b.attr[m]];
+    tiny += std::fabs(b.w[m]) + absmax[b.attr[m]];
   }
-  const double e = std::ldexp(rel, -13) + std::ldexp(tiny, -100);
-  float f = (float)e;
-  if ((double)f < e) f = std::nextafter(f, INFINITY);
-  return f;
+  const float e = std::ldexp(rel, -13) * (1.0f + 0x1p-16f) + std::ldexp(tiny, -100) * (1.0f + 0x1p-16f);
+  return std::nextafter(e, INFINITY);
 }
 
 // Batched exact top-k on the handle's primary stream (caller holds batch_mu):
@@ -694,7 +711,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
   std::vector<BatchQuery> q(nq);
   uint64_t best_total = 0, cand_total = 0;
-  uint32_t kmax = 1, capmax = 1;
+  uint32_t kmax = 1, capmax = 1, qmax = 1;
   for (uint64_t j = 0; j < nq; j++) {
     BatchQuery &b = q[j];
     std::memset(&b, 0, sizeof(b));
@@ -709,8 +726,10 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       b.attr[m] = attrs[j * astride + m];
       b.w[m] = weights[j * wstride + b.attr[m]];
     }
+    b.maxkey = 0xFFFFFFFFu;
     kmax = std::max(kmax, b.k);
     capmax = std::max(capmax, b.cand_cap);
+    qmax = std::max(qmax, b.qq);
   }
   if (best_total > 0xFFFFFFFFull || cand_total > 0xFFFFFFFFull)
     return fail(TOPK_ERR_UNSUPPORTED, "batch too large: split it");
@@ -741,18 +760,21 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (use_bf16) {
     std::vector<uint8_t> habf(bf16_query_bytes((uint32_t)nq), 0);
     for (uint64_t j = 0; j < nq; j++) {
-      double acc[kBf16MaxD] = {0};
-      for (uint32_t m = 0; m < q[j].qq; m++) acc[q[j].attr[m]] += (double)q[j].w[m];
-      float a[kBf16MaxD];
-      for (uint32_t m = 0; m < kBf16MaxD; m++) a[m] = (float)acc[m];
+      // a[m] = the sum of the weights on attribute m (repeated attributes add up; FP32,
+      // within 2^-19 of the exact sum for <= 32 terms, well inside the filter's bound)
+      float a[kBf16MaxD] = {0.0f};
+      for (uint32_t m = 0; m < q[j].qq; m++) a[q[j].attr[m]] += q[j].w[m];
       bf16_pack_query(a, (uint32_t)j, habf.data());
       q[j].err = bf16_error_bound(q[j], h->absmax);
+      q[j].maxkey = score_bound_key(q[j], h->colmax, h->colmin);
     }
     if ((st = ensure(h->b_abf, habf.size())) != TOPK_OK) return st;
+    if ((st = ensure(h->b_abf_act, habf.size())) != TOPK_OK) return st;
+    if ((st = ensure(h->b_amap, (nq + 1) * sizeof(uint32_t))) != TOPK_OK) return st;
     if ((st = ensure(h->b_err, sizeof(uint32_t))) != TOPK_OK) return st;
-    // survivor records: one log per filter CTA (at most max(num_sms, query groups) CTAs)
+    // survivor records: one log per filter CTA
     const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms, h->batch_qt);
-    log_ctas = std::max<uint64_t>((uint64_t)h->num_sms, fp.ngroups);
+    log_ctas = fp.grid;
     if ((st = ensure(h->b_log, log_ctas * kBf16LogCap * 8 * sizeof(uint4))) != TOPK_OK) return st;
     if ((st = ensure(h->b_logh, log_ctas * kBf16LogCap * sizeof(uint2))) != TOPK_OK) return st;
     CK(cudaMemcpyAsync(h->b_abf.p, habf.data(), habf.size(), cudaMemcpyHostToDevice, s));
@@ -769,6 +791,22 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if ((st = ensure(h->b_thr, nq * sizeof(float))) != TOPK_OK) return st;
   if (!h->b_ev0) CK(cudaEventCreate(&h->b_ev0));
   if (!h->b_ev1) CK(cudaEventCreate(&h->b_ev1));
+  // the plain FP32 scorer takes the queries ordered by attribute count, then by
+  // attribute list: a warp's lanes then run the same number of steps and mostly read
+  // the same rows of the staged tile at each step (shared-memory broadcast)
+  uint32_t *dorder = nullptr;
+  if (!use_bf16) {
+    std::vector<uint32_t> order(nq);
+    for (uint32_t j = 0; j < (uint32_t)nq; j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+      if (q[a].qq != q[b].qq) return q[a].qq < q[b].qq;
+      return std::memcmp(q[a].attr, q[b].attr, q[a].qq) < 0;
+    });
+    if ((st = ensure(h->b_order, nq * sizeof(uint32_t))) != TOPK_OK) return st;
+    dorder = static_cast<uint32_t *>(h->b_order.p);
+    CK(cudaMemcpyAsync(dorder, order.data(), nq * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // `order` is pageable and goes out of scope
+  }
   BatchQuery *dq = static_cast<BatchQuery *>(h->b_q.p);
   BatchState *dst = static_cast<BatchState *>(h->b_st.p);
   uint2 *dbest = static_cast<uint2 *>(h->b_best.p);
@@ -820,18 +858,22 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     if (use_bf16) {
       const FilterPlan fp = plan_bf16_filter(nqq, r, e, h->num_sms, h->batch_qt);
       if (fp.grid > log_ctas) return fail(TOPK_ERR_STATE, "filter grid %llu above its logs", (unsigned long long)fp.grid);
-      CK(launch_bf16_filter(fp, static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf.p), r, e,
-                            dq, nqq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
+      // the queries still served by the filter, as compact tiles
+      uint32_t *amap = static_cast<uint32_t *>(h->b_amap.p);
+      CK(launch_batch_active(dq, dst, nqq, static_cast<const uint8_t *>(h->b_abf.p),
+                             static_cast<uint8_t *>(h->b_abf_act.p), amap, amap + nq, s));
+      CK(launch_bf16_filter(fp, static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf_act.p),
+                            amap, amap + nq, r, e, dq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
                             static_cast<uint2 *>(h->b_logh.p), kBf16LogCap, h->wait_limit,
                             static_cast<uint32_t *>(h->b_err.p), s));
       // this chunk for every moved query; the previous one again for those that discarded it
-      CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, r, e, dq, dst, dcand, dsw + 2, dsw, nullptr, dwork,
-                                      h->num_sms, s));
+      CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, r, e, dq, dst, dcand, dsw + 2, dsw, nullptr, dwork, qmax,
+                                      true, h->num_sms, s));
       CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, prev_r, r, dq, dst, dcand, dsw + 2 + nq, dsw + 1,
-                                      dredo, dwork, h->num_sms, s));
+                                      dredo, dwork, qmax, true, h->num_sms, s));
       CK(launch_copy_word(dredo, dsw + 1, s));
     } else {
-      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, nullptr, s));
+      CK(launch_batch_score_fp32(h->table, h->ld, h->d, r, e, dq, nqq, dst, dcand, dorder, qmax, false, s));
     }
     CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
     prev_r = r;
@@ -839,7 +881,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   }
   if (use_bf16) {  // the last chunk again for the queries that discarded it (none: two empty launches)
     CK(launch_batch_score_fp32_list(h->table, h->ld, h->d, prev_r, h->n, dq, dst, dcand, dsw + 2 + nq, dsw + 1,
-                                    dredo, dwork, h->num_sms, s));
+                                    dredo, dwork, qmax, true, h->num_sms, s));
     CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
   }
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
@@ -851,11 +893,11 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   // pointer and scalar the captured launches take (a buffer that grew or a new model
   // margin makes a new shape).  The graph reads the query descriptors and states that
   // the stream uploaded and cleared before it.
-  std::vector<uint64_t> key = {nq, kmax, capmax, use_bf16, use_learned, h->n, h->d, h->ld, boot,
+  std::vector<uint64_t> key = {nq, kmax, capmax, qmax, use_bf16, use_learned, h->n, h->d, h->ld, boot,
                                (uint64_t)h->num_sms, log_ctas, h->wait_limit, h->num_parts, h->batch_qt};
   const void *key_ptrs[] = {h->table, dq, dst, dbest, dcand, h->b_ids.p, h->b_scores.p, h->b_count.p,
                             h->b_thr.p, h->xbf.p, h->b_abf.p, h->b_log.p, h->b_logh.p, h->b_err.p, h->b_sw.p,
-                            h->b_feat.p, h->b_pred.p, h->pstats, h->mlp};
+                            h->b_feat.p, h->b_pred.p, h->pstats, h->mlp, h->b_abf_act.p, h->b_amap.p, dorder};
   for (const void *ptr : key_ptrs) key.push_back((uint64_t)(uintptr_t)ptr);
   {
     uint32_t mb;
@@ -918,7 +960,10 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   if (use_bf16) CK(cudaMemcpyAsync(hsw, dsw, sizeof(hsw), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
-  uint64_t switched_total = hsw[0];
+  uint64_t switched_total = hsw[0], retired_total = 0;
+  if (use_bf16)
+    for (uint64_t j = 0; j < nq; j++)
+      if (!(hst[j].flags & kFlagFp32) && hst[j].thr != 0u && hst[j].thr > q[j].maxkey) ++retired_total;
   for (uint64_t j = 0; j < nq; j++) {  // queries answered again below overwrite theirs
     const uint32_t c = std::min<uint32_t>(hcnt[j], (uint32_t)std::min<uint64_t>(kmax, kstride));
     std::memcpy(ids + j * kstride, hid + j * kmax, (size_t)c * 8);
@@ -971,6 +1016,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     misses_total += h->last_batch_learned_misses;
     scans += h->last_batch_fallbacks;
     switched_total += h->last_batch_switched;
+    retired_total += h->last_batch_retired;
     return TOPK_OK;
   };
   std::vector<uint64_t> sub;
@@ -1006,6 +1052,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   h->last_batch_learned_misses = misses_total;
   h->last_batch_fallbacks = scans;
   h->last_batch_switched = switched_total;
+  h->last_batch_retired = retired_total;
   h->last_batch_method = use_learned ? TOPK_BATCH_LEARNED : use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
   return TOPK_OK;
 }
@@ -1379,6 +1426,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
   h->last_batch_ms = 0;
   h->last_batch_fallbacks = 0;
   h->last_batch_switched = 0;
+  h->last_batch_retired = 0;
   h->last_batch_cands = 0;
   h->last_batch_err_ratio = 0;
   h->last_batch_learned_misses = 0;
@@ -1493,6 +1541,12 @@ int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uin
   return TOPK_OK;
 }
 
+int topk_last_batch_retired(topk_table_t h, uint64_t *retired) {
+  if (!h || !retired) return fail(TOPK_ERR_ARG, "null argument");
+  *retired = h->last_batch_retired;
+  return TOPK_OK;
+}
+
 int topk_last_batch_switched(topk_table_t h, uint64_t *switched) {
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   std::lock_guard<std::mutex> lk(h->batch_mu);
@@ -1562,9 +1616,9 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
       return f;
     };
     const float mx = k2f(w[(size_t)m * kMinmaxWords]), mn = k2f(w[(size_t)m * kMinmaxWords + 1]);
-    const double range = (double)mx - (double)mn;
+    const float range = mx - mn;  // only decides the order of the rows, never a result
     lo_scale[m] = std::isfinite(mn) ? mn : 0.0f;
-    lo_scale[h->d + m] = (range > 0 && std::isfinite(range)) ? (float)(std::ldexp(1.0, (int)bits) / range) : 0.0f;
+    lo_scale[h->d + m] = (range > 0.0f && std::isfinite(range)) ? std::ldexp(1.0f, (int)bits) / range : 0.0f;
   }
   // release an older copy first (its memory may be needed)
   cudaFree(h->ptable);
@@ -1655,7 +1709,7 @@ int topk_query_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
                       uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats) {
   g_last_error.clear();
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
-  return run_pruned(h, k, qq, weights, attr, cut, ids, scores, count, threshold, stats);
+  return run_pruned(h, k, qq, weights, attr, cut, false, ids, scores, count, threshold, stats, nullptr);
 }
 
 }  // extern "C"
@@ -1727,8 +1781,8 @@ float query_scale(const BatchQuery &b) {
 // Training target of a query: qq * ln(gap / S), gap = largest bound - k-th score,
 // at least 1e-9 S (the largest bound bounds every score, so gap >= 0 up to rounding).
 float learned_target(float kth, float b1s, float S, uint32_t qq) {
-  const double g = std::max((double)b1s - (double)kth / (double)S, 1e-9);
-  return (float)((double)qq * std::log(g));
+  const float g = std::max(b1s - kth / S, 1e-9f);
+  return (float)qq * std::log(g);
 }
 
 int check_features_ready(topk_table_t h) {
@@ -2072,32 +2126,7 @@ extern "C" int topk_query_learned(topk_table_t h, uint64_t k, uint32_t qq, const
                        float *cut_out) {
   g_last_error.clear();
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
-  int st = check_query(h, k, qq, weights, attr);
-  if (st != TOPK_OK) return st;
-  if (qq > kBatchMaxQ) return fail(TOPK_ERR_UNSUPPORTED, "the learned path supports qq <= %u", kBatchMaxQ);
-  float cut = NAN;
-  {
-    std::lock_guard<std::mutex> lk(h->learned_mu);
-    if (!h->mlp || h->mlp_part_version != h->part_version || h->part_version != h->data_version)
-      return fail(TOPK_ERR_STATE, "no learned model for the current partitions");
-    DeviceGuard dg(h->device);
-    if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
-    const uint64_t k1 = k;
-    std::vector<BatchQuery> q = pack_queries(h, 1, &k1, &qq, weights, 0, attr, 0);
-    const size_t P = h->num_parts, d = h->d;
-    cudaStream_t s = h->primary->stream;
-    CK(cudaMemcpyAsync(h->lq_query, q.data(), sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
-    CK(launch_features(h->pstats, h->pstats + P * d, h->pstats + 2 * P * d, h->num_parts, h->d, h->lq_query, 1,
-                       h->lq_out, h->mlp, h->lq_out + kMlpMaxIn, s));
-    float out[kMlpMaxIn + 1];
-    CK(cudaMemcpyAsync(out, h->lq_out, sizeof(out), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    const float c =
-        learned_cut(out[kMlpMaxIn], out[feature_bound_col(h->d)], query_scale(q[0]), (float)qq, h->mlp_margin);
-    if (std::isfinite(c)) cut = c;
-  }
-  if (cut_out) *cut_out = cut;
-  return run_pruned(h, k, qq, weights, attr, cut, ids, scores, count, threshold, stats);
+  return run_pruned(h, k, qq, weights, attr, NAN, true, ids, scores, count, threshold, stats, cut_out);
 }
 
 extern "C" {

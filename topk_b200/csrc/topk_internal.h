@@ -26,7 +26,8 @@ struct ScanScratch {
   // Diagnostics of a TOPK_BOUNDS_CHECK build: first failed check (code, block,
   // tile, two values); the access it guarded was skipped.
   uint32_t diag[5];
-  uint32_t pad[6];
+  uint32_t acc_tiles;       // tiles scanned during this scan (partition mode)
+  uint32_t pad[5];
 };
 
 // TOPK_BOUNDS_CHECK codes
@@ -68,15 +69,22 @@ struct ScanParams {
   float *out_scores;
   float *out_threshold; // may be null
   uint32_t *out_count;  // may be null
-  uint32_t *out_stats;  // may be null: [0] entries merged at the root, [1] block-selects
+  uint32_t *out_stats;  // may be null: [0] entries merged at the root, [1] block-selects,
+                        // [2] tiles scanned (partition mode)
   // Partition mode (part_list != null): tile t covers rows
   //   part_list[t >> part_shift] << part_rows_log2  +  (t & ((1 << part_shift) - 1)) * tile
   // instead of tile_begin + t * tile; rows stay within [row_begin, row_end).
   const uint32_t *part_list;
+  // May be null.  part_key[i] = order key of an upper bound of every score in partition
+  // part_list[i], non-increasing in i: a CTA stops at its first tile whose bound is
+  // below its threshold (every later tile of that CTA is bounded lower still) -- the
+  // reference's stop rule (cpu/VTA.h:210-216, cpu/PTA.h:636-641) per partition.
+  const uint32_t *part_key;
   uint32_t part_shift;      // log2(tiles per partition)
   uint32_t part_rows_log2;  // log2(rows per partition)
   const uint32_t *row_ids;  // may be null: id of each row (a reordered table's original ids)
   uint32_t thr_seed;        // objects need key >= thr_seed from the start (0: none)
+  const uint32_t *thr_seed_dev;  // may be null: a further seed read from device memory at start
   uint8_t attr[kMaxQ];
   float w[kMaxQ];       // weights[attr[m]], gathered on the host
 };
@@ -153,6 +161,23 @@ int skyline_layers_device(const float *table, uint64_t ld, uint32_t d, uint64_t 
                           uint64_t *num_layers, std::string *msg);
 cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
                                float *ptable, int num_sms, cudaStream_t s);
+// One query's attributes and gathered weights, for partition bounds.
+struct PartQuery {
+  uint32_t qq;
+  uint8_t attr[kMaxQ];
+  float w[kMaxQ];  // weights[attr[m]]
+};
+// Partitions in descending order of the query's bound (the reference-order FP32 sum
+// over each partition's per-attribute max, or min for negative weights: an exact upper
+// bound of its rows' scores), ties by the lower partition number: plist[i] = partition,
+// pkey[i] = order key of its bound (0xFFFFFFFF for a NaN bound).  Up to
+// kPartOrderOneBlock partitions one block sorts them in shared memory; above, a radix
+// sort uses `temp` (part_order_temp_bytes(P) bytes).
+constexpr uint32_t kPartOrderOneBlock = 16384;
+size_t part_order_temp_bytes(uint32_t P);
+cudaError_t launch_part_order(const float *pmin, const float *pmax, uint32_t P, uint32_t d, const PartQuery &q,
+                              uint32_t *plist, uint32_t *pkey, void *temp, size_t temp_bytes, int num_sms,
+                              cudaStream_t s);
 // Per-partition min / max / mean of each attribute, [num_parts][d] each.
 cudaError_t launch_partition_stats(const float *ptable, uint64_t ld, uint32_t d, uint64_t n, uint32_t rows_log2,
                                    uint32_t num_parts, float *mins, float *maxs, float *means, cudaStream_t s);

@@ -47,6 +47,9 @@ Multi-GPU (torchrun): every rank holds its own replica and runs the same query
 steps (weak scaling, no collective on the data path); time = max over ranks.  The
 one-GPU secondary sections (pruned, loader, ta) run only when the job has one rank.
 
+`--sharded` times object-sharded single queries instead: the table split over the
+GPUs, one NCCL all_gather and a device merge per query (strong scaling).
+
 `--impl reference` runs the reference's own CPU TPAc on the host (rank 0 only).
 """
 import argparse
@@ -634,6 +637,59 @@ def run_ta(T, device, n=1 << 26, d=8, n_test=200, sample_rows=1 << 20, seed=8):
     return out
 
 
+def run_sharded(args, T, torch, dist, world, rank, local):
+    """Object-sharded single queries (strong scaling): the 2^28 x 16 table split into
+    world row ranges, one per GPU; each query scans the rank's rows
+    (Table.query_range_device into its exchange record), all_gathers the records over
+    NCCL and merges them on the device (topk_merge_lists) -- topk_b200/shard.py.  Time
+    = CUDA events around each step on the ranks' query stream, max over ranks."""
+    from topk_b200 import shard
+    n, d = args.n, args.d
+    queries = the_queries(d)
+    r0, r1 = shard.shard_rows(n, rank, world)
+    table = T.Table(r1 - r0, d, device=local)
+    table.generate(T.DIST_INDEPENDENT, rank)  # each shard its own seeded rows (timing only)
+    table.normalize()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def step():
+        for k, q, w, a in queries:
+            shard.sharded_query(table, n, k, w, a, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    table.close()
+    ms_per_step = ms / args.steps
+    return {
+        "metric": METRIC, "value": len(queries) * 1000.0 / ms_per_step, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded independent U[0,1) rows per shard, generated on each device, normalised",
+        "config": {"workload": "object-sharded single-query exact top-k, n=2^28 x d=16 split into row ranges over "
+                               "the GPUs, 16 queries/step (q in {2,4,8,16} x k in {16,64,256,1024}); per query: "
+                               "local fused scan, one NCCL all_gather of the k-entry records, device merge",
+                   "n": n, "d": d, "rows_per_gpu": r1 - r0, "parallelism": f"object shards x{world}"},
+        "gpu_launches": args.steps * len(queries) * 2,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -652,6 +708,8 @@ def main():
     ap.add_argument("--c5-q", type=int, default=C5_Q)
     ap.add_argument("--c5-methods", default="fp32,bf16,learned_bf16")
     ap.add_argument("--batched-methods", default="fp32,bf16,learned_bf16")
+    ap.add_argument("--sharded", action="store_true",
+                    help="object-sharded single queries over all GPUs (strong scaling) instead of replicas")
     ap.add_argument("--no-pruned", action="store_true")
     ap.add_argument("--no-loader", action="store_true")
     ap.add_argument("--no-ta", action="store_true")
@@ -689,10 +747,28 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
+    if world > 1 or args.sharded:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if world > 1:
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        else:  # a one-rank group: the sharded path's collective and merge still run
+            import socket
+            sk = socket.socket()
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+            sk.close()
+            dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                    timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    if args.sharded:
+        result = run_sharded(args, T, torch, dist, world, rank, local)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(result))
+        return 0
 
     n, d = args.n, args.d
     queries = the_queries(d)

@@ -185,6 +185,30 @@ int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
                       const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_threshold,
                       void *stream);
 
+/* topk_query_device over rows [row_begin, row_end) only (one shard of the objects):
+ * d_ids/d_scores receive min(k, row_end - row_begin) entries with global ids.  No
+ * reference counterpart: the device-side per-shard step of an object-sharded query
+ * (topk_b200/shard.py), whose lists topk_merge_lists combines. */
+int topk_query_range_device(topk_table_t h, uint64_t row_begin, uint64_t row_end, uint64_t k, uint32_t qq,
+                            const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores,
+                            float *d_threshold, void *stream);
+
+/* Merge per-shard top-k lists on the device (one block, exact): list j starts at
+ * d_lists + j * 12 * stride bytes and holds ids[stride] (uint64) then scores[stride]
+ * (float); its first counts[j] entries are valid, and id_base[j] (host array, may be
+ * NULL for all zero) is added to its ids -- a shard table numbers its rows from 0.
+ * The best min(k, sum of counts) of the union -- score descending, ties to the lower
+ * global id, the engine's order -- go to d_ids / d_scores ascending like every result,
+ * the k-th score to d_threshold (may be NULL), their number to *kept.  Enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) on CUDA device
+ * `device`.  nlists <= 64, k and stride <= TOPK_MAX_K, global ids < 2^32 - 1.
+ * Replaces the merge of the per-thread heaps in TPAc::findTopKthreads
+ * (cpu/TPAc.h:335-346) for shards held by different GPUs (the lists arrive by one
+ * all_gather). */
+int topk_merge_lists(int device, const void *d_lists, uint32_t nlists, uint64_t stride, const uint64_t *counts,
+                     const uint64_t *id_base, uint64_t k, uint64_t *d_ids, float *d_scores, float *d_threshold,
+                     uint64_t *kept, void *stream);
+
 /* The same exact top-k as topk_query_device, for callers that must not allocate GPU
  * memory: no handle, no cudaMalloc/cudaFree, nothing from an allocating library.
  * It serves host applications that own the whole device memory budget and hand it

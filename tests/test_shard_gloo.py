@@ -1,15 +1,20 @@
-"""CPU, world size 2 (gloo): the object-sharded query path.
+"""CPU, world size 2 (gloo): the exchange step of the object-sharded query.
 
-Each rank computes the exact top-k of its row shard (the oracle stands in for the
-per-GPU `Table.query(..., row_begin, row_end)` call, which returns global ids), the
-ranks all_gather and merge, and every rank must hold the single-process answer
-bit-for-bit, ties included.
+Each rank fills its exchange record (topk_b200/shard.py layout: ids then scores) with
+the exact top-k of its row shard -- the oracle stands in for the per-GPU
+`Table.query_range_device` call -- and the ranks run the product's `exchange`
+(all_gather_into_tensor of the records).  Every rank must then hold every rank's
+record byte for byte, and the best k of the gathered lists (score descending, lower
+id first: the merge kernel's order, restated here in numpy) must be the
+single-process answer bit for bit, ties included.  The device merge kernel itself
+runs in tests/test_gpu_shard.py.
 """
 import os
 import socket
 
 import numpy as np
 import pytest
+import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
@@ -22,6 +27,26 @@ def _free_port():
     port = s.getsockname()[1]
     s.close()
     return port
+
+
+def _keys(scores):
+    s = np.asarray(scores, np.float32)
+    u = s.view(np.uint32)
+    k = np.where(u & np.uint32(0x80000000), ~u, u | np.uint32(0x80000000)).astype(np.uint32)
+    return np.where(np.isnan(s), np.uint32(0), k)
+
+
+def merge_reference(records, counts, k, stride=None):
+    """The merge kernel's order on the host (test checker): best k by (key, -id)."""
+    stride = k if stride is None else stride
+    ids, sc = [], []
+    for rec, c in zip(records, counts):
+        ids.append(rec[: 8 * stride].view(np.uint64)[:c])
+        sc.append(rec[8 * stride: 12 * stride].view(np.float32)[:c])
+    ids, sc = np.concatenate(ids), np.concatenate(sc)
+    comp = (_keys(sc).astype(np.uint64) << np.uint64(32)) | (np.uint64(0xFFFFFFFF) - ids)
+    order = np.argsort(comp, kind="stable")[::-1][:k][::-1]
+    return ids[order], sc[order]
 
 
 def _worker(rank, world, port, results):
@@ -40,17 +65,24 @@ def _worker(rank, world, port, results):
             a = np.array(attr, np.uint8)
             r0, r1 = shard.shard_rows(n, rank, world)
             ids, sc, _ = O.topk_numpy(t, k, w, a, row0=r0, row1=r1)  # global ids
-            merged = shard.sharded_query((ids, sc), k)
+            rec = torch.zeros(shard.record_bytes(k), dtype=torch.uint8)
+            vi, vs = shard.record_views(rec, k)
+            vi[: len(ids)] = torch.from_numpy(ids.astype(np.int64))
+            vs[: len(sc)] = torch.from_numpy(sc)
+            got = shard.exchange(rec).numpy()
+            counts = shard.list_counts(n, world, k)
+            ok = got.shape == (world, shard.record_bytes(k)) and np.array_equal(got[rank], rec.numpy())
+            mids, msc = merge_reference(got, counts, k)
             want = O.topk_numpy(t, k, w, a)
-            out.append(bool(np.array_equal(merged[0], want[0]) and
-                            np.array_equal(merged[1].view(np.uint32), want[1].view(np.uint32))))
+            out.append(bool(ok and np.array_equal(mids, want[0]) and
+                            np.array_equal(msc.view(np.uint32), want[1].view(np.uint32))))
         results[rank] = all(out)
     finally:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def test_sharded_query_world_size_2():
+def test_sharded_exchange_world_size_2():
     world = 2
     ctx = mp.get_context("spawn")
     manager = ctx.Manager()
@@ -67,11 +99,16 @@ def test_sharded_query_world_size_2():
     assert dict(results) == {0: True, 1: True}
 
 
-def test_merge_and_shard_rows_helpers():
+def test_shard_rows_and_record_layout():
     assert [shard.shard_rows(10, r, 3) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
-    a = (np.array([5, 1], np.uint64), np.array([1.0, 2.0], np.float32))
-    b = (np.array([3, 0], np.uint64), np.array([2.0, 0.5], np.float32))
-    ids, sc, th = shard.merge_topk([a, b], 3)
-    assert ids.tolist() == [5, 3, 1] and sc.tolist() == [1.0, 2.0, 2.0] and th == 1.0
-    ids, sc, th = shard.merge_topk([a, b], 10)
-    assert ids.tolist() == [0, 5, 3, 1]
+    assert shard.list_counts(10, 3, 3).tolist() == [3, 3, 3]
+    assert shard.list_counts(10, 3, 5).tolist() == [4, 3, 3]
+    rec = torch.zeros(shard.record_bytes(4), dtype=torch.uint8)
+    ids, sc = shard.record_views(rec, 4)
+    ids[:] = torch.tensor([5, 1, 3, 0])
+    sc[:] = torch.tensor([1.0, 2.0, 2.0, 0.5])
+    r = rec.numpy()
+    assert r[:32].view(np.uint64).tolist() == [5, 1, 3, 0]
+    assert r[32:48].view(np.float32).tolist() == [1.0, 2.0, 2.0, 0.5]
+    mids, msc = merge_reference([r], [4], 3, stride=4)
+    assert mids.tolist() == [5, 3, 1] and msc.tolist() == [1.0, 2.0, 2.0]

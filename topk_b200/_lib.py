@@ -73,6 +73,10 @@ SIGNATURES = [
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
     ("topk_query_device", C.c_int, [_H, C.c_uint64, C.c_uint32, _f32p, _u8p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]),
+    ("topk_query_range_device", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, _f32p, _u8p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("topk_merge_lists", C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint64, _u64p, _u64p, C.c_uint64,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p]),
     ("topk_query_batch", C.c_int, [_H, C.c_uint64, _u64p, _u32p, _f32p, C.c_uint64, _u8p, C.c_uint64, _u64p, _f32p,
                                    C.c_uint64, C.c_void_p, C.c_void_p]),
     ("topk_build_partitions", C.c_int, [_H, C.c_uint32]),

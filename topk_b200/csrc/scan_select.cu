@@ -167,8 +167,9 @@ __device__ __forceinline__ float4 score_cols(const ScanParams &p, const float4 *
 // thread too few bytes in flight otherwise).
 constexpr int kPrefetchQ = 4;
 
-// QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).
-template <int QQ>
+// QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).  PART: partition
+// mode (p.part_list set): tiles of listed partitions of a reordered copy.
+template <int QQ, bool PART>
 __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + kOffCtl);
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   // tiles loaded ahead of the one being scored (two ahead for q <= 2 measured slower:
   // the extra registers cost a CTA per SM)
   constexpr int kDepth = 1;
-  const bool prefetch = QQ >= 1 && QQ <= kPrefetchQ && p.part_list == nullptr;
+  constexpr bool prefetch = QQ >= 1 && QQ <= kPrefetchQ && !PART;
   // queried columns: computed once for q >= 3; for q <= 2 per tile (two more 64-bit
   // registers would cost a CTA per SM there, measured slower)
   constexpr bool kHoist = kPQ >= 3;
@@ -238,15 +239,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   }
   // partition mode: the partition of the next tile (and its bound) is loaded one tile ahead
   const uint32_t pmask = (1u << p.part_shift) - 1u;
-  uint32_t part_next = (p.part_list && my_tiles) ? __ldg(p.part_list + (blockIdx.x >> p.part_shift)) : 0u;
-  uint32_t key_next = (p.part_key && my_tiles) ? __ldg(p.part_key + (blockIdx.x >> p.part_shift)) : 0xFFFFFFFFu;
-  uint32_t tiles_done = 0;
-  for (uint32_t i = 0; i < my_tiles; ++i) {
+  uint32_t part_next = 0, key_next = 0xFFFFFFFFu;
+  if (PART && my_tiles) {
+    part_next = __ldg(p.part_list + (blockIdx.x >> p.part_shift));
+    if (p.part_key) key_next = __ldg(p.part_key + (blockIdx.x >> p.part_shift));
+  }
+  uint32_t i = 0;  // after the loop: the tiles this CTA scanned
+  for (; i < my_tiles; ++i) {
     const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
     // every thread reads the same thresholds here (see SmemCtl::thr_g)
     const uint32_t thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
     uint64_t tile0;
-    if (p.part_list) {
+    if constexpr (PART) {
       // nothing in this partition (nor in any later one of this CTA) can reach thr
       if (key_next < thr) break;
       tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
@@ -258,7 +262,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     } else {
       tile0 = p.tile_begin + tix * kTile;
     }
-    ++tiles_done;
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
     float4 s;
@@ -315,14 +318,16 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
           ++base;
         }
     }
-    // thread 0 hands the next tile its copy of the global threshold (see SmemCtl::thr_g):
-    // it loads the global word every 8 tiles and applies it 7 tiles later, so the L2
-    // round trip is never waited on
+    // thread 0 hands the CTA its copy of the global threshold (see SmemCtl::thr_g): it
+    // loads the global word every 8 tiles and applies it 7 tiles later, so the L2 round
+    // trip is never waited on.  The new value goes to the slot the next tile reads, and
+    // on the tile after into the other slot too; between updates both slots agree.
     if (t == 0) {
-      uint32_t g = ctl->thr_g[i & 1u];
-      if ((i & 7u) == 7u) g = max(g, g_pending);
-      ctl->thr_g[(i + 1u) & 1u] = g;
-      if ((i & 7u) == 0u) g_pending = ld_volatile_u32(&p.scratch->g_thr);
+      if ((i & 7u) == 7u) ctl->thr_g[(i + 1u) & 1u] = max(ctl->thr_g[i & 1u], g_pending);
+      if ((i & 7u) == 0u) {
+        ctl->thr_g[(i + 1u) & 1u] = ctl->thr_g[i & 1u];
+        g_pending = ld_volatile_u32(&p.scratch->g_thr);
+      }
     }
     if (__syncthreads_or(after > cap - kTile)) {
       if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     bsync();
   }
   if (t == 0 && ctl->reductions) atomicAdd(&p.scratch->acc_reductions, ctl->reductions);
-  if (t == 0 && p.part_list) atomicAdd(&p.scratch->acc_tiles, tiles_done);
+  if (PART && t == 0) atomicAdd(&p.scratch->acc_tiles, i);
 
   // ---- merge tree ----
   const uint32_t k = p.k;
@@ -445,6 +450,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   if (t == 0) {
     if (p.out_threshold) *p.out_threshold = res_n ? key2f(res[res_n - 1].x) : 0.0f;
     if (p.out_count) *p.out_count = res_n;
+    if (p.out_kth_key) *p.out_kth_key = res_n == k ? res[res_n - 1].x : 0u;
     const uint32_t reds = ld_volatile_u32(&p.scratch->acc_reductions);
     const uint32_t tiles = ld_volatile_u32(&p.scratch->acc_tiles);
     p.scratch->last_cands = merged;
@@ -463,28 +469,32 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
 
 using ScanKernel = void (*)(ScanParams);
 
-// [q] for q = 1..16; [0] is the runtime-q kernel used for q > 16
-const ScanKernel kKernels[17] = {
-    scan_select_kernel<0>,  scan_select_kernel<1>,  scan_select_kernel<2>,  scan_select_kernel<3>,
-    scan_select_kernel<4>,  scan_select_kernel<5>,  scan_select_kernel<6>,  scan_select_kernel<7>,
-    scan_select_kernel<8>,  scan_select_kernel<9>,  scan_select_kernel<10>, scan_select_kernel<11>,
-    scan_select_kernel<12>, scan_select_kernel<13>, scan_select_kernel<14>, scan_select_kernel<15>,
-    scan_select_kernel<16>};
+// [part][q] for q = 1..16; [part][0] is the runtime-q kernel used for q > 16
+#define TOPK_SCAN_ROW(P)                                                                                \
+  {scan_select_kernel<0, P>,  scan_select_kernel<1, P>,  scan_select_kernel<2, P>,  scan_select_kernel<3, P>,  \
+   scan_select_kernel<4, P>,  scan_select_kernel<5, P>,  scan_select_kernel<6, P>,  scan_select_kernel<7, P>,  \
+   scan_select_kernel<8, P>,  scan_select_kernel<9, P>,  scan_select_kernel<10, P>, scan_select_kernel<11, P>, \
+   scan_select_kernel<12, P>, scan_select_kernel<13, P>, scan_select_kernel<14, P>, scan_select_kernel<15, P>, \
+   scan_select_kernel<16, P>}
+const ScanKernel kKernels[2][17] = {TOPK_SCAN_ROW(false), TOPK_SCAN_ROW(true)};
+#undef TOPK_SCAN_ROW
 
-ScanKernel kernel_for(uint32_t qq) { return kKernels[qq <= 16 ? qq : 0]; }
+ScanKernel kernel_for(uint32_t qq, bool part) { return kKernels[part ? 1 : 0][qq <= 16 ? qq : 0]; }
 
 }  // namespace
 
 cudaError_t scan_set_attributes(size_t smem_optin) {
-  for (ScanKernel f : kKernels) {
-    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(f),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_optin);
-    if (e != cudaSuccess) return e;
-  }
+  for (const auto &row : kKernels)
+    for (ScanKernel f : row) {
+      const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(f),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_optin);
+      if (e != cudaSuccess) return e;
+    }
   return cudaSuccess;
 }
 
-ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin, uint32_t max_ctas_per_sm) {
+ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin, uint32_t max_ctas_per_sm,
+                   bool part) {
   ScanPlan pl{};
   pl.tile = kTile;
   uint32_t P = 1;
@@ -509,7 +519,7 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   pl.smem = kScanSmemFixed + (size_t)mcap * 8;
   pl.stages = pl.smem <= smem_optin ? 1u : 0u;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reinterpret_cast<const void *>(kernel_for(qq)),
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reinterpret_cast<const void *>(kernel_for(qq, part)),
                                                     kScanThreads, pl.smem) != cudaSuccess || occ < 1)
     occ = 1;
   if (max_ctas_per_sm >= 1 && (uint32_t)occ > max_ctas_per_sm) occ = (int)max_ctas_per_sm;
@@ -544,7 +554,7 @@ void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *tot
 
 cudaError_t launch_scan(const ScanPlan &pl, const ScanParams &p, cudaStream_t stream) {
   if (pl.stages < 1) return cudaErrorInvalidValue;
-  kernel_for(p.qq)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
+  kernel_for(p.qq, p.part_list != nullptr)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
   return cudaGetLastError();
 }
 

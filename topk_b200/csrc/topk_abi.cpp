@@ -309,6 +309,7 @@ struct PartScan {
   uint32_t seed;           // objects need key >= seed (0: none)
   const uint32_t *d_key;   // bound key of each listed partition (null: no stop rule)
   const uint32_t *d_seed;  // a further seed in device memory (null: none)
+  uint32_t *d_kth;         // receives the k-th key when k objects were found, else 0 (may be null)
 };
 
 // Enqueue one fused scan over rows [r0, r1) (or over the partitions of `ps`)
@@ -317,7 +318,7 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
                  const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores, float *d_thr,
                  uint32_t *d_count, uint32_t *d_stats = nullptr, const PartScan *ps = nullptr) {
   const uint64_t rows = ps ? ((uint64_t)ps->count << h->part_log2) : r1 - r0;
-  ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin, h->max_ctas_per_sm);
+  ScanPlan pl = plan_scan(qq, (uint32_t)k, rows, h->num_sms, h->smem_optin, h->max_ctas_per_sm, ps != nullptr);
   if (pl.stages < 1) return fail(TOPK_ERR_UNSUPPORTED, "qq=%u, k=%llu do not fit in shared memory", qq, (unsigned long long)k);
   // keep the merge tree's slot entries (< (2 * grid + levels) * k) within the context budget
   const uint64_t max_grid_k = (c->slot_entries / k - (uint64_t)kMaxLevels) / 2;
@@ -349,6 +350,7 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     p.thr_seed = ps->seed;
     p.part_key = ps->d_key;
     p.thr_seed_dev = ps->d_seed;
+    p.out_kth_key = ps->d_kth;
     tiles = (uint64_t)ps->count << p.part_shift;
     if (tiles > 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "too many tiles");
   }
@@ -459,19 +461,24 @@ float host_key2f(uint32_t k) {
 std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs,
                                      const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride);
 
-// Exact top-k over the partitioned copy in one device pipeline on the context's
-// stream: a kernel orders the partitions by the query's bound (the reference-order
-// FP32 sum over each partition's extremes: an exact upper bound of its scores) and one
-// fused scan walks them in that order, each CTA stopping at its first partition whose
-// bound is below its running threshold -- the reference's stop rule per block
-// (cpu/VTA.h:210-216, cpu/PTA.h:636-641).  The scan's merge tree gives the result;
-// nothing is decided on the host between the launches.  With a seed (a predicted
-// lower bound of the k-th score: `cut`, or the learned model's cut computed on the
-// device), objects and partitions below it are left out from the start; the result
-// is accepted when it holds min(k, n) objects (then the true k-th score is at least
-// the seed, so every object of the true top-k was scanned), otherwise the same scan
-// runs again without the seed.  stats: partitions scanned (tiles scanned / tiles per
-// partition, over both scans), partitions, seed accepted (1/0), scans.
+// Exact top-k over the partitioned copy as one device pipeline on the context's
+// stream; nothing is decided on the host between the launches.
+//   1. A kernel orders the partitions by the query's bound (the reference-order FP32
+//      sum over each partition's extremes: an exact upper bound of its scores).
+//   2. Round 1 scans the first partitions of that order, about one wave of CTAs (and
+//      enough rows for k), and leaves its k-th key t1 in device memory: the k-th score
+//      of a subset, a lower bound of the true k-th.
+//   3. Round 2 scans the partitions in the same order seeded with t1 (ties at t1 kept),
+//      each CTA stopping at its first partition whose bound is below its running
+//      threshold -- the reference's stop rule per block (cpu/VTA.h:210-216,
+//      cpu/PTA.h:636-641); its merge tree gives the result.  (Round 1's partitions
+//      come again; rescanning them is cheaper than merging two results.)
+// With a seed (a predicted lower bound of the k-th score: `cut`, or the learned
+// model's cut computed on the device) round 2 alone runs with it, and its result is
+// accepted when it holds min(k, n) objects (then the true k-th score is at least the
+// seed, so every object of the true top-k was scanned); otherwise the two rounds run
+// without it.  stats: partitions scanned (tiles scanned / tiles per partition, over
+// every scan), partitions, seed accepted (1/0), scans.
 int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, const uint8_t *attr, float cut,
                bool learned, uint64_t *ids, float *scores, uint64_t *count, float *threshold, uint64_t *stats,
                float *cut_out) {
@@ -545,15 +552,35 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   const uint32_t seed_host = std::isfinite(cut) ? host_f2key(cut) : 0u;
   const bool seeded = learned || seed_host != 0u;
   const uint64_t tiles_per_part = (1ull << h->part_log2) / 1024u;
+  // round 1: about one wave of CTAs worth of the best partitions, and rows for k
+  const uint64_t R = 1ull << h->part_log2;
+  const ScanPlan wave = plan_scan(qq, (uint32_t)kk, h->n, h->num_sms, h->smem_optin, h->max_ctas_per_sm, true);
+  const uint32_t m1 = (uint32_t)std::min<uint64_t>(
+      P, std::max<uint64_t>((kk + R - 1) / R + 1, ((uint64_t)wave.grid + tiles_per_part - 1) / tiles_per_part));
+  uint32_t *d_t1 = reinterpret_cast<uint32_t *>(&dh->pad[0]);  // round 1's k-th key
   uint64_t tiles = 0, scans = 0, accepted = 0;
   const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
   float cut_seen = cut;
-  for (int round = 0; round < 2; round++) {
-    const bool use_seed = seeded && round == 0;
+  // the seeded attempt (if any), then the two rounds without a seed
+  for (int attempt = seeded ? 0 : 1; attempt < 2; attempt++) {
     CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), s));
-    PartScan ps{c->d_plist, P, use_seed ? seed_host : 0u, c->d_pkey, use_seed ? d_seed : nullptr};
-    st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count, dh->stats,
-                      &ps);
+    if (attempt == 0) {
+      PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr};
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+                        dh->stats, &ps);
+      scans += 1;
+    } else {
+      // round 1's statistics go to pad[1..3] (its tiles to pad[3]); round 2 overwrites
+      // the result and the header's own statistics
+      PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1};
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+                        &dh->pad[1], &p1);
+      if (st != TOPK_OK) return st;
+      PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr};
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+                        dh->stats, &p2);
+      scans += 2;
+    }
     if (st != TOPK_OK) return st;
     CK(cudaMemcpyAsync(c->h_res, dr, kHdr + kk * 12, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -564,10 +591,9 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
       if (sc.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
       return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
     }
-    if (learned && round == 0) cut_seen = hh->cut;
-    tiles += hh->stats[2];
-    scans++;
-    if (!use_seed) break;
+    if (learned && attempt == 0) cut_seen = hh->cut;
+    tiles += hh->stats[2] + (attempt == 1 ? hh->pad[3] : 0u);
+    if (attempt == 1) break;
     if (hh->count == kk) {
       accepted = 1;
       break;
@@ -1403,6 +1429,49 @@ int topk_query_device(topk_table_t h, uint64_t k, uint32_t qq, const float *weig
   DeviceGuard dg(h->device);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->primary->stream;
   return enqueue_scan(h, h->primary, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, d_threshold, nullptr);
+}
+
+int topk_query_range_device(topk_table_t h, uint64_t row_begin, uint64_t row_end, uint64_t k, uint32_t qq,
+                            const float *weights, const uint8_t *attr, uint64_t *d_ids, float *d_scores,
+                            float *d_threshold, void *stream) {
+  int st = check_query(h, k, qq, weights, attr);
+  if (st != TOPK_OK) return st;
+  if (row_end > h->n || row_begin >= row_end)
+    return fail(TOPK_ERR_ARG, "row range [%llu, %llu) empty or outside [0, %llu)", (unsigned long long)row_begin,
+                (unsigned long long)row_end, (unsigned long long)h->n);
+  if (!d_ids || !d_scores) return fail(TOPK_ERR_ARG, "null output buffer");
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", h->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->primary->stream;
+  return enqueue_scan(h, h->primary, s, row_begin, row_end, k, qq, weights, attr, d_ids, d_scores, d_threshold,
+                      nullptr);
+}
+
+int topk_merge_lists(int device, const void *d_lists, uint32_t nlists, uint64_t stride, const uint64_t *counts,
+                     const uint64_t *id_base, uint64_t k, uint64_t *d_ids, float *d_scores, float *d_threshold,
+                     uint64_t *kept, void *stream) {
+  g_last_error.clear();
+  if (!d_lists || !counts || !d_ids || !d_scores || !kept) return fail(TOPK_ERR_ARG, "null argument");
+  if (nlists == 0 || nlists > kMaxMergeLists)
+    return fail(TOPK_ERR_UNSUPPORTED, "nlists=%u: 1 to %u lists", nlists, kMaxMergeLists);
+  if (k == 0) return fail(TOPK_ERR_ARG, "k must be >= 1");
+  if (k > kMaxK) return fail(TOPK_ERR_UNSUPPORTED, "k=%llu exceeds TOPK_MAX_K=%u", (unsigned long long)k, kMaxK);
+  if (stride == 0 || stride > kMaxK) return fail(TOPK_ERR_ARG, "stride must be in [1, %u]", kMaxK);
+  if (reinterpret_cast<uintptr_t>(d_lists) % 8 != 0) return fail(TOPK_ERR_ARG, "d_lists must be 8-byte aligned");
+  uint32_t c32[kMaxMergeLists], b32[kMaxMergeLists];
+  for (uint32_t j = 0; j < nlists; j++) {
+    if (counts[j] > stride) return fail(TOPK_ERR_ARG, "counts[%u]=%llu above stride", j, (unsigned long long)counts[j]);
+    if (id_base && id_base[j] >= 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "id_base[%u] must be < 2^32 - 1", j);
+    c32[j] = (uint32_t)counts[j];
+    b32[j] = id_base ? (uint32_t)id_base[j] : 0u;
+  }
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(TOPK_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  uint32_t kk = 0;
+  CK(launch_merge_lists(static_cast<const unsigned char *>(d_lists), nlists, stride, c32, b32, (uint32_t)k, d_ids,
+                        d_scores, d_threshold, &kk, static_cast<cudaStream_t>(stream)));
+  *kept = kk;
+  return TOPK_OK;
 }
 
 int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs, const float *weights,

@@ -69,6 +69,7 @@ struct ScanParams {
   float *out_scores;
   float *out_threshold; // may be null
   uint32_t *out_count;  // may be null
+  uint32_t *out_kth_key; // may be null: the k-th entry's key when k entries were found, else 0
   uint32_t *out_stats;  // may be null: [0] entries merged at the root, [1] block-selects,
                         // [2] tiles scanned (partition mode)
   // Partition mode (part_list != null): tile t covers rows
@@ -103,12 +104,22 @@ struct ScanPlan {
 // Plan a launch for qq attributes and top-k over `rows` rows (max_ctas_per_sm 0 =
 // as many as fit).  stages == 0 means the request does not fit.
 ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin,
-                   uint32_t max_ctas_per_sm = 0);
+                   uint32_t max_ctas_per_sm = 0, bool part = false);
 // Fill the merge-tree fields of p for `grid` CTAs; returns slots and group
 // counters needed (entries = slots * k).
 void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *total_slots, uint32_t *total_groups);
 cudaError_t launch_scan(const ScanPlan &plan, const ScanParams &p, cudaStream_t stream);
 cudaError_t scan_set_attributes(size_t smem_optin);
+
+// Merge of per-shard top-k lists (merge.cu): list j at lists + j * 12 * stride holds
+// ids[stride] (u64) then scores[stride] (f32), counts[j] of them valid, base[j] (may
+// be null: 0) added to its ids; the best min(k, sum of counts) of the union (score
+// descending, then lower id) are written ascending to out_ids / out_scores, the k-th
+// score to out_thr (may be null).
+constexpr uint32_t kMaxMergeLists = 64;
+cudaError_t launch_merge_lists(const unsigned char *lists, uint32_t nlists, uint64_t stride, const uint32_t *counts,
+                               const uint32_t *base, uint32_t k, uint64_t *out_ids, float *out_scores, float *out_thr,
+                               uint32_t *kept, cudaStream_t s);
 
 // Set the calling thread's message returned by topk_last_error().
 void set_last_error(const char *msg);

@@ -160,6 +160,13 @@ class Table:
         check(_lib.load().topk_query_device(self._h, int(k), len(a), w, a, C.c_void_p(d_ids), C.c_void_p(d_scores),
                                             C.c_void_p(d_threshold or None), C.c_void_p(stream or None)))
 
+    def query_range_device(self, row_begin, row_end, k, weights, attr, d_ids, d_scores, d_threshold=0, stream=0):
+        """query_device over rows [row_begin, row_end) only; global ids."""
+        w, a = _weights(weights, self.d), _attr(attr)
+        check(_lib.load().topk_query_range_device(self._h, int(row_begin), int(row_end), int(k), len(a), w, a,
+                                                  C.c_void_p(d_ids), C.c_void_p(d_scores),
+                                                  C.c_void_p(d_threshold or None), C.c_void_p(stream or None)))
+
     def query_batch(self, ks, weights, attrs, qqs=None):
         """ks: (nq,), weights: (nq, >=d), attrs: (nq, astride) with qqs[j] valid ids each."""
         L = _lib.load()

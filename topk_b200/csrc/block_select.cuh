@@ -185,6 +185,16 @@ __device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, u
   return kept;
 }
 
+// Barrier after one stage of a bitonic network whose comparator i (thread i % NT, whole
+// warps) exchanges elements lo = 2i - (i & (stride - 1)) and lo + stride.  Up to stride
+// 32 the comparators of a warp touch only their own 64-element blocks, so the warp's
+// own barrier orders the stage; larger strides need the block's.  The caller ends each
+// size with a block barrier (the next size starts with its largest stride).
+__device__ __forceinline__ void bitonic_stage_sync(uint32_t stride) {
+  if (stride > 32) __syncthreads();
+  else __syncwarp();
+}
+
 // Sort a[0..n) descending by composite (bitonic, padded to a power of two; the
 // caller guarantees room for the padding).
 template <int NT>
@@ -207,8 +217,9 @@ __device__ void block_sort_desc(uint2 *a, uint32_t n) {
           a[hi] = x;
         }
       }
-      __syncthreads();
+      bitonic_stage_sync(stride);
     }
+    __syncthreads();
   }
 }
 

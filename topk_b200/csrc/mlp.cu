@@ -31,6 +31,7 @@
 #include <cstdint>
 
 #include "batch_internal.h"
+#include "block_select.cuh"
 #include "device_common.cuh"
 
 namespace topk {
@@ -274,9 +275,9 @@ __global__ void __launch_bounds__(128) mlp_predict_kernel(const float *__restric
 // ---------------------------------------------------------------- features
 // Bitonic sort of n (a power of two) floats in shared memory, descending.
 __device__ void sort_desc(float *a, uint32_t n) {
-  for (uint32_t size = 2; size <= n; size <<= 1)
+  __syncthreads();
+  for (uint32_t size = 2; size <= n; size <<= 1) {
     for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-      __syncthreads();
       for (uint32_t i = threadIdx.x; i < n / 2; i += blockDim.x) {
         const uint32_t lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
         const bool desc = (lo & size) == 0;
@@ -286,8 +287,10 @@ __device__ void sort_desc(float *a, uint32_t n) {
           a[hi] = x;
         }
       }
+      bitonic_stage_sync(stride);
     }
-  __syncthreads();
+    __syncthreads();
+  }
 }
 
 // One block per query: the F features (and, with params, the model's prediction

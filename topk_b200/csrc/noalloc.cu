@@ -46,10 +46,13 @@ constexpr uint32_t kNoAllocMaxGrid = 8 * 148;
 constexpr uint32_t kNoAllocSlotEntries = 1u << 20;  // 8 MiB
 constexpr uint32_t kNoAllocMaxSlots = 2 * kNoAllocMaxGrid + kMaxLevels;
 constexpr uint32_t kNoAllocMaxGroups = kNoAllocMaxGrid + kMaxLevels;
-// layout: ScanScratch | done[groups] | slot_count[slots] | pad | slots[entries]
+// published best keys before the merge: grid * M <= k + 2 * grid entries
+constexpr uint32_t kNoAllocPubEntries = kNoAllocMaxK + 2 * kNoAllocMaxGrid;
+// layout: ScanScratch | done[groups] | slot_count[slots] | pad | slots[entries] | pub[entries]
 constexpr size_t kMetaBytes = sizeof(ScanScratch) + (size_t)kNoAllocMaxGroups * 4;
 constexpr size_t kSlotsOff = (kMetaBytes + (size_t)kNoAllocMaxSlots * 4 + 255) / 256 * 256;
-constexpr size_t kNoAllocScratchBytes = kSlotsOff + (size_t)kNoAllocSlotEntries * sizeof(uint2);
+constexpr size_t kPubOff = kSlotsOff + (size_t)kNoAllocSlotEntries * sizeof(uint2);
+constexpr size_t kNoAllocScratchBytes = kPubOff + (size_t)kNoAllocPubEntries * sizeof(uint2);
 
 // The scratch.  In host code this name is only a stand-in for the symbol: its
 // device address comes from cudaGetSymbolAddress below, once per device.
@@ -162,6 +165,11 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   // and the threshold; a failure shows as a CUDA error on the stream.
   p.wait_limit = 1ull << 26;
   p.fault_mode = 0;
+  if (kk >= kPubMinK && (uint32_t)pl.grid >= kPubMinGrid) {
+    p.pub = reinterpret_cast<uint2 *>(blk + kPubOff);
+    p.pub_m = pub_keys_per_cta((uint32_t)kk, (uint32_t)pl.grid);
+    p.pub_wait = kPubWaitPolls;
+  }
   p.scratch = reinterpret_cast<ScanScratch *>(blk);
   p.done = reinterpret_cast<uint32_t *>(blk + sizeof(ScanScratch));
   p.slot_count = reinterpret_cast<uint32_t *>(blk + kMetaBytes);

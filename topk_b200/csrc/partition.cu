@@ -25,6 +25,7 @@
 
 #include <cstdint>
 
+#include "block_select.cuh"
 #include "device_common.cuh"
 #include "topk_internal.h"
 
@@ -266,8 +267,9 @@ __global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *
           ent[hi] = x;
         }
       }
-      __syncthreads();
+      bitonic_stage_sync(stride);
     }
+    __syncthreads();
   }
   for (uint32_t i = t; i < P; i += kOrderThreads) {
     const unsigned long long e = ent[i];

@@ -100,6 +100,9 @@ __device__ __forceinline__ float4 score4(const ScanParams &p, const float *wsm, 
 #pragma unroll
     for (int m = 0; m < QQ; ++m)
       x[m] = inb ? ld_stream(p.table + (uint64_t)p.attr[m] * p.ld + row0) : make_float4(0.f, 0.f, 0.f, 0.f);
+    // every load is issued before the first multiply (the compiler may not sink them
+    // below this point): QQ x 16 bytes in flight per thread
+    asm volatile("" ::: "memory");
 #pragma unroll
     for (int m = 0; m < QQ; ++m) {
       const float w = p.w[m];
@@ -167,10 +170,18 @@ __device__ __forceinline__ float4 score_cols(const ScanParams &p, const float4 *
 // thread too few bytes in flight otherwise).
 constexpr int kPrefetchQ = 4;
 
+// CTAs per SM the register budget is sized for: few queried columns need little data
+// in flight and gain from more CTAs (6: 42 registers); more columns need their loads
+// in flight without spills (5: 51 registers up to 8 columns, 4: 64 above).
+template <int QQ>
+constexpr int scan_min_blocks() {
+  return (QQ >= 1 && QQ <= 2) ? 6 : (QQ >= 3 && QQ <= 8) ? 5 : 4;
+}
+
 // QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).  PART: partition
 // mode (p.part_list set): tiles of listed partitions of a reordered copy.
 template <int QQ, bool PART>
-__global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_constant__ ScanParams p) {
+__global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_select_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + kOffCtl);
   uint64_t *never = reinterpret_cast<uint64_t *>(smem + kOffNever);
@@ -247,10 +258,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   uint32_t i = 0;  // after the loop: the tiles this CTA scanned
   for (; i < my_tiles; ++i) {
     const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
-    // every thread reads the same thresholds here (see SmemCtl::thr_g)
-    const uint32_t thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
+    // every thread reads the same thresholds in tile i (see SmemCtl::thr_g); in id
+    // order they are read after the scores, so they hold no register across the loads
+    uint32_t thr = 0;
     uint64_t tile0;
     if constexpr (PART) {
+      thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
       // nothing in this partition (nor in any later one of this CTA) can reach thr
       if (key_next < thr) break;
       tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
@@ -279,6 +292,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
       s = score4<QQ>(p, wsm, qq, row0, !interior);
     }
 
+    if constexpr (!PART) thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
     // key(score) >= thr  <=>  thr == 0 (everything, NaN included) or score >= thr_float(thr)
     const bool take_all = thr == 0u;
     const float thr_f = thr_float(thr);
@@ -369,6 +383,48 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
   }
   if (t == 0 && ctl->reductions) atomicAdd(&p.scratch->acc_reductions, ctl->reductions);
   if (PART && t == 0) atomicAdd(&p.scratch->acc_tiles, i);
+
+  // ---- a tight bound before the merge (p.pub set: large k) ----
+  // Each CTA's own k-th key is a weak bound of the global k-th (the best of one CTA's
+  // share), so without more every CTA would pass ~k entries up the merge tree.  Each
+  // CTA publishes the keys of its best M = pub_m entries; the last to arrive takes the
+  // k-th largest of all published keys -- k real objects score at least that, so it is
+  // a lower bound of the global k-th, close to it when the best objects are spread over
+  // the CTAs -- and raises the global threshold to it; the others wait for that (a
+  // bounded wait: if it runs out they go on with the threshold they have, which is
+  // still exact, only slower) and the merge tree then carries about k entries in all.
+  if (p.pub) {
+    uint2 *res0 = cand0 + (size_t)ctl->cur * cap;
+    uint2 *spare = cand0 + (size_t)(ctl->cur ^ 1u) * cap;
+    const uint32_t M = p.pub_m;
+    uint32_t n_pub = ctl->count;
+    const uint2 *top = res0;
+    if (n_pub > M) {
+      n_pub = block_reduce<kScanThreads>(res0, n_pub, spare, M, 0u, hist, &ctl->sel);
+      top = spare;
+    }
+    uint2 *mine = p.pub + (size_t)blockIdx.x * M;
+    for (uint32_t j = t; j < M; j += kScanThreads)  // (key, slot index): distinct composites
+      mine[j] = make_uint2(j < n_pub ? top[j].x : 0u, blockIdx.x * M + j);
+    __threadfence();
+    bsync();
+    if (t == 0) ctl->is_last = atomicAdd(&p.scratch->pub_arrived, 1u) == gridDim.x - 1u ? 1u : 0u;
+    bsync();
+    if (ctl->is_last) {
+      __threadfence();
+      // entries of key 0 are padding (or NaN scores, the lowest anyway): left out
+      const uint32_t kept = block_reduce<kScanThreads>(p.pub, gridDim.x * M, spare, p.k, 1u, hist, &ctl->sel);
+      if (t == 0) {
+        if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
+        __threadfence();
+        atomicExch(&p.scratch->pub_ready, 1u);
+      }
+    } else if (t == 0) {
+      for (uint32_t it = 0; it < p.pub_wait && !ld_volatile_u32(&p.scratch->pub_ready); ++it) __nanosleep(64);
+      __threadfence();  // the raised g_thr is read after the flag
+    }
+    bsync();
+  }
 
   // ---- merge tree ----
   const uint32_t k = p.k;
@@ -462,6 +518,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_select_kernel(const __grid_
     }
     p.scratch->acc_reductions = 0;
     p.scratch->acc_tiles = 0;
+    p.scratch->pub_arrived = 0;  // every CTA has left its wait: it published a slot above
+    p.scratch->pub_ready = 0;
     p.scratch->g_thr = 0;
     __threadfence();
   }

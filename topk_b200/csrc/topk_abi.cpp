@@ -89,6 +89,7 @@ struct Ctx {
   uint32_t *done = nullptr;
   uint32_t *slot_count = nullptr;
   uint2 *slots = nullptr;
+  uint2 *pub = nullptr;  // published best keys before the merge (kMaxK + 2 * max grid entries)
   uint32_t max_slots = 0, max_groups = 0;
   size_t slot_entries = 0;  // capacity of `slots`
   size_t meta_bytes = 0;    // bytes that must be zero between queries (header + done)
@@ -203,6 +204,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
   auto bail = [&](cudaError_t e, const char *what) {
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaFree(c->scratch);
+    cudaFree(c->pub);
     cudaFree(c->d_res);
     cudaFree(c->d_count2);
     if (c->h_res) cudaFreeHost(c->h_res);
@@ -229,6 +231,8 @@ int ctx_create(topk_table_t h, Ctx **out) {
   c->slot_count = reinterpret_cast<uint32_t *>(blk + c->meta_bytes);
   c->slots = reinterpret_cast<uint2 *>(blk + slots_off);
   if ((e = cudaMemset(blk, 0, slots_off)) != cudaSuccess) return bail(e, "scratch memset");
+  if ((e = cudaMalloc(&c->pub, ((size_t)kMaxK + 2 * (size_t)max_grid) * sizeof(uint2))) != cudaSuccess)
+    return bail(e, "publish area");
   if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
   if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
   if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK) + kStageBytes, cudaHostAllocDefault)) != cudaSuccess)
@@ -242,6 +246,7 @@ void ctx_free(Ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaFree(c->scratch);
+  cudaFree(c->pub);
   cudaFree(c->d_res);
   cudaFree(c->d_count2);
   cudaFree(c->d_ids_scratch);
@@ -374,6 +379,11 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     return fail(TOPK_ERR_UNSUPPORTED, "merge tree of %d CTAs does not fit the scratch", pl.grid);
   p.wait_limit = h->wait_limit;
   p.fault_mode = (uint32_t)h->fault_mode;
+  if (k >= kPubMinK && (uint32_t)pl.grid >= kPubMinGrid) {
+    p.pub = c->pub;
+    p.pub_m = pub_keys_per_cta((uint32_t)k, (uint32_t)pl.grid);
+    p.pub_wait = kPubWaitPolls;
+  }
   p.scratch = c->scratch;
   p.slots = c->slots;
   p.slot_count = c->slot_count;
@@ -554,9 +564,12 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   const uint64_t tiles_per_part = (1ull << h->part_log2) / 1024u;
   // round 1: about one wave of CTAs worth of the best partitions, and rows for k
   const uint64_t R = 1ull << h->part_log2;
+  // (the stop-rule scan keeps its first wave to max(SMs, tiles / 32) CTAs: see enqueue_scan)
   const ScanPlan wave = plan_scan(qq, (uint32_t)kk, h->n, h->num_sms, h->smem_optin, h->max_ctas_per_sm, true);
+  const uint64_t all_tiles = (uint64_t)P * tiles_per_part;
+  const uint64_t wave_ctas = std::min<uint64_t>((uint64_t)wave.grid, std::max<uint64_t>(h->num_sms, all_tiles / 32));
   const uint32_t m1 = (uint32_t)std::min<uint64_t>(
-      P, std::max<uint64_t>((kk + R - 1) / R + 1, ((uint64_t)wave.grid + tiles_per_part - 1) / tiles_per_part));
+      P, std::max<uint64_t>((kk + R - 1) / R + 1, (wave_ctas + tiles_per_part - 1) / tiles_per_part));
   uint32_t *d_t1 = reinterpret_cast<uint32_t *>(&dh->pad[0]);  // round 1's k-th key
   uint64_t tiles = 0, scans = 0, accepted = 0;
   const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);

@@ -27,7 +27,9 @@ struct ScanScratch {
   // tile, two values); the access it guarded was skipped.
   uint32_t diag[5];
   uint32_t acc_tiles;       // tiles scanned during this scan (partition mode)
-  uint32_t pad[5];
+  uint32_t pub_arrived;     // CTAs that published their best keys (ScanParams::pub)
+  uint32_t pub_ready;       // 1 once the bound from the published keys is in g_thr
+  uint32_t pad[3];
 };
 
 // TOPK_BOUNDS_CHECK codes
@@ -63,6 +65,12 @@ struct ScanParams {
   uint32_t fault_mode;  // 1: wait on a barrier nothing completes (timeout test)
   ScanScratch *scratch;
   uint2 *slots;         // merge-tree slots, k entries each (key, id)
+  // May be null.  Before the merge each CTA publishes the keys of its best pub_m
+  // entries here (grid * pub_m entries) and the k-th largest of them raises the global
+  // threshold; non-last CTAs wait at most pub_wait polls for it.
+  uint2 *pub;
+  uint32_t pub_m;
+  uint32_t pub_wait;
   uint32_t *slot_count; // entries per slot
   uint32_t *done;       // per-group arrival counters (zero between queries)
   uint64_t *out_ids;    // min(k, rows) ids, ascending by score
@@ -89,6 +97,14 @@ struct ScanParams {
   uint8_t attr[kMaxQ];
   float w[kMaxQ];       // weights[attr[m]], gathered on the host
 };
+
+// The published-keys bound before the merge (ScanParams::pub): used for k >= this and
+// grids of at least kPubMinGrid CTAs; M = ceil(k / grid) + 1 keys per CTA, so the
+// array needs grid * M <= k + 2 * grid entries.
+constexpr uint32_t kPubMinK = 64;
+constexpr uint32_t kPubMinGrid = 16;
+constexpr uint32_t kPubWaitPolls = 4096;  // ~64 ns each
+inline uint32_t pub_keys_per_cta(uint32_t k, uint32_t grid) { return (k + grid - 1) / grid + 1; }
 
 struct ScanPlan {
   uint32_t tile;     // objects per tile

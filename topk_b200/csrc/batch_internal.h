@@ -105,9 +105,16 @@ __host__ __device__ constexpr uint32_t feature_bound_col(uint32_t d) { return 2 
 uint32_t mlp_param_count(uint32_t F);
 cudaError_t launch_mlp_grad(const float *params, const float *X, const float *y, uint32_t B, uint32_t F, float *grad,
                             float *loss, cudaStream_t s);
+// Training on kTrainCtas CTAs (cooperative launch): scratch holds
+// mlp_train_scratch_bytes(F) bytes, zeroed by the caller, and epoch_loss is zeroed too;
+// every grid barrier waits at most wait_limit polls, after which the kernel stops and
+// mlp_train_failed (after the stream is synchronised) reports it.
+constexpr uint32_t kTrainCtas = 8;
+size_t mlp_train_scratch_bytes(uint32_t F);
 cudaError_t launch_mlp_train(float *params, float *m, float *v, const float *X, const float *y, uint64_t N, uint32_t F,
                              uint32_t B, uint32_t epochs, const uint64_t *mul, const uint64_t *add, float lr,
-                             float *epoch_loss, cudaStream_t s);
+                             float *epoch_loss, void *scratch, uint64_t wait_limit, cudaStream_t s);
+bool mlp_train_failed(const void *scratch, uint32_t F);
 cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, uint32_t F, float *out, int num_sms,
                                cudaStream_t s);
 cudaError_t launch_features(const float *pmin, const float *pmax, const float *pmean, uint32_t P, uint32_t d,

@@ -22,9 +22,9 @@
 //   cut = largest bound - S * exp((u + margin) / qq).
 //
 // Parameters, one flat FP32 array: W1[64][F] b1[64] W2[64][64] b2[64] w3[64] b3.
-// Training: one block runs every step (forward, backward, Adam) with the
-// parameters and gradients in shared memory and the Adam moments in global memory;
-// each epoch visits the samples in the order (a*i + c) mod N, gcd(a, N) = 1.
+// Training: kTrainCtas blocks, data-parallel over each batch, every step a gradient
+// reduction and an Adam update split over the blocks (mlp_train_kernel); each epoch
+// visits the samples in the order (a*i + c) mod N, gcd(a, N) = 1.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,11 +60,12 @@ __device__ __forceinline__ Net net_at(float *base, uint32_t F) {
   return n;
 }
 
-// Forward and backward of one batch (MSE loss); adds the gradient into g (each
-// element owned by one thread) and the batch's mean squared error into *loss.
+// Forward and backward of B samples of a batch of Bn (MSE loss over Bn); adds their
+// share of the gradient into g (each element owned by one thread) and of the batch's
+// mean squared error into *loss.
 // X [B][F], y [B], H1/H2 [B][64], dy [B] in shared memory; ends with a barrier.
 __device__ void batch_grad(const Net &p, const Net &g, const float *X, const float *y, uint32_t B, uint32_t F,
-                           float *H1, float *H2, float *dy, float *loss) {
+                           float *H1, float *H2, float *dy, float *loss, float Bn) {
   const int t = threadIdx.x;
   for (uint32_t e = t; e < B * kHid; e += kMT) {
     const uint32_t i = e / kHid, j = e % kHid;
@@ -84,8 +85,8 @@ __device__ void batch_grad(const Net &p, const Net &g, const float *X, const flo
     float s = p.b3[0];
     for (uint32_t j = 0; j < kHid; ++j) s = fmaf(p.w3[j], H2[i * kHid + j], s);
     const float r = s - y[i];
-    dy[i] = 2.0f * r / (float)B;
-    atomicAdd(loss, r * r / (float)B);
+    dy[i] = 2.0f * r / Bn;
+    atomicAdd(loss, r * r / Bn);
   }
   __syncthreads();
   for (uint32_t j = t; j < kHid; j += kMT) {
@@ -189,58 +190,105 @@ __global__ void __launch_bounds__(kMT) mlp_grad_kernel(const float *__restrict__
   for (uint32_t e = threadIdx.x; e < B; e += kMT) s.y[e] = y[e];
   if (threadIdx.x == 0) *s.loss = 0.0f;
   __syncthreads();
-  batch_grad(net_at(s.params, F), net_at(s.grad, F), s.X, s.y, B, F, s.H1, s.H2, s.dy, s.loss);
+  batch_grad(net_at(s.params, F), net_at(s.grad, F), s.X, s.y, B, F, s.H1, s.H2, s.dy, s.loss, (float)B);
   for (uint32_t e = threadIdx.x; e < P; e += kMT) grad[e] = s.grad[e];
   if (threadIdx.x == 0) *loss = *s.loss;
 }
 
-// Training: epochs x floor(N / B) Adam steps in one block.  mul/add: per-epoch
-// visiting order (mul coprime with N).  m, v: Adam moments (zeroed by the caller).
-// epoch_loss[e]: mean batch loss of epoch e.
+// Grid barrier with a bounded wait (the training kernel is launched cooperatively, so
+// every CTA is resident and the wait ends unless a CTA failed): returns false once a
+// wait ran out or another CTA's did, after setting bar->err.
+struct GridBar {
+  unsigned int count, gen, err, pad;
+};
+
+__device__ bool grid_barrier(GridBar *bar, uint64_t limit) {
+  __shared__ unsigned int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int g = ld_volatile_u32(&bar->gen);
+    __threadfence();
+    if (atomicAdd(&bar->count, 1u) == gridDim.x - 1u) {
+      bar->count = 0u;  // everyone has arrived: reset for the next barrier, then release
+      __threadfence();
+      atomicExch(&bar->gen, g + 1u);
+      ok_s = 1u;
+    } else {
+      uint64_t it = 0;
+      while (ld_volatile_u32(&bar->gen) == g && !ld_volatile_u32(&bar->err) && it < limit) {
+        __nanosleep(32);
+        ++it;
+      }
+      ok_s = ld_volatile_u32(&bar->gen) != g ? 1u : 0u;
+      if (!ok_s) atomicExch(&bar->err, 1u);
+    }
+    __threadfence();
+    if (ld_volatile_u32(&bar->err)) ok_s = 0u;  // one decision for the whole block
+  }
+  __syncthreads();
+  return ok_s != 0u;
+}
+
+// Training: epochs x floor(N / B) Adam steps, data-parallel over the grid.  In each
+// step CTA c computes the gradient of its share of the batch (samples
+// [c*B/G, (c+1)*B/G)) into gpart[c]; after a grid barrier CTA c sums the G partial
+// gradients (in CTA order: deterministic) for its slice of the parameters and applies
+// Adam to that slice in global memory; after a second barrier every CTA reloads the
+// parameters.  mul/add: per-epoch visiting order (mul coprime with N).  m, v: Adam
+// moments, epoch_loss: zeroed by the caller; epoch_loss[e] = mean batch loss of epoch e.
 __global__ void __launch_bounds__(kMT) mlp_train_kernel(float *__restrict__ params, float *__restrict__ m,
                                                         float *__restrict__ v, const float *__restrict__ X,
                                                         const float *__restrict__ y, uint64_t N, uint32_t F,
                                                         uint32_t B, uint32_t epochs, const uint64_t *__restrict__ mul,
                                                         const uint64_t *__restrict__ add, float lr,
-                                                        float *__restrict__ epoch_loss) {
+                                                        float *__restrict__ epoch_loss, float *__restrict__ gpart,
+                                                        GridBar *bar, uint64_t wait_limit) {
   extern __shared__ __align__(16) unsigned char smem[];
   MlpShared s = mlp_shared(smem, F);
   const uint32_t P = param_count(F);
+  const uint32_t G = gridDim.x, c = blockIdx.x;
+  const uint32_t i0 = (uint32_t)((uint64_t)B * c / G), i1 = (uint32_t)((uint64_t)B * (c + 1) / G);
+  const uint32_t nb = i1 - i0;
+  const uint32_t e0 = (uint32_t)((uint64_t)P * c / G), e1 = (uint32_t)((uint64_t)P * (c + 1) / G);
   for (uint32_t e = threadIdx.x; e < P; e += kMT) s.params[e] = params[e];
   const Net pn = net_at(s.params, F), gn = net_at(s.grad, F);
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   float b1t = 1.0f, b2t = 1.0f;
   const uint64_t steps = N / B;
+  float *mine = gpart + (size_t)c * P;
   for (uint32_t ep = 0; ep < epochs; ++ep) {
     if (threadIdx.x == 0) *s.loss = 0.0f;
     for (uint64_t st = 0; st < steps; ++st) {
       __syncthreads();
       for (uint32_t e = threadIdx.x; e < P; e += kMT) s.grad[e] = 0.0f;
-      for (uint32_t e = threadIdx.x; e < B * F; e += kMT) {
+      for (uint32_t e = threadIdx.x; e < nb * F; e += kMT) {
         const uint32_t i = e / F, f = e % F;
-        const uint64_t idx = (mul[ep] * (st * B + i) + add[ep]) % N;
+        const uint64_t idx = (mul[ep] * (st * B + i0 + i) + add[ep]) % N;
         s.X[e] = X[idx * F + f];
         if (f == 0) s.y[i] = y[idx];
       }
       __syncthreads();
-      batch_grad(pn, gn, s.X, s.y, B, F, s.H1, s.H2, s.dy, s.loss);
+      batch_grad(pn, gn, s.X, s.y, nb, F, s.H1, s.H2, s.dy, s.loss, (float)B);
+      for (uint32_t e = threadIdx.x; e < P; e += kMT) mine[e] = s.grad[e];
+      if (!grid_barrier(bar, wait_limit)) return;
       b1t *= b1;
       b2t *= b2;
       const float c1 = 1.0f / (1.0f - b1t), c2 = 1.0f / (1.0f - b2t);
-      for (uint32_t e = threadIdx.x; e < P; e += kMT) {
-        const float gr = s.grad[e];
+      for (uint32_t e = e0 + threadIdx.x; e < e1; e += kMT) {
+        float gr = 0.0f;
+        for (uint32_t j = 0; j < G; ++j) gr += __ldcg(gpart + (size_t)j * P + e);
         const float mm = b1 * m[e] + (1.0f - b1) * gr;
         const float vv = b2 * v[e] + (1.0f - b2) * gr * gr;
         m[e] = mm;
         v[e] = vv;
-        s.params[e] -= lr * (mm * c1) / (sqrtf(vv * c2) + eps);
+        params[e] = s.params[e] - lr * (mm * c1) / (sqrtf(vv * c2) + eps);
       }
+      if (!grid_barrier(bar, wait_limit)) return;
+      for (uint32_t e = threadIdx.x; e < P; e += kMT) s.params[e] = __ldcg(params + e);
     }
     __syncthreads();
-    if (threadIdx.x == 0) epoch_loss[ep] = steps ? *s.loss / (float)steps : 0.0f;
+    if (threadIdx.x == 0 && steps) atomicAdd(epoch_loss + ep, *s.loss / (float)steps);
   }
-  __syncthreads();
-  for (uint32_t e = threadIdx.x; e < P; e += kMT) params[e] = s.params[e];
 }
 
 // Inference: one thread per sample, parameters in shared memory, the hidden
@@ -294,8 +342,10 @@ __device__ void sort_desc(float *a, uint32_t n) {
 }
 
 // One block per query: the F features (and, with params, the model's prediction
-// of k-th score / S, the MLP forward in the same block).
-__global__ void __launch_bounds__(256) features_kernel(const float *__restrict__ pmin, const float *__restrict__ pmax,
+// of k-th score / S, the MLP forward in the same block).  NT threads: 256 for
+// batches (many blocks), 1024 for a single query (the sorts are its critical path).
+template <int NT>
+__global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ pmin, const float *__restrict__ pmax,
                                                        const float *__restrict__ pmean, uint32_t P, uint32_t Ppad,
                                                        uint32_t d, const BatchQuery *__restrict__ qs,
                                                        float *__restrict__ X, const float *__restrict__ params,
@@ -427,15 +477,32 @@ cudaError_t launch_mlp_grad(const float *params, const float *X, const float *y,
   return cudaGetLastError();
 }
 
+size_t mlp_train_scratch_bytes(uint32_t F) { return (size_t)kTrainCtas * mlp_param_count(F) * 4 + sizeof(GridBar); }
+
 cudaError_t launch_mlp_train(float *params, float *m, float *v, const float *X, const float *y, uint64_t N, uint32_t F,
                              uint32_t B, uint32_t epochs, const uint64_t *mul, const uint64_t *add, float lr,
-                             float *epoch_loss, cudaStream_t s) {
+                             float *epoch_loss, void *scratch, uint64_t wait_limit, cudaStream_t s) {
   if (B == 0 || B > kMB || F == 0 || F > kMlpMaxIn) return cudaErrorInvalidValue;
   const size_t smem = mlp_smem(F);
   cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  mlp_train_kernel<<<1, kMT, smem, s>>>(params, m, v, X, y, N, F, B, epochs, mul, add, lr, epoch_loss);
+  // the caller zeroed the scratch: partial gradients, then the barrier words
+  float *gpart = static_cast<float *>(scratch);
+  GridBar *bar = reinterpret_cast<GridBar *>(gpart + (size_t)kTrainCtas * mlp_param_count(F));
+  const uint32_t G = std::min<uint32_t>(kTrainCtas, B);
+  void *args[] = {&params, &m, &v, &X, &y, &N, &F, &B, &epochs, &mul, &add, &lr, &epoch_loss, &gpart, &bar, &wait_limit};
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(mlp_train_kernel), dim3(G), dim3(kMT), args, smem, s);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
+}
+
+bool mlp_train_failed(const void *scratch, uint32_t F) {
+  GridBar bar{};
+  const float *gpart = static_cast<const float *>(scratch);
+  if (cudaMemcpy(&bar, gpart + (size_t)kTrainCtas * mlp_param_count(F), sizeof(bar), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return true;
+  return bar.err != 0u;
 }
 
 cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, uint32_t F, float *out, int num_sms,
@@ -456,9 +523,15 @@ cudaError_t launch_features(const float *pmin, const float *pmax, const float *p
   uint32_t Ppad = 1;
   while (Ppad < P) Ppad <<= 1;
   const size_t smem = (2 * (size_t)Ppad + kMlpMaxIn + 2 * kHid) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(features_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  if (nq) features_kernel<<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+  if (nq <= 4) {
+    e = cudaFuncSetAttribute(features_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (nq) features_kernel<1024><<<nq, 1024, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+  } else {
+    features_kernel<256><<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+  }
   return cudaGetLastError();
 }
 

@@ -315,6 +315,7 @@ struct PartScan {
   const uint32_t *d_key;   // bound key of each listed partition (null: no stop rule)
   const uint32_t *d_seed;  // a further seed in device memory (null: none)
   uint32_t *d_kth;         // receives the k-th key when k objects were found, else 0 (may be null)
+  uint32_t max_ctas_per_sm;  // 0: as many as fit
 };
 
 // Enqueue one fused scan over rows [r0, r1) (or over the partitions of `ps`)
@@ -360,6 +361,8 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     if (tiles > 0xFFFFFFFFull) return fail(TOPK_ERR_UNSUPPORTED, "too many tiles");
   }
   p.num_tiles = (uint32_t)tiles;
+  if (ps && ps->max_ctas_per_sm && (uint64_t)pl.grid > (uint64_t)h->num_sms * ps->max_ctas_per_sm)
+    pl.grid = (int)((uint64_t)h->num_sms * ps->max_ctas_per_sm);
   if (ps && ps->d_key) {
     // With the stop rule, the first wave of CTAs scans its tiles before any threshold
     // exists; on a small copy keep that wave to about 1/32 of the tiles (one CTA per
@@ -471,6 +474,9 @@ float host_key2f(uint32_t k) {
 std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *qqs,
                                      const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride);
 
+constexpr uint32_t kPrunedCtasPerSm = 3;  // CTAs per SM of a pruned scan
+constexpr uint32_t kRound1CtasPerSm = 2;  // and of its first round
+
 // Exact top-k over the partitioned copy as one device pipeline on the context's
 // stream; nothing is decided on the host between the launches.
 //   1. A kernel orders the partitions by the query's bound (the reference-order FP32
@@ -564,10 +570,10 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   const uint64_t tiles_per_part = (1ull << h->part_log2) / 1024u;
   // round 1: about one wave of CTAs worth of the best partitions, and rows for k
   const uint64_t R = 1ull << h->part_log2;
-  // (the stop-rule scan keeps its first wave to max(SMs, tiles / 32) CTAs: see enqueue_scan)
-  const ScanPlan wave = plan_scan(qq, (uint32_t)kk, h->n, h->num_sms, h->smem_optin, h->max_ctas_per_sm, true);
-  const uint64_t all_tiles = (uint64_t)P * tiles_per_part;
-  const uint64_t wave_ctas = std::min<uint64_t>((uint64_t)wave.grid, std::max<uint64_t>(h->num_sms, all_tiles / 32));
+  // A pruned scan reads a small part of the table: a few CTAs per SM keep enough loads
+  // in flight for it, and fewer CTAs mean a shallower merge tree (kPrunedCtasPerSm).
+  // Round 1 is about one wave of its CTAs (and rows for k).
+  const uint64_t wave_ctas = (uint64_t)h->num_sms * kRound1CtasPerSm;
   const uint32_t m1 = (uint32_t)std::min<uint64_t>(
       P, std::max<uint64_t>((kk + R - 1) / R + 1, (wave_ctas + tiles_per_part - 1) / tiles_per_part));
   uint32_t *d_t1 = reinterpret_cast<uint32_t *>(&dh->pad[0]);  // round 1's k-th key
@@ -578,18 +584,18 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   for (int attempt = seeded ? 0 : 1; attempt < 2; attempt++) {
     CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), s));
     if (attempt == 0) {
-      PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr};
+      PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr, kPrunedCtasPerSm};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                         dh->stats, &ps);
       scans += 1;
     } else {
       // round 1's statistics go to pad[1..3] (its tiles to pad[3]); round 2 overwrites
       // the result and the header's own statistics
-      PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1};
+      PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1, kRound1CtasPerSm};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                         &dh->pad[1], &p1);
       if (st != TOPK_OK) return st;
-      PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr};
+      PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr, kPrunedCtasPerSm};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                         dh->stats, &p2);
       scans += 2;
@@ -1956,17 +1962,24 @@ int device_train(uint32_t in_dim, float *dp, const float *dX, const float *dy, u
   DevScope ds;
   float *dm, *dv, *dl;
   uint64_t *dmul, *dadd;
+  unsigned char *dscr;
+  const size_t scr = mlp_train_scratch_bytes(in_dim);
   CK(ds.alloc(&dm, P * 4));
   CK(ds.alloc(&dv, P * 4));
   CK(ds.alloc(&dl, mul.size() * 4));
   CK(ds.alloc(&dmul, mul.size() * 8));
   CK(ds.alloc(&dadd, mul.size() * 8));
+  CK(ds.alloc(&dscr, scr));
   CK(cudaMemset(dm, 0, P * 4));
   CK(cudaMemset(dv, 0, P * 4));
+  CK(cudaMemset(dl, 0, mul.size() * 4));
+  CK(cudaMemset(dscr, 0, scr));
   CK(cudaMemcpy(dmul, mul.data(), mul.size() * 8, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dadd, add.data(), add.size() * 8, cudaMemcpyHostToDevice));
-  CK(launch_mlp_train(dp, dm, dv, dX, dy, n, in_dim, batch, epochs, dmul, dadd, lr, dl, 0));
+  // a barrier wait of 2^24 polls (~1 s) only runs out if a CTA failed
+  CK(launch_mlp_train(dp, dm, dv, dX, dy, n, in_dim, batch, epochs, dmul, dadd, lr, dl, dscr, 1ull << 24, 0));
   CK(cudaDeviceSynchronize());
+  if (mlp_train_failed(dscr, in_dim)) return fail(TOPK_ERR_TIMEOUT, "training: a grid barrier wait ran out");
   if (epoch_loss) CK(cudaMemcpy(epoch_loss, dl, (size_t)epochs * 4, cudaMemcpyDeviceToHost));
   return TOPK_OK;
 }

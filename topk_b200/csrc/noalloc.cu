@@ -143,6 +143,7 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   p.row_end = n;
   p.tile_begin = 0;
   p.tile_end = (n + 3) & ~3ull;
+  p.tile_step = pl.tile;
   const uint64_t tiles = (p.tile_end + pl.tile - 1) / pl.tile;
   p.num_tiles = (uint32_t)tiles;
   if ((uint64_t)pl.grid > tiles) pl.grid = (int)tiles;

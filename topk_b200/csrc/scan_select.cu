@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
 #pragma unroll
   for (int m = 0; m < kPQ; ++m) col[m] = kHoist ? p.table + (uint64_t)p.attr[m] * p.ld : nullptr;
   auto load_tile = [&](uint32_t j, float4 *dst) {  // tile j of this CTA
-    const uint64_t tl = p.tile_begin + ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) * kTile;
+    const uint64_t tl = p.tile_begin + ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) * p.tile_step;
     const float *c[kPQ];
 #pragma unroll
     for (int m = 0; m < kPQ; ++m) c[m] = kHoist ? col[m] : p.table + (uint64_t)p.attr[m] * p.ld;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
         if (p.part_key) key_next = __ldg(p.part_key + nx);
       }
     } else {
-      tile0 = p.tile_begin + tix * kTile;
+      tile0 = p.tile_begin + tix * p.tile_step;
     }
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
@@ -410,10 +410,24 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     bsync();
     if (t == 0) ctl->is_last = atomicAdd(&p.scratch->pub_arrived, 1u) == gridDim.x - 1u ? 1u : 0u;
     bsync();
+    if (p.kth_only && !ctl->is_last) return;  // a threshold pass: only the last CTA goes on
     if (ctl->is_last) {
       __threadfence();
       // entries of key 0 are padding (or NaN scores, the lowest anyway): left out
       const uint32_t kept = block_reduce<kScanThreads>(p.pub, gridDim.x * M, spare, p.k, 1u, hist, &ctl->sel);
+      if (p.kth_only) {
+        // the bound is the pass's result; every other CTA has left: put the counters back
+        if (t == 0) {
+          *p.out_kth_key = kept == p.k ? ctl->sel.kept_min : 0u;
+          p.scratch->g_thr = 0;
+          p.scratch->acc_reductions = 0;
+          p.scratch->acc_tiles = 0;
+          p.scratch->pub_arrived = 0;
+          p.scratch->pub_ready = 0;
+          __threadfence();
+        }
+        return;
+      }
       if (t == 0) {
         if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
         __threadfence();

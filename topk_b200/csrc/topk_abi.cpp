@@ -90,6 +90,7 @@ struct Ctx {
   uint32_t *slot_count = nullptr;
   uint2 *slots = nullptr;
   uint2 *pub = nullptr;  // published best keys before the merge (kMaxK + 2 * max grid entries)
+  uint32_t *d_seed_word = nullptr;  // a threshold pass's bound, read by the scan after it
   uint32_t max_slots = 0, max_groups = 0;
   size_t slot_entries = 0;  // capacity of `slots`
   size_t meta_bytes = 0;    // bytes that must be zero between queries (header + done)
@@ -205,6 +206,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaFree(c->scratch);
     cudaFree(c->pub);
+    cudaFree(c->d_seed_word);
     cudaFree(c->d_res);
     cudaFree(c->d_count2);
     if (c->h_res) cudaFreeHost(c->h_res);
@@ -233,6 +235,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
   if ((e = cudaMemset(blk, 0, slots_off)) != cudaSuccess) return bail(e, "scratch memset");
   if ((e = cudaMalloc(&c->pub, ((size_t)kMaxK + 2 * (size_t)max_grid) * sizeof(uint2))) != cudaSuccess)
     return bail(e, "publish area");
+  if ((e = cudaMalloc(&c->d_seed_word, 256)) != cudaSuccess) return bail(e, "seed word");
   if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
   if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
   if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK) + kStageBytes, cudaHostAllocDefault)) != cudaSuccess)
@@ -247,6 +250,7 @@ void ctx_free(Ctx *c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaFree(c->scratch);
   cudaFree(c->pub);
+  cudaFree(c->d_seed_word);
   cudaFree(c->d_res);
   cudaFree(c->d_count2);
   cudaFree(c->d_ids_scratch);
@@ -337,6 +341,7 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   p.row_end = r1;
   p.tile_begin = r0 & ~3ull;
   p.tile_end = (r1 + 3) & ~3ull;
+  p.tile_step = pl.tile;
   const uint64_t span = p.tile_end - p.tile_begin;
   uint64_t tiles = (span + pl.tile - 1) / pl.tile;
   if (ps) {  // tiles of the listed partitions of the reordered copy, original ids
@@ -389,6 +394,28 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   }
   p.scratch = c->scratch;
   p.slots = c->slots;
+  // Large k over a large table in id order: a threshold pass over every
+  // kSampleStride-th tile first (its own launch, same kernel, no merge), whose bound
+  // seeds this scan, so its CTAs rarely need a select.
+  if (!ps && p.pub && k >= kSampleMinK && tiles >= kSampleMinTiles) {
+    ScanParams q = p;
+    q.num_tiles = (uint32_t)((tiles + kSampleStride - 1) / kSampleStride);
+    q.tile_step = (uint64_t)pl.tile * kSampleStride;
+    q.kth_only = 1;
+    q.out_kth_key = c->d_seed_word;
+    q.out_ids = nullptr;
+    q.out_scores = nullptr;
+    q.out_threshold = nullptr;
+    q.out_count = nullptr;
+    q.out_stats = nullptr;
+    ScanPlan qp = pl;
+    qp.grid = (int)std::min<uint64_t>((uint64_t)pl.grid, q.num_tiles);
+    if ((uint32_t)qp.grid >= kPubMinGrid) {
+      q.pub_m = pub_keys_per_cta((uint32_t)k, (uint32_t)qp.grid);
+      CK(launch_scan(qp, q, stream));
+      p.thr_seed_dev = c->d_seed_word;
+    }
+  }
   p.slot_count = c->slot_count;
   p.done = c->done;
   p.out_ids = d_ids;
@@ -572,10 +599,8 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   const uint64_t R = 1ull << h->part_log2;
   // A pruned scan reads a small part of the table: a few CTAs per SM keep enough loads
   // in flight for it, and fewer CTAs mean a shallower merge tree (kPrunedCtasPerSm).
-  // Round 1 is about one wave of its CTAs (and rows for k).
-  const uint64_t wave_ctas = (uint64_t)h->num_sms * kRound1CtasPerSm;
-  const uint32_t m1 = (uint32_t)std::min<uint64_t>(
-      P, std::max<uint64_t>((kk + R - 1) / R + 1, (wave_ctas + tiles_per_part - 1) / tiles_per_part));
+  // Round 1 takes the best 1/32 of the partitions (and rows for k).
+  const uint32_t m1 = (uint32_t)std::min<uint64_t>(P, std::max<uint64_t>((kk + R - 1) / R + 1, (P + 31) / 32));
   uint32_t *d_t1 = reinterpret_cast<uint32_t *>(&dh->pad[0]);  // round 1's k-th key
   uint64_t tiles = 0, scans = 0, accepted = 0;
   const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);

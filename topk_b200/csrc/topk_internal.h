@@ -51,6 +51,7 @@ struct ScanParams {
   uint64_t row_end;
   uint64_t tile_begin;  // row_begin rounded down to 4 (16-byte copies)
   uint64_t tile_end;    // row_end rounded up to 4 (<= ld)
+  uint64_t tile_step;   // rows from one tile to the next (the tile size; a multiple for a sample)
   uint32_t num_tiles;
   uint32_t qq;
   uint32_t k;
@@ -71,6 +72,11 @@ struct ScanParams {
   uint2 *pub;
   uint32_t pub_m;
   uint32_t pub_wait;
+  // Threshold pass (needs pub and out_kth_key): the published keys' k-th largest goes
+  // to *out_kth_key (0 when fewer than k were published) and the scan ends there, no
+  // merge and no result.  Run over a sample of the tiles (tile_step) it seeds the full
+  // scan that follows: k real objects score at least that key.
+  uint32_t kth_only;
   uint32_t *slot_count; // entries per slot
   uint32_t *done;       // per-group arrival counters (zero between queries)
   uint64_t *out_ids;    // min(k, rows) ids, ascending by score
@@ -105,6 +111,12 @@ constexpr uint32_t kPubMinK = 64;
 constexpr uint32_t kPubMinGrid = 16;
 constexpr uint32_t kPubWaitPolls = 4096;  // ~64 ns each
 inline uint32_t pub_keys_per_cta(uint32_t k, uint32_t grid) { return (k + grid - 1) / grid + 1; }
+// A full-table scan with k >= kSampleMinK first runs a threshold pass over every
+// kSampleStride-th tile (kth_only), when the table has at least kSampleMinTiles tiles,
+// and starts from its bound: few candidates ever reach the select.
+constexpr uint32_t kSampleMinK = 128;
+constexpr uint32_t kSampleStride = 64;
+constexpr uint64_t kSampleMinTiles = 1u << 16;
 
 struct ScanPlan {
   uint32_t tile;     // objects per tile

@@ -102,3 +102,23 @@ def test_fullsize_slice_vs_oracle(big):
             got = t.query(k, w, a, row_begin=r0, row_end=r1)
             want = O.topk_numpy(sl, k, w, a)
             H.assert_same_result(got, (want[0] + np.uint64(r0), want[1], want[2]))
+
+
+@pytest.mark.parametrize("dist", [1, 2])
+def test_large_k_full_scan_with_mixed_sign_weights_matches_oracle(dist):
+    """2^26 rows: large enough that a scan with k >= 128 first runs its threshold pass
+    over a tile sample; negative and mixed weights (scores below zero) and ties from
+    repeated attributes must still give the oracle's result bit for bit."""
+    n, d = (1 << 26) + 333, 4
+    raw = O.generate(n, d, dist, 31 + dist)
+    tn = raw.copy()
+    O.normalize(tn)
+    rng = np.random.default_rng(dist)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        for k in (128, 1024, 4096):
+            for w in (rng.uniform(-1, 0, d), rng.uniform(-1, 1, d), rng.uniform(0, 1, d)):
+                w = w.astype(np.float32)
+                a = np.array([3, 0, 3, 1], np.uint8)
+                H.assert_same_result(t.query(k, w, a), O.topk(tn, k, w, a))

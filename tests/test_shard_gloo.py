@@ -38,7 +38,7 @@ def _keys(scores):
 
 def merge_reference(records, counts, k, stride=None):
     """The merge kernel's order on the host (test checker): best k by (key, -id)."""
-    stride = k if stride is None else stride
+    stride = shard.record_stride(k) if stride is None else stride
     ids, sc = [], []
     for rec, c in zip(records, counts):
         ids.append(rec[: 8 * stride].view(np.uint64)[:c])
@@ -69,6 +69,7 @@ def _worker(rank, world, port, results):
             vi, vs = shard.record_views(rec, k)
             vi[: len(ids)] = torch.from_numpy(ids.astype(np.int64))
             vs[: len(sc)] = torch.from_numpy(sc)
+            assert rec.numel() % 8 == 0
             got = shard.exchange(rec).numpy()
             counts = shard.list_counts(n, world, k)
             ok = got.shape == (world, shard.record_bytes(k)) and np.array_equal(got[rank], rec.numpy())
@@ -103,6 +104,7 @@ def test_shard_rows_and_record_layout():
     assert [shard.shard_rows(10, r, 3) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
     assert shard.list_counts(10, 3, 3).tolist() == [3, 3, 3]
     assert shard.list_counts(10, 3, 5).tolist() == [4, 3, 3]
+    assert [shard.record_bytes(k) for k in (1, 2, 17)] == [24, 24, 216]  # stride rounded up to even
     rec = torch.zeros(shard.record_bytes(4), dtype=torch.uint8)
     ids, sc = shard.record_views(rec, 4)
     ids[:] = torch.tensor([5, 1, 3, 0])

@@ -394,6 +394,17 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   }
   p.scratch = c->scratch;
   p.slots = c->slots;
+  p.slot_count = c->slot_count;
+  p.done = c->done;
+  p.out_ids = d_ids;
+  p.out_scores = d_scores;
+  p.out_threshold = d_thr;
+  p.out_count = d_count;
+  p.out_stats = d_stats;
+  for (uint32_t m = 0; m < qq; m++) {
+    p.attr[m] = attr[m];
+    p.w[m] = weights[attr[m]];
+  }
   // Large k over a large table in id order: a threshold pass over every
   // kSampleStride-th tile first (its own launch, same kernel, no merge), whose bound
   // seeds this scan, so its CTAs rarely need a select.
@@ -415,17 +426,6 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
       CK(launch_scan(qp, q, stream));
       p.thr_seed_dev = c->d_seed_word;
     }
-  }
-  p.slot_count = c->slot_count;
-  p.done = c->done;
-  p.out_ids = d_ids;
-  p.out_scores = d_scores;
-  p.out_threshold = d_thr;
-  p.out_count = d_count;
-  p.out_stats = d_stats;
-  for (uint32_t m = 0; m < qq; m++) {
-    p.attr[m] = attr[m];
-    p.w[m] = weights[attr[m]];
   }
   CK(launch_scan(pl, p, stream));
   return TOPK_OK;

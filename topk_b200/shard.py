@@ -9,9 +9,10 @@ score descending, then the lower id) keeps the best k of the union, ascending li
 the reference's result (cpu/TPAc.h:198-206).  This is the reference's merge of its
 per-thread heaps (cpu/TPAc.h:335-346) with GPUs in place of threads.
 
-Exchange record of a rank, for a query with k entries per list (stride = k):
-    bytes [0, 8k)     ids, uint64 (global ids)
-    bytes [8k, 12k)   scores, float32
+Exchange record of a rank, for a query with k entries per list (stride s = k rounded up
+to even, so that every record of a gathered (world, 12 s) tensor starts 8-byte aligned):
+    bytes [0, 8s)     ids, uint64 (the first k valid)
+    bytes [8s, 12s)   scores, float32
 The number of valid entries of rank r is min(k, rows of r) -- known on every rank
 from the row split, so no count is exchanged.
 """
@@ -30,15 +31,21 @@ def shard_rows(n, rank, world):
     return begin, begin + base + (1 if rank < extra else 0)
 
 
+def record_stride(k):
+    """Entries per list in a record: k rounded up to even (8-byte aligned records)."""
+    return (int(k) + 1) // 2 * 2
+
+
 def record_bytes(k):
     """Bytes of one rank's exchange record for lists of k entries."""
-    return 12 * int(k)
+    return 12 * record_stride(k)
 
 
 def record_views(rec, k):
-    """(ids, scores) views of a uint8 torch record tensor of record_bytes(k) bytes."""
-    k = int(k)
-    return rec[: 8 * k].view(dtype=_torch().int64), rec[8 * k: 12 * k].view(dtype=_torch().float32)
+    """(ids, scores) views of a uint8 torch record tensor of record_bytes(k) bytes; the
+    first k entries of each are the list."""
+    s = record_stride(k)
+    return rec[: 8 * s].view(dtype=_torch().int64), rec[8 * s: 12 * s].view(dtype=_torch().float32)
 
 
 def list_counts(n, world, k):

@@ -23,8 +23,9 @@ flush is needed between queries.
           with the learned start; identical results checked, speed-ups and the
           filter's tensor roofline reported.
   pruned   the partitioned workload: 2^27 x 8 anticorrelated in 2^11 partitions of
-          2^16 rows, the learned model fitted on 10^5 exactly labelled queries,
-          2000 fresh queries by full scan, plain pruning and learned pruning:
+          2^16 rows, the learned model fitted on 10^6 exactly labelled queries (and
+          10^5 more to calibrate its margin), 10^4 fresh queries by full scan, plain
+          pruning and learned pruning:
           partitions scanned, fallback rate, speed-up, identical results; then
           500 of them pruned over partitions rebuilt in VTA's and in PTA's order
           (device index builds timed).
@@ -398,7 +399,7 @@ def reference_index_build(d, sample_rows=1 << 22):
     return out
 
 
-def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=100000, n_test=2000, seed=4):
+def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=1000000, n_test=10000, seed=4):
     """Partitioned workload: an anticorrelated n x d table in partitions of part_rows
     rows; the learned model fitted on n_train queries labelled exactly; n_test fresh
     queries (attribute subsets of size U{2..d}, k log-uniform in [16, 1024]) answered
@@ -714,7 +715,8 @@ def main():
     ap.add_argument("--no-loader", action="store_true")
     ap.add_argument("--no-ta", action="store_true")
     ap.add_argument("--pruned-n", type=int, default=1 << 27)
-    ap.add_argument("--pruned-queries", type=int, default=2000)
+    ap.add_argument("--pruned-queries", type=int, default=10000)
+    ap.add_argument("--pruned-train", type=int, default=1000000)
     ap.add_argument("--batched-n", type=int, default=BATCH_N)
     ap.add_argument("--batched-q", type=int, default=BATCH_Q)
     args = ap.parse_args()
@@ -735,7 +737,7 @@ def main():
         elif args.only == "ta":
             out = run_ta(T, 0)
         else:
-            out = run_pruned(T, 0, args.pruned_n, n_test=args.pruned_queries)
+            out = run_pruned(T, 0, args.pruned_n, n_train=args.pruned_train, n_test=args.pruned_queries)
         print(json.dumps(out))
         return 0
 
@@ -936,7 +938,7 @@ def main():
     # final barrier (process-group timeout 120 s) while rank 0 ran them, so they run
     # only when the job has one rank
     if not args.no_pruned and world == 1:
-        result["pruned"] = run_pruned(T, local, args.pruned_n, n_test=args.pruned_queries)
+        result["pruned"] = run_pruned(T, local, args.pruned_n, n_train=args.pruned_train, n_test=args.pruned_queries)
     if not args.no_loader and world == 1:
         result["loader"] = run_loader(T, local)
     if not args.no_ta and world == 1:

@@ -31,6 +31,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
+
 #include "block_select.cuh"
 #include "device_common.cuh"
 #include "topk_internal.h"
@@ -565,6 +568,34 @@ cudaError_t scan_set_attributes(size_t smem_optin) {
   return cudaSuccess;
 }
 
+namespace {
+
+// Shared memory of an SM that the unified L1 / shared memory can give (B200: 228 KB),
+// the L1 the scan keeps (its 128-bit loads land in L1 while in flight: with less, the
+// loads in flight per SM, and the bandwidth, shrink), and the per-CTA reserve.
+constexpr size_t kSmemPerSm = 228 * 1024;
+constexpr size_t kScanL1Keep = 60 * 1024;
+constexpr size_t kSmemPerCtaReserve = 1024;
+
+// The shared-memory carveout last set on each scan kernel, per device (the attribute
+// is per function and device; setting it again costs a driver call).
+std::mutex g_carveout_mu;
+int g_carveout[64][2][17];
+
+void set_carveout(const void *fn, bool part, uint32_t qq, int percent) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lk(g_carveout_mu);
+  int &cur = g_carveout[dev][part ? 1 : 0][qq <= 16 ? qq : 0];
+  if (cur == percent + 1) return;  // stored plus one: 0 means not set yet
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, percent) == cudaSuccess)
+    cur = percent + 1;
+  else
+    (void)cudaGetLastError();
+}
+
+}  // namespace
+
 ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin, uint32_t max_ctas_per_sm,
                    bool part) {
   ScanPlan pl{};
@@ -590,11 +621,34 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   pl.mcap = mcap;
   pl.smem = kScanSmemFixed + (size_t)mcap * 8;
   pl.stages = pl.smem <= smem_optin ? 1u : 0u;
+  // CTAs per SM: as many as registers and threads allow, and as the shared memory
+  // allows with kScanL1Keep left as L1 (or the caller's number); the carveout is set to
+  // just fit them, so the rest of the unified memory stays L1
+  const void *fn = reinterpret_cast<const void *>(kernel_for(qq, part));
+  set_carveout(fn, part, qq, 100);
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reinterpret_cast<const void *>(kernel_for(qq, part)),
-                                                    kScanThreads, pl.smem) != cudaSuccess || occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kScanThreads, pl.smem) != cudaSuccess || occ < 1) {
+    (void)cudaGetLastError();
     occ = 1;
-  if (max_ctas_per_sm >= 1 && (uint32_t)occ > max_ctas_per_sm) occ = (int)max_ctas_per_sm;
+  }
+  const size_t per_cta = pl.smem + kSmemPerCtaReserve;
+  const int by_l1 = (int)std::max<size_t>(1, (kSmemPerSm - kScanL1Keep) / per_cta);
+  if (max_ctas_per_sm >= 1) occ = std::min<int>(occ, (int)max_ctas_per_sm);
+  else occ = std::min(occ, by_l1);
+  // the smallest shared-memory size of the SM (KB) that holds them, as a percentage
+  static const size_t kSizesKb[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+  size_t want = per_cta * (size_t)occ, size_kb = 228;
+  for (size_t kb : kSizesKb)
+    if (kb * 1024 >= want) {
+      size_kb = kb;
+      break;
+    }
+  set_carveout(fn, part, qq, (int)((size_kb * 100 + 227) / 228));
+  int fit = 0;  // what the driver reports with that preference
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kScanThreads, pl.smem) == cudaSuccess && fit >= 1)
+    occ = std::min(occ, fit);
+  else
+    (void)cudaGetLastError();
   pl.ctas_per_sm = occ;
   const uint64_t tiles = (rows + 3 + kTile) / kTile;
   uint64_t grid = (uint64_t)num_sms * (uint64_t)occ;

@@ -461,6 +461,12 @@ int topk_last_batch_switched(topk_table_t h, uint64_t *switched);
  * other methods. */
 int topk_last_batch_retired(topk_table_t h, uint64_t *retired);
 
+/* The tensor-core work the last topk_query_batch ran under the BF16 filter: for every
+ * chunk, its served query tiles (128 queries each) times its object tiles (256 rows),
+ * three BF16 MMA passes of 2 * 16 flops per (query, object).  0 for the other methods.
+ * No reference counterpart (a measurement of this engine). */
+int topk_last_batch_filter_flops(topk_table_t h, double *flops);
+
 /* Device-side scan statistics of the last topk_query* on this thread:
  * candidates kept by the fused select and the number of block reductions. */
 int topk_last_stats(topk_table_t h, uint64_t *candidates, uint64_t *reductions);

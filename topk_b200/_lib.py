@@ -107,6 +107,7 @@ SIGNATURES = [
     ("topk_last_batch_info", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     ("topk_last_batch_switched", C.c_int, [_H, C.POINTER(C.c_uint64)]),
     ("topk_last_batch_retired", C.c_int, [_H, C.POINTER(C.c_uint64)]),
+    ("topk_last_batch_filter_flops", C.c_int, [_H, C.POINTER(C.c_double)]),
     ("topk_set_batch_tiles", C.c_int, [_H, C.c_uint32, C.c_uint32]),
     ("topk_build_partitions_ordered", C.c_int, [_H, C.c_uint32, C.c_int]),
     ("topk_partition_ids", C.c_int, [_H, _u32p]),

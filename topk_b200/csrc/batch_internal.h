@@ -92,9 +92,11 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
                                uint32_t *err, cudaStream_t s);
 // Before each chunk: the queries the filter still serves (neither moved to the FP32
 // scorer nor retired by BatchQuery::maxkey), their rows of abf copied into compact
-// tiles abf_act (same size as abf), amap[slot] = query, *nact = count.
+// tiles abf_act (same size as abf), amap[slot] = query, *nact = count (and, when
+// nact_log is not null, *nact_log = count: the chunk's entry of a per-batch record).
 cudaError_t launch_batch_active(const BatchQuery *qs, const BatchState *st, uint32_t nq, const uint8_t *abf,
-                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, cudaStream_t s);
+                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, uint32_t *nact_log,
+                                cudaStream_t s);
 // Learned k-th-score model (mlp.cu): in -> 64 -> 64 -> 1 ReLU MLP, features of
 // feature_dim(d) values per query from the partition statistics ([P][d] each).
 constexpr uint32_t kHid = 64;

@@ -500,7 +500,8 @@ __global__ void __launch_bounds__(kActThreads) batch_active_kernel(const BatchQu
                                                                  const uint8_t *__restrict__ abf,
                                                                  uint8_t *__restrict__ abf_act,
                                                                  uint32_t *__restrict__ amap,
-                                                                 uint32_t *__restrict__ nact) {
+                                                                 uint32_t *__restrict__ nact,
+                                                                 uint32_t *__restrict__ nact_log) {
   __shared__ uint32_t wsum[kActThreads / 32];
   __shared__ uint32_t base;
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
@@ -550,7 +551,10 @@ __global__ void __launch_bounds__(kActThreads) batch_active_kernel(const BatchQu
     dst[kQTileBytes / 32] = z;
     dst[kQTileBytes / 32 + 8] = z;
   }
-  if (t == 0) *nact = total;
+  if (t == 0) {
+    *nact = total;
+    if (nact_log) *nact_log = total;
+  }
 }
 
 }  // namespace
@@ -644,8 +648,9 @@ cudaError_t launch_bf16_filter(const FilterPlan &f, const uint8_t *xbf, const ui
 }
 
 cudaError_t launch_batch_active(const BatchQuery *qs, const BatchState *st, uint32_t nq, const uint8_t *abf,
-                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, cudaStream_t s) {
-  batch_active_kernel<<<1, kActThreads, 0, s>>>(qs, st, nq, abf, abf_act, amap, nact);
+                                uint8_t *abf_act, uint32_t *amap, uint32_t *nact, uint32_t *nact_log,
+                                cudaStream_t s) {
+  batch_active_kernel<<<1, kActThreads, 0, s>>>(qs, st, nq, abf, abf_act, amap, nact, nact_log);
   return cudaGetLastError();
 }
 

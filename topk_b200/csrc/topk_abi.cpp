@@ -177,6 +177,7 @@ struct topk_table_s {
   uint64_t last_batch_fallbacks = 0, last_batch_cands = 0, last_batch_learned_misses = 0;
   uint64_t last_batch_switched = 0;  // queries a hybrid batch moved from the filter to the FP32 scorer
   uint64_t last_batch_retired = 0;   // queries the filter retired (threshold above their score bound)
+  double last_batch_filter_flops = 0;  // MMA flops the filter ran (three BF16 passes)
   // pinned host copies of a batch's results (grow-only): copied at full link speed,
   // no page faults on the critical path
   void *hb_res = nullptr;
@@ -320,6 +321,7 @@ struct PartScan {
   const uint32_t *d_seed;  // a further seed in device memory (null: none)
   uint32_t *d_kth;         // receives the k-th key when k objects were found, else 0 (may be null)
   uint32_t max_ctas_per_sm;  // 0: as many as fit
+  bool kth_only;           // threshold pass: only the bound from the published keys, into d_kth
 };
 
 // Enqueue one fused scan over rows [r0, r1) (or over the partitions of `ps`)
@@ -404,6 +406,22 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   for (uint32_t m = 0; m < qq; m++) {
     p.attr[m] = attr[m];
     p.w[m] = weights[attr[m]];
+  }
+  if (ps && ps->kth_only) {
+    // every CTA publishes up to 4k / grid keys (as the publish area allows), so the
+    // bound stays close to the k-th of the scanned rows even when their best objects
+    // sit in few CTAs
+    const uint32_t cap_m = (uint32_t)(((size_t)kMaxK + 2 * (size_t)h->num_sms * 8u) / (uint32_t)pl.grid);
+    p.pub = c->pub;
+    p.pub_m = std::max<uint32_t>(1u, std::min<uint32_t>(cap_m, pub_keys_per_cta(4 * (uint32_t)k, (uint32_t)pl.grid)));
+    p.pub_wait = kPubWaitPolls;
+    p.kth_only = 1;
+    p.out_kth_key = ps->d_kth;
+    p.out_ids = nullptr;
+    p.out_scores = nullptr;
+    p.out_threshold = nullptr;
+    p.out_count = nullptr;
+    p.out_stats = nullptr;
   }
   // Large k over a large table in id order: a threshold pass over every
   // kSampleStride-th tile first (its own launch, same kernel, no merge), whose bound
@@ -609,18 +627,17 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   for (int attempt = seeded ? 0 : 1; attempt < 2; attempt++) {
     CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), s));
     if (attempt == 0) {
-      PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr, kPrunedCtasPerSm};
+      PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr, kPrunedCtasPerSm, false};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                         dh->stats, &ps);
       scans += 1;
     } else {
-      // round 1's statistics go to pad[1..3] (its tiles to pad[3]); round 2 overwrites
-      // the result and the header's own statistics
-      PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1, kRound1CtasPerSm};
+      // round 1: a threshold pass (no merge, no result) over its partitions
+      PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1, kRound1CtasPerSm, true};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
-                        &dh->pad[1], &p1);
+                        nullptr, &p1);
       if (st != TOPK_OK) return st;
-      PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr, kPrunedCtasPerSm};
+      PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr, kPrunedCtasPerSm, false};
       st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                         dh->stats, &p2);
       scans += 2;
@@ -636,7 +653,7 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
       return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
     }
     if (learned && attempt == 0) cut_seen = hh->cut;
-    tiles += hh->stats[2] + (attempt == 1 ? hh->pad[3] : 0u);
+    tiles += hh->stats[2] + (attempt == 1 ? (uint64_t)m1 * tiles_per_part : 0u);
     if (attempt == 1) break;
     if (hh->count == kk) {
       accepted = 1;
@@ -767,6 +784,9 @@ float bf16_error_bound(const BatchQuery &b, const std::vector<float> &absmax) {
   return std::nextafter(e, INFINITY);
 }
 
+// Chunks of a batch whose served query counts are recorded (a 2^32-row table needs 20).
+constexpr uint32_t kMaxChunkLog = 64;
+
 // Batched exact top-k on the handle's primary stream (caller holds batch_mu):
 // bootstrap over the first rows, doubling chunks (score + reduce), finish.  Queries
 // flagged for a candidate overflow are answered again by the single-query scan.
@@ -840,7 +860,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     }
     if ((st = ensure(h->b_abf, habf.size())) != TOPK_OK) return st;
     if ((st = ensure(h->b_abf_act, habf.size())) != TOPK_OK) return st;
-    if ((st = ensure(h->b_amap, (nq + 1) * sizeof(uint32_t))) != TOPK_OK) return st;
+    if ((st = ensure(h->b_amap, (nq + 1 + kMaxChunkLog) * sizeof(uint32_t))) != TOPK_OK) return st;
     if ((st = ensure(h->b_err, sizeof(uint32_t))) != TOPK_OK) return st;
     // survivor records: one log per filter CTA
     const FilterPlan fp = plan_bf16_filter(nqq_all, 0, h->n, h->num_sms, h->batch_qt);
@@ -907,8 +927,10 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     CK(cudaMemsetAsync(dredo, 0, sizeof(uint32_t), s));
   }
   uint32_t hsw[2] = {0, 0};
+  uint32_t chunk = 0;  // chunk index while the launches are issued
   // the device work of the batch, from the first threshold to the results
   auto issue = [&]() -> int {
+  chunk = 0;
   if (use_learned) {
     // features and the model in one kernel, then each query's threshold starts at
     // its cut (prediction - margin) * S; no bootstrap
@@ -930,8 +952,11 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       if (fp.grid > log_ctas) return fail(TOPK_ERR_STATE, "filter grid %llu above its logs", (unsigned long long)fp.grid);
       // the queries still served by the filter, as compact tiles
       uint32_t *amap = static_cast<uint32_t *>(h->b_amap.p);
+      // the chunk's active count also goes to its slot of the per-batch record
+      uint32_t *logslot = chunk < kMaxChunkLog ? amap + nq + 1 + chunk : nullptr;
+      ++chunk;
       CK(launch_batch_active(dq, dst, nqq, static_cast<const uint8_t *>(h->b_abf.p),
-                             static_cast<uint8_t *>(h->b_abf_act.p), amap, amap + nq, s));
+                             static_cast<uint8_t *>(h->b_abf_act.p), amap, amap + nq, logslot, s));
       CK(launch_bf16_filter(fp, static_cast<const uint8_t *>(h->xbf.p), static_cast<const uint8_t *>(h->b_abf_act.p),
                             amap, amap + nq, r, e, dq, dst, dcand, static_cast<uint4 *>(h->b_log.p),
                             static_cast<uint2 *>(h->b_logh.p), kBf16LogCap, h->wait_limit,
@@ -1026,10 +1051,25 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   CK(cudaMemcpyAsync(hth.data(), h->b_thr.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
   uint32_t herr = 0;
+  std::vector<uint32_t> hact(kMaxChunkLog, 0);
   if (use_bf16) CK(cudaMemcpyAsync(&herr, h->b_err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (use_bf16)
+    CK(cudaMemcpyAsync(hact.data(), static_cast<uint32_t *>(h->b_amap.p) + nq + 1, kMaxChunkLog * 4,
+                       cudaMemcpyDeviceToHost, s));
   if (use_bf16) CK(cudaMemcpyAsync(hsw, dsw, sizeof(hsw), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (herr) return fail(TOPK_ERR_TIMEOUT, "BF16 filter: a bounded device-side wait ran out");
+  // MMA work of the filter: every served query tile (128 queries) against every object
+  // tile of the chunk, three passes of 2 * 16 flops per (query, object)
+  double filter_flops = 0;
+  if (use_bf16) {
+    uint32_t c = 0;  // the chunks as issued (the graph replays the same sequence)
+    for (uint64_t r = r_start, size = h->batch_boot; r < h->n && c < kMaxChunkLog; size *= 2, ++c) {
+      const uint64_t e = std::min<uint64_t>(h->n, r + size);
+      filter_flops += (double)((hact[c] + 127) / 128 * 128) * (double)((e - r + 255) / 256 * 256) * 96.0;
+      r = e;
+    }
+  }
   uint64_t switched_total = hsw[0], retired_total = 0;
   if (use_bf16)
     for (uint64_t j = 0; j < nq; j++)
@@ -1087,6 +1127,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     scans += h->last_batch_fallbacks;
     switched_total += h->last_batch_switched;
     retired_total += h->last_batch_retired;
+    filter_flops += h->last_batch_filter_flops;
     return TOPK_OK;
   };
   std::vector<uint64_t> sub;
@@ -1123,6 +1164,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   h->last_batch_fallbacks = scans;
   h->last_batch_switched = switched_total;
   h->last_batch_retired = retired_total;
+  h->last_batch_filter_flops = filter_flops;
   h->last_batch_method = use_learned ? TOPK_BATCH_LEARNED : use_bf16 ? TOPK_BATCH_BF16 : TOPK_BATCH_FP32;
   return TOPK_OK;
 }
@@ -1540,6 +1582,7 @@ int topk_query_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint
   h->last_batch_fallbacks = 0;
   h->last_batch_switched = 0;
   h->last_batch_retired = 0;
+  h->last_batch_filter_flops = 0;
   h->last_batch_cands = 0;
   h->last_batch_err_ratio = 0;
   h->last_batch_learned_misses = 0;
@@ -1651,6 +1694,12 @@ int topk_last_batch_info(topk_table_t h, int *method, double *max_err_ratio, uin
   if (method) *method = h->last_batch_method;
   if (max_err_ratio) *max_err_ratio = h->last_batch_err_ratio;
   if (learned_misses) *learned_misses = h->last_batch_learned_misses;
+  return TOPK_OK;
+}
+
+int topk_last_batch_filter_flops(topk_table_t h, double *flops) {
+  if (!h || !flops) return fail(TOPK_ERR_ARG, "null argument");
+  *flops = h->last_batch_filter_flops;
   return TOPK_OK;
 }
 

@@ -319,12 +319,13 @@ class Table:
         check(L.topk_last_batch_stats(self._h, C.byref(ms), C.byref(fb), C.byref(cand)))
         method, ratio, miss = C.c_int(), C.c_double(), C.c_uint64()
         check(L.topk_last_batch_info(self._h, C.byref(method), C.byref(ratio), C.byref(miss)))
-        sw, ret = C.c_uint64(), C.c_uint64()
+        sw, ret, fl = C.c_uint64(), C.c_uint64(), C.c_double()
         check(L.topk_last_batch_switched(self._h, C.byref(sw)))
         check(L.topk_last_batch_retired(self._h, C.byref(ret)))
+        check(L.topk_last_batch_filter_flops(self._h, C.byref(fl)))
         return {"device_ms": ms.value, "fallbacks": fb.value, "candidates": cand.value, "method": method.value,
                 "max_err_ratio": ratio.value, "learned_misses": miss.value, "switched_fp32": sw.value,
-                "retired": ret.value}
+                "retired": ret.value, "filter_flops": fl.value}
 
     def set_scan_tuning(self, max_ctas_per_sm=0):
         check(_lib.load().topk_set_scan_tuning(self._h, int(max_ctas_per_sm)))

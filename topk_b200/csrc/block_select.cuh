@@ -185,6 +185,75 @@ __device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, u
   return kept;
 }
 
+// The k-th largest key among the entries src(0..count) with key >= min_key (keys only:
+// equal keys count once each, no ids): the key v with fewer than k entries above v and
+// at least k at or above it; 0 when fewer than k entries qualify.  Four 8-bit digit
+// passes from the top.  `count` must be the same in every thread; `hist` holds 256 bins.
+template <int NT, class Src>
+__device__ uint32_t block_kth_key(const Src &src, uint32_t count, uint32_t min_key, uint32_t k, uint32_t *hist,
+                                  SelShared *sh) {
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  uint32_t v = 0;
+  for (uint32_t j = t; j < count; j += NT) v += (src(j).x >= min_key);
+  v = warp_sum_u32(v);
+  if (t == 0) sh->valid = 0;
+  __syncthreads();
+  if (lane == 0) atomicAdd(&sh->valid, v);
+  __syncthreads();
+  if (sh->valid < k) return 0u;  // uniform
+  uint32_t prefix = 0, need = k;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = t; b < 256; b += NT) hist[b] = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < count; base += NT) {  // uniform trip count
+      const uint32_t j = base + t;
+      uint32_t bin = 0xFFFFFFFFu;
+      if (j < count) {
+        const uint32_t key = src(j).x;
+        if (key >= min_key && (shift == 24 || (key >> (shift + 8)) == (prefix >> (shift + 8))))
+          bin = (key >> shift) & 255u;
+      }
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+      if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (t < 32) {  // lane l owns bins [255-8l-7, 255-8l], visited from high to low
+      const int top = 255 - 8 * t;
+      uint32_t local[8], sum = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        local[b] = hist[top - b];
+        sum += local[b];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (t >= o) incl += y;
+      }
+      const uint32_t excl = incl - sum;
+      if (excl < need && need <= incl) {
+        uint32_t run = excl;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          if (run + local[b] >= need) {
+            sh->digit = (uint32_t)(top - b);
+            sh->above = run;
+            break;
+          }
+          run += local[b];
+        }
+      }
+    }
+    __syncthreads();
+    need -= sh->above;
+    prefix |= sh->digit << shift;
+    __syncthreads();  // everyone has read the result before the next pass rewrites it
+  }
+  return prefix;
+}
+
 // Barrier after one stage of a bitonic network whose comparator i (thread i % NT, whole
 // warps) exchanges elements lo = 2i - (i & (stride - 1)) and lo + stride.  Up to stride
 // 32 the comparators of a warp touch only their own 64-element blocks, so the warp's

@@ -46,8 +46,8 @@ constexpr uint32_t kNoAllocMaxGrid = 8 * 148;
 constexpr uint32_t kNoAllocSlotEntries = 1u << 20;  // 8 MiB
 constexpr uint32_t kNoAllocMaxSlots = 2 * kNoAllocMaxGrid + kMaxLevels;
 constexpr uint32_t kNoAllocMaxGroups = kNoAllocMaxGrid + kMaxLevels;
-// published best keys before the merge: grid * M <= k + 2 * grid entries
-constexpr uint32_t kNoAllocPubEntries = kNoAllocMaxK + 2 * kNoAllocMaxGrid;
+// published best keys before the merge: at most 8 * kPubMaxPerWarp per CTA
+constexpr uint32_t kNoAllocPubEntries = 8 * kPubMaxPerWarp * kNoAllocMaxGrid;
 // layout: ScanScratch | done[groups] | slot_count[slots] | pad | slots[entries] | pub[entries]
 constexpr size_t kMetaBytes = sizeof(ScanScratch) + (size_t)kNoAllocMaxGroups * 4;
 constexpr size_t kSlotsOff = (kMetaBytes + (size_t)kNoAllocMaxSlots * 4 + 255) / 256 * 256;

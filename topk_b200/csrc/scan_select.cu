@@ -368,11 +368,11 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     }
   }
 
-  // ---- end of scan: reduce to <= k ----
+  // ---- end of scan: reduce to <= k (a threshold pass publishes from its buffer as is) ----
   bsync();
   if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
   bsync();
-  if (ctl->count > p.k) {
+  if (ctl->count > p.k && !p.kth_only) {
     const uint32_t c = ctl->cur;
     const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
                                                      cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
@@ -397,18 +397,47 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   // bounded wait: if it runs out they go on with the threshold they have, which is
   // still exact, only slower) and the merge tree then carries about k entries in all.
   if (p.pub) {
-    uint2 *res0 = cand0 + (size_t)ctl->cur * cap;
-    uint2 *spare = cand0 + (size_t)(ctl->cur ^ 1u) * cap;
-    const uint32_t M = p.pub_m;
-    uint32_t n_pub = ctl->count;
-    const uint2 *top = res0;
-    if (n_pub > M) {
-      n_pub = block_reduce<kScanThreads>(res0, n_pub, spare, M, 0u, hist, &ctl->sel);
-      top = spare;
+    const uint2 *res0 = cand0 + (size_t)ctl->cur * cap;
+    // Each warp publishes the best r = pub_m / 8 entries of its share of the buffer
+    // (entries j = t, t + 256, ...): every thread keeps its own best r, then r rounds of
+    // a warp maximum, each taken from the lane that holds it.  The CTA's pub_m keys are
+    // the best of 8 disjoint shares -- keys of distinct real objects, which is all the
+    // bound needs.  Unused places publish key 0.
+    {
+      constexpr int kR = kPubMaxPerWarp;
+      const uint32_t r = p.pub_m / 8u;
+      const uint32_t n = ctl->count;
+      uint64_t best[kR];
+#pragma unroll
+      for (int i = 0; i < kR; ++i) best[i] = 0ull;
+      for (uint32_t j = t; j < n; j += kScanThreads) {
+        const uint2 e = res0[j];
+        uint64_t c = composite(e.x, e.y);
+#pragma unroll
+        for (int i = 0; i < kR; ++i)  // insertion into the descending list
+          if (c > best[i]) {
+            const uint64_t x = best[i];
+            best[i] = c;
+            c = x;
+          }
+      }
+      uint2 *mine = p.pub + (size_t)blockIdx.x * p.pub_m + (size_t)(t >> 5) * r;
+      for (uint32_t i = 0; i < r; ++i) {
+        uint64_t m = best[0];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const uint64_t y = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+          m = y > m ? y : m;
+        }
+        if (m != 0ull && best[0] == m) {  // the one lane that holds it pops it
+#pragma unroll
+          for (int x = 0; x + 1 < kR; ++x) best[x] = best[x + 1];
+          best[kR - 1] = 0ull;
+        }
+        // (key, place): distinct entries even for padding
+        if (lane == 0) mine[i] = make_uint2((uint32_t)(m >> 32), blockIdx.x * p.pub_m + (t >> 5) * r + i);
+      }
     }
-    uint2 *mine = p.pub + (size_t)blockIdx.x * M;
-    for (uint32_t j = t; j < M; j += kScanThreads)  // (key, slot index): distinct composites
-      mine[j] = make_uint2(j < n_pub ? top[j].x : 0u, blockIdx.x * M + j);
     __threadfence();
     bsync();
     if (t == 0) ctl->is_last = atomicAdd(&p.scratch->pub_arrived, 1u) == gridDim.x - 1u ? 1u : 0u;
@@ -416,12 +445,13 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     if (p.kth_only && !ctl->is_last) return;  // a threshold pass: only the last CTA goes on
     if (ctl->is_last) {
       __threadfence();
-      // entries of key 0 are padding (or NaN scores, the lowest anyway): left out
-      const uint32_t kept = block_reduce<kScanThreads>(p.pub, gridDim.x * M, spare, p.k, 1u, hist, &ctl->sel);
+      // the k-th largest published key; entries of key 0 are padding (or NaN scores,
+      // the lowest anyway): left out
+      const uint32_t kth = block_kth_key<kScanThreads>(SmemSrc{p.pub}, gridDim.x * p.pub_m, 1u, p.k, hist, &ctl->sel);
       if (p.kth_only) {
         // the bound is the pass's result; every other CTA has left: put the counters back
         if (t == 0) {
-          *p.out_kth_key = kept == p.k ? ctl->sel.kept_min : 0u;
+          *p.out_kth_key = kth;
           p.scratch->g_thr = 0;
           p.scratch->acc_reductions = 0;
           p.scratch->acc_tiles = 0;
@@ -432,7 +462,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
         return;
       }
       if (t == 0) {
-        if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
+        if (kth) atomicMax(&p.scratch->g_thr, kth);
         __threadfence();
         atomicExch(&p.scratch->pub_ready, 1u);
       }

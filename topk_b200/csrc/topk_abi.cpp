@@ -89,7 +89,7 @@ struct Ctx {
   uint32_t *done = nullptr;
   uint32_t *slot_count = nullptr;
   uint2 *slots = nullptr;
-  uint2 *pub = nullptr;  // published best keys before the merge (kMaxK + 2 * max grid entries)
+  uint2 *pub = nullptr;  // published best keys before the merge (8 * kPubMaxPerWarp per CTA of the largest grid)
   uint32_t *d_seed_word = nullptr;  // a threshold pass's bound, read by the scan after it
   uint32_t max_slots = 0, max_groups = 0;
   size_t slot_entries = 0;  // capacity of `slots`
@@ -234,7 +234,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
   c->slot_count = reinterpret_cast<uint32_t *>(blk + c->meta_bytes);
   c->slots = reinterpret_cast<uint2 *>(blk + slots_off);
   if ((e = cudaMemset(blk, 0, slots_off)) != cudaSuccess) return bail(e, "scratch memset");
-  if ((e = cudaMalloc(&c->pub, ((size_t)kMaxK + 2 * (size_t)max_grid) * sizeof(uint2))) != cudaSuccess)
+  if ((e = cudaMalloc(&c->pub, (size_t)8 * kPubMaxPerWarp * max_grid * sizeof(uint2))) != cudaSuccess)
     return bail(e, "publish area");
   if ((e = cudaMalloc(&c->d_seed_word, 256)) != cudaSuccess) return bail(e, "seed word");
   if ((e = cudaMalloc(&c->d_res, result_bytes(kMaxK))) != cudaSuccess) return bail(e, "result block");
@@ -408,12 +408,11 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     p.w[m] = weights[attr[m]];
   }
   if (ps && ps->kth_only) {
-    // every CTA publishes up to 4k / grid keys (as the publish area allows), so the
+    // every CTA publishes up to 4k / grid keys (at most 8 * kPubMaxPerWarp), so the
     // bound stays close to the k-th of the scanned rows even when their best objects
     // sit in few CTAs
-    const uint32_t cap_m = (uint32_t)(((size_t)kMaxK + 2 * (size_t)h->num_sms * 8u) / (uint32_t)pl.grid);
     p.pub = c->pub;
-    p.pub_m = std::max<uint32_t>(1u, std::min<uint32_t>(cap_m, pub_keys_per_cta(4 * (uint32_t)k, (uint32_t)pl.grid)));
+    p.pub_m = pub_keys_per_cta(4 * (uint32_t)k, (uint32_t)pl.grid);
     p.pub_wait = kPubWaitPolls;
     p.kth_only = 1;
     p.out_kth_key = ps->d_kth;

@@ -105,12 +105,19 @@ struct ScanParams {
 };
 
 // The published-keys bound before the merge (ScanParams::pub): used for k >= this and
-// grids of at least kPubMinGrid CTAs; M = ceil(k / grid) + 1 keys per CTA, so the
-// array needs grid * M <= k + 2 * grid entries.
+// grids of at least kPubMinGrid CTAs; pub_keys_per_cta(k, grid) keys per CTA, so the
+// array needs grid * 8 * kPubMaxPerWarp entries.
 constexpr uint32_t kPubMinK = 64;
 constexpr uint32_t kPubMinGrid = 16;
 constexpr uint32_t kPubWaitPolls = 4096;  // ~64 ns each
-inline uint32_t pub_keys_per_cta(uint32_t k, uint32_t grid) { return (k + grid - 1) / grid + 1; }
+// Keys published per CTA: a multiple of its 8 warps, at least ceil(k / grid) + 1, at
+// most 8 * kPubMaxPerWarp.
+constexpr uint32_t kPubMaxPerWarp = 4;
+inline uint32_t pub_keys_per_cta(uint32_t k, uint32_t grid) {
+  const uint32_t want = (k + grid - 1) / grid + 1;
+  const uint32_t r = (want + 7) / 8;
+  return 8 * (r < kPubMaxPerWarp ? r : kPubMaxPerWarp);
+}
 // A full-table scan with k >= kSampleMinK first runs a threshold pass over every
 // kSampleStride-th tile (kth_only), when the table has at least kSampleMinTiles tiles,
 // and starts from its bound: few candidates ever reach the select.

@@ -544,11 +544,13 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
 
   // ---- root: sort and write the result (res has room for the padding) ----
   block_sort_desc<kScanThreads>(res, res_n);
-  for (uint32_t r = t; r < res_n; r += kScanThreads) {
-    const uint2 e = res[r];
-    const uint32_t pos = res_n - 1 - r;  // ascending output
-    p.out_ids[pos] = (uint64_t)e.y;
-    p.out_scores[pos] = key2f(e.x);
+  if (p.out_ids) {  // (a round that only wants the k-th key has no result arrays)
+    for (uint32_t r = t; r < res_n; r += kScanThreads) {
+      const uint2 e = res[r];
+      const uint32_t pos = res_n - 1 - r;  // ascending output
+      p.out_ids[pos] = (uint64_t)e.y;
+      p.out_scores[pos] = key2f(e.x);
+    }
   }
   if (t == 0) {
     if (p.out_threshold) *p.out_threshold = res_n ? key2f(res[res_n - 1].x) : 0.0f;

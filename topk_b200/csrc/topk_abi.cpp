@@ -408,13 +408,18 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
     p.w[m] = weights[attr[m]];
   }
   if (ps && ps->kth_only) {
-    // every CTA publishes up to 4k / grid keys (at most 8 * kPubMaxPerWarp), so the
+    // Every CTA publishes up to 4k / grid keys (at most 8 * kPubMaxPerWarp), so the
     // bound stays close to the k-th of the scanned rows even when their best objects
-    // sit in few CTAs
-    p.pub = c->pub;
-    p.pub_m = pub_keys_per_cta(4 * (uint32_t)k, (uint32_t)pl.grid);
-    p.pub_wait = kPubWaitPolls;
-    p.kth_only = 1;
+    // sit in few CTAs.  When the grid is too small for that (few tiles, large k) the
+    // round runs the merge tree instead, whose root writes the exact k-th key of the
+    // rows it scanned.
+    const uint32_t m = pub_keys_per_cta(4 * (uint32_t)k, (uint32_t)pl.grid);
+    if ((uint64_t)m * (uint64_t)pl.grid >= 4 * k) {
+      p.pub = c->pub;
+      p.pub_m = m;
+      p.pub_wait = kPubWaitPolls;
+      p.kth_only = 1;
+    }
     p.out_kth_key = ps->d_kth;
     p.out_ids = nullptr;
     p.out_scores = nullptr;

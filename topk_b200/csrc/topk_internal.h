@@ -79,7 +79,7 @@ struct ScanParams {
   uint32_t kth_only;
   uint32_t *slot_count; // entries per slot
   uint32_t *done;       // per-group arrival counters (zero between queries)
-  uint64_t *out_ids;    // min(k, rows) ids, ascending by score
+  uint64_t *out_ids;    // min(k, rows) ids, ascending by score (null with out_scores: none written)
   float *out_scores;
   float *out_threshold; // may be null
   uint32_t *out_count;  // may be null

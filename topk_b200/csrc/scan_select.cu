@@ -182,8 +182,12 @@ constexpr int scan_min_blocks() {
 }
 
 // QQ: compile-time attribute count (0 = runtime, any qq <= kMaxQ).  PART: partition
-// mode (p.part_list set): tiles of listed partitions of a reordered copy.
-template <int QQ, bool PART>
+// mode (p.part_list set): tiles of listed partitions of a reordered copy.  KTH: a
+// threshold pass (p.kth_only, p.pub set): no candidate buffer, no select and no merge;
+// each thread keeps the best kPubMaxPerWarp (key, row) words of its own objects in
+// registers, each warp publishes its best pub_m / 8 of them, and the last CTA writes
+// the k-th largest published key.
+template <int QQ, bool PART, bool KTH>
 __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_select_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem + kOffCtl);
@@ -258,6 +262,9 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     part_next = __ldg(p.part_list + (blockIdx.x >> p.part_shift));
     if (p.part_key) key_next = __ldg(p.part_key + (blockIdx.x >> p.part_shift));
   }
+  uint64_t kbest[KTH ? kPubMaxPerWarp : 1];  // KTH: this thread's best words, descending
+#pragma unroll
+  for (int b = 0; b < (KTH ? (int)kPubMaxPerWarp : 1); ++b) kbest[b] = 0ull;
   uint32_t i = 0;  // after the loop: the tiles this CTA scanned
   for (; i < my_tiles; ++i) {
     const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
@@ -266,9 +273,11 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     uint32_t thr = 0;
     uint64_t tile0;
     if constexpr (PART) {
-      thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
-      // nothing in this partition (nor in any later one of this CTA) can reach thr
-      if (key_next < thr) break;
+      if constexpr (!KTH) {
+        thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
+        // nothing in this partition (nor in any later one of this CTA) can reach thr
+        if (key_next < thr) break;
+      }
       tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
       if (i + 1 < my_tiles) {
         const uint64_t nx = (tix + gridDim.x) >> p.part_shift;
@@ -295,6 +304,23 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       s = score4<QQ>(p, wsm, qq, row0, !interior);
     }
 
+    if constexpr (KTH) {
+      // a threshold pass: every object of the tile against this thread's best words
+      const float sk[4] = {s.x, s.y, s.z, s.w};
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const bool ok = interior || (row0 + v >= p.row_begin && row0 + v < p.row_end);
+        uint64_t c = ok ? composite(f2key(sk[v]), (uint32_t)(row0 + v)) : 0ull;
+#pragma unroll
+        for (int b = 0; b < (int)kPubMaxPerWarp; ++b)
+          if (c > kbest[b]) {
+            const uint64_t x = kbest[b];
+            kbest[b] = c;
+            c = x;
+          }
+      }
+      continue;
+    }
     if constexpr (!PART) thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
     // key(score) >= thr  <=>  thr == 0 (everything, NaN included) or score >= thr_float(thr)
     const bool take_all = thr == 0u;
@@ -372,7 +398,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   bsync();
   if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
   bsync();
-  if (ctl->count > p.k && !p.kth_only) {
+  if (!KTH && ctl->count > p.k && !p.kth_only) {
     const uint32_t c = ctl->cur;
     const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
                                                      cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
@@ -396,7 +422,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   // the CTAs -- and raises the global threshold to it; the others wait for that (a
   // bounded wait: if it runs out they go on with the threshold they have, which is
   // still exact, only slower) and the merge tree then carries about k entries in all.
-  if (p.pub) {
+  if (KTH || p.pub) {
     const uint2 *res0 = cand0 + (size_t)ctl->cur * cap;
     // Each warp publishes the best r = pub_m / 8 entries of its share of the buffer
     // (entries j = t, t + 256, ...): every thread keeps its own best r, then r rounds of
@@ -409,8 +435,8 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       const uint32_t n = ctl->count;
       uint64_t best[kR];
 #pragma unroll
-      for (int i = 0; i < kR; ++i) best[i] = 0ull;
-      for (uint32_t j = t; j < n; j += kScanThreads) {
+      for (int i = 0; i < kR; ++i) best[i] = KTH ? kbest[i] : 0ull;
+      for (uint32_t j = t; !KTH && j < n; j += kScanThreads) {
         const uint2 e = res0[j];
         uint64_t c = composite(e.x, e.y);
 #pragma unroll
@@ -442,13 +468,13 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     bsync();
     if (t == 0) ctl->is_last = atomicAdd(&p.scratch->pub_arrived, 1u) == gridDim.x - 1u ? 1u : 0u;
     bsync();
-    if (p.kth_only && !ctl->is_last) return;  // a threshold pass: only the last CTA goes on
+    if ((KTH || p.kth_only) && !ctl->is_last) return;  // a threshold pass: only the last CTA goes on
     if (ctl->is_last) {
       __threadfence();
       // the k-th largest published key; entries of key 0 are padding (or NaN scores,
       // the lowest anyway): left out
       const uint32_t kth = block_kth_key<kScanThreads>(SmemSrc{p.pub}, gridDim.x * p.pub_m, 1u, p.k, hist, &ctl->sel);
-      if (p.kth_only) {
+      if (KTH || p.kth_only) {
         // the bound is the pass's result; every other CTA has left: put the counters back
         if (t == 0) {
           *p.out_kth_key = kth;
@@ -472,6 +498,8 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     }
     bsync();
   }
+
+  if constexpr (KTH) return;  // (the last CTA has returned above)
 
   // ---- merge tree ----
   const uint32_t k = p.k;
@@ -576,27 +604,32 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
 
 using ScanKernel = void (*)(ScanParams);
 
-// [part][q] for q = 1..16; [part][0] is the runtime-q kernel used for q > 16
-#define TOPK_SCAN_ROW(P)                                                                                \
-  {scan_select_kernel<0, P>,  scan_select_kernel<1, P>,  scan_select_kernel<2, P>,  scan_select_kernel<3, P>,  \
-   scan_select_kernel<4, P>,  scan_select_kernel<5, P>,  scan_select_kernel<6, P>,  scan_select_kernel<7, P>,  \
-   scan_select_kernel<8, P>,  scan_select_kernel<9, P>,  scan_select_kernel<10, P>, scan_select_kernel<11, P>, \
-   scan_select_kernel<12, P>, scan_select_kernel<13, P>, scan_select_kernel<14, P>, scan_select_kernel<15, P>, \
-   scan_select_kernel<16, P>}
-const ScanKernel kKernels[2][17] = {TOPK_SCAN_ROW(false), TOPK_SCAN_ROW(true)};
+// [kth][part][q] for q = 1..16; [..][0] is the runtime-q kernel used for q > 16
+#define TOPK_SCAN_ROW(P, K)                                                                                   \
+  {scan_select_kernel<0, P, K>,  scan_select_kernel<1, P, K>,  scan_select_kernel<2, P, K>,                   \
+   scan_select_kernel<3, P, K>,  scan_select_kernel<4, P, K>,  scan_select_kernel<5, P, K>,                   \
+   scan_select_kernel<6, P, K>,  scan_select_kernel<7, P, K>,  scan_select_kernel<8, P, K>,                   \
+   scan_select_kernel<9, P, K>,  scan_select_kernel<10, P, K>, scan_select_kernel<11, P, K>,                  \
+   scan_select_kernel<12, P, K>, scan_select_kernel<13, P, K>, scan_select_kernel<14, P, K>,                  \
+   scan_select_kernel<15, P, K>, scan_select_kernel<16, P, K>}
+const ScanKernel kKernels[2][2][17] = {{TOPK_SCAN_ROW(false, false), TOPK_SCAN_ROW(true, false)},
+                                       {TOPK_SCAN_ROW(false, true), TOPK_SCAN_ROW(true, true)}};
 #undef TOPK_SCAN_ROW
 
-ScanKernel kernel_for(uint32_t qq, bool part) { return kKernels[part ? 1 : 0][qq <= 16 ? qq : 0]; }
+ScanKernel kernel_for(uint32_t qq, bool part, bool kth = false) {
+  return kKernels[kth ? 1 : 0][part ? 1 : 0][qq <= 16 ? qq : 0];
+}
 
 }  // namespace
 
 cudaError_t scan_set_attributes(size_t smem_optin) {
-  for (const auto &row : kKernels)
-    for (ScanKernel f : row) {
-      const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(f),
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_optin);
-      if (e != cudaSuccess) return e;
-    }
+  for (const auto &mode : kKernels)
+    for (const auto &row : mode)
+      for (ScanKernel f : row) {
+        const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(f),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_optin);
+        if (e != cudaSuccess) return e;
+      }
   return cudaSuccess;
 }
 
@@ -612,13 +645,13 @@ constexpr size_t kSmemPerCtaReserve = 1024;
 // The shared-memory carveout last set on each scan kernel, per device (the attribute
 // is per function and device; setting it again costs a driver call).
 std::mutex g_carveout_mu;
-int g_carveout[64][2][17];
+int g_carveout[64][2][2][17];
 
-void set_carveout(const void *fn, bool part, uint32_t qq, int percent) {
+void set_carveout(const void *fn, bool part, uint32_t qq, int percent, bool kth = false) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
   std::lock_guard<std::mutex> lk(g_carveout_mu);
-  int &cur = g_carveout[dev][part ? 1 : 0][qq <= 16 ? qq : 0];
+  int &cur = g_carveout[dev][kth ? 1 : 0][part ? 1 : 0][qq <= 16 ? qq : 0];
   if (cur == percent + 1) return;  // stored plus one: 0 means not set yet
   if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, percent) == cudaSuccess)
     cur = percent + 1;
@@ -676,6 +709,9 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
       break;
     }
   set_carveout(fn, part, qq, (int)((size_kb * 100 + 227) / 228));
+  // the threshold-pass form of the kernel runs with the same plan
+  set_carveout(reinterpret_cast<const void *>(kernel_for(qq, part, true)), part, qq,
+               (int)((size_kb * 100 + 227) / 228), true);
   int fit = 0;  // what the driver reports with that preference
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kScanThreads, pl.smem) == cudaSuccess && fit >= 1)
     occ = std::min(occ, fit);
@@ -712,7 +748,10 @@ void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *tot
 
 cudaError_t launch_scan(const ScanPlan &pl, const ScanParams &p, cudaStream_t stream) {
   if (pl.stages < 1) return cudaErrorInvalidValue;
-  kernel_for(p.qq, p.part_list != nullptr)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
+  // a threshold pass needs the published-keys area
+  if (p.kth_only && (!p.pub || !p.out_kth_key || p.pub_m == 0 || p.pub_m > 8 * kPubMaxPerWarp))
+    return cudaErrorInvalidValue;
+  kernel_for(p.qq, p.part_list != nullptr, p.kth_only != 0)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
   return cudaGetLastError();
 }
 

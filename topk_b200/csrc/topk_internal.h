@@ -75,7 +75,9 @@ struct ScanParams {
   // Threshold pass (needs pub and out_kth_key): the published keys' k-th largest goes
   // to *out_kth_key (0 when fewer than k were published) and the scan ends there, no
   // merge and no result.  Run over a sample of the tiles (tile_step) it seeds the full
-  // scan that follows: k real objects score at least that key.
+  // scan that follows: k real objects score at least that key.  It runs the kernel's
+  // threshold-pass form: each thread keeps its best kPubMaxPerWarp (key, row) words in
+  // registers (no candidate buffer, no select), so pub_m <= 8 * kPubMaxPerWarp.
   uint32_t kth_only;
   uint32_t *slot_count; // entries per slot
   uint32_t *done;       // per-group arrival counters (zero between queries)

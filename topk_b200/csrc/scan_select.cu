@@ -229,79 +229,72 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   }
 
   uint32_t g_pending = 0;  // thread 0's in-flight copy of the global threshold
-  // next-tile prefetch (rows in id order only; a partition list resolves a tile's rows
-  // one tile ahead, too late to issue its loads early)
+  // next-tile prefetch: the loads of tile i + 1 are in flight while tile i is scored
   constexpr int kPQ = (QQ >= 1 && QQ <= kPrefetchQ) ? QQ : 1;
-  // tiles loaded ahead of the one being scored (two ahead for q <= 2 measured slower:
-  // the extra registers cost a CTA per SM)
-  constexpr int kDepth = 1;
-  constexpr bool prefetch = QQ >= 1 && QQ <= kPrefetchQ && !PART;
+  constexpr bool prefetch = QQ >= 1 && QQ <= kPrefetchQ;
   // queried columns: computed once for q >= 3; for q <= 2 per tile (two more 64-bit
   // registers would cost a CTA per SM there, measured slower)
   constexpr bool kHoist = kPQ >= 3;
   const float *col[kPQ];
 #pragma unroll
   for (int m = 0; m < kPQ; ++m) col[m] = kHoist ? p.table + (uint64_t)p.attr[m] * p.ld : nullptr;
-  auto load_tile = [&](uint32_t j, float4 *dst) {  // tile j of this CTA
-    const uint64_t tl = p.tile_begin + ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) * p.tile_step;
+  // partition mode: the partitions (and bounds) of tiles i and i + 1 are known at the
+  // start of tile i, the one of tile i + 2 is loaded during it
+  const uint32_t pmask = (1u << p.part_shift) - 1u;
+  uint32_t part_cur = 0, key_cur = 0xFFFFFFFFu, part_nx = 0, key_nx = 0xFFFFFFFFu;
+  auto part_of = [&](uint32_t j, uint32_t &part, uint32_t &key) {
+    const uint64_t x = ((uint64_t)blockIdx.x + (uint64_t)j * gridDim.x) >> p.part_shift;
+    part = __ldg(p.part_list + x);
+    if (p.part_key) key = __ldg(p.part_key + x);
+  };
+  if (PART) {
+    if (my_tiles > 0) part_of(0, part_cur, key_cur);
+    if (my_tiles > 1) part_of(1, part_nx, key_nx);
+  }
+  auto tile_row = [&](uint32_t j, uint32_t part) -> uint64_t {  // first row of tile j of this CTA
+    const uint64_t tix = blockIdx.x + (uint64_t)j * gridDim.x;
+    if constexpr (PART) return ((uint64_t)part << p.part_rows_log2) + (tix & pmask) * kTile;
+    return p.tile_begin + tix * p.tile_step;
+  };
+  auto load_tile = [&](uint32_t j, uint32_t part, float4 *dst) {
+    const uint64_t tl = tile_row(j, part);
     const float *c[kPQ];
 #pragma unroll
     for (int m = 0; m < kPQ; ++m) c[m] = kHoist ? col[m] : p.table + (uint64_t)p.attr[m] * p.ld;
     load_cols<kPQ>(p, c, tl + (uint64_t)t * kVec, !(tl >= p.row_begin && tl + kTile <= p.row_end), dst);
   };
-  float4 xn[kDepth][kPQ];
-  if (prefetch) {
-#pragma unroll
-    for (int dd = 0; dd < kDepth; ++dd)
-      if ((uint32_t)dd < my_tiles) load_tile(dd, xn[dd]);
-  }
-  // partition mode: the partition of the next tile (and its bound) is loaded one tile ahead
-  const uint32_t pmask = (1u << p.part_shift) - 1u;
-  uint32_t part_next = 0, key_next = 0xFFFFFFFFu;
-  if (PART && my_tiles) {
-    part_next = __ldg(p.part_list + (blockIdx.x >> p.part_shift));
-    if (p.part_key) key_next = __ldg(p.part_key + (blockIdx.x >> p.part_shift));
-  }
+  float4 xn[kPQ];
+  if (prefetch && my_tiles) load_tile(0, part_cur, xn);
   uint64_t kbest[KTH ? kPubMaxPerWarp : 1];  // KTH: this thread's best words, descending
 #pragma unroll
   for (int b = 0; b < (KTH ? (int)kPubMaxPerWarp : 1); ++b) kbest[b] = 0ull;
   uint32_t i = 0;  // after the loop: the tiles this CTA scanned
   for (; i < my_tiles; ++i) {
-    const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
     // every thread reads the same thresholds in tile i (see SmemCtl::thr_g); in id
     // order they are read after the scores, so they hold no register across the loads
     uint32_t thr = 0;
-    uint64_t tile0;
-    if constexpr (PART) {
-      if constexpr (!KTH) {
-        thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
-        // nothing in this partition (nor in any later one of this CTA) can reach thr
-        if (key_next < thr) break;
-      }
-      tile0 = ((uint64_t)part_next << p.part_rows_log2) + (uint64_t)(tix & pmask) * kTile;
-      if (i + 1 < my_tiles) {
-        const uint64_t nx = (tix + gridDim.x) >> p.part_shift;
-        part_next = __ldg(p.part_list + nx);
-        if (p.part_key) key_next = __ldg(p.part_key + nx);
-      }
-    } else {
-      tile0 = p.tile_begin + tix * p.tile_step;
+    if constexpr (PART && !KTH) {
+      thr = max(ctl->thr_local, ctl->thr_g[i & 1u]);
+      // nothing in this partition (nor in any later one of this CTA) can reach thr
+      if (key_cur < thr) break;
     }
+    const uint64_t tile0 = tile_row(i, part_cur);
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
     const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
     float4 s;
     if (prefetch) {
       float4 x[kPQ];
 #pragma unroll
-      for (int m = 0; m < kPQ; ++m) x[m] = xn[0][m];
-#pragma unroll
-      for (int dd = 0; dd + 1 < kDepth; ++dd)
-#pragma unroll
-        for (int m = 0; m < kPQ; ++m) xn[dd][m] = xn[dd + 1][m];
-      if (i + kDepth < my_tiles) load_tile(i + kDepth, xn[kDepth - 1]);
+      for (int m = 0; m < kPQ; ++m) x[m] = xn[m];
+      if (i + 1 < my_tiles) load_tile(i + 1, part_nx, xn);
       s = score_cols<kPQ>(p, x);
     } else {
       s = score4<QQ>(p, wsm, qq, row0, !interior);
+    }
+    if constexpr (PART) {
+      part_cur = part_nx;
+      key_cur = key_nx;
+      if (i + 2 < my_tiles) part_of(i + 2, part_nx, key_nx);
     }
 
     if constexpr (KTH) {

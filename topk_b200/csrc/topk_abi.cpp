@@ -524,7 +524,7 @@ std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t
                                      const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride);
 
 constexpr uint32_t kPrunedCtasPerSm = 3;  // CTAs per SM of a pruned scan
-constexpr uint32_t kRound1CtasPerSm = 2;  // and of its first round
+constexpr uint32_t kRound1CtasPerSm = 0;  // and of its first round (0: as many as fit)
 
 // Exact top-k over the partitioned copy as one device pipeline on the context's
 // stream; nothing is decided on the host between the launches.

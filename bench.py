@@ -412,19 +412,21 @@ def reference_index_build(d, sample_rows=1 << 22):
 
 def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=1000000, n_test=10000, seed=4):
     """Partitioned workload: an anticorrelated n x d table in partitions of part_rows
-    rows; the learned model fitted on n_train queries labelled exactly; n_test fresh
-    queries (attribute subsets of size U{2..d}, k log-uniform in [16, 1024]) answered
-    by the plain full scan, the plain pruned method and the learned pruned method,
-    results checked identical; host wall time per query (each call is synchronous).
-    Then the partitions are rebuilt in VTA's order (one range and the threaded build's
-    16), then in PTA's, each time the first 500 queries answered pruned again (checked
-    identical); the reference's own VTA and PTA index builds are timed on a 2^22-row
-    sample on the host."""
+    rows (the kd order: median splits along the attribute of widest spread); the
+    learned model fitted on n_train queries labelled exactly; n_test fresh queries
+    (attribute subsets of size U{2..d}, k log-uniform in [16, 1024]) answered by the
+    plain full scan, the plain pruned method and the learned pruned method, results
+    checked identical; host wall time per query (each call is synchronous).  Then the
+    partitions are rebuilt in the Morton order, in VTA's order (one range and the
+    threaded build's 16), then in PTA's, each time the first 500 queries answered
+    pruned again (checked identical); the reference's own VTA and PTA index builds are
+    timed on a 2^22-row sample on the host."""
     t = T.Table(n, d, device=device)
     t.generate(T.DIST_ANTICORRELATED, 0)
     t.normalize()
+    t.build_partitions(part_rows, order=T.ORDER_KD)  # first build: module loading, allocations
     b0 = time.perf_counter()
-    t.build_partitions(part_rows)
+    t.build_partitions(part_rows, order=T.ORDER_KD)
     build_s = time.perf_counter() - b0
     fit = t.learned_fit(n_train=n_train, n_val=max(1000, n_train // 10), kmin=16, kmax=1024, qmin=2, qmax=d,
                         epochs=30, miss_rate=0.01, seed=seed)
@@ -466,8 +468,8 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=1000000, n_test=100
     # the first n_vta queries again over partitions in VTA's and in PTA's order
     # (cpu/VTA.h:121-135, cpu/PTA.h:88-236)
     index_orders = {}
-    for name, order in (("vta_order", T.ORDER_VTA), ("vta_threads_order", T.ORDER_VTA_THREADS),
-                        ("pta_order", T.ORDER_PTA)):
+    for name, order in (("morton_order", T.ORDER_MORTON), ("vta_order", T.ORDER_VTA),
+                        ("vta_threads_order", T.ORDER_VTA_THREADS), ("pta_order", T.ORDER_PTA)):
         b0 = time.perf_counter()
         t.build_partitions(part_rows, order=order)  # first build: module loading, allocations
         first_s = time.perf_counter() - b0
@@ -491,7 +493,7 @@ def run_pruned(T, device, n, d=8, part_rows=1 << 16, n_train=1000000, n_test=100
     t.close()
     qps = {key: n_test / v for key, v in times.items()}
     return {
-        "workload": f"anticorrelated n={n} x {d}, {P} partitions of {part_rows} rows; {n_test} test queries, "
+        "workload": f"anticorrelated n={n} x {d}, {P} partitions of {part_rows} rows (kd order); {n_test} test queries, "
                     f"|attrs| U{{2..{d}}}, k log-uniform [16, 1024]; model fitted on {n_train} queries",
         "queries_per_s": qps,
         "speedup_pruned_vs_full_scan": qps["pruned"] / qps["full_scan"],

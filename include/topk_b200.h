@@ -273,6 +273,15 @@ int topk_build_partitions(topk_table_t h, uint32_t part_rows);
                              * VTA's order, layers by number.  Needs d <= 32 and
                              * n <= TOPK_SKYLINE_MAX_ROWS; the layer build compares
                              * O(n^2 d) pairs. */
+#define TOPK_ORDER_KD 5     /* No reference counterpart: the partitions are the leaves of a
+                             * balanced binary tree over the rows; each node (a range of
+                             * whole partitions) is split at its middle partition boundary
+                             * after its rows are sorted, stably, by the attribute whose
+                             * values spread widest in it (FP32 max - min, the lower
+                             * attribute on a tie).  Boxes shrink in the attributes that
+                             * vary most, so partition bounds are tighter than in the
+                             * Morton order.  n < 2^31; about 20*n + 8*P*d bytes of scratch
+                             * while it runs. */
 /* In the VTA and PTA orders ties go to the lower row id (the reference's sorts are not
  * stable and leave them unspecified: rows sharing a minimum position, equal values);
  * PTA's angles order as their tangents, which are compared. */

@@ -102,6 +102,66 @@ def pta_order(table):
     return np.lexsort((np.arange(n), minpos)).astype(np.uint32)
 
 
+def key2f(k):
+    k = np.asarray(k, np.uint64)
+    u = np.where(k & 0x80000000, k & 0x7FFFFFFF, (~k) & 0xFFFFFFFF).astype(np.uint32)
+    return u.view(np.float32)
+
+
+def kd_nodes(parts, P, level):
+    """Node id at `level` of every partition number in `parts`: the path from the root
+    over [0, P), each node [lo, hi) split at lo + ceil((hi - lo) / 2), left 0, right 1."""
+    parts = np.asarray(parts, np.int64)
+    lo = np.zeros_like(parts)
+    hi = np.full_like(parts, P)
+    node = np.zeros_like(parts)
+    for _ in range(level):
+        mid = lo + (hi - lo + 1) // 2
+        right = parts >= mid
+        node = 2 * node + right
+        lo = np.where(right, mid, lo)
+        hi = np.where(right, hi, mid)
+    return node
+
+
+def kd_order(table, part_rows):
+    """The kd order of this library's partitioned copy (no reference counterpart; the
+    device build is topk_b200/csrc/partition.cu): level by level, every node's rows are
+    sorted stably by the attribute whose values spread widest in the node (FP32 max -
+    min over the non-NaN values, 0 for a node without any; the lower attribute on a
+    tie), the node's range splitting at its middle partition boundary.  Returns the row
+    permutation (uint32)."""
+    d, n = table.shape
+    lg = int(part_rows).bit_length() - 1
+    P = (n + part_rows - 1) // part_rows
+    levels = max(0, (P - 1).bit_length())
+    perm = np.arange(n, dtype=np.int64)
+    parts = np.arange(n, dtype=np.int64) >> lg
+    for level in range(levels):
+        nodes = 1 << level
+        node = kd_nodes(parts, P, level)
+        vals = table[:, perm]
+        keys = f2key(vals)
+        nan = np.isnan(vals)
+        spread = np.zeros((nodes, d), np.float32)
+        # nodes are ranges of positions in node order: reduce over each range
+        present, starts = np.unique(node, return_index=True)
+        for m in range(d):
+            kmax = np.zeros(nodes, np.uint64)
+            kmin = np.full(nodes, 0xFFFFFFFF, np.uint64)
+            kmax[present] = np.maximum.reduceat(np.where(nan[m], 0, keys[m]), starts)
+            kmin[present] = np.minimum.reduceat(np.where(nan[m], 0xFFFFFFFF, keys[m]).astype(np.uint64), starts)
+            has = kmax != 0
+            sp = np.zeros(nodes, np.float32)
+            sp[has] = key2f(kmax[has]) - key2f(kmin[has])
+            sp[np.isnan(sp)] = 0.0
+            spread[:, m] = sp
+        attr = np.argmax(spread, axis=1)  # first of equal maxima
+        k = (node.astype(np.uint64) << np.uint64(32)) | keys[attr[node], np.arange(n)]
+        perm = perm[np.argsort(k, kind="stable")]
+    return perm.astype(np.uint32)
+
+
 def same_order_up_to_ties(table, groups, perm_a, perm_b):
     """True when two row orders agree up to the ties the reference leaves unspecified:
     the same group and the same minimum position at every place (rows sharing both

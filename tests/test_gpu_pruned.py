@@ -145,7 +145,7 @@ def test_pruned_ties_in_reordered_rows_go_to_the_lower_original_id():
                 assert got[3][2] == 1
 
 
-@pytest.mark.parametrize("order", ["vta", "vta16", "pta"])
+@pytest.mark.parametrize("order", ["vta", "vta16", "pta", "kd"])
 @pytest.mark.parametrize("n,d,dist,ties", [(200003, 6, 0, False), (200003, 6, 1, False), (200003, 6, 2, False),
                                           (200003, 6, 3, False), (200003, 6, 0, True), (65536, 1, 0, False),
                                           (70001, 2, 2, False), (50001, 20, 0, False)])
@@ -154,9 +154,10 @@ def test_index_order_matches_oracle(order, n, d, dist, ties):
     VTA::init (one row range, or 16 as its threaded build) and PTA::polar +
     create_partitions, ties by the lower id; the partitioned copy holds the rows in
     that order and its block bounds are those rows' maxima."""
-    from oracle.vta_oracle import pta_order, vta_order
-    codes = {"vta": T.ORDER_VTA, "vta16": T.ORDER_VTA_THREADS, "pta": T.ORDER_PTA}
-    want = {"vta": lambda x: vta_order(x), "vta16": lambda x: vta_order(x, 16), "pta": pta_order}
+    from oracle.vta_oracle import kd_order, pta_order, vta_order
+    codes = {"vta": T.ORDER_VTA, "vta16": T.ORDER_VTA_THREADS, "pta": T.ORDER_PTA, "kd": T.ORDER_KD}
+    want = {"vta": lambda x: vta_order(x), "vta16": lambda x: vta_order(x, 16), "pta": pta_order,
+            "kd": lambda x: kd_order(x, 1024)}
     with T.Table(n, d) as t:
         t.generate(dist, 11 + dist)
         t.normalize()
@@ -172,7 +173,7 @@ def test_index_order_matches_oracle(order, n, d, dist, ties):
         assert np.array_equal(maxs, blocks.max(axis=2).T)
 
 
-@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("order", [1, 2, 3, 5])
 @pytest.mark.parametrize("dist", [2, 0])
 def test_pruned_on_vta_pta_partitions_matches_oracle(dist, order):
     n, d = (1 << 19) + 77, 8
@@ -194,6 +195,55 @@ def test_pruned_on_vta_pta_partitions_matches_oracle(dist, order):
         t.build_partitions(4096)
         w, a = H.random_query(rng, d)
         H.assert_same_result(t.query_pruned(64, w, a)[:3], O.topk_numpy(tn, 64, w, a))
+
+
+def test_kd_order_with_nan_and_constant_columns_matches_oracle():
+    """The kd order on a table with NaN values, a constant column and infinities: the
+    spread rule leaves NaN out and counts a NaN or missing spread as 0; the device
+    permutation equals the restatement and pruned queries stay exact."""
+    from oracle.vta_oracle import kd_order
+    n, d = 150001, 5
+    rng = np.random.default_rng(8)
+    x = rng.random((d, n), dtype=np.float32)
+    x[1] = 0.25  # constant column: spread 0 in every node
+    x[2, rng.integers(0, n, 500)] = np.nan
+    x[3, rng.integers(0, n, 50)] = np.inf
+    x[4, :4096] = np.nan  # a long run of NaN values in one attribute
+    with T.Table(n, d) as t:
+        t.upload(x)
+        t.build_partitions(1024, order=T.ORDER_KD)
+        assert np.array_equal(t.partition_ids(), kd_order(x, 1024))
+        for k in (1, 100, 1000):
+            w, a = H.random_query(rng, d)
+            a = np.array([0, 1, 3], np.uint8)
+            H.assert_same_result(t.query_pruned(k, w, a)[:3], O.topk_numpy(x, k, w, a))
+
+
+def test_kd_order_prunes_more_than_morton_on_anticorrelated_data():
+    """The kd order's partition boxes follow the attributes that vary most, so on
+    anticorrelated data a query scans fewer partitions than over the Morton order."""
+    n, d = 1 << 22, 8
+    rng = np.random.default_rng(77)
+    fr = {}
+    with T.Table(n, d) as t:
+        t.generate(2, 9)
+        t.normalize()
+        tn = t.download()
+        qs = []
+        for j in range(40):
+            w, a = H.random_query(rng, d)
+            qs.append((int(rng.choice([16, 100, 1000])), w, a))
+        for order in (T.ORDER_MORTON, T.ORDER_KD):
+            t.build_partitions(4096, order=order)
+            sc = []
+            for k, w, a in qs:
+                ids, s_, th, st = t.query_pruned(k, w, a)
+                if len(sc) < 5:
+                    H.assert_same_result((ids, s_, th), O.topk_numpy(tn, k, w, a))
+                sc.append(st[0] / st[1])
+            fr[order] = float(np.mean(sc))
+    print(f"fraction of partitions scanned: Morton {fr[T.ORDER_MORTON]:.3f}, kd {fr[T.ORDER_KD]:.3f}")
+    assert fr[T.ORDER_KD] < fr[T.ORDER_MORTON]
 
 
 def test_partition_order_errors():

@@ -144,3 +144,55 @@ def test_orders_pinned_to_reference(d, imp, n):
     if imp == 2:  # PTA does not depend on IMP
         ref_perm = rows_to_ids(tn, ref_index_rows("pta", raw, imp)[0])
         assert same_order_up_to_ties(tn, pta_part_ids(tn), ref_perm, pta_order(tn))
+
+
+def kd_order_loops(table, part_rows):
+    """The kd order node by node with Python's stable sort: a node is a range of whole
+    partitions [lo, hi) of the order, split at lo + ceil((hi - lo) / 2) after its rows
+    are sorted by the attribute of widest spread (FP32 max - min over non-NaN values,
+    the lower attribute on a tie)."""
+    d, n = table.shape
+    P = (n + part_rows - 1) // part_rows
+    order = list(range(n))
+
+    def split(lo, hi):
+        if hi - lo <= 1:
+            return
+        a, b = lo * part_rows, min(n, hi * part_rows)
+        rows = order[a:b]
+        best, bs = 0, np.float32(0)
+        for m in range(d):
+            v = [table[m, r] for r in rows if not np.isnan(table[m, r])]
+            s = np.float32(max(v)) - np.float32(min(v)) if v else np.float32(0)
+            if np.isnan(s):
+                s = np.float32(0)
+            if m == 0 or s > bs:
+                best, bs = m, s
+        key = lambda r: (0, 0.0) if np.isnan(table[best, r]) else (1, float(table[best, r]))
+        order[a:b] = sorted(rows, key=key)
+        mid = lo + (hi - lo + 1) // 2
+        split(lo, mid)
+        split(mid, hi)
+
+    split(0, P)
+    return np.array(order, np.uint32)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_kd_order_matches_node_by_node_loops(seed):
+    """The level-by-level numpy kd order puts the same rows in every partition as the
+    node-by-node recursion (stable sorts: equal values keep the order of the level
+    before).  Inside a partition the orders may differ: the level form sorts a node
+    that is already a single partition again at the later levels."""
+    from oracle.vta_oracle import kd_order
+    rng = np.random.default_rng(100 + seed)
+    d, n, R = int(rng.integers(1, 6)), int(rng.integers(1, 3000)), int(2 ** rng.integers(4, 8))
+    if seed % 2:
+        table = rng.integers(0, 4, size=(d, n)).astype(np.float32) / 4
+    else:
+        table = rng.random((d, n), dtype=np.float32)
+    if seed % 3 == 0 and n > 10:
+        table[0, rng.integers(0, n, n // 10)] = np.nan
+    a, b = kd_order(table, R), kd_order_loops(table, R)
+    for p0 in range(0, n, R):
+        assert np.array_equal(np.sort(a[p0:p0 + R]), np.sort(b[p0:p0 + R]))

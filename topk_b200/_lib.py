@@ -28,7 +28,7 @@ DIST_CORRELATED, DIST_INDEPENDENT, DIST_ANTICORRELATED, DIST_MIXED = 0, 1, 2, 3
 
 # topk_query_batch methods (TOPK_BATCH_* in include/topk_b200.h)
 BATCH_AUTO, BATCH_LOOP, BATCH_FP32, BATCH_BF16, BATCH_LEARNED = 0, 1, 2, 3, 4
-ORDER_MORTON, ORDER_VTA, ORDER_PTA, ORDER_VTA_THREADS, ORDER_SLA = 0, 1, 2, 3, 4
+ORDER_MORTON, ORDER_VTA, ORDER_PTA, ORDER_VTA_THREADS, ORDER_SLA, ORDER_KD = 0, 1, 2, 3, 4, 5
 
 
 class TopKError(RuntimeError):

@@ -189,13 +189,25 @@ __device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, u
 // equal keys count once each, no ids): the key v with fewer than k entries above v and
 // at least k at or above it; 0 when fewer than k entries qualify.  Four 8-bit digit
 // passes from the top.  `count` must be the same in every thread; `hist` holds 256 bins.
+// The source may live in global memory: each thread loads kKthBatch entries before it
+// uses any, so a pass waits for one load latency per NT * kKthBatch entries.
+constexpr int kKthBatch = 16;
 template <int NT, class Src>
 __device__ uint32_t block_kth_key(const Src &src, uint32_t count, uint32_t min_key, uint32_t k, uint32_t *hist,
                                   SelShared *sh) {
   const int t = threadIdx.x;
   const int lane = t & 31;
   uint32_t v = 0;
-  for (uint32_t j = t; j < count; j += NT) v += (src(j).x >= min_key);
+  for (uint32_t base = 0; base < count; base += NT * kKthBatch) {
+    uint32_t key[kKthBatch];
+#pragma unroll
+    for (int u = 0; u < kKthBatch; ++u) {
+      const uint32_t j = base + (uint32_t)u * NT + t;
+      key[u] = j < count ? src(j).x : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kKthBatch; ++u) v += (base + (uint32_t)u * NT + t < count && key[u] >= min_key);
+  }
   v = warp_sum_u32(v);
   if (t == 0) sh->valid = 0;
   __syncthreads();
@@ -206,16 +218,22 @@ __device__ uint32_t block_kth_key(const Src &src, uint32_t count, uint32_t min_k
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int b = t; b < 256; b += NT) hist[b] = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < count; base += NT) {  // uniform trip count
-      const uint32_t j = base + t;
-      uint32_t bin = 0xFFFFFFFFu;
-      if (j < count) {
-        const uint32_t key = src(j).x;
-        if (key >= min_key && (shift == 24 || (key >> (shift + 8)) == (prefix >> (shift + 8))))
-          bin = (key >> shift) & 255u;
+    for (uint32_t base = 0; base < count; base += NT * kKthBatch) {  // uniform trip count
+      uint32_t key[kKthBatch];
+#pragma unroll
+      for (int u = 0; u < kKthBatch; ++u) {
+        const uint32_t j = base + (uint32_t)u * NT + t;
+        key[u] = j < count ? src(j).x : 0u;
       }
-      const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
-      if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+#pragma unroll
+      for (int u = 0; u < kKthBatch; ++u) {
+        uint32_t bin = 0xFFFFFFFFu;
+        if (base + (uint32_t)u * NT + t < count && key[u] >= min_key &&
+            (shift == 24 || (key[u] >> (shift + 8)) == (prefix >> (shift + 8))))
+          bin = (key[u] >> shift) & 255u;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+        if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+      }
     }
     __syncthreads();
     if (t < 32) {  // lane l owns bins [255-8l-7, 255-8l], visited from high to low

@@ -243,6 +243,30 @@ __device__ __forceinline__ uint32_t part_bound_key(const float *__restrict__ pmi
 // partition number) in shared memory by a bitonic network; plist[i] = partition of
 // rank i, pkey[i] = its bound key.
 constexpr uint32_t kOrderThreads = 1024;
+
+// Stages with strides st, st/2, .., 1 (st <= 32) of a descending bitonic sort's merge of
+// `size`, on the 64-entry chunk at `base` that one warp holds: x0 = entry base + lane,
+// x1 = entry base + 32 + lane.  Entry i is compared with i ^ stride; the lower of the
+// two keeps the larger value where (i & size) == 0, the smaller elsewhere.
+__device__ __forceinline__ void warp_bitonic_stages(unsigned long long &x0, unsigned long long &x1, uint32_t base,
+                                                    uint32_t size, uint32_t st, uint32_t lane) {
+  for (uint32_t stride = st; stride > 0; stride >>= 1) {
+    if (stride == 32) {
+      const bool desc = ((base + lane) & size) == 0;
+      const unsigned long long hi = x0 > x1 ? x0 : x1, lo = x0 > x1 ? x1 : x0;
+      x0 = desc ? hi : lo;
+      x1 = desc ? lo : hi;
+    } else {
+      const unsigned long long y0 = __shfl_xor_sync(0xFFFFFFFFu, x0, stride);
+      const unsigned long long y1 = __shfl_xor_sync(0xFFFFFFFFu, x1, stride);
+      const uint32_t i0 = base + lane, i1 = base + 32 + lane;
+      const bool k0 = ((i0 & stride) == 0) == ((i0 & size) == 0);  // keep the larger
+      const bool k1 = ((i1 & stride) == 0) == ((i1 & size) == 0);
+      x0 = k0 ? (x0 > y0 ? x0 : y0) : (x0 < y0 ? x0 : y0);
+      x1 = k1 ? (x1 > y1 ? x1 : y1) : (x1 < y1 ? x1 : y1);
+    }
+  }
+}
 __global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *__restrict__ pmin,
                                                                   const float *__restrict__ pmax, uint32_t P,
                                                                   uint32_t Ppad, uint32_t d, const PartQuery q,
@@ -255,8 +279,20 @@ __global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *
   for (uint32_t i = t; i < Ppad; i += kOrderThreads)
     ent[i] = i < P ? ((unsigned long long)part_bound_key(pmin, pmax, d, i, q) << 32) | (0xFFFFFFFFu - i) : 0ull;
   __syncthreads();
-  for (uint32_t size = 2; size <= Ppad; size <<= 1) {
-    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+  // Bitonic sort, descending.  Strides up to 32 run in registers: a warp holds a chunk
+  // of 64 entries (lane l: entries base + l and base + 32 + l) and exchanges by
+  // shuffles; larger strides run in shared memory with a block barrier each.
+  const uint32_t lane = t & 31, warp = t >> 5;
+  for (uint32_t c = warp; c < Ppad / 64; c += kOrderThreads / 32) {  // sizes 2 .. 64
+    const uint32_t base = c * 64;
+    unsigned long long x0 = ent[base + lane], x1 = ent[base + 32 + lane];
+    for (uint32_t size = 2; size <= 64; size <<= 1) warp_bitonic_stages(x0, x1, base, size, size >> 1, lane);
+    ent[base + lane] = x0;
+    ent[base + 32 + lane] = x1;
+  }
+  __syncthreads();
+  for (uint32_t size = 128; size <= Ppad; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride >= 64; stride >>= 1) {
       for (uint32_t i = t; i < Ppad / 2; i += kOrderThreads) {
         const uint32_t lo = 2 * i - (i & (stride - 1));
         const uint32_t hi = lo + stride;
@@ -267,7 +303,14 @@ __global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *
           ent[hi] = x;
         }
       }
-      bitonic_stage_sync(stride);
+      __syncthreads();
+    }
+    for (uint32_t c = warp; c < Ppad / 64; c += kOrderThreads / 32) {  // strides 32 .. 1
+      const uint32_t base = c * 64;
+      unsigned long long x0 = ent[base + lane], x1 = ent[base + 32 + lane];
+      warp_bitonic_stages(x0, x1, base, size, 32, lane);
+      ent[base + lane] = x0;
+      ent[base + 32 + lane] = x1;
     }
     __syncthreads();
   }
@@ -363,6 +406,170 @@ cudaError_t launch_index_order(const float *table, uint64_t ld, uint32_t d, uint
   return cudaGetLastError();
 }
 
+namespace {
+
+// ---- kd order: median splits along the attribute of widest spread ----
+//
+// The partitions are the leaves of a balanced binary tree over the rows: a node is a
+// range of whole partitions [lo, hi) of the order; it splits into [lo, mid) and
+// [mid, hi), mid = lo + ceil((hi - lo) / 2), by sorting its rows by the attribute
+// whose values spread widest in it (largest max - min, FP32; the lower attribute on a
+// tie), so the first half holds its lower values.  Level L sorts every node of level L
+// at once: a stable radix sort of (node << 32 | order key of the value) with the row
+// ids, which keeps each node's rows in its own range.  Node ids at level L follow the
+// path from the root (left 0, right 1), so they increase along the rows.
+
+__device__ __forceinline__ uint32_t kd_node_of(uint32_t part, uint32_t P, uint32_t level) {
+  uint32_t lo = 0, hi = P, id = 0;
+  for (uint32_t l = 0; l < level; ++l) {
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    const uint32_t right = part >= mid ? 1u : 0u;
+    id = 2 * id + right;
+    if (right) lo = mid; else hi = mid;
+  }
+  return id;
+}
+
+// Per node and attribute: the largest and smallest order key of the node's values
+// (NaN left out).  One block per chunk of 1024 positions (a chunk lies in one
+// partition, so in one node); stats: [node][d] max keys, then [node][d] min keys.
+__global__ void __launch_bounds__(256) kd_stats_kernel(const float *__restrict__ table, uint64_t ld, uint32_t d,
+                                                       uint64_t n, const uint32_t *__restrict__ perm, uint32_t lg,
+                                                       uint32_t P, uint32_t level, uint32_t nodes,
+                                                       uint32_t *__restrict__ stats) {
+  __shared__ uint32_t smax[32], smin[32];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t chunks = (n + 1023) / 1024;
+  for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+    const uint64_t base = c * 1024;
+    const uint32_t node = kd_node_of((uint32_t)(base >> lg), P, level);
+    uint32_t id[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const uint64_t pos = base + threadIdx.x + 256u * v;
+      id[v] = pos < n ? perm[pos] : 0xFFFFFFFFu;
+    }
+    for (uint32_t m0 = 0; m0 < d; m0 += 32) {
+      const uint32_t dm = min(32u, d - m0);
+      if (threadIdx.x < dm) {
+        smax[threadIdx.x] = 0u;
+        smin[threadIdx.x] = 0xFFFFFFFFu;
+      }
+      __syncthreads();
+      for (uint32_t m = 0; m < dm; ++m) {
+        uint32_t kmax = 0u, kmin = 0xFFFFFFFFu;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          if (id[v] == 0xFFFFFFFFu) continue;
+          const float x = __ldg(table + (uint64_t)(m0 + m) * ld + id[v]);
+          if (x != x) continue;
+          const uint32_t k = f2key(x);
+          kmax = max(kmax, k);
+          kmin = min(kmin, k);
+        }
+        kmax = __reduce_max_sync(0xFFFFFFFFu, kmax);
+        kmin = __reduce_min_sync(0xFFFFFFFFu, kmin);
+        if (lane == 0) {
+          atomicMax(&smax[m], kmax);
+          atomicMin(&smin[m], kmin);
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < dm) {
+        atomicMax(stats + (size_t)node * d + m0 + threadIdx.x, smax[threadIdx.x]);
+        atomicMin(stats + (size_t)nodes * d + (size_t)node * d + m0 + threadIdx.x, smin[threadIdx.x]);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Per node: the attribute of widest spread (0 for a node without values).
+__global__ void kd_split_kernel(const uint32_t *__restrict__ stats, uint32_t d, uint32_t nodes,
+                                uint32_t *__restrict__ attr) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nodes; j += gridDim.x * blockDim.x) {
+    uint32_t best = 0;
+    float bspread = 0.0f;
+    for (uint32_t m = 0; m < d; ++m) {
+      const uint32_t kmax = stats[(size_t)j * d + m], kmin = stats[(size_t)nodes * d + (size_t)j * d + m];
+      float spread = 0.0f;
+      if (kmax != 0u) {
+        spread = __fsub_rn(key2f(kmax), key2f(kmin));
+        if (spread != spread) spread = 0.0f;
+      }
+      if (m == 0 || spread > bspread) {
+        bspread = spread;
+        best = m;
+      }
+    }
+    attr[j] = best;
+  }
+}
+
+// Sort keys of level `level`: (node << 32 | order key of the row's value in the node's
+// split attribute), with the row ids.
+__global__ void kd_keys_kernel(const float *__restrict__ table, uint64_t ld, uint64_t n,
+                               const uint32_t *__restrict__ perm, uint32_t lg, uint32_t P, uint32_t level,
+                               const uint32_t *__restrict__ attr, unsigned long long *__restrict__ keys,
+                               uint32_t *__restrict__ ids) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = kd_node_of((uint32_t)(i >> lg), P, level);
+    const uint32_t id = perm[i];
+    const float x = __ldg(table + (uint64_t)attr[node] * ld + id);
+    keys[i] = ((unsigned long long)node << 32) | f2key(x);
+    ids[i] = id;
+  }
+}
+
+}  // namespace
+
+uint32_t kd_levels(uint32_t P) {
+  uint32_t L = 0;
+  while ((1ull << L) < P) ++L;
+  return L;
+}
+
+uint64_t kd_order_work_words(uint64_t n, uint32_t d, uint32_t P) {
+  return 5 * n + 2 * (uint64_t)P * d + P;
+}
+
+cudaError_t launch_kd_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint32_t part_log2,
+                            uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
+                            cudaStream_t s) {
+  if (n > 0x7FFFFFFFull || d == 0) return cudaErrorInvalidValue;
+  const uint32_t P = (uint32_t)((n + (1ull << part_log2) - 1) >> part_log2);
+  const uint32_t L = kd_levels(P);
+  const int nn = (int)n;
+  // work: keys in / out (2n words each), ids (n words), per-node stats, split attributes
+  unsigned long long *kin = reinterpret_cast<unsigned long long *>(work);
+  unsigned long long *kout = kin + n;
+  uint32_t *ids = work + 4 * n;
+  uint32_t *stats = work + 5 * n;
+  uint32_t *attr = stats + 2 * (uint64_t)P * d;
+  if (!temp) {  // size query
+    return cub::DeviceRadixSort::SortPairs(nullptr, *temp_bytes, kin, kout, ids, perm, nn, 0, 64, s);
+  }
+  const int g = grid_for(n, num_sms);
+  size_t tb = *temp_bytes;
+  iota_kernel<<<g, 256, 0, s>>>(perm, n);
+  cudaError_t e = cudaGetLastError();
+  for (uint32_t level = 0; e == cudaSuccess && level < L; ++level) {
+    const uint32_t nodes = 1u << level;
+    e = cudaMemsetAsync(stats, 0, (size_t)nodes * d * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats + (size_t)nodes * d, 0xFF, (size_t)nodes * d * sizeof(uint32_t), s);
+    if (e != cudaSuccess) break;
+    const uint64_t chunks = (n + 1023) / 1024;
+    const int gs = (int)std::min<uint64_t>(chunks, (uint64_t)num_sms * 8);
+    kd_stats_kernel<<<gs, 256, 0, s>>>(table, ld, d, n, perm, part_log2, P, level, nodes, stats);
+    kd_split_kernel<<<(nodes + 255) / 256, 256, 0, s>>>(stats, d, nodes, attr);
+    kd_keys_kernel<<<g, 256, 0, s>>>(table, ld, n, perm, part_log2, P, level, attr, kin, ids);
+    e = cudaGetLastError();
+    // the sorted ids are the next order; node ids < 2^level sit above the 32 key bits
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(temp, tb, kin, kout, ids, perm, nn, 0, 32 + (int)level, s);
+  }
+  return e;
+}
+
 cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
                                float *ptable, int num_sms, cudaStream_t s) {
   gather_rows_kernel<<<grid_for(n, num_sms), 256, 0, s>>>(table, ld, d, n, perm, ptable);
@@ -388,7 +595,7 @@ cudaError_t launch_part_order(const float *pmin, const float *pmax, uint32_t P, 
                               cudaStream_t s) {
   if (P == 0) return cudaSuccess;
   if (P <= kPartOrderOneBlock) {
-    uint32_t Ppad = 1;
+    uint32_t Ppad = 64;  // whole 64-entry chunks (padding entries are 0, sorted last)
     while (Ppad < P) Ppad <<= 1;
     const size_t smem = (size_t)Ppad * 8;
     cudaError_t e = cudaFuncSetAttribute(part_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -60,8 +60,11 @@ constexpr int kOffCtl = 0;        // SmemCtl (80 B)
 constexpr int kOffNever = 96;     // test barrier (u64)
 constexpr int kOffHist = 128;     // 256-bin radix histogram
 constexpr int kOffWsm = 1152;     // weights of the runtime-q path (kMaxQ floats)
+constexpr int kOffScnt = 1408;    // entry counts of a merge group's slots (kMaxFanin words)
 constexpr int kOffCand = kScanSmemFixed;
-static_assert(kOffWsm + 4 * (int)kMaxQ <= kScanSmemFixed, "fixed shared block");
+constexpr uint32_t kMaxFanin = 8;
+static_assert(kOffWsm + 4 * (int)kMaxQ <= kOffScnt && kOffScnt + 4 * (int)kMaxFanin <= kScanSmemFixed,
+              "fixed shared block");
 static_assert(sizeof(SmemCtl) <= kOffNever, "control block layout");
 static_assert(kScanThreads == 256, "one histogram bin per thread");
 
@@ -194,6 +197,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   uint64_t *never = reinterpret_cast<uint64_t *>(smem + kOffNever);
   uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffHist);
   float *wsm = reinterpret_cast<float *>(smem + kOffWsm);
+  uint32_t *scnt = reinterpret_cast<uint32_t *>(smem + kOffScnt);
   uint2 *cand0 = reinterpret_cast<uint2 *>(smem + kOffCand);  // two buffers of cap entries
   uint2 *mbuf = cand0;                                         // merge area (reuses both)
 
@@ -530,25 +534,37 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     bsync();
     if (!ctl->is_last) return;
     __threadfence();
-    // the last arrival merges the group's slots
+    // the last arrival merges the group's slots: their counts first, then all their
+    // entries as one flat index space, kMergeBatch loads per thread in flight at a time
     if (t == 0) {
       ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       ctl->sel.wcount = 0;
     }
+    if (t < (int)gsize) scnt[t] = __ldcg(&p.slot_count[p.slot_off[level] + first + t]);
     bsync();
     {
       const uint32_t g = ctl->red_g;
       const uint32_t lim = p.fanin * k;
-      (void)lim;
-      for (uint32_t si = 0; si < gsize; ++si) {
-        const uint32_t so = p.slot_off[level] + first + si;
-        const uint32_t cnt = __ldcg(&p.slot_count[so]);
-        const uint2 *src = p.slots + (size_t)so * k;
-        for (uint32_t j = t; j < cnt; j += kScanThreads) {
-          const uint2 e = __ldcg(src + j);
-          if (e.x >= g) {
+      uint32_t total = 0;
+      for (uint32_t si = 0; si < gsize; ++si) total += scnt[si];
+      constexpr int kMergeBatch = 4;
+      for (uint32_t base = 0; base < total; base += kScanThreads * kMergeBatch) {
+        uint2 e[kMergeBatch];
+#pragma unroll
+        for (int u = 0; u < kMergeBatch; ++u) {
+          uint32_t f = base + (uint32_t)u * kScanThreads + t;
+          e[u] = make_uint2(0u, 0u);
+          if (f < total) {
+            uint32_t si = 0;
+            while (f >= scnt[si]) f -= scnt[si++];  // f < total: ends inside a slot
+            e[u] = __ldcg(p.slots + (size_t)(p.slot_off[level] + first + si) * k + f);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kMergeBatch; ++u) {
+          if (base + (uint32_t)u * kScanThreads + t < total && e[u].x >= g) {
             const uint32_t pos = atomicAdd(&ctl->sel.wcount, 1u);
-            if (TOPK_CHECK(pos < lim, kDiagMerge, level, pos, lim)) mbuf[pos] = e;
+            if (TOPK_CHECK(pos < lim, kDiagMerge, level, pos, lim)) mbuf[pos] = e[u];
           }
         }
       }

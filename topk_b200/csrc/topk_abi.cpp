@@ -1737,12 +1737,12 @@ int topk_partition_ids(topk_table_t h, uint32_t *ids) {
 int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order) {
   g_last_error.clear();
   if (order != TOPK_ORDER_MORTON && order != TOPK_ORDER_VTA && order != TOPK_ORDER_PTA &&
-      order != TOPK_ORDER_VTA_THREADS && order != TOPK_ORDER_SLA)
+      order != TOPK_ORDER_VTA_THREADS && order != TOPK_ORDER_SLA && order != TOPK_ORDER_KD)
     return fail(TOPK_ERR_ARG, "unknown order %d", order);
   if (!h) return fail(TOPK_ERR_ARG, "null handle");
   if (!h->has_data) return fail(TOPK_ERR_STATE, "no table data");
   if (order != TOPK_ORDER_MORTON && h->n > 0x7FFFFFFFull)
-    return fail(TOPK_ERR_UNSUPPORTED, "VTA and PTA orders need n < 2^31 rows");
+    return fail(TOPK_ERR_UNSUPPORTED, "the VTA, PTA, SLA and kd orders need n < 2^31 rows");
   if (order == TOPK_ORDER_PTA && (h->n < 2 || h->d > 32))
     return fail(TOPK_ERR_UNSUPPORTED, "PTA order needs n >= 2 and d <= 32");
   if (order == TOPK_ORDER_SLA && h->d > 32) return fail(TOPK_ERR_UNSUPPORTED, "SLA order needs d <= 32");
@@ -1813,7 +1813,21 @@ int topk_build_partitions_ordered(topk_table_t h, uint32_t part_rows, int order)
   if (e == cudaSuccess && order == TOPK_ORDER_MORTON)
     e = launch_partition_build(h->table, h->ld, h->d, h->n, dls, dls + h->d, bits, keys, hist, h->pids, h->ptable,
                                h->num_sms, s);
-  if (e == cudaSuccess && order != TOPK_ORDER_MORTON) {
+  if (e == cudaSuccess && order == TOPK_ORDER_KD) {
+    uint32_t *work = nullptr;
+    void *temp = nullptr;
+    size_t temp_bytes = 0;
+    e = launch_kd_order(h->table, h->ld, h->d, h->n, lg, h->pids, nullptr, nullptr, &temp_bytes, h->num_sms, s);
+    if (e == cudaSuccess) e = cudaMalloc(&work, kd_order_work_words(h->n, h->d, (uint32_t)P) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&temp, std::max<size_t>(temp_bytes, 16));
+    if (e == cudaSuccess)
+      e = launch_kd_order(h->table, h->ld, h->d, h->n, lg, h->pids, work, temp, &temp_bytes, h->num_sms, s);
+    if (e == cudaSuccess) e = launch_gather_rows(h->table, h->ld, h->d, h->n, h->pids, h->ptable, h->num_sms, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // before the scratch goes
+    cudaFree(work);
+    cudaFree(temp);
+  }
+  if (e == cudaSuccess && order != TOPK_ORDER_MORTON && order != TOPK_ORDER_KD) {
     const IndexOrder kind = order == TOPK_ORDER_PTA           ? IndexOrder::kPta
                             : order == TOPK_ORDER_VTA_THREADS ? IndexOrder::kVtaThreads
                             : order == TOPK_ORDER_SLA         ? IndexOrder::kGroups

@@ -209,6 +209,15 @@ int skyline_layers_device(const float *table, uint64_t ld, uint32_t d, uint64_t 
                           uint64_t *num_layers, std::string *msg);
 cudaError_t launch_gather_rows(const float *table, uint64_t ld, uint32_t d, uint64_t n, const uint32_t *perm,
                                float *ptable, int num_sms, cudaStream_t s);
+// kd order (partition.cu): the partitions of 2^part_log2 rows are the leaves of a
+// balanced binary tree; each node is split at its middle partition boundary after its
+// rows are sorted by the attribute of widest spread in it.  n < 2^31.  work:
+// kd_order_work_words(n, d, P) words; temp: CUB storage (size query with temp null).
+uint32_t kd_levels(uint32_t P);
+uint64_t kd_order_work_words(uint64_t n, uint32_t d, uint32_t P);
+cudaError_t launch_kd_order(const float *table, uint64_t ld, uint32_t d, uint64_t n, uint32_t part_log2,
+                            uint32_t *perm, uint32_t *work, void *temp, size_t *temp_bytes, int num_sms,
+                            cudaStream_t s);
 // One query's attributes and gathered weights, for partition bounds.
 struct PartQuery {
   uint32_t qq;

@@ -208,8 +208,8 @@ class Table:
 
     # -- partitions and pruned queries -------------------------------------
     def build_partitions(self, part_rows=1 << 16, order=0):
-        """order: ORDER_MORTON (0), ORDER_VTA (1), ORDER_PTA (2), ORDER_VTA_THREADS (3) or
-        ORDER_SLA (4), see topk_build_partitions_ordered."""
+        """order: ORDER_MORTON (0), ORDER_VTA (1), ORDER_PTA (2), ORDER_VTA_THREADS (3),
+        ORDER_SLA (4) or ORDER_KD (5), see topk_build_partitions_ordered."""
         check(_lib.load().topk_build_partitions_ordered(self._h, int(part_rows), int(order)))
 
     def skyline_layers(self):

@@ -191,7 +191,7 @@ __device__ uint32_t block_reduce(const uint2 *src, uint32_t count, uint2 *dst, u
 // passes from the top.  `count` must be the same in every thread; `hist` holds 256 bins.
 // The source may live in global memory: each thread loads kKthBatch entries before it
 // uses any, so a pass waits for one load latency per NT * kKthBatch entries.
-constexpr int kKthBatch = 16;
+constexpr int kKthBatch = 8;
 template <int NT, class Src>
 __device__ uint32_t block_kth_key(const Src &src, uint32_t count, uint32_t min_key, uint32_t k, uint32_t *hist,
                                   SelShared *sh) {

@@ -321,29 +321,47 @@ __global__ void __launch_bounds__(128) mlp_predict_kernel(const float *__restric
 }
 
 // ---------------------------------------------------------------- features
-// Bitonic sort of n (a power of two) floats in shared memory, descending.
-__device__ void sort_desc(float *a, uint32_t n) {
+struct FloatKeys {  // order keys of a float array (NaN lowest), as block_kth_key reads them
+  const float *p;
+  __device__ uint2 operator()(uint32_t j) const { return make_uint2(f2key(p[j]), 0u); }
+};
+
+// The K = min(P, 128) largest of v[0..P) in descending order into out[0..K): the K-th
+// largest order key by a block radix select, the entries strictly above it (fewer than
+// K) placed by their rank among themselves, the rest of out[] the K-th value itself.
+// Ranks 1, 2, 4, .. 128 are all the features need, so nothing else is sorted.
+template <int NT>
+__device__ void top_desc(const float *v, uint32_t P, float *out, uint32_t *hist, SelShared *sh, float *buf,
+                         uint32_t *bkey, uint32_t *cnt) {
+  const uint32_t K = min(P, 128u);
+  const uint32_t kth = block_kth_key<NT>(FloatKeys{v}, P, 0u, K, hist, sh);
+  if (threadIdx.x == 0) *cnt = 0;
   __syncthreads();
-  for (uint32_t size = 2; size <= n; size <<= 1) {
-    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-      for (uint32_t i = threadIdx.x; i < n / 2; i += blockDim.x) {
-        const uint32_t lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
-        const bool desc = (lo & size) == 0;
-        const float x = a[lo], y2 = a[hi];
-        if ((x < y2) == desc) {
-          a[lo] = y2;
-          a[hi] = x;
-        }
-      }
-      bitonic_stage_sync(stride);
+  for (uint32_t j = threadIdx.x; j < P; j += NT) {
+    const uint32_t key = f2key(v[j]);
+    if (key > kth) {
+      const uint32_t pos = atomicAdd(cnt, 1u);  // < K
+      buf[pos] = v[j];
+      bkey[pos] = key;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  const uint32_t c = *cnt;
+  for (uint32_t i = threadIdx.x; i < K; i += NT) {
+    if (i < c) {
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < c; ++j) rank += (bkey[j] > bkey[i] || (bkey[j] == bkey[i] && j < i)) ? 1u : 0u;
+      out[rank] = buf[i];
+    } else {
+      out[i] = key2f(kth);
+    }
+  }
+  __syncthreads();
 }
 
 // One block per query: the F features (and, with params, the model's prediction
 // of k-th score / S, the MLP forward in the same block).  NT threads: 256 for
-// batches (many blocks), 1024 for a single query (the sorts are its critical path).
+// batches (many blocks), 1024 for a single query (the selects are its critical path).
 template <int NT>
 __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ pmin, const float *__restrict__ pmax,
                                                        const float *__restrict__ pmean, uint32_t P, uint32_t Ppad,
@@ -356,6 +374,9 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
   float *feat = mu + Ppad;          // kMlpMaxIn
   float *h = feat + kMlpMaxIn;      // 2 * kHid
   __shared__ float S;
+  __shared__ uint32_t hist[256], bkey[128], cnt;
+  __shared__ SelShared sel;
+  __shared__ float tb[128], tm[128], buf[128];
   const BatchQuery &q = qs[blockIdx.x];
   const uint32_t F = feature_dim(d);
   if (threadIdx.x == 0) {
@@ -380,8 +401,8 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
   }
   for (uint32_t m = threadIdx.x; m < kMlpMaxIn; m += blockDim.x) feat[m] = 0.0f;
   __syncthreads();
-  sort_desc(bnd, Ppad);
-  sort_desc(mu, Ppad);
+  top_desc<NT>(bnd, P, tb, hist, &sel, buf, bkey, &cnt);
+  top_desc<NT>(mu, P, tm, hist, &sel, buf, bkey, &cnt);
   if (threadIdx.x == 0) {
     const float inv = 1.0f / S;
     for (uint32_t m = 0; m < q.qq; ++m) feat[q.attr[m]] += q.w[m] * inv;
@@ -390,8 +411,8 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
     feat[2 * d + 1] = (float)q.qq * (1.0f / 16.0f);
     for (uint32_t r = 0; r < 8; ++r) {
       const uint32_t at = min((1u << r), P) - 1u;
-      feat[2 * d + 2 + r] = bnd[at] * inv;
-      feat[2 * d + 10 + r] = mu[at] * inv;
+      feat[2 * d + 2 + r] = tb[at] * inv;
+      feat[2 * d + 10 + r] = tm[at] * inv;
     }
   }
   __syncthreads();

@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       const uint32_t lim = p.fanin * k;
       uint32_t total = 0;
       for (uint32_t si = 0; si < gsize; ++si) total += scnt[si];
-      constexpr int kMergeBatch = 4;
+      constexpr int kMergeBatch = 2;
       for (uint32_t base = 0; base < total; base += kScanThreads * kMergeBatch) {
         uint2 e[kMergeBatch];
 #pragma unroll

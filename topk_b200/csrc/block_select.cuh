@@ -28,6 +28,10 @@ struct SmemSrc {
   const uint2 *p;
   __device__ uint2 operator()(uint32_t j) const { return p[j]; }
 };
+struct KeySrc {  // bare keys (no ids), as a source of (key, 0) entries
+  const uint32_t *p;
+  __device__ uint2 operator()(uint32_t j) const { return make_uint2(p[j], 0u); }
+};
 
 // Block-wide radix select over `count` entries of `src` with key >= min_key: finds
 // (prefix, mask) such that exactly `need` valid entries satisfy

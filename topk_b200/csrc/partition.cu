@@ -22,7 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-
+#include <atomic>
 #include <cstdint>
 
 #include "block_select.cuh"
@@ -244,80 +244,79 @@ __device__ __forceinline__ uint32_t part_bound_key(const float *__restrict__ pmi
 // rank i, pkey[i] = its bound key.
 constexpr uint32_t kOrderThreads = 1024;
 
-// Stages with strides st, st/2, .., 1 (st <= 32) of a descending bitonic sort's merge of
-// `size`, on the 64-entry chunk at `base` that one warp holds: x0 = entry base + lane,
-// x1 = entry base + 32 + lane.  Entry i is compared with i ^ stride; the lower of the
-// two keeps the larger value where (i & size) == 0, the smaller elsewhere.
-__device__ __forceinline__ void warp_bitonic_stages(unsigned long long &x0, unsigned long long &x1, uint32_t base,
-                                                    uint32_t size, uint32_t st, uint32_t lane) {
-  for (uint32_t stride = st; stride > 0; stride >>= 1) {
-    if (stride == 32) {
-      const bool desc = ((base + lane) & size) == 0;
-      const unsigned long long hi = x0 > x1 ? x0 : x1, lo = x0 > x1 ? x1 : x0;
-      x0 = desc ? hi : lo;
-      x1 = desc ? lo : hi;
-    } else {
-      const unsigned long long y0 = __shfl_xor_sync(0xFFFFFFFFu, x0, stride);
-      const unsigned long long y1 = __shfl_xor_sync(0xFFFFFFFFu, x1, stride);
-      const uint32_t i0 = base + lane, i1 = base + 32 + lane;
-      const bool k0 = ((i0 & stride) == 0) == ((i0 & size) == 0);  // keep the larger
-      const bool k1 = ((i1 & stride) == 0) == ((i1 & size) == 0);
-      x0 = k0 ? (x0 > y0 ? x0 : y0) : (x0 < y0 ? x0 : y0);
-      x1 = k1 ? (x1 > y1 ? x1 : y1) : (x1 < y1 ? x1 : y1);
-    }
-  }
-}
+// The partitions in bound order by a counting sort into kOrderThreads buckets over the
+// range of the bound keys (bucket 0 = the highest keys); within a bucket in arrival
+// order.  pkey[i] is the largest key of i's bucket: an upper bound of every score in
+// each of its partitions, and non-increasing along the list (a bucket's keys all lie
+// above the next bucket's), which is what the stop rule needs; the bucket width only
+// costs pruning where bounds within (kmax - kmin) / 1024 of each other are split.  A
+// NaN bound (key 0xFFFFFFFF) lands in bucket 0 and keeps its partition.
 __global__ void __launch_bounds__(kOrderThreads) part_order_kernel(const float *__restrict__ pmin,
                                                                   const float *__restrict__ pmax, uint32_t P,
-                                                                  uint32_t Ppad, uint32_t d, const PartQuery q,
+                                                                  uint32_t d, const PartQuery q,
                                                                   uint32_t *__restrict__ plist,
                                                                   uint32_t *__restrict__ pkey) {
-  extern __shared__ unsigned long long ent[];
-  const uint32_t t = threadIdx.x;
-  // (key, ~partition): descending composite = key descending, then partition ascending;
-  // padding entries are 0, below every real one
-  for (uint32_t i = t; i < Ppad; i += kOrderThreads)
-    ent[i] = i < P ? ((unsigned long long)part_bound_key(pmin, pmax, d, i, q) << 32) | (0xFFFFFFFFu - i) : 0ull;
-  __syncthreads();
-  // Bitonic sort, descending.  Strides up to 32 run in registers: a warp holds a chunk
-  // of 64 entries (lane l: entries base + l and base + 32 + l) and exchanges by
-  // shuffles; larger strides run in shared memory with a block barrier each.
-  const uint32_t lane = t & 31, warp = t >> 5;
-  for (uint32_t c = warp; c < Ppad / 64; c += kOrderThreads / 32) {  // sizes 2 .. 64
-    const uint32_t base = c * 64;
-    unsigned long long x0 = ent[base + lane], x1 = ent[base + 32 + lane];
-    for (uint32_t size = 2; size <= 64; size <<= 1) warp_bitonic_stages(x0, x1, base, size, size >> 1, lane);
-    ent[base + lane] = x0;
-    ent[base + 32 + lane] = x1;
+  extern __shared__ uint32_t keys[];  // P bound keys
+  __shared__ uint32_t cnt[kOrderThreads], bmax[kOrderThreads], wsum[32];
+  __shared__ uint32_t kmin_s, kmax_s;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  cnt[t] = 0;
+  bmax[t] = 0;
+  if (t == 0) {
+    kmin_s = 0xFFFFFFFFu;
+    kmax_s = 0;
   }
-  __syncthreads();
-  for (uint32_t size = 128; size <= Ppad; size <<= 1) {
-    for (uint32_t stride = size >> 1; stride >= 64; stride >>= 1) {
-      for (uint32_t i = t; i < Ppad / 2; i += kOrderThreads) {
-        const uint32_t lo = 2 * i - (i & (stride - 1));
-        const uint32_t hi = lo + stride;
-        const bool desc = (lo & size) == 0;
-        const unsigned long long x = ent[lo], y = ent[hi];
-        if (desc ? (x < y) : (x > y)) {
-          ent[lo] = y;
-          ent[hi] = x;
-        }
-      }
-      __syncthreads();
-    }
-    for (uint32_t c = warp; c < Ppad / 64; c += kOrderThreads / 32) {  // strides 32 .. 1
-      const uint32_t base = c * 64;
-      unsigned long long x0 = ent[base + lane], x1 = ent[base + 32 + lane];
-      warp_bitonic_stages(x0, x1, base, size, 32, lane);
-      ent[base + lane] = x0;
-      ent[base + 32 + lane] = x1;
-    }
-    __syncthreads();
-  }
+  uint32_t lmin = 0xFFFFFFFFu, lmax = 0;
   for (uint32_t i = t; i < P; i += kOrderThreads) {
-    const unsigned long long e = ent[i];
-    plist[i] = 0xFFFFFFFFu - (uint32_t)e;
-    pkey[i] = (uint32_t)(e >> 32);
+    const uint32_t k = part_bound_key(pmin, pmax, d, i, q);
+    keys[i] = k;
+    lmin = min(lmin, k);
+    lmax = max(lmax, k);
+  }
+  lmin = __reduce_min_sync(0xFFFFFFFFu, lmin);
+  lmax = __reduce_max_sync(0xFFFFFFFFu, lmax);
+  __syncthreads();
+  if (lane == 0) {
+    atomicMin(&kmin_s, lmin);
+    atomicMax(&kmax_s, lmax);
+  }
+  __syncthreads();
+  const uint32_t kmax = kmax_s;
+  const uint64_t span = (uint64_t)(kmax - kmin_s) + 1;
+  auto bucket = [&](uint32_t k) { return (uint32_t)(((uint64_t)(kmax - k) * kOrderThreads) / span); };
+  for (uint32_t i = t; i < P; i += kOrderThreads) {
+    const uint32_t b = bucket(keys[i]);
+    atomicAdd(&cnt[b], 1u);
+    atomicMax(&bmax[b], keys[i]);
+  }
+  __syncthreads();
+  // exclusive scan of the bucket counts, one bucket per thread
+  const uint32_t c = cnt[t];
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = wsum[lane], wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= (uint32_t)o) wi += y;
+    }
+    wsum[lane] = wi - w;
+  }
+  __syncthreads();
+  cnt[t] = wsum[warp] + incl - c;  // the bucket's first place
+  __syncthreads();
+  for (uint32_t i = t; i < P; i += kOrderThreads) {
+    const uint32_t b = bucket(keys[i]);
+    const uint32_t pos = atomicAdd(&cnt[b], 1u);
+    plist[pos] = i;
+    pkey[pos] = bmax[b];
   }
 }
 
@@ -595,12 +594,20 @@ cudaError_t launch_part_order(const float *pmin, const float *pmax, uint32_t P, 
                               cudaStream_t s) {
   if (P == 0) return cudaSuccess;
   if (P <= kPartOrderOneBlock) {
-    uint32_t Ppad = 64;  // whole 64-entry chunks (padding entries are 0, sorted last)
-    while (Ppad < P) Ppad <<= 1;
-    const size_t smem = (size_t)Ppad * 8;
-    cudaError_t e = cudaFuncSetAttribute(part_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = (size_t)P * 4;
+    // the largest size once per device (a driver call on every query otherwise)
+    static std::atomic<uint64_t> opted{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    part_order_kernel<<<1, kOrderThreads, smem, s>>>(pmin, pmax, P, Ppad, d, q, plist, pkey);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(opted.load(std::memory_order_acquire) & bit)) {
+      e = cudaFuncSetAttribute(part_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(kPartOrderOneBlock * 4));
+      if (e != cudaSuccess) return e;
+      opted.fetch_or(bit, std::memory_order_release);
+    }
+    part_order_kernel<<<1, kOrderThreads, smem, s>>>(pmin, pmax, P, d, q, plist, pkey);
     return cudaGetLastError();
   }
   // keys_in | ids_in after the radix sort's own scratch

@@ -32,7 +32,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "block_select.cuh"
 #include "device_common.cuh"
@@ -469,8 +471,33 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     if (ctl->is_last) {
       __threadfence();
       // the k-th largest published key; entries of key 0 are padding (or NaN scores,
-      // the lowest anyway): left out
-      const uint32_t kth = block_kth_key<kScanThreads>(SmemSrc{p.pub}, gridDim.x * p.pub_m, 1u, p.k, hist, &ctl->sel);
+      // the lowest anyway): left out.  The keys go to this CTA's free candidate space
+      // first (independent loads, kStageBatch in flight per thread), so the select's
+      // five passes read shared memory, not L2.
+      const uint32_t np = gridDim.x * p.pub_m;
+      uint32_t *stage = reinterpret_cast<uint32_t *>(KTH ? cand0 : cand0 + (size_t)(ctl->cur ^ 1u) * cap);
+      const uint32_t stage_cap = KTH ? 2u * p.mcap : 2u * cap;
+      uint32_t kth;
+      if (np <= stage_cap) {
+        constexpr int kStageBatch = 8;
+        for (uint32_t base = 0; base < np; base += kScanThreads * kStageBatch) {
+          uint32_t v[kStageBatch];
+#pragma unroll
+          for (int u = 0; u < kStageBatch; ++u) {
+            const uint32_t j = base + (uint32_t)u * kScanThreads + t;
+            v[u] = j < np ? __ldcg(&p.pub[j].x) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < kStageBatch; ++u) {
+            const uint32_t j = base + (uint32_t)u * kScanThreads + t;
+            if (j < np) stage[j] = v[u];
+          }
+        }
+        bsync();
+        kth = block_kth_key<kScanThreads>(KeySrc{stage}, np, 1u, p.k, hist, &ctl->sel);
+      } else {
+        kth = block_kth_key<kScanThreads>(SmemSrc{p.pub}, np, 1u, p.k, hist, &ctl->sel);
+      }
       if (KTH || p.kth_only) {
         // the bound is the pass's result; every other CTA has left: put the counters back
         if (t == 0) {
@@ -670,8 +697,48 @@ void set_carveout(const void *fn, bool part, uint32_t qq, int percent, bool kth 
 
 }  // namespace
 
+namespace {
+
+// Plans by (device, q, k, partition mode, CTA cap): the occupancy queries behind a plan
+// are driver calls, a few microseconds each, on every query's critical path otherwise.
+struct PlanEntry {
+  ScanPlan pl;
+  int carveout;
+};
+std::mutex g_plan_mu;
+std::map<std::tuple<int, uint32_t, uint32_t, bool, uint32_t>, PlanEntry> g_plans;
+
+}  // namespace
+
 ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t smem_optin, uint32_t max_ctas_per_sm,
                    bool part) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    dev = -1;
+  }
+  const auto key = std::make_tuple(dev, qq <= 16 ? qq : 0u, k, part, max_ctas_per_sm);
+  const void *fn = reinterpret_cast<const void *>(kernel_for(qq, part));
+  const void *fn_kth = reinterpret_cast<const void *>(kernel_for(qq, part, true));
+  const uint64_t tiles = (rows + 3 + kTile) / kTile;
+  auto finish = [&](ScanPlan pl) {
+    uint64_t grid = (uint64_t)num_sms * (uint64_t)pl.ctas_per_sm;
+    if (grid > tiles) grid = tiles;
+    if (grid < 1) grid = 1;
+    pl.grid = (int)grid;
+    return pl;
+  };
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    const auto it = g_plans.find(key);
+    if (it != g_plans.end()) {
+      const PlanEntry pe = it->second;
+      // the carveout is per function: another plan may have changed it since
+      set_carveout(fn, part, qq, pe.carveout);
+      set_carveout(fn_kth, part, qq, pe.carveout, true);
+      return finish(pe.pl);
+    }
+  }
   ScanPlan pl{};
   pl.tile = kTile;
   uint32_t P = 1;
@@ -698,7 +765,6 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   // CTAs per SM: as many as registers and threads allow, and as the shared memory
   // allows with kScanL1Keep left as L1 (or the caller's number); the carveout is set to
   // just fit them, so the rest of the unified memory stays L1
-  const void *fn = reinterpret_cast<const void *>(kernel_for(qq, part));
   set_carveout(fn, part, qq, 100);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kScanThreads, pl.smem) != cudaSuccess || occ < 1) {
@@ -717,22 +783,21 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
       size_kb = kb;
       break;
     }
-  set_carveout(fn, part, qq, (int)((size_kb * 100 + 227) / 228));
+  const int carveout = (int)((size_kb * 100 + 227) / 228);
+  set_carveout(fn, part, qq, carveout);
   // the threshold-pass form of the kernel runs with the same plan
-  set_carveout(reinterpret_cast<const void *>(kernel_for(qq, part, true)), part, qq,
-               (int)((size_kb * 100 + 227) / 228), true);
+  set_carveout(fn_kth, part, qq, carveout, true);
   int fit = 0;  // what the driver reports with that preference
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kScanThreads, pl.smem) == cudaSuccess && fit >= 1)
     occ = std::min(occ, fit);
   else
     (void)cudaGetLastError();
   pl.ctas_per_sm = occ;
-  const uint64_t tiles = (rows + 3 + kTile) / kTile;
-  uint64_t grid = (uint64_t)num_sms * (uint64_t)occ;
-  if (grid > tiles) grid = tiles;
-  if (grid < 1) grid = 1;
-  pl.grid = (int)grid;
-  return pl;
+  if (dev >= 0) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans[key] = PlanEntry{pl, carveout};
+  }
+  return finish(pl);
 }
 
 void plan_merge_tree(ScanParams &p, uint32_t grid, uint32_t fanin, uint32_t *total_slots, uint32_t *total_groups) {

@@ -226,10 +226,12 @@ struct PartQuery {
 };
 // Partitions in descending order of the query's bound (the reference-order FP32 sum
 // over each partition's per-attribute max, or min for negative weights: an exact upper
-// bound of its rows' scores), ties by the lower partition number: plist[i] = partition,
-// pkey[i] = order key of its bound (0xFFFFFFFF for a NaN bound).  Up to
-// kPartOrderOneBlock partitions one block sorts them in shared memory; above, a radix
-// sort uses `temp` (part_order_temp_bytes(P) bytes).
+// bound of its rows' scores): plist[i] = partition, pkey[i] = order key of an upper
+// bound of its scores, non-increasing in i (0xFFFFFFFF for a NaN bound).  Up to
+// kPartOrderOneBlock partitions one block orders them by a counting sort into 1024
+// buckets over the range of the keys, pkey[i] = the largest key of i's bucket,
+// partitions of one bucket in no set order; above, an exact radix sort (ties by the
+// lower partition number) uses `temp` (part_order_temp_bytes(P) bytes).
 constexpr uint32_t kPartOrderOneBlock = 16384;
 size_t part_order_temp_bytes(uint32_t P);
 cudaError_t launch_part_order(const float *pmin, const float *pmax, uint32_t P, uint32_t d, const PartQuery &q,

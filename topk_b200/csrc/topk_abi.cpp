@@ -96,6 +96,11 @@ struct Ctx {
   size_t meta_bytes = 0;    // bytes that must be zero between queries (header + done)
   unsigned char *d_res = nullptr;  // device result block (kMaxK capacity)
   unsigned char *h_res = nullptr;  // pinned mirror
+  // Result block of the synchronous queries in mapped pinned memory (h_out on the host,
+  // d_out its device address): the scan's root writes ids, scores and the header
+  // straight to the host, so no copy follows the scan.
+  unsigned char *h_out = nullptr;
+  unsigned char *d_out = nullptr;
   unsigned long long *d_count2 = nullptr;
   uint64_t *d_ids_scratch = nullptr;  // gather ids
   float *d_rows = nullptr;
@@ -211,6 +216,7 @@ int ctx_create(topk_table_t h, Ctx **out) {
     cudaFree(c->d_res);
     cudaFree(c->d_count2);
     if (c->h_res) cudaFreeHost(c->h_res);
+    if (c->h_out) cudaFreeHost(c->h_out);
     delete c;
     return cuda_fail(e, what);
   };
@@ -241,6 +247,10 @@ int ctx_create(topk_table_t h, Ctx **out) {
   if ((e = cudaMalloc(&c->d_count2, 2 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "count");
   if ((e = cudaHostAlloc(&c->h_res, result_bytes(kMaxK) + kStageBytes, cudaHostAllocDefault)) != cudaSuccess)
     return bail(e, "pinned result");
+  if ((e = cudaHostAlloc(&c->h_out, result_bytes(kMaxK), cudaHostAllocMapped)) != cudaSuccess)
+    return bail(e, "mapped result");
+  if ((e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_out), c->h_out, 0)) != cudaSuccess)
+    return bail(e, "mapped result address");
   *out = c;
   return TOPK_OK;
 }
@@ -261,6 +271,7 @@ void ctx_free(Ctx *c) {
   cudaFree(c->d_ptemp);
   cudaFree(c->d_lq);
   if (c->h_res) cudaFreeHost(c->h_res);
+  if (c->h_out) cudaFreeHost(c->h_out);
   delete c;
 }
 
@@ -472,19 +483,18 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
   CtxLease lease(h);
   if (lease.status != TOPK_OK) return lease.status;
   Ctx *c = lease.c;
-  unsigned char *dr = c->d_res;
+  // the result goes straight to the mapped block (no copy after the scan)
+  unsigned char *dr = c->d_out;
   ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
   uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
   float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
+  volatile ResultHeader *hh = reinterpret_cast<volatile ResultHeader *>(c->h_out);
   // a sentinel count tells a completed scan from one that left early
-  CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), c->stream));
+  hh->count = 0xFFFFFFFFu;
   st = enqueue_scan(h, c, c->stream, r0, r1, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
                     dh->stats);
   if (st != TOPK_OK) return st;
-  const size_t bytes = kHdr + kk * 12;
-  CK(cudaMemcpyAsync(c->h_res, dr, bytes, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
   if (hh->count != (uint32_t)kk) {
     ScanScratch s{};
     cudaMemcpy(&s, c->scratch, sizeof(s), cudaMemcpyDeviceToHost);
@@ -493,10 +503,11 @@ int run_query_sync(topk_table_t h, uint64_t r0, uint64_t r1, uint64_t k, uint32_
       return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls); diag %u block %u tile %u [%u %u]",
                   (unsigned long long)h->wait_limit, s.diag[0], s.diag[1], s.diag[2], s.diag[3], s.diag[4]);
     return fail(TOPK_ERR_CUDA, "scan did not complete (count %u, expected %llu, error 0x%x); diag %u block %u tile %u [%u %u]",
-                hh->count, (unsigned long long)kk, s.error, s.diag[0], s.diag[1], s.diag[2], s.diag[3], s.diag[4]);
+                (uint32_t)hh->count, (unsigned long long)kk, s.error, s.diag[0], s.diag[1], s.diag[2], s.diag[3],
+                s.diag[4]);
   }
-  std::memcpy(ids, c->h_res + kHdr, kk * 8);
-  std::memcpy(scores, c->h_res + kHdr + kk * 8, kk * 4);
+  std::memcpy(ids, c->h_out + kHdr, kk * 8);
+  std::memcpy(scores, c->h_out + kHdr + kk * 8, kk * 4);
   if (count) *count = kk;
   if (threshold) *threshold = hh->threshold;
   g_last_cands = hh->stats[0];
@@ -583,10 +594,14 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
     if (c->ptemp_bytes) CK(cudaMalloc(&c->d_ptemp, c->ptemp_bytes));
     c->plist_cap = P;
   }
-  unsigned char *dr = c->d_res;
-  ResultHeader *dh = reinterpret_cast<ResultHeader *>(dr);
-  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dr + kHdr);
-  float *d_scores = reinterpret_cast<float *>(dr + kHdr + kk * 8);
+  // device-side words (round 1's bound) in the device block; the result and the cut
+  // the host reads go straight to the mapped block
+  ResultHeader *dh = reinterpret_cast<ResultHeader *>(c->d_res);
+  unsigned char *dro = c->d_out;
+  ResultHeader *dho = reinterpret_cast<ResultHeader *>(dro);
+  uint64_t *d_ids = reinterpret_cast<uint64_t *>(dro + kHdr);
+  float *d_scores = reinterpret_cast<float *>(dro + kHdr + kk * 8);
+  volatile ResultHeader *hh = reinterpret_cast<volatile ResultHeader *>(c->h_out);
   const uint32_t *d_seed = nullptr;
   if (learned) {
     // descriptor | features (kMlpMaxIn) | prediction | seed word
@@ -603,7 +618,7 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
     CK(cudaMemcpyAsync(dq, stage, sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
     const size_t Pd = (size_t)P * h->d;
     CK(launch_features(h->pstats, h->pstats + Pd, h->pstats + 2 * Pd, P, h->d, dq, 1, X, mlp, X + kMlpMaxIn, s));
-    CK(launch_learned_seed_one(X + kMlpMaxIn, X, h->d, dq, margin, seed, &dh->cut, s));
+    CK(launch_learned_seed_one(X + kMlpMaxIn, X, h->d, dq, margin, seed, &dho->cut, s));
     d_seed = seed;
   }
   PartQuery pq{};
@@ -625,36 +640,35 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
   const uint32_t m1 = (uint32_t)std::min<uint64_t>(P, std::max<uint64_t>((kk + R - 1) / R + 1, (P + 31) / 32));
   uint32_t *d_t1 = reinterpret_cast<uint32_t *>(&dh->pad[0]);  // round 1's k-th key
   uint64_t tiles = 0, scans = 0, accepted = 0;
-  const ResultHeader *hh = reinterpret_cast<const ResultHeader *>(c->h_res);
   float cut_seen = cut;
   // the seeded attempt (if any), then the two rounds without a seed
   for (int attempt = seeded ? 0 : 1; attempt < 2; attempt++) {
-    CK(cudaMemsetAsync(&dh->count, 0xFF, sizeof(uint32_t), s));
+    hh->count = 0xFFFFFFFFu;  // sentinel: a completed scan writes its count
     if (attempt == 0) {
       PartScan ps{c->d_plist, P, seed_host, c->d_pkey, d_seed, nullptr, kPrunedCtasPerSm, false};
-      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
-                        dh->stats, &ps);
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dho->threshold, &dho->count,
+                        dho->stats, &ps);
       scans += 1;
     } else {
       // round 1: a threshold pass (no merge, no result) over its partitions
       PartScan p1{c->d_plist, m1, 0u, nullptr, nullptr, d_t1, kRound1CtasPerSm, true};
-      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dho->threshold, &dho->count,
                         nullptr, &p1);
       if (st != TOPK_OK) return st;
       PartScan p2{c->d_plist, P, 0u, c->d_pkey, d_t1, nullptr, kPrunedCtasPerSm, false};
-      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dh->threshold, &dh->count,
-                        dh->stats, &p2);
+      st = enqueue_scan(h, c, s, 0, h->n, k, qq, weights, attr, d_ids, d_scores, &dho->threshold, &dho->count,
+                        dho->stats, &p2);
       scans += 2;
     }
     if (st != TOPK_OK) return st;
-    CK(cudaMemcpyAsync(c->h_res, dr, kHdr + kk * 12, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (hh->count > kk) {
       ScanScratch sc{};
       cudaMemcpy(&sc, c->scratch, sizeof(sc), cudaMemcpyDeviceToHost);
       cudaMemset(c->scratch, 0, c->meta_bytes);
       if (sc.error & 1u) return fail(TOPK_ERR_TIMEOUT, "device wait gave up (limit %llu polls)", (unsigned long long)h->wait_limit);
-      return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", hh->count, sc.error);
+      return fail(TOPK_ERR_CUDA, "partition scan did not complete (count %u, error 0x%x)", (uint32_t)hh->count,
+                  sc.error);
     }
     if (learned && attempt == 0) cut_seen = hh->cut;
     tiles += hh->stats[2] + (attempt == 1 ? (uint64_t)m1 * tiles_per_part : 0u);
@@ -665,8 +679,8 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
     }
   }
   const uint32_t cnt = hh->count;
-  std::memcpy(ids, c->h_res + kHdr, (size_t)cnt * 8);
-  std::memcpy(scores, c->h_res + kHdr + kk * 8, (size_t)cnt * 4);
+  std::memcpy(ids, c->h_out + kHdr, (size_t)cnt * 8);
+  std::memcpy(scores, c->h_out + kHdr + kk * 8, (size_t)cnt * 4);
   if (count) *count = cnt;
   if (threshold) *threshold = hh->threshold;
   if (cut_out) *cut_out = cut_seen;

@@ -120,16 +120,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-#define TOPK_RW8(i) "+r"(v[i]), "+r"(v[i + 1]), "+r"(v[i + 2]), "+r"(v[i + 3]), "+r"(v[i + 4]), "+r"(v[i + 5]), \
-                    "+r"(v[i + 6]), "+r"(v[i + 7])
-// The wait for this thread's TMEM loads, with the 32 registers of one load as operands:
-// every use of them is ordered after the wait, so the load can stay in flight while
-// other work runs.
-__device__ __forceinline__ void tmem_wait_ld_regs(uint32_t *v) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" : TOPK_RW8(0), TOPK_RW8(8), TOPK_RW8(16), TOPK_RW8(24) : : "memory");
-}
-#undef TOPK_RW8
-
 // Largest of 32 FP32 values (three-input max, a tree of depth 4).  A NaN value is
 // ignored, as a NaN also fails the compare it replaces.
 __device__ __forceinline__ float max3f(float a, float b, float c) {
@@ -334,19 +324,13 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
       const uint32_t ql = qt * kQTile + quarter * 32u + lane;  // this thread's query, CTA-relative
       const float cut = scut[ql];
       const uint64_t obj0 = t * kOTile + part * kWarpCols;
-      // Round trip rt compares 32 columns while the next 32 are loaded (two register
-      // sets, the loop unrolled so each keeps its registers).  The accumulator is free
-      // once its last columns are in registers.
-      uint32_t va[32], vb[32];
-      tmem_ld32(tcol, va);
-      tmem_wait_ld_regs(va);
-#pragma unroll
+#pragma unroll 1
       for (uint32_t rt = 0; rt < kWarpCols / 32u; ++rt) {
-        uint32_t *v = (rt & 1u) ? vb : va;
-        uint32_t *vn = (rt & 1u) ? va : vb;
-        if (rt + 1 < kWarpCols / 32u) {
-          tmem_ld32(tcol + (rt + 1u) * 32u, vn);
-        } else {
+        uint32_t v[32];
+        tmem_ld32(tcol + rt * 32u, v);
+        tmem_wait_ld();
+        if (rt + 1 == kWarpCols / 32u) {
+          // the accumulator is free once its last columns are in registers
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(acce + grp);
@@ -355,25 +339,22 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
         const float m = max32(v);
         const bool hit = m >= cut;
         const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
-        if (b != 0u) {
-          // cold path: each thread with a hit stores its 32 values as one record (eight
-          // asynchronous 16-byte stores); which objects pass is worked out after the
-          // pipeline, where no accumulator waits on it
-          const uint32_t e = wcnt + __popc(b & lt_mask);
-          wcnt += __popc(b);
-          if (hit) {
-            if (e < seg_cap) {
-              uint4 *dst = wrecv + (size_t)e * 8u;
+        if (b == 0u) continue;  // common case
+        // cold path: each thread with a hit stores its 32 values as one record (eight
+        // asynchronous 16-byte stores); which objects pass is worked out after the
+        // pipeline, where no accumulator waits on it
+        const uint32_t e = wcnt + __popc(b & lt_mask);
+        wcnt += __popc(b);
+        if (hit) {
+          if (e < seg_cap) {
+            uint4 *dst = wrecv + (size_t)e * 8u;
 #pragma unroll
-              for (int c = 0; c < 8; ++c) dst[c] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
-              wrech[e] = make_uint2((uint32_t)(obj0 + rt * 32u), ql);
-            } else {
-              atomicOr(&p.st[p.amap[q0 + ql]].flags, kFlagOverflow);  // lost: the query moves to the exact scorer
-            }
+            for (int c = 0; c < 8; ++c) dst[c] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+            wrech[e] = make_uint2((uint32_t)(obj0 + rt * 32u), ql);
+          } else {
+            atomicOr(&p.st[p.amap[q0 + ql]].flags, kFlagOverflow);  // lost: the query moves to the exact scorer
           }
-          __syncwarp();  // converged for the aligned wait
         }
-        if (rt + 1 < kWarpCols / 32u) tmem_wait_ld_regs(vn);
       }
       qt += kAcc;
       while (qt >= nqt) {

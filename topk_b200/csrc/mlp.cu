@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "batch_internal.h"
@@ -544,11 +545,21 @@ cudaError_t launch_features(const float *pmin, const float *pmax, const float *p
   uint32_t Ppad = 1;
   while (Ppad < P) Ppad <<= 1;
   const size_t smem = (2 * (size_t)Ppad + kMlpMaxIn + 2 * kHid) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(features_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the largest size, once per device (a driver call on every query otherwise)
+  static std::atomic<uint64_t> opted{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (nq <= 4) {
-    e = cudaFuncSetAttribute(features_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(opted.load(std::memory_order_acquire) & bit)) {
+    const int most = (int)((2 * (size_t)kMaxFeatureParts + kMlpMaxIn + 2 * kHid) * sizeof(float));
+    e = cudaFuncSetAttribute(features_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(features_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     if (e != cudaSuccess) return e;
+    opted.fetch_or(bit, std::memory_order_release);
+  }
+  if (nq <= 4) {
     if (nq) features_kernel<1024><<<nq, 1024, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
   } else {
     features_kernel<256><<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);

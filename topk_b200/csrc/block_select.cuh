@@ -93,6 +93,7 @@ __device__ void block_radix_select(const Src &src, uint32_t count, uint32_t min_
           if ((c & mask) == prefix) bin = (uint32_t)(c >> lob) & dmask;
         }
       }
+      if (!__any_sync(0xFFFFFFFFu, bin != 0xFFFFFFFFu)) continue;  // warp-uniform: nothing to count
       const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
       if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
     }
@@ -231,10 +232,12 @@ __device__ uint32_t block_kth_key(const Src &src, uint32_t count, uint32_t min_k
       }
 #pragma unroll
       for (int u = 0; u < kKthBatch; ++u) {
+        if (base + (uint32_t)u * NT >= count) break;  // uniform: no entry of this slot in range
         uint32_t bin = 0xFFFFFFFFu;
         if (base + (uint32_t)u * NT + t < count && key[u] >= min_key &&
             (shift == 24 || (key[u] >> (shift + 8)) == (prefix >> (shift + 8))))
           bin = (key[u] >> shift) & 255u;
+        if (!__any_sync(0xFFFFFFFFu, bin != 0xFFFFFFFFu)) continue;  // warp-uniform: nothing to count
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
         if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
       }

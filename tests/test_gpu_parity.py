@@ -163,6 +163,27 @@ def test_adversarial_orders_and_ties():
                 H.assert_same_result(t.query(k, w, a), O.topk_numpy(tn, k, w, a))
 
 
+def test_queries_after_high_scoring_ones_stay_exact():
+    """A query with low scores right after queries with high ones, few tiles per CTA:
+    every CTA's threshold copies must start from this query's own bounds (a slot left
+    unset once held the previous kernel's shared-memory contents, a threshold far
+    above this query's k-th score)."""
+    n, d = 1 << 20, 8
+    rng = np.random.default_rng(21)
+    with T.Table(n, d) as t:
+        t.generate(1, 4)
+        t.normalize()
+        tn = t.download()
+        w = (0.1 * np.arange(1, d + 1)).astype(np.float32)
+        for rep in range(3):
+            for k in (16, 64, 256, 1024):
+                for q in (8, 6, 2, 1, 2):
+                    a = np.arange(d - q, d, dtype=np.uint8)
+                    if rep == 2:
+                        a = np.sort(rng.choice(d, q, replace=False)).astype(np.uint8)
+                    H.assert_same_result(t.query(k, w, a)[:3], O.topk_numpy(tn, k, w, a))
+
+
 def test_nan_scores_rank_last():
     n, d = 5000, 2
     raw = O.generate(n, d, 1, 8)

@@ -49,8 +49,11 @@ struct SmemCtl {
   uint32_t cur;        // which of the two candidate buffers is current
   uint32_t thr_local;  // min key that can still enter (k-th CTA key + 1)
   uint32_t thr_g[2];   // CTA copy of the global threshold: tile i reads [i & 1], thread 0
-                       // writes [(i + 1) & 1] before tile i's barrier, so every thread of
-                       // a tile reads the same value
+                       // writes [(i + 1) & 1] before tile i's barrier, so with a vote
+                       // barrier every tile (partition mode, whose stop rule needs it)
+                       // every thread of a tile reads the same value; with a vote every
+                       // two tiles a thread may read a slot before or after an update,
+                       // both valid bounds
   uint32_t reductions;
   uint32_t is_last;
   uint32_t red_g;      // threshold snapshot shared by the block
@@ -178,6 +181,11 @@ __device__ __forceinline__ float4 score_cols(const ScanParams &p, const float4 *
 // thread too few bytes in flight otherwise).
 constexpr int kPrefetchQ = 4;
 
+// Tiles between two select votes of the scan (see scan_select_kernel).
+__host__ __device__ constexpr uint32_t scan_vote_tiles(int qq, bool part) {
+  return (qq >= 1 && qq <= 2 && !part) ? 2u : 1u;
+}
+
 // CTAs per SM the register budget is sized for: few queried columns need little data
 // in flight and gain from more CTAs (6: 42 registers); more columns need their loads
 // in flight without spills (5: 51 registers up to 8 columns, 4: 64 above).
@@ -219,7 +227,9 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     ctl->thr_local = 0;
     const uint32_t seed = max(p.thr_seed, p.thr_seed_dev ? *p.thr_seed_dev : 0u);
     if (seed) atomicMax(&p.scratch->g_thr, seed);  // every later read includes it
-    ctl->thr_g[0] = max(ld_volatile_u32(&p.scratch->g_thr), seed);
+    // both slots hold a valid bound from the start: with two tiles per vote a thread
+    // can read the second slot before thread 0's first copy into it
+    ctl->thr_g[0] = ctl->thr_g[1] = max(ld_volatile_u32(&p.scratch->g_thr), seed);
     ctl->reductions = 0;
   }
   bsync();
@@ -271,6 +281,11 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   };
   float4 xn[kPQ];
   if (prefetch && my_tiles) load_tile(0, part_cur, xn);
+  // tiles between two select votes: 2 for q <= 2 in id order (a thread's work per tile
+  // is small there and the vote's barrier was the top stall), 1 elsewhere; the buffer
+  // has room for that many tiles above its select mark (plan_scan)
+  constexpr uint32_t kVoteTiles = scan_vote_tiles(QQ, PART);
+  uint32_t after = 0;  // fill after this thread's warp last appended, since the last vote
   uint64_t kbest[KTH ? kPubMaxPerWarp : 1];  // KTH: this thread's best words, descending
 #pragma unroll
   for (int b = 0; b < (KTH ? (int)kPubMaxPerWarp : 1); ++b) kbest[b] = 0ull;
@@ -332,11 +347,10 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       if (!interior) pv = pv && row0 + v >= p.row_begin && row0 + v < p.row_end;
       pass_mask |= (unsigned)pv << v;
     }
-    // `after` = fill after this warp's append.  The warp that appends last in a tile
-    // sees the tile's final count, so OR-voting "after > cap - TILE" at the barrier
-    // gives every thread the same reduce decision.  (Reading ctl->count after a
-    // barrier would not: a fast warp may already be appending the next tile.)
-    uint32_t after = 0;
+    // `after` = fill after this warp's append.  The warp that appends last before a
+    // vote sees the final count, so OR-voting "after > cap - kVoteTiles * TILE" at the
+    // barrier gives every thread the same reduce decision.  (Reading ctl->count after
+    // a barrier would not: a fast warp may already be appending the next tile.)
     if (__ballot_sync(0xFFFFFFFFu, pass_mask != 0u)) {  // warp-uniform: some lane passed
       uint2 *cand = cand0 + (size_t)ctl->cur * cap;
       const uint32_t npass = __popc(pass_mask);
@@ -371,7 +385,11 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
         g_pending = ld_volatile_u32(&p.scratch->g_thr);
       }
     }
-    if (__syncthreads_or(after > cap - kTile)) {
+    // (uniform: every thread takes the same votes)
+    if (kVoteTiles > 1 && (i % kVoteTiles) != kVoteTiles - 1 && i + 1 < my_tiles) continue;
+    const bool full = __syncthreads_or(after > cap - kVoteTiles * kTile);
+    after = 0;
+    if (full) {
       if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       bsync();
       const uint32_t c = ctl->cur;
@@ -743,9 +761,12 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   pl.tile = kTile;
   uint32_t P = 1;
   while (P < k) P <<= 1;
-  // after a select the buffer holds <= k entries; one tile adds <= kTile, and a select
-  // runs once the fill exceeds cap - kTile
-  uint32_t cap = k + kTile + kTile / 2;
+  // after a select the buffer holds <= k entries; kVoteTiles tiles add <= that many times
+  // kTile, and a select runs once the fill exceeds cap - kVoteTiles * kTile
+  // (plus half a tile of slack when every tile votes; with two tiles per vote the
+  // rounding below leaves some, and more would cost q <= 2 a CTA per SM)
+  const uint32_t vote_tiles = scan_vote_tiles(qq <= 16 ? (int)qq : 0, part);
+  uint32_t cap = k + vote_tiles * kTile + (vote_tiles == 1 ? kTile / 2 : 0u);
   if (cap < P) cap = P;
   if (cap < 2048) cap = 2048;
   cap = (cap + kScanThreads - 1) / kScanThreads * kScanThreads;

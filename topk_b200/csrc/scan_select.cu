@@ -67,7 +67,7 @@ constexpr int kOffHist = 128;     // 256-bin radix histogram
 constexpr int kOffWsm = 1152;     // weights of the runtime-q path (kMaxQ floats)
 constexpr int kOffScnt = 1408;    // entry counts of a merge group's slots (kMaxFanin words)
 constexpr int kOffCand = kScanSmemFixed;
-constexpr uint32_t kMaxFanin = 8;
+constexpr uint32_t kMaxFanin = 32;  // merge-tree fan-in at most (small k: two levels for 592 CTAs)
 static_assert(kOffWsm + 4 * (int)kMaxQ <= kOffScnt && kOffScnt + 4 * (int)kMaxFanin <= kScanSmemFixed,
               "fixed shared block");
 static_assert(sizeof(SmemCtl) <= kOffNever, "control block layout");
@@ -774,7 +774,7 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   // the merge reuses the two candidate buffers: fan-in G needs G*k + P entries
   uint32_t mcap = 2 * cap;
   uint32_t G = (mcap - P) / k;
-  if (G > 8) G = 8;
+  if (G > kMaxFanin) G = kMaxFanin;
   if (G < 2) {
     G = 2;
     mcap = 2 * k + P;

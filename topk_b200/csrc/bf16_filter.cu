@@ -73,9 +73,14 @@ constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxQTPerCta = 16;
 constexpr uint32_t kAcc = kTmemCols / kOTile;            // TMEM accumulators in flight
-constexpr uint32_t kGroupWarps = kEpiWarps / kAcc;        // epilogue warps draining one accumulator
-constexpr uint32_t kWarpCols = kOTile * 4 / kGroupWarps;  // objects of one warp per pair
-static_assert(kGroupWarps % 4 == 0 && kEpiWarps % kAcc == 0, "whole TMEM lane quarters per group");
+// Epilogue groups: group g drains the pairs seq = g mod kDrainGroups.  One group (all
+// epilogue warps on every pair, each warp 2 round trips of 32 columns) drains a pair in
+// about half the time of two groups of eight (4 round trips each), and the drain, not
+// the MMAs, sets the pipeline's pace.
+constexpr uint32_t kDrainGroups = 1;
+constexpr uint32_t kGroupWarps = kEpiWarps / kDrainGroups;  // epilogue warps draining one pair
+constexpr uint32_t kWarpCols = kOTile * 4 / kGroupWarps;    // objects of one warp per pair
+static_assert(kGroupWarps % 4 == 0 && kEpiWarps % kDrainGroups == 0, "whole TMEM lane quarters per group");
 static_assert(kQTile == 128 && kWarpCols % 32 == 0, "a query per TMEM lane; whole 32-column round trips");
 constexpr size_t kMinFilterSmem = 120 * 1024;  // more than half an SM: one CTA per SM
 
@@ -213,7 +218,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
     for (uint32_t b = 0; b < kAcc; ++b) {
       mbar_init(accf + b, 1);
-      mbar_init(acce + b, kGroupWarps);  // the epilogue warps of the accumulator's group
+      mbar_init(acce + b, kGroupWarps);  // the epilogue warps that drain a pair
     }
     mbar_init(qfull, 1);
     mbar_init(mdone, 1);
@@ -302,24 +307,24 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    // warps kGroupWarps*g.. drain accumulator g, i.e. every kAcc-th pair.  Thread
-    // (warp w, lane l) owns TMEM lane 32*(w%4)+l, one query of the pair's query tile,
-    // and reads kWarpCols of its objects in round trips of 32 columns: one cut in a
-    // register, the largest value against it, a warp vote.  Each SM sub-partition
-    // holds warps of both groups, which work on different pairs.
+    // warps kGroupWarps*g.. drain the pairs seq = g mod kDrainGroups, pair seq in
+    // accumulator seq mod kAcc.  Thread (warp w, lane l) owns TMEM lane 32*(w%4)+l, one
+    // query of the pair's query tile, and reads kWarpCols of its objects in round trips
+    // of 32 columns: one cut in a register, the largest value against it, a warp vote.
     const uint32_t quarter = warp & 3u, grp = warp / kGroupWarps, part = (warp % kGroupWarps) >> 2;
-    const uint32_t tcol = tmem + ((quarter * 32u) << 16) + grp * kOTile + part * kWarpCols;
+    const uint32_t tcol0 = tmem + ((quarter * 32u) << 16) + part * kWarpCols;
     // this warp's record segment and its fill, the same in every lane (no atomics)
     uint4 *wrecv = recv + (size_t)warp * seg_cap * 8u;
     uint2 *wrech = rech + (size_t)warp * seg_cap;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t wcnt = 0;
     const uint64_t npairs = (te - tb) * nqt;
-    uint32_t parity = 0;
     uint32_t qt = grp % nqt;       // query tile and
     uint64_t t = tb + grp / nqt;   // object tile of pair seq = t * nqt + qt
-    for (uint64_t seq = grp; seq < npairs; seq += kAcc, parity ^= 1u) {
-      if (!__all_sync(0xFFFFFFFFu, fwait(accf + grp, parity, limit, abort_flag))) break;
+    for (uint64_t seq = grp; seq < npairs; seq += kDrainGroups) {
+      const uint32_t buf = (uint32_t)(seq % kAcc), parity = (uint32_t)((seq / kAcc) & 1u);
+      const uint32_t tcol = tcol0 + buf * kOTile;
+      if (!__all_sync(0xFFFFFFFFu, fwait(accf + buf, parity, limit, abort_flag))) break;
       tc_fence_after();
       const uint32_t ql = qt * kQTile + quarter * 32u + lane;  // this thread's query, CTA-relative
       const float cut = scut[ql];
@@ -333,7 +338,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
           // the accumulator is free once its last columns are in registers
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(acce + grp);
+          if (lane == 0) mbar_arrive(acce + buf);
         }
         // hot path: the largest of the 32 values against the thread's cut
         const float m = max32(v);
@@ -356,7 +361,7 @@ __global__ void __launch_bounds__(kFThreads, 1) bf16_filter_kernel(const FilterA
           }
         }
       }
-      qt += kAcc;
+      qt += kDrainGroups;
       while (qt >= nqt) {
         qt -= nqt;
         ++t;

@@ -73,11 +73,12 @@ constexpr uint32_t kFThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxQTPerCta = 16;
 constexpr uint32_t kAcc = kTmemCols / kOTile;            // TMEM accumulators in flight
-// Epilogue groups: group g drains the pairs seq = g mod kDrainGroups.  One group (all
-// epilogue warps on every pair, each warp 2 round trips of 32 columns) drains a pair in
-// about half the time of two groups of eight (4 round trips each), and the drain, not
-// the MMAs, sets the pipeline's pace.
-constexpr uint32_t kDrainGroups = 1;
+// Epilogue groups: group g drains the pairs seq = g mod kDrainGroups, so with two
+// groups each accumulator has its own eight warps (4 round trips of 32 columns each).
+// One group of all sixteen warps on every pair (2 round trips each) measured slower
+// (C3 batch 34.1 against 31.7 ms): the drain is bound by its throughput, not by the
+// latency of one warp's round trips.
+constexpr uint32_t kDrainGroups = 2;
 constexpr uint32_t kGroupWarps = kEpiWarps / kDrainGroups;  // epilogue warps draining one pair
 constexpr uint32_t kWarpCols = kOTile * 4 / kGroupWarps;    // objects of one warp per pair
 static_assert(kGroupWarps % 4 == 0 && kEpiWarps % kDrainGroups == 0, "whole TMEM lane quarters per group");

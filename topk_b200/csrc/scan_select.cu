@@ -46,7 +46,6 @@ namespace {
 
 struct SmemCtl {
   uint32_t count;      // entries in the current candidate buffer
-  uint32_t cur;        // which of the two candidate buffers is current
   uint32_t thr_local;  // min key that can still enter (k-th CTA key + 1)
   uint32_t thr_g[2];   // CTA copy of the global threshold: tile i reads [i & 1], thread 0
                        // writes [(i + 1) & 1] before tile i's barrier, so with a vote
@@ -208,8 +207,11 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffHist);
   float *wsm = reinterpret_cast<float *>(smem + kOffWsm);
   uint32_t *scnt = reinterpret_cast<uint32_t *>(smem + kOffScnt);
-  uint2 *cand0 = reinterpret_cast<uint2 *>(smem + kOffCand);  // two buffers of cap entries
-  uint2 *mbuf = cand0;                                         // merge area (reuses both)
+  // the candidate buffer (cap entries), then the select's output (the rest of mcap);
+  // the merge reuses both
+  uint2 *cand0 = reinterpret_cast<uint2 *>(smem + kOffCand);
+  uint2 *selb = cand0 + p.cap;
+  uint2 *mbuf = cand0;
 
   const int t = threadIdx.x;
   const int lane = t & 31;
@@ -223,7 +225,6 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     mbar_init(never, 1);
     fence_barrier_init();
     ctl->count = 0;
-    ctl->cur = 0;
     ctl->thr_local = 0;
     const uint32_t seed = max(p.thr_seed, p.thr_seed_dev ? *p.thr_seed_dev : 0u);
     if (seed) atomicMax(&p.scratch->g_thr, seed);  // every later read includes it
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     // barrier gives every thread the same reduce decision.  (Reading ctl->count after
     // a barrier would not: a fast warp may already be appending the next tile.)
     if (__ballot_sync(0xFFFFFFFFu, pass_mask != 0u)) {  // warp-uniform: some lane passed
-      uint2 *cand = cand0 + (size_t)ctl->cur * cap;
+      uint2 *cand = cand0;
       const uint32_t npass = __popc(pass_mask);
       uint32_t incl = npass;
 #pragma unroll
@@ -392,11 +393,10 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     if (full) {
       if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
       bsync();
-      const uint32_t c = ctl->cur;
-      const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
-                                                       cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
+      // the best k into the output area, then back to the front of the buffer
+      const uint32_t kept = block_reduce<kScanThreads>(cand0, ctl->count, selb, p.k, ctl->red_g, hist, &ctl->sel);
+      for (uint32_t j = t; j < kept; j += kScanThreads) cand0[j] = selb[j];
       if (t == 0) {
-        ctl->cur = c ^ 1u;
         ctl->count = kept;
         ctl->reductions++;
         if (kept == p.k) {  // the CTA knows a k-th key
@@ -416,11 +416,9 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
   bsync();
   if (!KTH && ctl->count > p.k && !p.kth_only) {
-    const uint32_t c = ctl->cur;
-    const uint32_t kept = block_reduce<kScanThreads>(cand0 + (size_t)c * cap, ctl->count,
-                                                     cand0 + (size_t)(c ^ 1u) * cap, p.k, ctl->red_g, hist, &ctl->sel);
+    const uint32_t kept = block_reduce<kScanThreads>(cand0, ctl->count, selb, p.k, ctl->red_g, hist, &ctl->sel);
+    for (uint32_t j = t; j < kept; j += kScanThreads) cand0[j] = selb[j];
     if (t == 0) {
-      ctl->cur = c ^ 1u;
       ctl->count = kept;
       ctl->reductions++;
       if (kept == p.k) atomicMax(&p.scratch->g_thr, ctl->sel.kept_min);
@@ -440,7 +438,7 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   // bounded wait: if it runs out they go on with the threshold they have, which is
   // still exact, only slower) and the merge tree then carries about k entries in all.
   if (KTH || p.pub) {
-    const uint2 *res0 = cand0 + (size_t)ctl->cur * cap;
+    const uint2 *res0 = cand0;
     // Each warp publishes the best r = pub_m / 8 entries of its share of the buffer
     // (entries j = t, t + 256, ...): every thread keeps its own best r, then r rounds of
     // a warp maximum, each taken from the lane that holds it.  The CTA's pub_m keys are
@@ -493,8 +491,9 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       // first (independent loads, kStageBatch in flight per thread), so the select's
       // five passes read shared memory, not L2.
       const uint32_t np = gridDim.x * p.pub_m;
-      uint32_t *stage = reinterpret_cast<uint32_t *>(KTH ? cand0 : cand0 + (size_t)(ctl->cur ^ 1u) * cap);
-      const uint32_t stage_cap = KTH ? 2u * p.mcap : 2u * cap;
+      // (a threshold pass has no candidates; a scan's <= k sit at the buffer's front)
+      uint32_t *stage = reinterpret_cast<uint32_t *>(KTH ? cand0 : cand0 + p.k);
+      const uint32_t stage_cap = KTH ? 2u * p.mcap : 2u * (p.mcap - p.k);
       uint32_t kth;
       if (np <= stage_cap) {
         constexpr int kStageBatch = 8;
@@ -545,10 +544,12 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
 
   // ---- merge tree ----
   const uint32_t k = p.k;
-  uint2 *res = cand0 + (size_t)ctl->cur * cap;
+  uint2 *res = cand0;
   uint32_t res_n = ctl->count;
   uint32_t level = 0, slot = blockIdx.x, merged = res_n;
-  uint2 *outb = mbuf + (size_t)p.fanin * k;
+  uint32_t kpad = 1;  // k rounded up to a power of two: the kept entries and the sort's padding
+  while (kpad < k) kpad <<= 1;
+  uint2 *outb = mbuf + (p.mcap - kpad);
   while (p.nslots[level] > 1) {
     // publish my result into slot (level, slot), filtered by the current threshold
     if (t == 0) {
@@ -580,45 +581,54 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     if (!ctl->is_last) return;
     __threadfence();
     // the last arrival merges the group's slots: their counts first, then all their
-    // entries as one flat index space, kMergeBatch loads per thread in flight at a time
-    if (t == 0) {
-      ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
-      ctl->sel.wcount = 0;
-    }
+    // entries as one flat index space, kMergeBatch loads per thread in flight at a
+    // time, in chunks that fit the shared input area; the best k so far (in `outb`)
+    // open each chunk after the first
+    if (t == 0) ctl->red_g = ld_volatile_u32(&p.scratch->g_thr);
     if (t < (int)gsize) scnt[t] = __ldcg(&p.slot_count[p.slot_off[level] + first + t]);
     bsync();
     {
       const uint32_t g = ctl->red_g;
-      const uint32_t lim = p.fanin * k;
+      const uint32_t in_cap = p.mcap - kpad;  // input area [0, in_cap), outb after it
       uint32_t total = 0;
       for (uint32_t si = 0; si < gsize; ++si) total += scnt[si];
-      constexpr int kMergeBatch = 2;
-      for (uint32_t base = 0; base < total; base += kScanThreads * kMergeBatch) {
-        uint2 e[kMergeBatch];
+      uint32_t kept = 0, done = 0;
+      merged = 0;
+      do {
+        for (uint32_t j = t; j < kept; j += kScanThreads) mbuf[j] = outb[j];
+        if (t == 0) ctl->sel.wcount = kept;
+        bsync();
+        const uint32_t n_load = min(total - done, in_cap - kept);
+        constexpr int kMergeBatch = 2;
+        for (uint32_t base = 0; base < n_load; base += kScanThreads * kMergeBatch) {
+          uint2 e[kMergeBatch];
 #pragma unroll
-        for (int u = 0; u < kMergeBatch; ++u) {
-          uint32_t f = base + (uint32_t)u * kScanThreads + t;
-          e[u] = make_uint2(0u, 0u);
-          if (f < total) {
-            uint32_t si = 0;
-            while (f >= scnt[si]) f -= scnt[si++];  // f < total: ends inside a slot
-            e[u] = __ldcg(p.slots + (size_t)(p.slot_off[level] + first + si) * k + f);
+          for (int u = 0; u < kMergeBatch; ++u) {
+            const uint32_t j = base + (uint32_t)u * kScanThreads + t;
+            e[u] = make_uint2(0u, 0u);
+            if (j < n_load) {
+              uint32_t f = done + j, si = 0;
+              while (f >= scnt[si]) f -= scnt[si++];  // done + j < total: ends inside a slot
+              e[u] = __ldcg(p.slots + (size_t)(p.slot_off[level] + first + si) * k + f);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kMergeBatch; ++u) {
+            if (base + (uint32_t)u * kScanThreads + t < n_load && e[u].x >= g) {
+              const uint32_t pos = atomicAdd(&ctl->sel.wcount, 1u);
+              if (TOPK_CHECK(pos < in_cap, kDiagMerge, level, pos, in_cap)) mbuf[pos] = e[u];
+            }
           }
         }
-#pragma unroll
-        for (int u = 0; u < kMergeBatch; ++u) {
-          if (base + (uint32_t)u * kScanThreads + t < total && e[u].x >= g) {
-            const uint32_t pos = atomicAdd(&ctl->sel.wcount, 1u);
-            if (TOPK_CHECK(pos < lim, kDiagMerge, level, pos, lim)) mbuf[pos] = e[u];
-          }
-        }
-      }
+        bsync();
+        const uint32_t loaded = min(ctl->sel.wcount, in_cap);
+        bsync();  // every thread has `loaded` before block_reduce resets wcount
+        merged += loaded - kept;
+        kept = block_reduce<kScanThreads>(mbuf, loaded, outb, k, 0u, hist, &ctl->sel);
+        done += n_load;
+      } while (done < total);
+      res_n = kept;
     }
-    bsync();
-    const uint32_t loaded = min(ctl->sel.wcount, p.fanin * k);
-    bsync();  // every thread has `loaded` before block_reduce resets wcount
-    merged = loaded;
-    res_n = block_reduce<kScanThreads>(mbuf, loaded, outb, k, 0u, hist, &ctl->sel);
     res = outb;
     level += 1;
     slot = grp;
@@ -771,14 +781,13 @@ ScanPlan plan_scan(uint32_t qq, uint32_t k, uint64_t rows, int num_sms, size_t s
   if (cap < 2048) cap = 2048;
   cap = (cap + kScanThreads - 1) / kScanThreads * kScanThreads;
   pl.cap = cap;
-  // the merge reuses the two candidate buffers: fan-in G needs G*k + P entries
-  uint32_t mcap = 2 * cap;
-  uint32_t G = (mcap - P) / k;
+  // the select writes <= k entries (padded to P for the sort) after the buffer; the
+  // merge reuses both, its input in chunks of up to cap entries, so the fan-in is not
+  // bound by it: G = what two buffers of cap would hold, 4 to kMaxFanin
+  uint32_t mcap = cap + P;
+  uint32_t G = (2 * cap - P) / k;
   if (G > kMaxFanin) G = kMaxFanin;
-  if (G < 2) {
-    G = 2;
-    mcap = 2 * k + P;
-  }
+  if (G < 4) G = 4;
   pl.fanin = G;
   pl.mcap = mcap;
   pl.smem = kScanSmemFixed + (size_t)mcap * 8;

@@ -535,7 +535,7 @@ std::vector<BatchQuery> pack_queries(topk_table_t h, uint64_t nq, const uint64_t
                                      const float *weights, uint64_t wstride, const uint8_t *attrs, uint64_t astride);
 
 constexpr uint32_t kPrunedCtasPerSm = 3;  // CTAs per SM of a pruned scan
-constexpr uint32_t kRound1CtasPerSm = 0;  // and of its first round (0: as many as fit)
+constexpr uint32_t kRound1CtasPerSm = 4;  // and of its first round (more CTAs publish more keys)
 
 // Exact top-k over the partitioned copy as one device pipeline on the context's
 // stream; nothing is decided on the host between the launches.

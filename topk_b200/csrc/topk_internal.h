@@ -55,8 +55,9 @@ struct ScanParams {
   uint32_t num_tiles;
   uint32_t qq;
   uint32_t k;
-  uint32_t cap;         // entries of each of the two shared candidate buffers
-  uint32_t mcap;        // shared entries available to the merge (both buffers reused)
+  uint32_t cap;         // entries of the shared candidate buffer
+  uint32_t mcap;        // shared entries: the buffer, then a select's output (<= k, padded
+                        // to a power of two); the merge reuses all of them
   uint32_t fanin;       // merge-tree fan-in G
   uint32_t levels;      // merge-tree levels below the root (level l has nslots[l] slots)
   uint32_t nslots[kMaxLevels];

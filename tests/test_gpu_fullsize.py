@@ -106,9 +106,10 @@ def test_fullsize_slice_vs_oracle(big):
 
 @pytest.mark.parametrize("dist", [1, 2])
 def test_large_k_full_scan_with_mixed_sign_weights_matches_oracle(dist):
-    """2^26 rows: large enough that a scan with k >= 128 first runs its threshold pass
-    over a tile sample; negative and mixed weights (scores below zero) and ties from
-    repeated attributes must still give the oracle's result bit for bit."""
+    """2^26 rows: large enough that a scan with large k first runs its threshold pass
+    over a tile sample (from k = 128 at two attributes, from k = 512 at four);
+    negative and mixed weights (scores below zero) and ties from repeated attributes
+    must still give the oracle's result bit for bit."""
     n, d = (1 << 26) + 333, 4
     raw = O.generate(n, d, dist, 31 + dist)
     tn = raw.copy()
@@ -120,5 +121,5 @@ def test_large_k_full_scan_with_mixed_sign_weights_matches_oracle(dist):
         for k in (128, 1024, 4096):
             for w in (rng.uniform(-1, 0, d), rng.uniform(-1, 1, d), rng.uniform(0, 1, d)):
                 w = w.astype(np.float32)
-                a = np.array([3, 0, 3, 1], np.uint8)
-                H.assert_same_result(t.query(k, w, a), O.topk(tn, k, w, a))
+                for a in (np.array([3, 0, 3, 1], np.uint8), np.array([2, 0], np.uint8)):
+                    H.assert_same_result(t.query(k, w, a), O.topk(tn, k, w, a))

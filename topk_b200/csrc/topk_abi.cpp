@@ -441,7 +441,7 @@ int enqueue_scan(topk_table_t h, Ctx *c, cudaStream_t stream, uint64_t r0, uint6
   // Large k over a large table in id order: a threshold pass over every
   // kSampleStride-th tile first (its own launch, same kernel, no merge), whose bound
   // seeds this scan, so its CTAs rarely need a select.
-  if (!ps && p.pub && k >= kSampleMinK && tiles >= kSampleMinTiles) {
+  if (!ps && p.pub && k >= sample_min_k(qq) && tiles >= kSampleMinTiles) {
     ScanParams q = p;
     q.num_tiles = (uint32_t)((tiles + kSampleStride - 1) / kSampleStride);
     q.tile_step = (uint64_t)pl.tile * kSampleStride;

@@ -111,9 +111,10 @@ def measured_peaks():
 # the launches of one query on a 2^26-row table (the scan, plus for k >= 128 its
 # threshold pass over every 64th tile; every object is read once, so traffic grows with
 # the rows scanned) scaled x4, the mean over k in {16, 64, 256, 1024}.
-TRAFFIC_PER_LAUNCH = {2: 2.1652e9, 4: 4.3304e9, 8: 8.6592e9, 16: 1.7317e10}
+TRAFFIC_PER_LAUNCH = {2: 2.1687e9, 4: 4.3131e9, 8: 8.6261e9, 16: 1.7183e10}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the launches of each query on a "
-                  "2^26-row table (scan + threshold pass), scaled x4 to 2^28 rows")
+                  "2^26-row table (scan + threshold pass where it runs), mean over the four k, scaled x4 to "
+                  "2^28 rows")
 
 
 class Clocks:

@@ -322,39 +322,100 @@ __global__ void __launch_bounds__(128) mlp_predict_kernel(const float *__restric
 }
 
 // ---------------------------------------------------------------- features
-struct FloatKeys {  // order keys of a float array (NaN lowest), as block_kth_key reads them
-  const float *p;
-  __device__ uint2 operator()(uint32_t j) const { return make_uint2(f2key(p[j]), 0u); }
-};
 
-// The K = min(P, 128) largest of v[0..P) in descending order into out[0..K): the K-th
-// largest order key by a block radix select, the entries strictly above it (fewer than
-// K) placed by their rank among themselves, the rest of out[] the K-th value itself.
+// The K = min(P, 128) largest of each of two arrays a[0..P), b[0..P) in descending
+// order into oa[0..K), ob[0..K): the K-th largest order key of each by a radix select
+// (four 8-bit digit passes from the top, both arrays in the same passes, histogram
+// updates aggregated per warp), the entries strictly above it (fewer than K) placed
+// by their rank among themselves, the rest of the output the K-th value itself.
 // Ranks 1, 2, 4, .. 128 are all the features need, so nothing else is sorted.
+// hist: 512 words; buf / bkey: 2 * 128 entries; cnt: 2 words; sel: 4 words.
 template <int NT>
-__device__ void top_desc(const float *v, uint32_t P, float *out, uint32_t *hist, SelShared *sh, float *buf,
-                         uint32_t *bkey, uint32_t *cnt) {
-  const uint32_t K = min(P, 128u);
-  const uint32_t kth = block_kth_key<NT>(FloatKeys{v}, P, 0u, K, hist, sh);
-  if (threadIdx.x == 0) *cnt = 0;
+__device__ void top_desc_two(const float *a, const float *b, uint32_t P, float *oa, float *ob, uint32_t *hist,
+                             float *buf, uint32_t *bkey, uint32_t *cnt, uint32_t *sel) {
+  const uint32_t t = threadIdx.x, lane = t & 31, K = min(P, 128u);
+  uint32_t prefix[2] = {0u, 0u}, need[2] = {K, K};
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (uint32_t i = t; i < 512; i += NT) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < P; base += NT) {  // uniform trip count
+      const uint32_t j = base + t;
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        uint32_t bin = 0xFFFFFFFFu;
+        if (j < P) {
+          const uint32_t key = f2key((s2 ? b : a)[j]);
+          if (shift == 24 || (key >> (shift + 8)) == (prefix[s2] >> (shift + 8))) bin = (key >> shift) & 255u;
+        }
+        if (!__any_sync(0xFFFFFFFFu, bin != 0xFFFFFFFFu)) continue;  // warp-uniform
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+        if (bin != 0xFFFFFFFFu && lane == __ffs(peers) - 1)
+          atomicAdd(&hist[256 * s2 + bin], (uint32_t)__popc(peers));
+      }
+    }
+    __syncthreads();
+    if (t < 64) {  // warp s2: lane l owns bins [255-8l-7, 255-8l] of array s2, high to low
+      const uint32_t s2 = t >> 5;
+      const int top = 255 - 8 * (int)lane;
+      uint32_t local[8], sum = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        local[q] = hist[256 * s2 + top - q];
+        sum += local[q];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t excl = incl - sum;
+      if (excl < need[s2] && need[s2] <= incl) {
+        uint32_t run = excl;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (run + local[q] >= need[s2]) {
+            sel[2 * s2] = (uint32_t)(top - q);
+            sel[2 * s2 + 1] = run;
+            break;
+          }
+          run += local[q];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s2 = 0; s2 < 2; ++s2) {
+      need[s2] -= sel[2 * s2 + 1];
+      prefix[s2] |= sel[2 * s2] << shift;
+    }
+    __syncthreads();  // everyone has read the result before the next pass rewrites it
+  }
+  if (t < 2) cnt[t] = 0;
   __syncthreads();
-  for (uint32_t j = threadIdx.x; j < P; j += NT) {
-    const uint32_t key = f2key(v[j]);
-    if (key > kth) {
-      const uint32_t pos = atomicAdd(cnt, 1u);  // < K
-      buf[pos] = v[j];
-      bkey[pos] = key;
+  for (uint32_t j = t; j < P; j += NT) {
+#pragma unroll
+    for (int s2 = 0; s2 < 2; ++s2) {
+      const float v = (s2 ? b : a)[j];
+      const uint32_t key = f2key(v);
+      if (key > prefix[s2]) {
+        const uint32_t pos = atomicAdd(&cnt[s2], 1u);  // < K
+        buf[128 * s2 + pos] = v;
+        bkey[128 * s2 + pos] = key;
+      }
     }
   }
   __syncthreads();
-  const uint32_t c = *cnt;
-  for (uint32_t i = threadIdx.x; i < K; i += NT) {
+  for (uint32_t x = t; x < 2 * K; x += NT) {
+    const uint32_t s2 = x / K, i = x % K, c = cnt[s2];
+    float *out = s2 ? ob : oa;
+    const uint32_t *bk = bkey + 128 * s2;
     if (i < c) {
       uint32_t rank = 0;
-      for (uint32_t j = 0; j < c; ++j) rank += (bkey[j] > bkey[i] || (bkey[j] == bkey[i] && j < i)) ? 1u : 0u;
-      out[rank] = buf[i];
+      for (uint32_t j = 0; j < c; ++j) rank += (bk[j] > bk[i] || (bk[j] == bk[i] && j < i)) ? 1u : 0u;
+      out[rank] = buf[128 * s2 + i];
     } else {
-      out[i] = key2f(kth);
+      out[i] = key2f(prefix[s2]);
     }
   }
   __syncthreads();
@@ -375,9 +436,8 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
   float *feat = mu + Ppad;          // kMlpMaxIn
   float *h = feat + kMlpMaxIn;      // 2 * kHid
   __shared__ float S;
-  __shared__ uint32_t hist[256], bkey[128], cnt;
-  __shared__ SelShared sel;
-  __shared__ float tb[128], tm[128], buf[128];
+  __shared__ uint32_t hist[512], bkey[256], cnt[2], selw[4];
+  __shared__ float tb[128], tm[128], buf[256];
   const BatchQuery &q = qs[blockIdx.x];
   const uint32_t F = feature_dim(d);
   if (threadIdx.x == 0) {
@@ -402,8 +462,7 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
   }
   for (uint32_t m = threadIdx.x; m < kMlpMaxIn; m += blockDim.x) feat[m] = 0.0f;
   __syncthreads();
-  top_desc<NT>(bnd, P, tb, hist, &sel, buf, bkey, &cnt);
-  top_desc<NT>(mu, P, tm, hist, &sel, buf, bkey, &cnt);
+  top_desc_two<NT>(bnd, mu, P, tb, tm, hist, buf, bkey, cnt, selw);
   if (threadIdx.x == 0) {
     const float inv = 1.0f / S;
     for (uint32_t m = 0; m < q.qq; ++m) feat[q.attr[m]] += q.w[m] * inv;

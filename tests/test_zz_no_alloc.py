@@ -58,6 +58,38 @@ def test_noalloc_matches_regular_entry_point_twice():
             H.assert_same_result(got, t.query(k, w, a))
 
 
+def test_noalloc_large_table_large_k_matches_regular_entry_point():
+    """2^26 rows: large enough that a large-k query first runs the threshold pass
+    over a tile sample (from k = 128 at two attributes, from k = 512 at four), in
+    this entry point as in topk_query; mixed-sign weights and a repeated attribute."""
+    torch = pytest.importorskip("torch")
+    L = T.load()
+    n, d = (1 << 26) + 333, 4
+    ld = (n + 63) // 64 * 64
+    raw = O.generate(n, d, O.ANTICORRELATED, 41)
+    with T.Table(n, d) as t:
+        t.upload(raw)
+        t.normalize()
+        host = np.zeros((d, ld), np.float32)
+        host[:, :n] = t.download()
+        dt = torch.from_numpy(host).cuda()
+        del host
+        ids = torch.empty(1024, dtype=torch.int64, device="cuda")
+        sc = torch.empty(1024, dtype=torch.float32, device="cuda")
+        th = torch.empty(1, dtype=torch.float32, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        rng = np.random.default_rng(9)
+        for k in (128, 1024):
+            for w in (rng.uniform(-1, 1, d), rng.uniform(0, 1, d)):
+                w = w.astype(np.float32)
+                for a in (np.array([2, 0], np.uint8), np.array([3, 0, 3, 1], np.uint8)):
+                    st = _noalloc(L, dt, n, ld, d, k, w, a, ids, sc, th, stream)
+                    assert st == _lib.OK, L.topk_last_error()
+                    torch.cuda.synchronize()
+                    got = (ids[:k].cpu().numpy().astype(np.uint64), sc[:k].cpu().numpy(), float(th.cpu()[0]))
+                    H.assert_same_result(got, t.query(k, w, a))
+
+
 def test_noalloc_k_above_n_matches_regular_entry_point():
     torch = pytest.importorskip("torch")
     L = T.load()

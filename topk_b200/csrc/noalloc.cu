@@ -188,6 +188,28 @@ extern "C" int topk_query_noalloc(const float *d_table, uint64_t n, uint64_t ld,
   // arrival counters (the scan expects them at zero when it starts).
   if ((e = cudaMemsetAsync(blk, 0, kMetaBytes, s)) != cudaSuccess)
     return fail(TOPK_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+  // Large k over a large table: the threshold pass over every kSampleStride-th tile
+  // first, as topk_query runs it; its bound goes to a spare word of the array's header
+  // (zeroed above) and seeds the scan.
+  if (p.pub && kk >= sample_min_k(qq) && tiles >= kSampleMinTiles) {
+    uint32_t *seed_word = &p.scratch->pad[0];
+    ScanParams q = p;
+    q.num_tiles = (uint32_t)((tiles + kSampleStride - 1) / kSampleStride);
+    q.tile_step = (uint64_t)pl.tile * kSampleStride;
+    q.kth_only = 1;
+    q.out_kth_key = seed_word;
+    q.out_ids = nullptr;
+    q.out_scores = nullptr;
+    q.out_threshold = nullptr;
+    ScanPlan qp = pl;
+    qp.grid = (int)std::min<uint64_t>((uint64_t)pl.grid, q.num_tiles);
+    if ((uint32_t)qp.grid >= kPubMinGrid) {
+      q.pub_m = pub_keys_per_cta((uint32_t)kk, (uint32_t)qp.grid);
+      if ((e = launch_scan(qp, q, s)) != cudaSuccess)
+        return fail(TOPK_ERR_CUDA, "threshold pass launch: %s", cudaGetErrorString(e));
+      p.thr_seed_dev = seed_word;
+    }
+  }
   if ((e = launch_scan(pl, p, s)) != cudaSuccess)
     return fail(TOPK_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
   return TOPK_OK;

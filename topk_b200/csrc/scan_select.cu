@@ -249,12 +249,8 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
   // next-tile prefetch: the loads of tile i + 1 are in flight while tile i is scored
   constexpr int kPQ = (QQ >= 1 && QQ <= kPrefetchQ) ? QQ : 1;
   constexpr bool prefetch = QQ >= 1 && QQ <= kPrefetchQ;
-  // queried columns: computed once for q >= 3; for q <= 2 per tile (two more 64-bit
-  // registers would cost a CTA per SM there, measured slower)
-  constexpr bool kHoist = kPQ >= 3;
-  const float *col[kPQ];
-#pragma unroll
-  for (int m = 0; m < kPQ; ++m) col[m] = kHoist ? p.table + (uint64_t)p.attr[m] * p.ld : nullptr;
+  // queried columns of the prefetching forms: read from the parameter block (colp), no
+  // registers held
   // partition mode: the partitions (and bounds) of tiles i and i + 1 are known at the
   // start of tile i, the one of tile i + 2 is loaded during it
   const uint32_t pmask = (1u << p.part_shift) - 1u;
@@ -273,15 +269,26 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
     if constexpr (PART) return ((uint64_t)part << p.part_rows_log2) + (tix & pmask) * kTile;
     return p.tile_begin + tix * p.tile_step;
   };
-  auto load_tile = [&](uint32_t j, uint32_t part, float4 *dst) {
-    const uint64_t tl = tile_row(j, part);
+  auto load_rows = [&](uint64_t tl, float4 *dst) {  // the tile that starts at row tl
     const float *c[kPQ];
 #pragma unroll
-    for (int m = 0; m < kPQ; ++m) c[m] = kHoist ? col[m] : p.table + (uint64_t)p.attr[m] * p.ld;
+    for (int m = 0; m < kPQ; ++m) c[m] = p.colp[m];
     load_cols<kPQ>(p, c, tl + (uint64_t)t * kVec, !(tl >= p.row_begin && tl + kTile <= p.row_end), dst);
   };
+  // id order with prefetch: first row and index of the tile whose loads went out last;
+  // tile j lies wholly inside [row_begin, row_end) iff j - int_lo < int_n (unsigned)
+  uint64_t next_row = p.tile_begin + (uint64_t)blockIdx.x * p.tile_step;
+  uint32_t next_tix = blockIdx.x;
+  auto load_next = [&](float4 *dst) {
+    const uint64_t r = next_row + (uint64_t)t * kVec;
+    const bool inner = next_tix - p.int_lo < p.int_n;
+    load_cols<kPQ>(p, p.colp, r, !inner, dst);
+  };
   float4 xn[kPQ];
-  if (prefetch && my_tiles) load_tile(0, part_cur, xn);
+  if (prefetch && my_tiles) {
+    if constexpr (PART) load_rows(tile_row(0, part_cur), xn);
+    else load_next(xn);
+  }
   // tiles between two select votes: 2 for q <= 2 in id order (a thread's work per tile
   // is small there and the vote's barrier was the top stall), 1 elsewhere; the buffer
   // has room for that many tiles above its select mark (plan_scan)
@@ -300,15 +307,24 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
       // nothing in this partition (nor in any later one of this CTA) can reach thr
       if (key_cur < thr) break;
     }
-    const uint64_t tile0 = tile_row(i, part_cur);
+    const uint64_t tile0 = (prefetch && !PART) ? next_row : tile_row(i, part_cur);
     const uint64_t row0 = tile0 + (uint64_t)t * kVec;
-    const bool interior = tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
+    const bool interior = (prefetch && !PART) ? next_tix - p.int_lo < p.int_n
+                                              : tile0 >= p.row_begin && tile0 + kTile <= p.row_end;  // uniform
     float4 s;
     if (prefetch) {
       float4 x[kPQ];
 #pragma unroll
       for (int m = 0; m < kPQ; ++m) x[m] = xn[m];
-      if (i + 1 < my_tiles) load_tile(i + 1, part_nx, xn);
+      if (i + 1 < my_tiles) {
+        if constexpr (PART) {
+          load_rows(tile_row(i + 1, part_nx), xn);
+        } else {
+          next_row += p.grid_rows;
+          next_tix += gridDim.x;
+          load_next(xn);
+        }
+      }
       s = score_cols<kPQ>(p, x);
     } else {
       s = score4<QQ>(p, wsm, qq, row0, !interior);
@@ -855,7 +871,16 @@ cudaError_t launch_scan(const ScanPlan &pl, const ScanParams &p, cudaStream_t st
   // a threshold pass needs the published-keys area
   if (p.kth_only && (!p.pub || !p.out_kth_key || p.pub_m == 0 || p.pub_m > 8 * kPubMaxPerWarp))
     return cudaErrorInvalidValue;
-  kernel_for(p.qq, p.part_list != nullptr, p.kth_only != 0)<<<pl.grid, kScanThreads, pl.smem, stream>>>(p);
+  ScanParams q = p;
+  for (uint32_t m = 0; m < 4; ++m) q.colp[m] = m < p.qq ? p.table + (uint64_t)p.attr[m] * p.ld : p.table;
+  q.grid_rows = (uint64_t)pl.grid * p.tile_step;
+  // id order: tiles [int_lo, int_lo + int_n) lie wholly inside [row_begin, row_end)
+  q.int_lo = p.tile_begin < p.row_begin ? 1u : 0u;
+  uint64_t hi = 0;
+  if (p.row_end >= p.tile_begin + kTile) hi = (p.row_end - p.tile_begin - kTile) / p.tile_step + 1;
+  if (hi > p.num_tiles) hi = p.num_tiles;
+  q.int_n = hi > q.int_lo ? (uint32_t)(hi - q.int_lo) : 0u;
+  kernel_for(p.qq, p.part_list != nullptr, p.kth_only != 0)<<<pl.grid, kScanThreads, pl.smem, stream>>>(q);
   return cudaGetLastError();
 }
 

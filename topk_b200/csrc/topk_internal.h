@@ -105,6 +105,13 @@ struct ScanParams {
   const uint32_t *thr_seed_dev;  // may be null: a further seed read from device memory at start
   uint8_t attr[kMaxQ];
   float w[kMaxQ];       // weights[attr[m]], gathered on the host
+  // Set by launch_scan: the first four queried columns (table + attr[m] * ld), the
+  // rows from one tile of a CTA to its next in id order (grid * tile_step), and the
+  // tiles [int_lo, int_lo + int_n) that lie wholly inside [row_begin, row_end).
+  const float *colp[4];
+  uint64_t grid_rows;
+  uint32_t int_lo;
+  uint32_t int_n;
 };
 
 // The published-keys bound before the merge (ScanParams::pub): used for k >= this and

@@ -298,6 +298,10 @@ __global__ void __launch_bounds__(kScanThreads, scan_min_blocks<QQ>()) scan_sele
 #pragma unroll
   for (int b = 0; b < (KTH ? (int)kPubMaxPerWarp : 1); ++b) kbest[b] = 0ull;
   uint32_t i = 0;  // after the loop: the tiles this CTA scanned
+  // q <= 2 in id order: two tiles per loop pass, so the prefetched registers swap roles
+  // instead of being copied (q = 2 on 2^28 rows: 0.420 -> 0.406 ms)
+  constexpr int kUnroll = kVoteTiles == 2 ? 2 : 1;
+#pragma unroll(kUnroll)
   for (; i < my_tiles; ++i) {
     // every thread reads the same thresholds in tile i (see SmemCtl::thr_g); in id
     // order they are read after the scores, so they hold no register across the loads

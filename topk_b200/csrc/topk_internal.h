@@ -116,8 +116,9 @@ struct ScanParams {
 
 // The published-keys bound before the merge (ScanParams::pub): used for k >= this and
 // grids of at least kPubMinGrid CTAs; pub_keys_per_cta(k, grid) keys per CTA, so the
-// array needs grid * 8 * kPubMaxPerWarp entries.
-constexpr uint32_t kPubMinK = 64;
+// array needs grid * 8 * kPubMaxPerWarp entries.  (From k = 128: at k = 64 the bound
+// cost more than it saved, 0.447 against 0.439 ms at q = 2 on 2^28 rows.)
+constexpr uint32_t kPubMinK = 128;
 constexpr uint32_t kPubMinGrid = 16;
 constexpr uint32_t kPubWaitPolls = 4096;  // ~64 ns each
 // Keys published per CTA: a multiple of its 8 warps, at least ceil(k / grid) + 1, at

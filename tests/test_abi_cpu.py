@@ -99,3 +99,38 @@ def test_null_handle_calls_of_the_file_index_and_ta_entries():
     n, d = C.c_uint64(), C.c_uint64()
     assert L.topk_csv_shape(None, C.byref(n), C.byref(d)) == _lib.ERR_ARG
     assert L.topk_binary_shape(b"/nonexistent.bin", C.byref(n), C.byref(d)) == _lib.ERR_ARG
+
+
+def test_lean_bindings_match_the_checked_ones():
+    """The per-query Table methods call lean bindings (plain addresses); each has the
+    checked binding's argument count and returns the same status on a null handle."""
+    import numpy as np
+    from topk_b200.table import _call_block
+    L, F = T.load(), _lib.lean()
+    checked = {name: args for name, _, args in _lib.SIGNATURES}
+    for name, res, args in _lib.LEAN_SIGNATURES:
+        assert len(args) == len(checked[name]), name
+    b = _call_block()
+    assert b is _call_block()  # one block per thread, reused
+    assert b.buf.ctypes.data % 16 == 0 and b.p_st % 8 == 0 and b.p_cnt % 8 == 0
+    assert len(b.ids) == _lib.MAX_K and len(b.sc) == _lib.MAX_K and len(b.w) >= _lib.MAX_D
+    assert F.topk_query(None, 4, 2, b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt, b.p_th) == _lib.ERR_ARG
+    assert F.topk_query_range(None, 0, 4, 4, 2, b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt, b.p_th) == _lib.ERR_ARG
+    assert F.topk_query_pruned(None, 4, 2, b.p_w, b.p_a, 0.0, b.p_ids, b.p_sc, b.p_cnt, b.p_th,
+                               b.p_st) == _lib.ERR_ARG
+    assert F.topk_query_learned(None, 4, 2, b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt, b.p_th, b.p_st,
+                                b.p_cut) == _lib.ERR_ARG
+    # arguments that do not fit the block go to the checked bindings
+    assert not b.args_in(np.ones(8, np.float32), np.zeros(_lib.MAX_Q + 1, np.uint8), 8)
+    w = np.arange(1, 9, dtype=np.float32)
+    assert b.args_in(w, np.array([7, 2], np.uint8), 8)
+    assert b.w[:8].tobytes() == w.tobytes() and list(b.a[:2]) == [7, 2]
+    # results come out as copies
+    b.cnt[0] = 2
+    b.ids[:2] = [5, 9]
+    b.sc[:2] = [0.25, 0.5]
+    b.f[0] = 0.25
+    ids, sc, th = b.results()
+    b.ids[:2] = 0
+    assert list(ids) == [5, 9] and list(sc) == [0.25, 0.5] and th == 0.25
+    assert ids.dtype == np.uint64 and sc.dtype == np.float32

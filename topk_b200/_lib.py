@@ -5,6 +5,7 @@ raises, and there is no CPU fallback anywhere in the package.
 """
 import ctypes as C
 import os
+import types
 
 import numpy as np
 
@@ -123,7 +124,37 @@ SIGNATURES = [
     ("topk_version", C.c_char_p, []),
 ]
 
+_V = C.c_void_p
+# Lean bindings of the per-query entry points, used by the Table methods that run
+# once per query: every pointer is a plain address.  The ndpointer checks above cost
+# about 1.4 us per array and call; these methods pass the addresses of their own
+# per-thread call buffers instead (table.py, _CallBlock), so a call converts integers
+# only.
+LEAN_SIGNATURES = [
+    ("topk_query", C.c_int, [_H, C.c_uint64, C.c_uint32, _V, _V, _V, _V, _V, _V]),
+    ("topk_query_range", C.c_int, [_H, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, _V, _V, _V, _V, _V, _V]),
+    ("topk_query_pruned", C.c_int, [_H, C.c_uint64, C.c_uint32, _V, _V, C.c_float, _V, _V, _V, _V, _V]),
+    ("topk_query_learned", C.c_int, [_H, C.c_uint64, C.c_uint32, _V, _V, _V, _V, _V, _V, _V, _V]),
+]
+
 _lib = None
+_lean = None
+
+
+def lean():
+    """The entry points of LEAN_SIGNATURES bound with address arguments (separate
+    function objects: the checked bindings of load() stay as they are)."""
+    global _lean
+    if _lean is None:
+        L = load()
+        fns = {}
+        for name, res, args in LEAN_SIGNATURES:
+            fn = L[name]  # a new function object, with its own argtypes
+            fn.restype = res
+            fn.argtypes = args
+            fns[name] = fn
+        _lean = types.SimpleNamespace(**fns)
+    return _lean
 
 
 def load():

@@ -1,6 +1,7 @@
 """Python handle over the C ABI: one n x d FP32 table resident on one GPU."""
 import ctypes as C
 import os
+import threading
 
 import numpy as np
 
@@ -17,6 +18,63 @@ def _weights(w, d):
 
 def _attr(a):
     return np.ascontiguousarray(a, np.uint8).reshape(-1)
+
+
+class _CallBlock:
+    """One host thread's argument and result buffers for the per-query calls, at
+    fixed addresses: ids (MAX_K u64), scores (MAX_K f32), weights (MAX_D f32),
+    attributes (MAX_Q u8), stats (4 u64), count (u64), threshold and cut (f32).
+    A call copies its weights and attributes in and its results out, so the
+    buffers are free again when the method returns."""
+
+    _IDS, _SC = 0, 8 * _lib.MAX_K
+    _W = _SC + 4 * _lib.MAX_K
+    _A = _W + 4 * 256
+    _ST = _A + _lib.MAX_Q
+    _CNT = _ST + 32
+    _TH = _CNT + 8
+    _CUT = _TH + 4
+    _BYTES = _CUT + 4
+
+    def __init__(self):
+        b = np.zeros(self._BYTES, np.uint8)
+        self.buf = b
+        base = b.ctypes.data
+        self.ids = b[self._IDS:self._SC].view(np.uint64)
+        self.sc = b[self._SC:self._W].view(np.float32)
+        self.w = b[self._W:self._A].view(np.float32)
+        self.a = b[self._A:self._ST]
+        self.st = b[self._ST:self._CNT].view(np.uint64)
+        self.cnt = b[self._CNT:self._TH].view(np.uint64)
+        self.f = b[self._TH:self._BYTES].view(np.float32)  # threshold, cut
+        self.p_ids, self.p_sc, self.p_w, self.p_a = (base + self._IDS, base + self._SC, base + self._W,
+                                                     base + self._A)
+        self.p_st, self.p_cnt, self.p_th, self.p_cut = (base + self._ST, base + self._CNT, base + self._TH,
+                                                        base + self._CUT)
+
+    def args_in(self, w, a, d):
+        """Copy a query's weights (the first d) and attributes into the block; False
+        when they do not fit (the caller then takes the checked bindings, whose C
+        call reports the error)."""
+        if len(a) > _lib.MAX_Q or d > 256:
+            return False
+        self.w[:d] = w[:d]
+        self.a[:len(a)] = a
+        return True
+
+    def results(self):
+        c = int(self.cnt[0])
+        return self.ids[:c].copy(), self.sc[:c].copy(), float(self.f[0])
+
+
+_tls = threading.local()
+
+
+def _call_block():
+    b = getattr(_tls, "blk", None)
+    if b is None:
+        b = _tls.blk = _CallBlock()
+    return b
 
 
 class Table:
@@ -112,11 +170,20 @@ class Table:
     # -- queries ------------------------------------------------------------
     def query(self, k, weights, attr, row_begin=None, row_end=None):
         """Exact top-k; returns (ids uint64, scores float32, threshold) ascending by score."""
-        L = _lib.load()
         w, a = _weights(weights, self.d), _attr(attr)
         r0 = 0 if row_begin is None else int(row_begin)
         r1 = self.n if row_end is None else int(row_end)
         cap = max(1, min(int(k), max(r1 - r0, 0)))
+        b = _call_block()
+        if cap <= _lib.MAX_K and b.args_in(w, a, self.d):
+            F = _lib.lean()
+            if row_begin is None and row_end is None:
+                check(F.topk_query(self._h, int(k), len(a), b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt, b.p_th))
+            else:
+                check(F.topk_query_range(self._h, r0, r1, int(k), len(a), b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt,
+                                         b.p_th))
+            return b.results()
+        L = _lib.load()
         ids = np.empty(cap, np.uint64)
         sc = np.empty(cap, np.float32)
         cnt = C.c_uint64()
@@ -242,6 +309,11 @@ class Table:
         partitions, cut accepted, scans)."""
         w, a = _weights(weights, self.d), _attr(attr)
         cap = max(1, min(int(k), self.n))
+        b = _call_block()
+        if cap <= _lib.MAX_K and b.args_in(w, a, self.d):
+            check(_lib.lean().topk_query_pruned(self._h, int(k), len(a), b.p_w, b.p_a, float(cut), b.p_ids, b.p_sc,
+                                                b.p_cnt, b.p_th, b.p_st))
+            return b.results() + (tuple(b.st.tolist()),)
         ids = np.empty(cap, np.uint64)
         sc = np.empty(cap, np.float32)
         st = np.zeros(4, np.uint64)
@@ -290,6 +362,11 @@ class Table:
         """Exact top-k through the model; returns (ids, scores, threshold, stats, cut)."""
         w, a = _weights(weights, self.d), _attr(attr)
         cap = max(1, min(int(k), self.n))
+        b = _call_block()
+        if cap <= _lib.MAX_K and b.args_in(w, a, self.d):
+            check(_lib.lean().topk_query_learned(self._h, int(k), len(a), b.p_w, b.p_a, b.p_ids, b.p_sc, b.p_cnt,
+                                                 b.p_th, b.p_st, b.p_cut))
+            return b.results() + (tuple(b.st.tolist()), float(b.f[1]))
         ids = np.empty(cap, np.uint64)
         sc = np.empty(cap, np.float32)
         st = np.zeros(4, np.uint64)

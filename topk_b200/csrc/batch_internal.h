@@ -119,9 +119,11 @@ cudaError_t launch_mlp_train(float *params, float *m, float *v, const float *X, 
 bool mlp_train_failed(const void *scratch, uint32_t F);
 cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, uint32_t F, float *out, int num_sms,
                                cudaStream_t s);
+// With seed (one query, params given): also *seed = key of its learned cut (0: none)
+// and *cut = the cut (NaN when not finite), from the same launch.
 cudaError_t launch_features(const float *pmin, const float *pmax, const float *pmean, uint32_t P, uint32_t d,
                             const BatchQuery *qs, uint32_t nq, float *X, const float *params, float *pred,
-                            cudaStream_t s);
+                            cudaStream_t s, float margin = 0.0f, uint32_t *seed = nullptr, float *cut = nullptr);
 // The learned cut: largest bound - S * exp((u + margin) / qq), u the model's output
 // (b1s: the largest partition bound / S, a feature).
 __host__ __device__ inline float learned_cut(float u, float b1s, float S, float qq, float margin) {
@@ -130,10 +132,6 @@ __host__ __device__ inline float learned_cut(float u, float b1s, float S, float 
 // Start each query's state at its learned cut (pred: model outputs; X: features).
 cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
                                 BatchState *st, uint32_t nq, cudaStream_t s);
-// One query (device descriptor q): *seed = key of its learned cut (0: none), *cut = the
-// cut (NaN when not finite).
-cudaError_t launch_learned_seed_one(const float *pred, const float *X, uint32_t d, const BatchQuery *q, float margin,
-                                    uint32_t *seed, float *cut, cudaStream_t s);
 cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
                                 uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
                                 uint32_t *out_count, float *out_thr, cudaStream_t s);

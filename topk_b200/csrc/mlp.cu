@@ -429,7 +429,8 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
                                                        const float *__restrict__ pmean, uint32_t P, uint32_t Ppad,
                                                        uint32_t d, const BatchQuery *__restrict__ qs,
                                                        float *__restrict__ X, const float *__restrict__ params,
-                                                       float *__restrict__ pred) {
+                                                       float *__restrict__ pred, float margin,
+                                                       uint32_t *__restrict__ seed, float *__restrict__ cut_out) {
   extern __shared__ __align__(16) unsigned char smem[];
   float *bnd = reinterpret_cast<float *>(smem);
   float *mu = bnd + Ppad;
@@ -450,11 +451,26 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
     if (p < P) {
       b = 0.0f;
       u = 0.0f;
-      for (uint32_t m = 0; m < q.qq; ++m) {
-        const size_t o = (size_t)p * d + q.attr[m];
-        const float w = q.w[m];
-        b += w * (w >= 0.0f ? pmax[o] : pmin[o]);
-        u += w * pmean[o];
+      // eight attributes' loads in flight before their sums (the statistics are
+      // mostly out of L2 here: one DRAM round trip per attribute otherwise)
+      for (uint32_t m0 = 0; m0 < q.qq; m0 += 8) {
+        float xb[8], xm[8];
+#pragma unroll
+        for (uint32_t v = 0; v < 8; ++v) {
+          xb[v] = xm[v] = 0.0f;
+          if (m0 + v < q.qq) {
+            const size_t o = (size_t)p * d + q.attr[m0 + v];
+            xb[v] = q.w[m0 + v] >= 0.0f ? pmax[o] : pmin[o];
+            xm[v] = pmean[o];
+          }
+        }
+#pragma unroll
+        for (uint32_t v = 0; v < 8; ++v)
+          if (m0 + v < q.qq) {
+            const float w = q.w[m0 + v];
+            b += w * xb[v];
+            u += w * xm[v];
+          }
       }
     }
     bnd[p] = b;
@@ -497,6 +513,17 @@ __global__ void __launch_bounds__(NT) features_kernel(const float *__restrict__ 
     float s = p.b3[0];
     for (uint32_t j = 0; j < kHid; ++j) s = fmaf(p.w3[j], h[kHid + j], s);
     pred[blockIdx.x] = s;
+    if (seed) {
+      // a single pruned query: its seed key (0: none) and the cut itself, here rather
+      // than in a launch of its own; S as the batched seed takes it (a NaN weight
+      // gives a NaN cut: no seed)
+      float Sw = 0.0f;
+      for (uint32_t m = 0; m < q.qq; ++m) Sw += fabsf(q.w[m]);
+      if (Sw == 0.0f) Sw = 1.0f;
+      const float cut = learned_cut(s, feat[feature_bound_col(d)], Sw, (float)q.qq, margin);
+      *seed = isfinite(cut) ? f2key(cut) : 0u;
+      *cut_out = isfinite(cut) ? cut : __int_as_float(0x7FC00000);
+    }
   }
 }
 
@@ -519,27 +546,9 @@ __global__ void learned_seed_kernel(const float *__restrict__ pred, const float 
   st[j] = s;
 }
 
-// One query (a pruned single query): its seed key (0: none) and the cut itself.
-__global__ void learned_seed_one_kernel(const float *__restrict__ pred, const float *__restrict__ X, uint32_t bcol,
-                                        const BatchQuery *__restrict__ q, float margin, uint32_t *__restrict__ seed,
-                                        float *__restrict__ cut_out) {
-  float S = 0.0f;
-  for (uint32_t m = 0; m < q->qq; ++m) S += fabsf(q->w[m]);
-  if (S == 0.0f) S = 1.0f;
-  const float cut = learned_cut(pred[0], X[bcol], S, (float)q->qq, margin);
-  *seed = isfinite(cut) ? f2key(cut) : 0u;
-  *cut_out = isfinite(cut) ? cut : __int_as_float(0x7FC00000);
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-cudaError_t launch_learned_seed_one(const float *pred, const float *X, uint32_t d, const BatchQuery *q, float margin,
-                                    uint32_t *seed, float *cut, cudaStream_t s) {
-  learned_seed_one_kernel<<<1, 1, 0, s>>>(pred, X, feature_bound_col(d), q, margin, seed, cut);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
                                 BatchState *st, uint32_t nq, cudaStream_t s) {
   if (nq)
@@ -599,7 +608,8 @@ cudaError_t launch_mlp_predict(const float *params, const float *X, uint64_t N, 
 
 cudaError_t launch_features(const float *pmin, const float *pmax, const float *pmean, uint32_t P, uint32_t d,
                             const BatchQuery *qs, uint32_t nq, float *X, const float *params, float *pred,
-                            cudaStream_t s) {
+                            cudaStream_t s, float margin, uint32_t *seed, float *cut) {
+  if (seed && (nq != 1 || !params || !cut)) return cudaErrorInvalidValue;
   if (feature_dim(d) > kMlpMaxIn || P == 0 || P > kMaxFeatureParts) return cudaErrorInvalidValue;
   uint32_t Ppad = 1;
   while (Ppad < P) Ppad <<= 1;
@@ -619,9 +629,12 @@ cudaError_t launch_features(const float *pmin, const float *pmax, const float *p
     opted.fetch_or(bit, std::memory_order_release);
   }
   if (nq <= 4) {
-    if (nq) features_kernel<1024><<<nq, 1024, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+    if (nq)
+      features_kernel<1024><<<nq, 1024, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred, margin, seed,
+                                                   cut);
   } else {
-    features_kernel<256><<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred);
+    features_kernel<256><<<nq, 256, smem, s>>>(pmin, pmax, pmean, P, Ppad, d, qs, X, params, pred, 0.0f, nullptr,
+                                               nullptr);
   }
   return cudaGetLastError();
 }

@@ -227,14 +227,28 @@ int grid_for(uint64_t n, int num_sms) {
 // addition round monotonically, so no row of p scores above it (no slack needed, and
 // a partition whose every queried value sits at its maximum scores exactly it).  The
 // order key of the bound, or 0xFFFFFFFF (keep) when it is NaN.
+// The extremes are read kBoundBatch attributes at a time, all loads of a batch issued
+// before the first multiply: the statistics are usually out of L2 by the time a query
+// reads them (the scans stream past it), and one DRAM round trip per attribute was the
+// bound's whole cost.  The sum keeps the reference order.
+constexpr uint32_t kBoundBatch = 8;
 __device__ __forceinline__ uint32_t part_bound_key(const float *__restrict__ pmin, const float *__restrict__ pmax,
                                                    uint32_t d, uint32_t p, const PartQuery &q) {
   float sacc = 0.0f;
-  for (uint32_t m = 0; m < q.qq; ++m) {
-    const float w = q.w[m];
-    const size_t o = (size_t)p * d + q.attr[m];
-    const float x = w >= 0.0f ? __ldg(pmax + o) : __ldg(pmin + o);
-    sacc = __fadd_rn(sacc, __fmul_rn(x, w));
+  for (uint32_t m0 = 0; m0 < q.qq; m0 += kBoundBatch) {
+    float x[kBoundBatch];
+#pragma unroll
+    for (uint32_t u = 0; u < kBoundBatch; ++u) {
+      const uint32_t m = m0 + u;
+      x[u] = 0.0f;
+      if (m < q.qq) {
+        const size_t o = (size_t)p * d + q.attr[m];
+        x[u] = q.w[m] >= 0.0f ? __ldg(pmax + o) : __ldg(pmin + o);
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kBoundBatch; ++u)
+      if (m0 + u < q.qq) sacc = __fadd_rn(sacc, __fmul_rn(x[u], q.w[m0 + u]));
   }
   return sacc != sacc ? 0xFFFFFFFFu : f2key(sacc);
 }

@@ -619,8 +619,8 @@ int run_pruned(topk_table_t h, uint64_t k, uint32_t qq, const float *weights, co
     uint32_t *seed = reinterpret_cast<uint32_t *>(X + kMlpMaxIn + 1);
     CK(cudaMemcpyAsync(dq, stage, sizeof(BatchQuery), cudaMemcpyHostToDevice, s));
     const size_t Pd = (size_t)P * h->d;
-    CK(launch_features(h->pstats, h->pstats + Pd, h->pstats + 2 * Pd, P, h->d, dq, 1, X, mlp, X + kMlpMaxIn, s));
-    CK(launch_learned_seed_one(X + kMlpMaxIn, X, h->d, dq, margin, seed, &dho->cut, s));
+    CK(launch_features(h->pstats, h->pstats + Pd, h->pstats + 2 * Pd, P, h->d, dq, 1, X, mlp, X + kMlpMaxIn, s,
+                       margin, seed, &dho->cut));
     d_seed = seed;
   }
   PartQuery pq{};

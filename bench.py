@@ -21,7 +21,11 @@ flush is needed between queries.
           U{2..16}, k U{1..1024}) over a 2^26 x 16 table, plain batched FP32
           against the BF16 tensor-core filter with exact rescoring, without and
           with the learned start; identical results checked, speed-ups and the
-          filter's tensor roofline reported.
+          filter's tensor roofline reported.  e2e_ms: host wall time of the
+          topk_query_batch call (query upload, the batch, result download and the
+          copy into the caller's arrays), writing into result arrays the caller
+          keeps across its calls, as a serving loop does (fresh zeroed arrays per
+          call add their first-touch page faults, 10-40 ms at these sizes).
   pruned   the partitioned workload: 2^27 x 8 anticorrelated in 2^11 partitions of
           2^16 rows, the learned model fitted on 10^6 exactly labelled queries (and
           10^5 more to calibrate its margin), 10^4 fresh queries by full scan, plain
@@ -320,13 +324,21 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
             # after the plain FP32 timing, which keeps the default tiles
             out["tuned"] = t.tune_batch(ks, W, A, qqs)
         res[name] = t.query_batch(ks, W, A, qqs)  # warm-up (and the BF16 table split)
+        # the caller's result arrays, kept across the timed calls (their pages resident)
+        bufs = tuple(np.ones_like(x) for x in res[name])
         ms, walls = [], []
         for _ in range(r):
             w0 = time.perf_counter()
-            t.query_batch(ks, W, A, qqs)
+            t.query_batch(ks, W, A, qqs, out=bufs)
             walls.append(time.perf_counter() - w0)
             ms.append(t.last_batch_stats()["device_ms"])
         st = t.last_batch_stats()
+        # the kept arrays hold the same results as the fresh ones of the warm-up call
+        kept_same = all(np.array_equal(x.view(np.uint8), y.view(np.uint8)) for x, y in zip(bufs[2:], res[name][2:]))
+        live = np.arange(bufs[0].shape[1])[None, :] < res[name][2].astype(np.int64)[:, None]
+        kept_same = kept_same and all(np.array_equal(x[live].view(np.uint8), y[live].view(np.uint8))
+                                      for x, y in zip(bufs[:2], res[name][:2]))
+        del bufs, live
         dev = statistics.median(ms)
         wall = statistics.median(walls) * 1e3
         if dist:
@@ -334,7 +346,8 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             dev, wall = float(tt[0].item()), float(tt[1].item())
         out[name] = {"device_ms": dev, "queries_per_s": nq * 1000.0 / dev, "e2e_ms": wall,
-                     "e2e_queries_per_s": nq * 1000.0 / wall, "fallbacks": st["fallbacks"],
+                     "e2e_queries_per_s": nq * 1000.0 / wall, "e2e_results_identical": kept_same,
+                     "fallbacks": st["fallbacks"],
                      "candidates": st["candidates"], "method_ran": st["method"],
                      "switched_fp32": st["switched_fp32"]}
         if name != "fp32":
@@ -348,6 +361,7 @@ def run_batched(T, torch, dist, device, n, nq, d=16, reps=3, methods=("fp32", "b
     names = list(res)
     same = all(np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
                for other in names[1:] for x, y in zip(res[names[0]], res[other]))
+    same = same and all(out[m]["e2e_results_identical"] for m in names)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

@@ -134,3 +134,53 @@ def test_lean_bindings_match_the_checked_ones():
     b.ids[:2] = 0
     assert list(ids) == [5, 9] and list(sc) == [0.25, 0.5] and th == 0.25
     assert ids.dtype == np.uint64 and sc.dtype == np.float32
+
+
+def test_query_batch_writes_into_kept_arrays(monkeypatch):
+    """Table.query_batch(out=...) hands the caller's arrays to topk_query_batch and
+    returns them; shapes and dtypes are checked before the call.  The C call is
+    replaced by a stand-in that writes counts[j] entries per row, as the library
+    does, so this runs without a GPU."""
+    import numpy as np
+    from topk_b200 import table as TB
+
+    calls = []
+
+    class FakeLib:
+        def topk_query_batch(self, h, nq, ks, qqs, W, wstride, A, astride, ids, sc, kstride, pcnt, pth):
+            calls.append((nq, kstride))
+            cnt = np.ctypeslib.as_array(C.cast(pcnt, C.POINTER(C.c_uint64)), (nq,))
+            th = np.ctypeslib.as_array(C.cast(pth, C.POINTER(C.c_float)), (nq,))
+            ids2, sc2 = ids.reshape(nq, kstride), sc.reshape(nq, kstride)
+            for j in range(nq):
+                c = int(min(ks[j], kstride))
+                ids2[j, :c] = np.arange(c) + 100 * j
+                sc2[j, :c] = np.linspace(1.0, 0.5, c, dtype=np.float32)
+                cnt[j] = c
+                th[j] = sc2[j, c - 1]
+            return _lib.OK
+
+    monkeypatch.setattr(_lib, "load", lambda: FakeLib())
+    t = TB.Table.__new__(TB.Table)
+    t._h, t.n, t.d = None, 1000, 4
+    ks = np.array([3, 5, 1], np.uint64)
+    W = np.ones((3, 4), np.float32)
+    A = np.array([[0, 1], [2, 3], [1, 2]], np.uint8)
+    fresh = t.query_batch(ks, W, A)
+    bufs = (np.full((3, 5), 7, np.uint64), np.full((3, 5), 9, np.float32), np.zeros(3, np.uint64),
+            np.zeros(3, np.float32))
+    got = t.query_batch(ks, W, A, out=bufs)
+    assert all(g is b for g, b in zip(got, bufs))
+    assert calls == [(3, 5), (3, 5)]
+    for j in range(3):
+        c = int(fresh[2][j])
+        assert int(bufs[2][j]) == c
+        assert np.array_equal(bufs[0][j, :c], fresh[0][j, :c]) and np.array_equal(bufs[1][j, :c], fresh[1][j, :c])
+        assert np.all(fresh[0][j, c:] == 0) and np.all(bufs[0][j, c:] == 7)  # kept rows keep their tail
+    assert np.array_equal(bufs[3], fresh[3])
+    # wrong shape, dtype or layout: refused before the call
+    for bad in ((np.zeros((3, 4), np.uint64),) + bufs[1:], (bufs[0].astype(np.int64),) + bufs[1:],
+                bufs[:1] + (np.zeros((5, 3), np.float32).T,) + bufs[2:], bufs[:2] + (np.zeros(3, np.uint32),) + bufs[3:]):
+        with pytest.raises(ValueError):
+            t.query_batch(ks, W, A, out=bad)
+    assert len(calls) == 2

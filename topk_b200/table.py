@@ -234,8 +234,18 @@ class Table:
                                                   C.c_void_p(d_ids), C.c_void_p(d_scores),
                                                   C.c_void_p(d_threshold or None), C.c_void_p(stream or None)))
 
-    def query_batch(self, ks, weights, attrs, qqs=None):
-        """ks: (nq,), weights: (nq, >=d), attrs: (nq, astride) with qqs[j] valid ids each."""
+    def query_batch(self, ks, weights, attrs, qqs=None, out=None):
+        """ks: (nq,), weights: (nq, >=d), attrs: (nq, astride) with qqs[j] valid ids each.
+        Returns (ids, scores, counts, thresholds); row j of ids and scores holds
+        counts[j] entries, the rest of the row is zero.
+
+        out: optional (ids, scores, counts, thresholds) arrays to write into, of dtypes
+        uint64, float32, uint64, float32 and shapes (nq, kstride), (nq, kstride), (nq,),
+        (nq,) with kstride = min(max(ks), n), C-contiguous.  A caller that answers
+        batches of one shape in a loop keeps them across calls instead of taking fresh
+        zeroed arrays each time (whose first-touch page faults cost more than the copy
+        of the results into them); then only the first counts[j] entries of row j are
+        written, the rest of the row keeps what was there.  Returns the same arrays."""
         L = _lib.load()
         ks = np.ascontiguousarray(ks, np.uint64)
         nq = len(ks)
@@ -243,10 +253,19 @@ class Table:
         A = np.ascontiguousarray(attrs, np.uint8).reshape(nq, -1)
         qqs = np.full(nq, A.shape[1], np.uint32) if qqs is None else np.ascontiguousarray(qqs, np.uint32)
         kstride = int(max(1, min(int(ks.max()) if nq else 1, self.n)))
-        ids = np.zeros((nq, kstride), np.uint64)
-        sc = np.zeros((nq, kstride), np.float32)
-        counts = np.zeros(nq, np.uint64)
-        ths = np.zeros(nq, np.float32)
+        if out is None:
+            ids = np.zeros((nq, kstride), np.uint64)
+            sc = np.zeros((nq, kstride), np.float32)
+            counts = np.zeros(nq, np.uint64)
+            ths = np.zeros(nq, np.float32)
+        else:
+            ids, sc, counts, ths = out
+            for x, dt, shape, name in ((ids, np.uint64, (nq, kstride), "ids"), (sc, np.float32, (nq, kstride), "scores"),
+                                       (counts, np.uint64, (nq,), "counts"), (ths, np.float32, (nq,), "thresholds")):
+                if (not isinstance(x, np.ndarray) or x.dtype != dt or x.shape != shape or not x.flags.c_contiguous
+                        or not x.flags.writeable):
+                    raise ValueError(f"out {name}: need a writeable C-contiguous {np.dtype(dt).name} array of shape "
+                                     f"{shape}")
         check(L.topk_query_batch(self._h, nq, ks, qqs, W.reshape(-1), W.shape[1], A.reshape(-1), A.shape[1],
                                  ids.reshape(-1), sc.reshape(-1), kstride, counts.ctypes.data, ths.ctypes.data))
         return ids, sc, counts, ths

@@ -374,8 +374,10 @@ __global__ void __launch_bounds__(kBT) batch_finish_kernel(const BatchQuery *__r
   for (uint32_t j = t; j < cnt; j += kBT) a[j] = best[q.best_off + j];
   __syncthreads();
   block_sort_desc<kBT>(a, cnt);
-  uint64_t *ids = out_ids + (uint64_t)blockIdx.x * kstride;
-  float *sc = out_scores + (uint64_t)blockIdx.x * kstride;
+  // kstride 0: compact, each query's entries at its best_off (sum of k entries in all)
+  const uint64_t off = kstride ? (uint64_t)blockIdx.x * kstride : (uint64_t)q.best_off;
+  uint64_t *ids = out_ids + off;
+  float *sc = out_scores + off;
   for (uint32_t r = t; r < cnt; r += kBT) {
     const uint2 e = a[r];
     ids[cnt - 1 - r] = e.y;

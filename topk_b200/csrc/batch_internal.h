@@ -132,6 +132,8 @@ __host__ __device__ inline float learned_cut(float u, float b1s, float S, float 
 // Start each query's state at its learned cut (pred: model outputs; X: features).
 cudaError_t launch_learned_seed(const float *pred, const float *X, uint32_t d, const BatchQuery *qs, float margin,
                                 BatchState *st, uint32_t nq, cudaStream_t s);
+// Each query's result, ascending, at out + j * kstride, or at out + its best_off when
+// kstride is 0 (compact: sum of k entries in all).
 cudaError_t launch_batch_finish(const BatchQuery *qs, uint32_t nq, const BatchState *st, const uint2 *best,
                                 uint32_t kmax, uint64_t *out_ids, float *out_scores, uint64_t kstride,
                                 uint32_t *out_count, float *out_thr, cudaStream_t s);

@@ -999,8 +999,9 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
                                     dredo, dwork, qmax, true, h->num_sms, s));
     CK(launch_batch_reduce(h->table, h->ld, dq, nqq, dst, dbest, dcand, kmax, capmax, use_bf16, dsw, s));
   }
+  // results compact (each query's at its best_off), so the download moves sum(k) entries
   CK(launch_batch_finish(dq, nqq, dst, dbest, kmax, static_cast<uint64_t *>(h->b_ids.p),
-                         static_cast<float *>(h->b_scores.p), kmax, static_cast<uint32_t *>(h->b_count.p),
+                         static_cast<float *>(h->b_scores.p), 0, static_cast<uint32_t *>(h->b_count.p),
                          static_cast<float *>(h->b_thr.p), s));
   return TOPK_OK;
   };
@@ -1051,7 +1052,7 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
   CK(cudaEventRecord(h->b_ev1, s));
   // results through the handle's pinned buffers (grown once), then into the caller's
   // arrays before anything below runs a nested batch that reuses them
-  const size_t res_bytes = (size_t)nq * kmax * 12;
+  const size_t res_bytes = (size_t)best_total * 12;
   if (h->hb_bytes < res_bytes) {
     if (h->hb_res) cudaFreeHost(h->hb_res);
     h->hb_res = nullptr;
@@ -1061,12 +1062,12 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
     h->hb_bytes = res_bytes;
   }
   uint64_t *hid = static_cast<uint64_t *>(h->hb_res);
-  float *hsc = reinterpret_cast<float *>(hid + nq * kmax);
+  float *hsc = reinterpret_cast<float *>(hid + best_total);
   std::vector<float> hth(nq);
   std::vector<uint32_t> hcnt(nq);
   std::vector<BatchState> hst(nq);
-  CK(cudaMemcpyAsync(hid, h->b_ids.p, nq * kmax * 8, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(hsc, h->b_scores.p, nq * kmax * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hid, h->b_ids.p, best_total * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hsc, h->b_scores.p, best_total * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hcnt.data(), h->b_count.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hth.data(), h->b_thr.p, nq * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), dst, nq * sizeof(BatchState), cudaMemcpyDeviceToHost, s));
@@ -1096,8 +1097,8 @@ int run_batch(topk_table_t h, uint64_t nq, const uint64_t *ks, const uint32_t *q
       if (!(hst[j].flags & kFlagFp32) && hst[j].thr != 0u && hst[j].thr > q[j].maxkey) ++retired_total;
   for (uint64_t j = 0; j < nq; j++) {  // queries answered again below overwrite theirs
     const uint32_t c = std::min<uint32_t>(hcnt[j], (uint32_t)std::min<uint64_t>(kmax, kstride));
-    std::memcpy(ids + j * kstride, hid + j * kmax, (size_t)c * 8);
-    std::memcpy(scores + j * kstride, hsc + j * kmax, (size_t)c * 4);
+    std::memcpy(ids + j * kstride, hid + q[j].best_off, (size_t)c * 8);
+    std::memcpy(scores + j * kstride, hsc + q[j].best_off, (size_t)c * 4);
   }
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->b_ev0, h->b_ev1));
